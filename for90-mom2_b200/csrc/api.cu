@@ -1,0 +1,516 @@
+// C ABI of the B200 PMCHWT library: context, problem upload and the entry
+// points that replace sysmat_pmchwt, srcvec, solve_systems, cs_prtsrf and
+// rcs of the reference (declarations and citations in include/mom_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "mom_internal.h"
+
+namespace mom {
+
+int fail(Ctx *c, int code, const std::string &msg) {
+  if (c) c->last_error = msg;
+  return code;
+}
+
+int cuda_fail(Ctx *c, cudaError_t e, const char *where) {
+  return fail(c, MOM_ERR_CUDA, std::string(cudaGetErrorString(e)) + " in " + where);
+}
+
+int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes) {
+  if (*p && *cap >= bytes) return MOM_OK;
+  if (*p) {
+    MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+  }
+  const size_t want = std::max<size_t>(bytes, 1 << 20);
+  if (cudaMalloc(p, want) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(c, MOM_ERR_ALLOC, "device allocation of " + std::to_string(want) + " bytes failed");
+  }
+  *cap = want;
+  return MOM_OK;
+}
+
+namespace {
+
+void free_domain(DomDev &D) {
+  cudaFree(D.qrel);
+  cudaFree(D.qabs);
+  cudaFree(D.cp);
+  cudaFree(D.area);
+  cudaFree(D.nrm);
+  cudaFree(D.mu);
+  cudaFree(D.sl);
+  cudaFree(D.hpar);
+  cudaFree(D.eh);
+  cudaFree(D.epar);
+  cudaFree(D.near_m);
+  cudaFree(D.near_n);
+  cudaFree(D.near_static);
+  D = DomDev();
+}
+
+void free_problem(Ctx *c) {
+  for (auto &D : c->dom) free_domain(D);
+  c->dom.clear();
+  cudaFree(c->A);
+  cudaFree(c->A32);
+  cudaFree(c->blk);
+  cudaFree(c->ipiv);
+  cudaFree(c->invd);
+  cudaFree(c->B);
+  cudaFree(c->X);
+  c->A = nullptr;
+  c->A32 = nullptr;
+  c->blk = nullptr;
+  c->ipiv = nullptr;
+  c->invd = nullptr;
+  c->B = c->X = nullptr;
+  c->BX_cap = 0;
+  c->have_problem = false;
+  c->assembled = 0;
+  c->factored = -1;
+}
+
+template <typename T>
+int upload(Ctx *c, T **dst, const std::vector<T> &h) {
+  MOM_CUDA(c, cudaMalloc(dst, sizeof(T) * std::max<size_t>(1, h.size())));
+  if (!h.empty()) MOM_CUDA(c, cudaMemcpyAsync(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream));
+  return MOM_OK;
+}
+
+inline void cross(const double *a, const double *b, double *r) {
+  r[0] = a[1] * b[2] - a[2] * b[1];
+  r[1] = a[2] * b[0] - a[0] * b[2];
+  r[2] = a[0] * b[1] - a[1] * b[0];
+}
+inline double nrm(const double *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// Geometry of one domain as compute_basis_data / average_edge_length /
+// quad_tri_points compute it (mesh.f90:138-153, 1265-1322; quad.f90:352-367).
+int build_domain(Ctx *c, const mom_mesh &m, DomDev &D) {
+  const int F = m.nfaces, Nd = m.nedges, nq = c->nq;
+  if (F <= 0 || Nd <= 0 || m.nnodes <= 0 || !m.nodes || !m.face_nodes || !m.face_edges || !m.edge_nodes ||
+      !m.edge_faces || !m.edge_bnodes || !m.edge_parent)
+    return fail(c, MOM_ERR_ARG, "incomplete domain mesh");
+  for (int i = 0; i < 3 * F; i++)
+    if (m.face_nodes[i] < 0 || m.face_nodes[i] >= m.nnodes || m.face_edges[i] < 0 || m.face_edges[i] >= Nd)
+      return fail(c, MOM_ERR_MESH, "face index out of range");
+  for (int e = 0; e < Nd; e++) {
+    if (m.edge_parent[e] < 0 || m.edge_parent[e] >= c->N) return fail(c, MOM_ERR_MESH, "edge parent out of range");
+    for (int k = 0; k < 2; k++) {
+      if (m.edge_faces[2 * e + k] >= F || m.edge_nodes[2 * e + k] < 0 || m.edge_nodes[2 * e + k] >= m.nnodes)
+        return fail(c, MOM_ERR_MESH, "edge index out of range");
+      if (m.edge_faces[2 * e + k] >= 0 && (m.edge_bnodes[2 * e + k] < 0 || m.edge_bnodes[2 * e + k] >= m.nnodes))
+        return fail(c, MOM_ERR_MESH, "edge free vertex out of range");
+    }
+  }
+  D.F = F;
+  D.Nd = Nd;
+  const double *P = m.nodes;
+  D.h_cp.resize(3 * (size_t)F);
+  D.h_area.resize(F);
+  D.h_nrm.resize(3 * (size_t)F);
+  D.h_qrel.resize((size_t)F * nq * 3);
+  D.h_qabs.resize((size_t)F * nq * 3);
+  D.h_mu.resize(9 * (size_t)F);
+  D.h_sl.resize(3 * (size_t)F);
+  D.h_hpar.resize(3 * (size_t)F);
+  D.h_fv.resize(9 * (size_t)F);
+  D.h_fs.resize(9 * (size_t)F);
+  D.h_fm.resize(9 * (size_t)F);
+  D.h_bn.resize(9 * (size_t)F);
+  std::vector<double> elen(Nd);
+  double ave = 0.0;
+  for (int e = 0; e < Nd; e++) {
+    const double *a = P + 3 * m.edge_nodes[2 * e], *b = P + 3 * m.edge_nodes[2 * e + 1];
+    double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+    elen[e] = nrm(d);
+    ave = ave + elen[e];
+  }
+  D.avelen = ave / Nd;
+  for (int f = 0; f < F; f++) {
+    const double *p1 = P + 3 * m.face_nodes[3 * f], *p2 = P + 3 * m.face_nodes[3 * f + 1],
+                 *p3 = P + 3 * m.face_nodes[3 * f + 2];
+    double a[3], b[3], cc[3], p21[3], p32[3], p13[3];
+    for (int i = 0; i < 3; i++) {
+      a[i] = p2[i] - p1[i];
+      cc[i] = p3[i] - p1[i];
+      p21[i] = p2[i] - p1[i];
+      p32[i] = p3[i] - p2[i];
+      p13[i] = p1[i] - p3[i];
+    }
+    cross(a, cc, b);
+    const double nb = nrm(b);
+    double *n = &D.h_nrm[3 * (size_t)f];
+    for (int i = 0; i < 3; i++) n[i] = b[i] / nb;
+    double *s = &D.h_fs[9 * (size_t)f], *mm = &D.h_fm[9 * (size_t)f];
+    const double l21 = nrm(p21), l32 = nrm(p32), l13 = nrm(p13);
+    for (int i = 0; i < 3; i++) {
+      s[i] = p21[i] / l21;
+      s[3 + i] = p32[i] / l32;
+      s[6 + i] = p13[i] / l13;
+    }
+    for (int e = 0; e < 3; e++) {
+      cross(s + 3 * e, n, mm + 3 * e);
+      const double l = nrm(mm + 3 * e);
+      for (int i = 0; i < 3; i++) mm[3 * e + i] = mm[3 * e + i] / l;
+    }
+    double mp13[3] = {-p13[0], -p13[1], -p13[2]}, cr[3];
+    cross(mp13, p32, cr);
+    const double A = 0.5 * nrm(cr);
+    D.h_area[f] = A;
+    double *cp = &D.h_cp[3 * (size_t)f];
+    for (int i = 0; i < 3; i++) cp[i] = (p1[i] + p2[i] + p3[i]) / 3.0;
+    for (int i = 0; i < 3; i++) {
+      D.h_fv[9 * (size_t)f + i] = p1[i];
+      D.h_fv[9 * (size_t)f + 3 + i] = p2[i];
+      D.h_fv[9 * (size_t)f + 6 + i] = p3[i];
+    }
+    for (int t = 0; t < nq; t++)
+      for (int i = 0; i < 3; i++) {
+        const double q = c->qn[t][2] * p1[i] + c->qn[t][0] * p2[i] + c->qn[t][1] * p3[i];
+        D.h_qabs[((size_t)f * nq + t) * 3 + i] = q;
+        D.h_qrel[((size_t)f * nq + t) * 3 + i] = q - cp[i];
+      }
+    for (int e = 0; e < 3; e++) {
+      const int ge = m.face_edges[3 * f + e];
+      double sign;
+      int bn;
+      if (m.edge_faces[2 * ge] == f) {
+        sign = 1.0;
+        bn = m.edge_bnodes[2 * ge];
+      } else if (m.edge_faces[2 * ge + 1] == f) {
+        sign = -1.0;
+        bn = m.edge_bnodes[2 * ge + 1];
+      } else {
+        return fail(c, MOM_ERR_MESH,
+                    "Error evaluating mesh face sign (this could imply corrupted mesh connectivity)!");
+      }
+      D.h_sl[3 * (size_t)f + e] = sign * elen[ge];
+      D.h_hpar[3 * (size_t)f + e] = m.edge_parent[ge];
+      for (int i = 0; i < 3; i++) {
+        D.h_bn[9 * (size_t)f + 3 * e + i] = P[3 * bn + i];
+        D.h_mu[9 * (size_t)f + 3 * e + i] = P[3 * bn + i] - cp[i];
+      }
+    }
+  }
+  D.h_eh.assign(2 * (size_t)Nd, -1);
+  D.h_epar.resize(Nd);
+  for (int e = 0; e < Nd; e++) {
+    D.h_epar[e] = m.edge_parent[e];
+    for (int k = 0; k < 2; k++) {
+      const int f = m.edge_faces[2 * e + k];
+      if (f < 0) continue;
+      for (int p = 0; p < 3; p++)
+        if (m.face_edges[3 * f + p] == e) D.h_eh[2 * e + k] = 3 * f + p;
+    }
+  }
+  MOM_TRY(upload(c, &D.qrel, D.h_qrel));
+  MOM_TRY(upload(c, &D.qabs, D.h_qabs));
+  MOM_TRY(upload(c, &D.cp, D.h_cp));
+  MOM_TRY(upload(c, &D.area, D.h_area));
+  MOM_TRY(upload(c, &D.nrm, D.h_nrm));
+  MOM_TRY(upload(c, &D.mu, D.h_mu));
+  MOM_TRY(upload(c, &D.sl, D.h_sl));
+  MOM_TRY(upload(c, &D.hpar, D.h_hpar));
+  MOM_TRY(upload(c, &D.eh, D.h_eh));
+  MOM_TRY(upload(c, &D.epar, D.h_epar));
+  return MOM_OK;
+}
+
+int ensure_rhs(Ctx *c, int nsrc) {
+  const size_t need = sizeof(double2) * (size_t)c->n * nsrc;
+  if (c->B && c->BX_cap >= need) return MOM_OK;
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  cudaFree(c->B);
+  cudaFree(c->X);
+  c->B = c->X = nullptr;
+  c->BX_cap = 0;
+  if (cudaMalloc(&c->B, need) != cudaSuccess || cudaMalloc(&c->X, need) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, MOM_ERR_ALLOC, "right-hand side allocation failed");
+  }
+  c->BX_cap = need;
+  return MOM_OK;
+}
+
+int ensure_a32(Ctx *c) {
+  if (c->A32) return MOM_OK;
+  const size_t bytes = sizeof(float2) * (size_t)c->lda * c->n;
+  if (cudaMalloc(&c->A32, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, MOM_ERR_ALLOC, "FP32 matrix allocation failed");
+  }
+  c->A32_bytes = bytes;
+  return MOM_OK;
+}
+
+// Copy a 2N x ncol column block of device data (ld = c->n) to host (ld).
+int copy_block_to_host(Ctx *c, const double2 *dev, int64_t ncol, double *host, int64_t ld) {
+  const int64_t rows = 2 * (int64_t)c->N;
+  MOM_CUDA(c, cudaMemcpy2DAsync(host, sizeof(double2) * ld, dev, sizeof(double2) * c->n, sizeof(double2) * rows, ncol,
+                                cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int check_prec(Ctx *c, int p) {
+  if (p != MOM_PREC_FP64 && p != MOM_PREC_MIXED) return fail(c, MOM_ERR_ARG, "unknown precision");
+  return MOM_OK;
+}
+
+}  // namespace
+}  // namespace mom
+
+using namespace mom;
+
+struct mom_ctx : public Ctx {};
+
+extern "C" {
+
+int mom_gpu_create(int32_t device, mom_ctx **out) {
+  if (!out) return MOM_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return MOM_ERR_CUDA;
+  }
+  mom_ctx *c = new (std::nothrow) mom_ctx();
+  if (!c) return MOM_ERR_ALLOC;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return MOM_ERR_CUDA;
+  }
+  if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS || cublasSetStream(c->blas, c->stream) != CUBLAS_STATUS_SUCCESS) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return MOM_ERR_CUDA;
+  }
+  *out = c;
+  return MOM_OK;
+}
+
+void mom_gpu_destroy(mom_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  free_problem(c);
+  cudaFree(c->ws);
+  cudaFree(c->Xh);
+  cudaFree(c->dinfo);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  cublasDestroy(c->blas);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char *mom_gpu_strerror(int32_t s) {
+  switch (s) {
+    case MOM_OK: return "success";
+    case MOM_ERR_ARG: return "invalid argument";
+    case MOM_ERR_ALLOC: return "allocation failed";
+    case MOM_ERR_CUDA: return "CUDA error";
+    case MOM_ERR_SINGULAR: return "Matrix factorization failed! (singular matrix)";
+    case MOM_ERR_TIMEOUT: return "device wait timed out";
+    case MOM_ERR_STATE: return "call order violated";
+    case MOM_ERR_MESH: return "inconsistent mesh";
+    case MOM_ERR_NOCONV: return "iterative refinement did not converge";
+    case MOM_ERR_IO: return "could not read mesh file";
+    default: return "unknown status";
+  }
+}
+
+const char *mom_gpu_last_error(mom_ctx *c) { return c ? c->last_error.c_str() : ""; }
+
+int mom_gpu_set_problem(mom_ctx *c, int32_t nedges_total, int32_t ndom, const mom_mesh *doms, int32_t nq,
+                        const double *qw, const double *qnodes) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (nedges_total <= 0 || ndom <= 0 || !doms || nq <= 0 || nq > kMaxQ || !qw || !qnodes)
+    return fail(c, MOM_ERR_ARG, "invalid problem description");
+  if (nq != 1 && nq != 3 && nq != 4 && nq != 7 && nq != 13)
+    return fail(c, MOM_ERR_ARG, "triangle rule must have 1, 3, 4, 7 or 13 points");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  free_problem(c);
+  c->N = nedges_total;
+  c->ndom = ndom;
+  c->nq = nq;
+  for (int i = 0; i < kMaxQ; i++) {
+    c->qw[i] = i < nq ? qw[i] : 0.0;
+    for (int k = 0; k < 3; k++) c->qn[i][k] = i < nq ? qnodes[3 * i + k] : 0.0;
+  }
+  MOM_TRY(upload_quadrature(c));
+  c->dom.resize(ndom);
+  size_t maxF = 0;
+  for (int d = 0; d < ndom; d++) {
+    MOM_TRY(build_domain(c, doms[d], c->dom[d]));
+    maxF = std::max<size_t>(maxF, c->dom[d].F);
+  }
+  for (int d = 0; d < ndom; d++) MOM_TRY(near_precompute(c, d));
+  const int64_t n2 = 2 * (int64_t)c->N;
+  c->nb = 64;
+  c->n = (n2 + c->nb - 1) / c->nb * c->nb;
+  c->lda = c->n;
+  c->A_bytes = sizeof(double2) * (size_t)c->lda * c->n;
+  c->blk_bytes = sizeof(double2) * 18 * maxF * maxF;
+  if (cudaMalloc(&c->A, c->A_bytes) != cudaSuccess || cudaMalloc(&c->blk, c->blk_bytes) != cudaSuccess ||
+      cudaMalloc(&c->ipiv, sizeof(int) * c->n) != cudaSuccess ||
+      cudaMalloc(&c->invd, sizeof(double2) * 2 * (size_t)c->nb * c->n) != cudaSuccess) {
+    cudaGetLastError();
+    free_problem(c);
+    return fail(c, MOM_ERR_ALLOC, "device allocation for the system matrix failed");
+  }
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_problem = true;
+  return MOM_OK;
+}
+
+int mom_gpu_sysmat(mom_ctx *c, double omega, const double *ri, int32_t precision, double *A_host, int64_t lda) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before sysmat");
+  if (!ri || !(omega > 0)) return fail(c, MOM_ERR_ARG, "invalid omega or refractive indices");
+  MOM_TRY(check_prec(c, precision));
+  if (A_host && lda < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "lda < 2N");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  if (precision == MOM_PREC_MIXED) MOM_TRY(ensure_a32(c));
+  MOM_TRY(assemble(c, omega, ri, precision));
+  if (A_host) MOM_TRY(copy_block_to_host(c, c->A, 2 * (int64_t)c->N, A_host, lda));
+  return MOM_OK;
+}
+
+int mom_gpu_srcvec(mom_ctx *c, double omega, const double *ri1, int32_t nsrc, const mom_src *src, double *q_host,
+                   int64_t ldq) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before srcvec");
+  if (!ri1 || nsrc <= 0 || !src || !(omega > 0)) return fail(c, MOM_ERR_ARG, "invalid sources");
+  if (q_host && ldq < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldq < 2N");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  MOM_TRY(ensure_rhs(c, nsrc));
+  MOM_TRY(rhs_build(c, omega, ri1, nsrc, src));
+  c->nsrc = nsrc;
+  c->srcs.assign(src, src + nsrc);
+  c->omega_rhs = omega;
+  c->ri1[0] = ri1[0];
+  c->ri1[1] = ri1[1];
+  if (q_host) MOM_TRY(copy_block_to_host(c, c->B, nsrc, q_host, ldq));
+  return MOM_OK;
+}
+
+int mom_gpu_solve(mom_ctx *c, int32_t precision, double tol, int32_t maxit, double *x_host, int64_t ldx,
+                  int32_t *iters_out) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  MOM_TRY(check_prec(c, precision));
+  if (!c->assembled && c->factored != precision)
+    return fail(c, MOM_ERR_STATE, "build the system matrix before solving");
+  if (c->nsrc <= 0) return fail(c, MOM_ERR_STATE, "compute source vectors before solving");
+  if (x_host && ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+  if (precision == MOM_PREC_MIXED && (!c->A32 || maxit <= 0 || !(tol > 0)))
+    return fail(c, MOM_ERR_ARG, "mixed solve needs a mixed sysmat and tol > 0, maxit > 0");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  if (c->factored != precision) MOM_TRY(lu_factor(c, precision));
+  int it = 0;
+  MOM_TRY(lu_solve(c, precision, tol, maxit, &it));
+  if (precision == MOM_PREC_FP64) c->assembled = 0;  // the matrix now holds its LU factors
+  if (iters_out) *iters_out = it;
+  if (x_host) MOM_TRY(copy_block_to_host(c, c->X, c->nsrc, x_host, ldx));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int mom_gpu_solve_wavelength(mom_ctx *c, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                             int32_t precision, double tol, int32_t maxit, double *x_host, int64_t ldx,
+                             int32_t *iters_out) {
+  int r = mom_gpu_sysmat(c, omega, ri, precision, nullptr, 0);
+  if (r) return r;
+  r = mom_gpu_srcvec(c, omega, ri, nsrc, src, nullptr, 0);
+  if (r) return r;
+  return mom_gpu_solve(c, precision, tol, maxit, x_host, ldx, iters_out);
+}
+
+int mom_gpu_cross_sections(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t nsrc,
+                           const mom_src *src, const double *x_host, int64_t ldx, double *csca, double *cabs) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (dom < 0 || dom >= c->ndom || nsrc <= 0 || !src || !ri || !csca || !cabs || !(omega > 0))
+    return fail(c, MOM_ERR_ARG, "invalid cross-section arguments");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  const double2 *xd = c->X;
+  int64_t ld = c->n;
+  if (x_host) {
+    if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n * nsrc));
+    MOM_CUDA(c, cudaMemcpy2DAsync(c->Xh, sizeof(double2) * c->n, x_host, sizeof(double2) * ldx,
+                                  sizeof(double2) * 2 * c->N, nsrc, cudaMemcpyHostToDevice, c->stream));
+    xd = c->Xh;
+  } else if (nsrc > c->nsrc) {
+    return fail(c, MOM_ERR_STATE, "no device solution for that many sources");
+  }
+  return cross_sections(c, dom, omega, ri, nsrc, src, xd, ld, csca, cabs);
+}
+
+int mom_gpu_rcs(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
+                int64_t ldx, int32_t ntheta, int32_t nphi, double *rcs) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (dom < 0 || dom >= c->ndom || ntheta < 2 || nphi < 2 || !rcs || !ri || isrc < 0 || !(omega > 0))
+    return fail(c, MOM_ERR_ARG, "invalid far-field arguments");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  const double2 *xd;
+  if (x_host) {
+    if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n));
+    MOM_CUDA(c, cudaMemcpyAsync(c->Xh, x_host + 2 * (size_t)isrc * ldx, sizeof(double2) * 2 * c->N,
+                                cudaMemcpyHostToDevice, c->stream));
+    xd = c->Xh;
+  } else {
+    if (isrc >= c->nsrc) return fail(c, MOM_ERR_STATE, "no device solution for that source");
+    xd = c->X + (size_t)isrc * c->n;
+  }
+  return far_field(c, dom, omega, ri, xd, ntheta, nphi, rcs);
+}
+
+int mom_gpu_device_matrix(mom_ctx *c, void **A_dev, int64_t *lda) {
+  if (!c || !A_dev || !lda) return MOM_ERR_ARG;
+  *A_dev = c->A;
+  *lda = c->lda;
+  return MOM_OK;
+}
+
+int mom_gpu_device_solution(mom_ctx *c, void **x_dev, int64_t *ldx, int32_t *nsrc) {
+  if (!c || !x_dev || !ldx || !nsrc) return MOM_ERR_ARG;
+  *x_dev = c->X;
+  *ldx = c->n;
+  *nsrc = c->nsrc;
+  return MOM_OK;
+}
+
+int mom_gpu_synchronize(mom_ctx *c) {
+  if (!c) return MOM_ERR_ARG;
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int64_t mom_gpu_launch_count(mom_ctx *c) { return c ? c->launches : 0; }
+
+}  // extern "C"

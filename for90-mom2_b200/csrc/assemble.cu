@@ -1,0 +1,815 @@
+// PMCHWT system-matrix assembly on sm_100a.
+//
+// Replaces sysmat_pmchwt / computeD / computeH / computeK (sysmat.f90:18-519)
+// with the intK1/intK2/intK4 source integrals (srcint.f90:57-448), the
+// Green's functions (green.f90:40-151) and the closed-form singular terms
+// (int.f90:15-407).
+//
+// Formulation.  For a test face m (centroid c_m, points r = c_m + rho) and a
+// source face n (centroid c_n, points r' = c_n + rho'), with d = c_m - c_n,
+// one pass over the NQ x NQ point pairs evaluates G = e^{ikR}/(4 pi R) and
+// the gradient phasor phi = e^{ikR}(1/R^3 - ik/R^2)/(4 pi) once per pair and
+// reduces them into 18 complex moments; the 3 x 3 edge-pair blocks of D+H
+// and K follow in closed form from those moments (the RWG functions are
+// affine in the point), e.g.
+//   D(p,q) = c1 sl_p sl_q / 4 * sum_r w_r (rho - mu_p).sum_r' w' G (rho' - nu_q)
+// with mu_p, nu_q the free RWG vertices relative to the centroids and
+// sl = sign * edge length.  The reference evaluates intK2 per test point
+// (srcint.f90:158) and contracts afterwards (sysmat.f90:326-343); the sums
+// are the same, only the rounding order differs.
+//
+// Kernels:
+//   pair_kernel<T>    all face pairs with the regular G (T = double for the
+//                     FP64 path, float for the mixed path in units of the
+//                     domain's average edge length);
+//   near_static_kernel  once per geometry: the wavelength-independent
+//                     closed-form integrals (int.f90) of every near pair,
+//                     contracted with the test functions;
+//   near_kernel       per wavelength, FP64: the smoothed-G quadrature of the
+//                     near pairs plus the closed-form terms scaled by
+//                     1/(4 pi) and k^2/(8 pi) (srcint.f90:21-53,121-154,
+//                     330-366); overwrites the near blocks;
+//   gather_kernel     sums the (up to) four face-pair blocks of every
+//                     edge pair and adds them to A with the Zsi and sign
+//                     factors of sysmat.f90:70-99.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "mom_internal.h"
+
+namespace mom {
+
+__constant__ double c_qw[kMaxQ];
+__constant__ double c_qn[kMaxQ][3];
+
+namespace {
+
+constexpr int kPairThreads = 128;
+constexpr int kTestPerCta = 8;
+constexpr double kOofpi = 1.0 / (4.0 * kPi);  // green.f90:20-21
+
+template <typename T>
+struct Cx {
+  T re, im;
+};
+
+__device__ __forceinline__ void fsincos(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ void fsincos(float x, float *s, float *c) { __sincosf(x, s, c); }
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+__device__ __forceinline__ float fexp(float x) { return __expf(x); }
+__device__ __forceinline__ double frsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float frsqrt(float x) { return rsqrtf(x); }
+
+// The 18 moments of one face pair (without the 1/(4 pi) factor).
+template <typename T>
+struct Moments {
+  Cx<T> TA, TD, KG;
+  Cx<T> TB[3], TC[3], KC[3], KE[3], KF[3];
+};
+
+template <typename T>
+__device__ __forceinline__ void zero(Cx<T> &a) {
+  a.re = 0;
+  a.im = 0;
+}
+
+// Point-pair loop.  rho_t: test point offsets (stride 3), rho_s: source
+// offsets with stride sstride between coordinates; w from constant memory.
+// SMOOTH selects the singularity-subtracted kernels (green.f90:40-97).
+template <typename T, int NQ, bool SMOOTH>
+__device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int sstride, const T d[3], T kr, T ki,
+                                             Moments<T> &M) {
+  zero(M.TA);
+  zero(M.TD);
+  zero(M.KG);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    zero(M.TB[i]);
+    zero(M.TC[i]);
+    zero(M.KC[i]);
+    zero(M.KE[i]);
+    zero(M.KF[i]);
+  }
+  // k^2 for the smoothed kernels
+  const T k2r = kr * kr - ki * ki, k2i = 2 * kr * ki;
+#pragma unroll 1
+  for (int t = 0; t < NQ; t++) {
+    const T rx = rho_t[3 * t], ry = rho_t[3 * t + 1], rz = rho_t[3 * t + 2];
+    const T wt = (T)c_qw[t];
+    const T ax = d[0] + rx, ay = d[1] + ry, az = d[2] + rz;
+    Cx<T> G0 = {0, 0}, P0 = {0, 0}, G1[3] = {{0, 0}, {0, 0}, {0, 0}}, P1[3] = {{0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int s = 0; s < NQ; s++) {
+      const T sx = rho_s[(3 * s) * sstride], sy = rho_s[(3 * s + 1) * sstride], sz = rho_s[(3 * s + 2) * sstride];
+      const T ws = (T)c_qw[s];
+      const T dx = ax - sx, dy = ay - sy, dz = az - sz;
+      const T R2 = dx * dx + dy * dy + dz * dz;
+      T gre, gim, pre, pim;
+      if (R2 > 0) {
+        const T iR = frsqrt(R2);
+        const T R = R2 * iR;
+        T sn, cs;
+        fsincos(kr * R, &sn, &cs);
+        const T ea = fexp(-ki * R);
+        const T er = ea * cs, ei = ea * sn;  // e^{ikR}
+        const T iR2 = iR * iR;
+        const T iR3 = iR2 * iR;
+        // q = 1/R^3 - i k / R^2 = (iR3 + ki iR2) - i kr iR2
+        const T qr = iR3 + ki * iR2, qi = -kr * iR2;
+        if (SMOOTH) {
+          // Gs*4pi = (e - 1)/R + k^2 R / 2 ; phis*4pi = e q - 1/R^3 - k^2/(2R)
+          gre = ((er - (T)1) * iR + (T)0.5 * k2r * R) * ws;
+          gim = (ei * iR + (T)0.5 * k2i * R) * ws;
+          pre = (er * qr - ei * qi - iR3 - (T)0.5 * k2r * iR) * ws;
+          pim = (er * qi + ei * qr - (T)0.5 * k2i * iR) * ws;
+        } else {
+          const T g = iR * ws;
+          gre = er * g;
+          gim = ei * g;
+          pre = (er * qr - ei * qi) * ws;
+          pim = (er * qi + ei * qr) * ws;
+        }
+      } else {
+        if (SMOOTH) {  // R = 0 limits: Gs = ik/(4 pi), grad Gs = 0
+          gre = -ki * ws;
+          gim = kr * ws;
+        } else {
+          gre = 0;
+          gim = 0;
+        }
+        pre = 0;
+        pim = 0;
+      }
+      G0.re += gre;
+      G0.im += gim;
+      P0.re += pre;
+      P0.im += pim;
+      G1[0].re += gre * sx; G1[0].im += gim * sx;
+      G1[1].re += gre * sy; G1[1].im += gim * sy;
+      G1[2].re += gre * sz; G1[2].im += gim * sz;
+      P1[0].re += pre * sx; P1[0].im += pim * sx;
+      P1[1].re += pre * sy; P1[1].im += pim * sy;
+      P1[2].re += pre * sz; P1[2].im += pim * sz;
+    }
+    // Test-side sums.
+    const T rr[3] = {rx, ry, rz};
+    M.TA.re += wt * (rx * G1[0].re + ry * G1[1].re + rz * G1[2].re);
+    M.TA.im += wt * (rx * G1[0].im + ry * G1[1].im + rz * G1[2].im);
+    M.TD.re += wt * G0.re;
+    M.TD.im += wt * G0.im;
+    M.KG.re += wt * P0.re;
+    M.KG.im += wt * P0.im;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      M.TB[i].re += wt * G0.re * rr[i];
+      M.TB[i].im += wt * G0.im * rr[i];
+      M.TC[i].re += wt * G1[i].re;
+      M.TC[i].im += wt * G1[i].im;
+      M.KC[i].re += wt * P0.re * rr[i];
+      M.KC[i].im += wt * P0.im * rr[i];
+      M.KF[i].re += wt * P1[i].re;
+      M.KF[i].im += wt * P1[i].im;
+    }
+    // KE += w rho x P1
+    M.KE[0].re += wt * (ry * P1[2].re - rz * P1[1].re);
+    M.KE[0].im += wt * (ry * P1[2].im - rz * P1[1].im);
+    M.KE[1].re += wt * (rz * P1[0].re - rx * P1[2].re);
+    M.KE[1].im += wt * (rz * P1[0].im - rx * P1[2].im);
+    M.KE[2].re += wt * (rx * P1[1].re - ry * P1[0].re);
+    M.KE[2].im += wt * (rx * P1[1].im - ry * P1[0].im);
+  }
+}
+
+struct Cd {
+  double re, im;
+};
+__device__ __forceinline__ Cd cmul(Cd a, Cd b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+// Closed-form 3x3 blocks from the moments (FP64).  mu[p][3], nu[q][3], d in
+// the kernel's length unit; fD, fH, fK carry c1, c2, 1/(16 pi) and the unit
+// scale.  Writes S = D + H and K, interleaved, 18 double2 values.
+template <typename T>
+__device__ __forceinline__ void blocks_from_moments(const Moments<T> &Mt, const double mu[3][3], const double nu[3][3],
+                                                    const double slp[3], const double slq[3], const double d[3],
+                                                    Cd fD, Cd fH, double fK, bool self, double2 *out) {
+  auto cv = [](const Cx<T> &a) -> Cd { return {(double)a.re, (double)a.im}; };
+  Cd TA = cv(Mt.TA), TD = cv(Mt.TD), KG = cv(Mt.KG);
+  Cd TB[3], TC[3], KC[3], KE[3], KF[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    TB[i] = cv(Mt.TB[i]);
+    TC[i] = cv(Mt.TC[i]);
+    KC[i] = cv(Mt.KC[i]);
+    KE[i] = cv(Mt.KE[i]);
+    KF[i] = cv(Mt.KF[i]);
+  }
+  // K helpers: KBv = d x KF + KE, KDv = d KG + KC, dKE = d . KE
+  Cd KBv[3], KDmF[3];
+  KBv[0] = {d[1] * KF[2].re - d[2] * KF[1].re + KE[0].re, d[1] * KF[2].im - d[2] * KF[1].im + KE[0].im};
+  KBv[1] = {d[2] * KF[0].re - d[0] * KF[2].re + KE[1].re, d[2] * KF[0].im - d[0] * KF[2].im + KE[1].im};
+  KBv[2] = {d[0] * KF[1].re - d[1] * KF[0].re + KE[2].re, d[0] * KF[1].im - d[1] * KF[0].im + KE[2].im};
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    KDmF[i] = {d[i] * KG.re + KC[i].re - KF[i].re, d[i] * KG.im + KC[i].im - KF[i].im};
+  Cd dKE = {d[0] * KE[0].re + d[1] * KE[1].re + d[2] * KE[2].re, d[0] * KE[0].im + d[1] * KE[1].im + d[2] * KE[2].im};
+  // per q: beta_q = nu.TB, bq = (d x nu).KC, cq = nu.KE
+  Cd beta[3], bq[3], cq[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const double *v = nu[q];
+    beta[q] = {v[0] * TB[0].re + v[1] * TB[1].re + v[2] * TB[2].re, v[0] * TB[0].im + v[1] * TB[1].im + v[2] * TB[2].im};
+    double dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
+    bq[q] = {dn[0] * KC[0].re + dn[1] * KC[1].re + dn[2] * KC[2].re, dn[0] * KC[0].im + dn[1] * KC[1].im + dn[2] * KC[2].im};
+    cq[q] = {v[0] * KE[0].re + v[1] * KE[1].re + v[2] * KE[2].re, v[0] * KE[0].im + v[1] * KE[1].im + v[2] * KE[2].im};
+  }
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    const double *u = mu[p];
+    Cd alpha = {u[0] * TC[0].re + u[1] * TC[1].re + u[2] * TC[2].re, u[0] * TC[0].im + u[1] * TC[1].im + u[2] * TC[2].im};
+    Cd ap = {u[0] * KBv[0].re + u[1] * KBv[1].re + u[2] * KBv[2].re, u[0] * KBv[0].im + u[1] * KBv[1].im + u[2] * KBv[2].im};
+    // Z_p = mu_p x (KDv - KF)
+    Cd Z[3] = {{u[1] * KDmF[2].re - u[2] * KDmF[1].re, u[1] * KDmF[2].im - u[2] * KDmF[1].im},
+               {u[2] * KDmF[0].re - u[0] * KDmF[2].re, u[2] * KDmF[0].im - u[0] * KDmF[2].im},
+               {u[0] * KDmF[1].re - u[1] * KDmF[0].re, u[0] * KDmF[1].im - u[1] * KDmF[0].im}};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const double *v = nu[q];
+      const double uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+      const double ss = slp[p] * slq[q];
+      Cd cD = {TA.re - beta[q].re - alpha.re + uv * TD.re, TA.im - beta[q].im - alpha.im + uv * TD.im};
+      Cd S1 = cmul(fD, cD), S2 = cmul(fH, TD);
+      double2 sv = make_double2(ss * (S1.re + S2.re), ss * (S1.im + S2.im));
+      double2 kv = make_double2(0.0, 0.0);
+      if (!self) {
+        Cd cK = {-dKE.re - ap.re - bq[q].re + cq[q].re + v[0] * Z[0].re + v[1] * Z[1].re + v[2] * Z[2].re,
+                 -dKE.im - ap.im - bq[q].im + cq[q].im + v[0] * Z[0].im + v[1] * Z[1].im + v[2] * Z[2].im};
+        kv = make_double2(ss * fK * cK.re, ss * fK * cK.im);
+      }
+      out[2 * (3 * p + q)] = sv;
+      out[2 * (3 * p + q) + 1] = kv;
+    }
+  }
+}
+
+struct PairArgs {
+  int F;
+  const double *qrel;  // [F][NQ][3]
+  const double *cp;    // [F][3]
+  const double *mu;    // [F][3][3]
+  const double *sl;    // [F][3]
+  double inv_unit;     // 1/L0
+  double kr, ki;       // k * L0
+  Cd fD, fH;
+  double fK;
+  double2 *blk;        // [F][F][18]
+};
+
+// One thread per source face n; the CTA walks kTestPerCta test faces.
+template <typename T, int NQ>
+__global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
+  __shared__ T s_src[NQ * 3][kPairThreads];
+  __shared__ T s_tst[NQ * 3];
+  __shared__ double s_tmu[9], s_tsl[3], s_tcp[3];
+  const int tid = threadIdx.x;
+  const int n = blockIdx.x * kPairThreads + tid;
+  const bool active = n < a.F;
+  double ncp[3] = {0, 0, 0}, nu[3][3], slq[3];
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NQ * 3; i++) s_src[i][tid] = (T)(a.qrel[(size_t)n * NQ * 3 + i] * a.inv_unit);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      ncp[i] = a.cp[3 * n + i];
+      slq[i] = a.sl[3 * n + i] * a.inv_unit;
+#pragma unroll
+      for (int j = 0; j < 3; j++) nu[i][j] = a.mu[9 * n + 3 * i + j] * a.inv_unit;
+    }
+  }
+  const int m0 = blockIdx.y * kTestPerCta;
+  for (int mi = 0; mi < kTestPerCta; mi++) {
+    const int m = m0 + mi;
+    if (m >= a.F) break;
+    __syncthreads();
+    if (tid < NQ * 3) s_tst[tid] = (T)(a.qrel[(size_t)m * NQ * 3 + tid] * a.inv_unit);
+    if (tid < 9) s_tmu[tid] = a.mu[9 * m + tid] * a.inv_unit;
+    if (tid < 3) {
+      s_tsl[tid] = a.sl[3 * m + tid] * a.inv_unit;
+      s_tcp[tid] = a.cp[3 * m + tid];
+    }
+    __syncthreads();
+    if (!active) continue;
+    double dd[3];
+    T dT[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      dd[i] = (s_tcp[i] - ncp[i]) * a.inv_unit;
+      dT[i] = (T)dd[i];
+    }
+    Moments<T> Mt;
+    pair_moments<T, NQ, false>(s_tst, &s_src[0][tid], kPairThreads, dT, (T)a.kr, (T)a.ki, Mt);
+    double mu[3][3], slp[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      slp[i] = s_tsl[i];
+#pragma unroll
+      for (int j = 0; j < 3; j++) mu[i][j] = s_tmu[3 * i + j];
+    }
+    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, m == n, a.blk + ((size_t)m * a.F + n) * 18);
+  }
+}
+
+// ---- closed-form static integrals (int.f90), FP64 ------------------------
+
+struct FaceGeo {
+  double v[3][3];   // vertices
+  double s[3][3];   // edge unit vectors s(:,e)
+  double mm[3][3];  // in-plane edge normals m(:,e)
+  double n[3];      // unit normal
+};
+
+__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ double norm3(const double *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+// int.f90:15-53 intLm1
+__device__ double d_intLm1(const double *r, const FaceGeo &g, int e) {
+  const double *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
+  double a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
+  double Rp = norm3(a), Rm = norm3(b);
+  double sp = -dot3(a, s), sm = -dot3(b, s);
+  double div1 = Rp - sp, div2 = Rm + sm;
+  if (fabs(div1) > fabs(div2)) return log((Rm - sm) / div1);
+  return log((Rp + sp) / div2);
+}
+
+// int.f90:55-96 intL1 and 98-135 intL3 together (they share R02, Rp, Rm).
+__device__ void d_intL13(const double *r, const FaceGeo &g, int e, const double *n, double lm1, double *L1, double *L3) {
+  const double *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
+  double rp[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) rp[i] = r[i] - 0.5 * (p1[i] + p2[i]);
+  double h = dot3(n, rp), t = dot3(g.mm[e], rp);
+  double R02 = t * t + h * h;
+  double a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
+  double Rp = norm3(a), Rm = norm3(b);
+  double sp = -dot3(a, s), sm = -dot3(b, s);
+  double l1 = (R02 == 0) ? 0.5 * (sp * Rp - sm * Rm) : 0.5 * R02 * lm1 + 0.5 * (sp * Rp - sm * Rm);
+  *L1 = l1;
+  *L3 = 0.75 * R02 * l1 + 0.25 * (sp * (Rp * Rp * Rp) - sm * (Rm * Rm * Rm));
+}
+
+// int.f90:137-162 intSm3h
+__device__ double d_intSm3h(const double *r, const FaceGeo &g) {
+  double a[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double v[3] = {g.v[k][0] - r[0], g.v[k][1] - r[1], g.v[k][2] - r[2]};
+    double l = norm3(v);
+#pragma unroll
+    for (int i = 0; i < 3; i++) a[k][i] = v[i] / l;
+  }
+  double x = 1.0 + dot3(a[0], a[1]) + dot3(a[0], a[2]) + dot3(a[1], a[2]);
+  double c[3] = {a[1][1] * a[2][2] - a[1][2] * a[2][1], a[1][2] * a[2][0] - a[1][0] * a[2][2],
+                 a[1][0] * a[2][1] - a[1][1] * a[2][0]};
+  double y = fabs(dot3(a[0], c));
+  double om = 2.0 * atan2(y, x);
+  double rp1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
+  return dot3(g.n, rp1) > 0.0 ? fabs(om) : -fabs(om);
+}
+
+struct StaticArgs {
+  int64_t nnear;
+  const int *near_m, *near_n;
+  const FaceGeo *geo;  // [F]
+  const double *qabs;  // [F][NQ][3]
+  const double *area;  // [F]
+  const double *sl;    // [F][3]
+  const double *bn;    // [F][3][3] free vertex (absolute) of local edge e
+  double *out;         // [nnear][6][9]
+};
+
+// One thread per near pair: the k-independent closed-form integrals of
+// source face n at the test points of face m, contracted with the test RWG
+// functions: Dm1, D1, Hm1, H1, Km1, K1 (each 3x3, row p = test edge).
+template <int NQ>
+__global__ void __launch_bounds__(128) near_static_kernel(StaticArgs a) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.nnear) return;
+  const int m = a.near_m[j], n = a.near_n[j];
+  const FaceGeo g = a.geo[n];
+  const double An = a.area[n], Am = a.area[m];
+  double acc[6][9];
+#pragma unroll
+  for (int o = 0; o < 6; o++)
+#pragma unroll
+    for (int i = 0; i < 9; i++) acc[o][i] = 0.0;
+  for (int t = 0; t < NQ; t++) {
+    const double *r = a.qabs + ((size_t)m * NQ + t) * 3;
+    const double wt = c_qw[t];
+    double Lm1[3], L1[3], L3[3];
+    // intSm1 (int.f90:181-226) decides per edge whether intLm1 is needed
+    // when h == 0; intL1 always calls intLm1 unless R02 == 0.
+    double r1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
+    double h = dot3(g.n, r1);
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      Lm1[e] = d_intLm1(r, g, e);
+      d_intL13(r, g, e, g.n, Lm1[e], &L1[e], &L3[e]);
+    }
+    double tt[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      double re[3] = {r[0] - g.v[e][0], r[1] - g.v[e][1], r[2] - g.v[e][2]};
+      tt[e] = dot3(g.mm[e], re);
+    }
+    double Sm3h = d_intSm3h(r, g);
+    double Sm1;
+    if (h == 0) {
+      double e1 = tt[0] == 0 ? 0.0 : Lm1[0], e2 = tt[1] == 0 ? 0.0 : Lm1[1], e3 = tt[2] == 0 ? 0.0 : Lm1[2];
+      Sm1 = -(tt[0] * e1 + tt[1] * e2 + tt[2] * e3);
+    } else {
+      Sm1 = -h * Sm3h - (tt[0] * Lm1[0] + tt[1] * Lm1[1] + tt[2] * Lm1[2]);
+    }
+    double S1 = (h * h) / 3.0 * Sm1 - 1.0 / 3.0 * (tt[0] * L1[0] + tt[1] * L1[1] + tt[2] * L1[2]);
+    double rho[3], K3m1[3], K31[3], mL1[3], mL3[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      rho[i] = r[i] - h * g.n[i];
+      mL1[i] = g.mm[0][i] * L1[0] + g.mm[1][i] * L1[1] + g.mm[2][i] * L1[2];
+      mL3[i] = g.mm[0][i] * L3[0] + g.mm[1][i] * L3[1] + g.mm[2][i] * L3[2];
+      K3m1[i] = g.mm[0][i] * Lm1[0] + g.mm[1][i] * Lm1[1] + g.mm[2][i] * Lm1[2] + g.n[i] * Sm3h;
+      K31[i] = (h == 0) ? mL1[i] : mL1[i] - h * g.n[i] * Sm1;
+    }
+    // test functions at r: f_p = sl_p/(2 Am) (r - u_p), div f_p = sl_p / Am
+    double fp[3][3], dvp[3];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const double slp = a.sl[3 * m + p];
+      const double *u = a.bn + 9 * m + 3 * p;
+#pragma unroll
+      for (int i = 0; i < 3; i++) fp[p][i] = slp / (2.0 * Am) * (r[i] - u[i]);
+      dvp[p] = slp / Am;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const double slq = a.sl[3 * n + q];
+      const double cq = slq / (2.0 * An);
+      const double *pq = a.bn + 9 * n + 3 * q;
+      double K2m1[3], K21[3], K4m1[3], K41[3], rpq[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        K2m1[i] = cq * (mL1[i] + (rho[i] - pq[i]) * Sm1);
+        K21[i] = cq * (1.0 / 3.0 * mL3[i] + (rho[i] - pq[i]) * S1);
+        rpq[i] = r[i] - pq[i];
+      }
+      K4m1[0] = -cq * (rpq[1] * K3m1[2] - rpq[2] * K3m1[1]);
+      K4m1[1] = -cq * (rpq[2] * K3m1[0] - rpq[0] * K3m1[2]);
+      K4m1[2] = -cq * (rpq[0] * K3m1[1] - rpq[1] * K3m1[0]);
+      K41[0] = -cq * (rpq[1] * K31[2] - rpq[2] * K31[1]);
+      K41[1] = -cq * (rpq[2] * K31[0] - rpq[0] * K31[2]);
+      K41[2] = -cq * (rpq[0] * K31[1] - rpq[1] * K31[0]);
+      const double K1m1 = slq / An * Sm1, K11 = slq / An * S1;
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+        const int pq_ = 3 * p + q;
+        acc[0][pq_] += wt * dot3(fp[p], K2m1);
+        acc[1][pq_] += wt * dot3(fp[p], K21);
+        acc[2][pq_] += wt * dvp[p] * K1m1;
+        acc[3][pq_] += wt * dvp[p] * K11;
+        acc[4][pq_] += wt * dot3(fp[p], K4m1);
+        acc[5][pq_] += wt * dot3(fp[p], K41);
+      }
+    }
+  }
+  double *o = a.out + j * 54;
+  const bool self = (m == n);
+#pragma unroll
+  for (int k = 0; k < 6; k++)
+#pragma unroll
+    for (int i = 0; i < 9; i++) o[9 * k + i] = (self && k >= 4) ? 0.0 : acc[k][i] * Am;
+}
+
+struct NearArgs {
+  int64_t nnear;
+  int F;
+  const int *near_m, *near_n;
+  const double *qrel, *cp, *mu, *sl;
+  const double *stat;  // [nnear][54]
+  double kr, ki;
+  Cd c1, c2;           // -i w mu0, -1/(i w eps0 n^2)
+  Cd k2;               // k^2
+  double2 *blk;
+};
+
+// Per wavelength, FP64: smoothed-G quadrature of each near pair (one thread
+// per pair) plus the closed-form terms; overwrites the pair's block.
+template <int NQ>
+__global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.nnear) return;
+  const int m = a.near_m[j], n = a.near_n[j];
+  double d[3], mu[3][3], nu[3][3], slp[3], slq[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    d[i] = a.cp[3 * m + i] - a.cp[3 * n + i];
+    slp[i] = a.sl[3 * m + i];
+    slq[i] = a.sl[3 * n + i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      mu[i][k] = a.mu[9 * m + 3 * i + k];
+      nu[i][k] = a.mu[9 * n + 3 * i + k];
+    }
+  }
+  Moments<double> Mt;
+  pair_moments<double, NQ, true>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)n * NQ * 3, 1, d, a.kr, a.ki, Mt);
+  double2 out[18];
+  const Cd fD = {a.c1.re * kOofpi / 4.0, a.c1.im * kOofpi / 4.0};
+  const Cd fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
+  blocks_from_moments<double>(Mt, mu, nu, slp, slq, d, fD, fH, kOofpi / 4.0, m == n, out);
+  // closed-form parts: (1/(4 pi)) X_m1 - (k^2/(8 pi)) X_1
+  const double *st = a.stat + j * 54;
+  const double f4 = 1.0 / (4.0 * kPi);
+  const Cd f8 = {a.k2.re / (8.0 * kPi), a.k2.im / (8.0 * kPi)};
+  double2 *dst = a.blk + ((size_t)m * a.F + n) * 18;
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    Cd dterm = {f4 * st[i] - f8.re * st[9 + i], -f8.im * st[9 + i]};
+    Cd hterm = {f4 * st[18 + i] - f8.re * st[27 + i], -f8.im * st[27 + i]};
+    Cd kterm = {f4 * st[36 + i] - f8.re * st[45 + i], -f8.im * st[45 + i]};
+    Cd sD = cmul(a.c1, dterm), sH = cmul(a.c2, hterm);
+    double2 s = out[2 * i], k = out[2 * i + 1];
+    s.x += sD.re + sH.re;
+    s.y += sD.im + sH.im;
+    k.x += kterm.re;
+    k.y += kterm.im;
+    dst[2 * i] = s;
+    dst[2 * i + 1] = k;
+  }
+}
+
+struct GatherArgs {
+  int F, Nd, N;
+  const int *eh;    // [Nd][2]
+  const int *epar;  // [Nd]
+  const double2 *blk;
+  Cd Zsi;
+  double2 *A;
+  int64_t lda;
+};
+
+// Thread per domain edge pair (e1 fastest): S = sum of the face-pair blocks
+// over the (+,-) halves of e1 and e2, then the four PMCHWT blocks.
+__global__ void __launch_bounds__(256) gather_kernel(GatherArgs a) {
+  const int e1 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e2 = blockIdx.y;
+  if (e1 >= a.Nd) return;
+  const int h1[2] = {a.eh[2 * e1], a.eh[2 * e1 + 1]};
+  const int h2[2] = {a.eh[2 * e2], a.eh[2 * e2 + 1]};
+  double sr = 0, si = 0, kr = 0, ki = 0;
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    if (h1[i] < 0) continue;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      if (h2[j] < 0) continue;
+      const int m = h1[i] / 3, p = h1[i] % 3, n = h2[j] / 3, q = h2[j] % 3;
+      const double4 v = *reinterpret_cast<const double4 *>(a.blk + ((size_t)m * a.F + n) * 18 + 2 * (3 * p + q));
+      sr += v.x;
+      si += v.y;
+      kr += v.z;
+      ki += v.w;
+    }
+  }
+  const int64_t r = a.epar[e1], c = a.epar[e2];
+  const int64_t N = a.N;
+  double2 *A = a.A;
+  double2 t;
+  t = A[r + c * a.lda];
+  t.x += sr;
+  t.y += si;
+  A[r + c * a.lda] = t;
+  t = A[(r + N) + (c + N) * a.lda];
+  t.x += a.Zsi.re * sr - a.Zsi.im * si;
+  t.y += a.Zsi.re * si + a.Zsi.im * sr;
+  A[(r + N) + (c + N) * a.lda] = t;
+  t = A[(r + N) + c * a.lda];
+  t.x += kr;
+  t.y += ki;
+  A[(r + N) + c * a.lda] = t;
+  t = A[r + (c + N) * a.lda];
+  t.x -= kr;
+  t.y -= ki;
+  A[r + (c + N) * a.lda] = t;
+}
+
+// Rows/columns 2N..n-1 pad the matrix to a multiple of the panel width with
+// an identity block, which leaves the LU of the leading 2N x 2N part as is.
+__global__ void pad_identity(double2 *A, int64_t lda, int64_t n2, int64_t n) {
+  const int64_t i = n2 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[i + i * lda] = make_double2(1.0, 0.0);
+}
+
+__global__ void convert_to_fp32(const double2 *__restrict__ A, float2 *__restrict__ B, int64_t count) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; i < count; i += stride) {
+    double2 v = A[i];
+    B[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+template <typename T>
+int launch_pair(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
+  switch (nq) {
+    case 1: pair_kernel<T, 1><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 3: pair_kernel<T, 3><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 4: pair_kernel<T, 4><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 7: pair_kernel<T, 7><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 13: pair_kernel<T, 13><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+  }
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+}  // namespace
+
+
+int upload_quadrature(Ctx *c) {
+  MOM_CUDA(c, cudaMemcpyToSymbolAsync(c_qw, c->qw, sizeof(c->qw), 0, cudaMemcpyHostToDevice, c->stream));
+  MOM_CUDA(c, cudaMemcpyToSymbolAsync(c_qn, c->qn, sizeof(c->qn), 0, cudaMemcpyHostToDevice, c->stream));
+  return MOM_OK;
+}
+
+// Near pairs of domain d (sysmat.f90:233-260: |cp_m - cp_n|^2 < (3 avelen)^2
+// with the domain's own average edge length) and their closed-form terms.
+// The list is wavelength independent and built once per geometry.
+int near_precompute(Ctx *c, int d) {
+  DomDev &D = c->dom[d];
+  const int F = D.F;
+  const double thr = D.avelen * 3;
+  std::vector<int> nm, nn;
+  for (int m = 0; m < F; m++) {
+    const double *cm = &D.h_cp[3 * (size_t)m];
+    for (int n = 0; n < F; n++) {
+      const double *cn = &D.h_cp[3 * (size_t)n];
+      const double d0 = cm[0] - cn[0], d1 = cm[1] - cn[1], d2 = cm[2] - cn[2];
+      const double distsq = d0 * d0 + d1 * d1 + d2 * d2;
+      if (distsq < thr * thr) {
+        nm.push_back(m);
+        nn.push_back(n);
+      }
+    }
+  }
+  D.nnear = (int64_t)nm.size();
+  const size_t cap = (size_t)std::max<int64_t>(1, D.nnear);
+  MOM_CUDA(c, cudaMalloc(&D.near_m, sizeof(int) * cap));
+  MOM_CUDA(c, cudaMalloc(&D.near_n, sizeof(int) * cap));
+  MOM_CUDA(c, cudaMalloc(&D.near_static, sizeof(double) * 54 * cap));
+  if (D.nnear == 0) return MOM_OK;
+  MOM_CUDA(c, cudaMemcpyAsync(D.near_m, nm.data(), sizeof(int) * D.nnear, cudaMemcpyHostToDevice, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(D.near_n, nn.data(), sizeof(int) * D.nnear, cudaMemcpyHostToDevice, c->stream));
+  std::vector<FaceGeo> geo(F);
+  for (int f = 0; f < F; f++) {
+    FaceGeo &g = geo[f];
+    for (int k = 0; k < 3; k++)
+      for (int i = 0; i < 3; i++) {
+        g.v[k][i] = D.h_fv[9 * (size_t)f + 3 * k + i];
+        g.s[k][i] = D.h_fs[9 * (size_t)f + 3 * k + i];
+        g.mm[k][i] = D.h_fm[9 * (size_t)f + 3 * k + i];
+      }
+    for (int i = 0; i < 3; i++) g.n[i] = D.h_nrm[3 * (size_t)f + i];
+  }
+  FaceGeo *dgeo = nullptr;
+  double *dbn = nullptr;
+  MOM_CUDA(c, cudaMalloc(&dgeo, sizeof(FaceGeo) * F));
+  MOM_CUDA(c, cudaMalloc(&dbn, sizeof(double) * 9 * F));
+  MOM_CUDA(c, cudaMemcpyAsync(dgeo, geo.data(), sizeof(FaceGeo) * F, cudaMemcpyHostToDevice, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(dbn, D.h_bn.data(), sizeof(double) * 9 * F, cudaMemcpyHostToDevice, c->stream));
+  StaticArgs a;
+  a.nnear = D.nnear;
+  a.near_m = D.near_m;
+  a.near_n = D.near_n;
+  a.geo = dgeo;
+  a.qabs = D.qabs;
+  a.area = D.area;
+  a.sl = D.sl;
+  a.bn = dbn;
+  a.out = D.near_static;
+  const unsigned blocks = (unsigned)((D.nnear + 127) / 128);
+  switch (c->nq) {
+    case 1: near_static_kernel<1><<<blocks, 128, 0, c->stream>>>(a); break;
+    case 3: near_static_kernel<3><<<blocks, 128, 0, c->stream>>>(a); break;
+    case 4: near_static_kernel<4><<<blocks, 128, 0, c->stream>>>(a); break;
+    case 7: near_static_kernel<7><<<blocks, 128, 0, c->stream>>>(a); break;
+    case 13: near_static_kernel<13><<<blocks, 128, 0, c->stream>>>(a); break;
+    default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+  }
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  cudaFree(dgeo);
+  cudaFree(dbn);
+  return MOM_OK;
+}
+
+// sysmat_pmchwt (sysmat.f90:18-105), identity group: A = 0, then for every
+// domain the face-pair blocks (far pairs in the requested precision, near
+// pairs in FP64) are gathered into the four PMCHWT blocks.
+int assemble(Ctx *c, double omega, const double *ri, int precision) {
+  const int64_t n = c->n, lda = c->lda;
+  MOM_CUDA(c, cudaMemsetAsync(c->A, 0, sizeof(double2) * (size_t)lda * n, c->stream));
+  const int64_t n2 = 2 * (int64_t)c->N;
+  if (n > n2) {
+    pad_identity<<<(unsigned)((n - n2 + 127) / 128), 128, 0, c->stream>>>(c->A, lda, n2, n);
+    c->launches++;
+  }
+  for (int d = 0; d < c->ndom; d++) {
+    DomDev &D = c->dom[d];
+    const Cd rid = {ri[2 * d], ri[2 * d + 1]};
+    // k = ri omega / c0 ; c1 = -i omega mu0 ; c2 = -1/(i omega eps0 ri^2) ; Zsi = ri^2/eta0^2
+    const double kr = rid.re * omega / kC0, ki = rid.im * omega / kC0;
+    const Cd c1 = {0.0, -omega * kMu0};
+    const Cd ri2 = {rid.re * rid.re - rid.im * rid.im, 2 * rid.re * rid.im};
+    const Cd den = {-omega * kEps0 * ri2.im, omega * kEps0 * ri2.re};  // i omega eps0 ri^2
+    const double dn2 = den.re * den.re + den.im * den.im;
+    const Cd c2 = {-den.re / dn2, den.im / dn2};
+    const Cd Zsi = {ri2.re / (kEta0 * kEta0), ri2.im / (kEta0 * kEta0)};
+    const double L0 = (precision == MOM_PREC_MIXED) ? D.avelen : 1.0;
+    PairArgs pa;
+    pa.F = D.F;
+    pa.qrel = D.qrel;
+    pa.cp = D.cp;
+    pa.mu = D.mu;
+    pa.sl = D.sl;
+    pa.inv_unit = 1.0 / L0;
+    pa.kr = kr * L0;
+    pa.ki = ki * L0;
+    pa.fD = {c1.re * L0 * L0 * L0 * kOofpi / 4.0, c1.im * L0 * L0 * L0 * kOofpi / 4.0};
+    pa.fH = {c2.re * L0 * kOofpi, c2.im * L0 * kOofpi};
+    pa.fK = L0 * L0 * kOofpi / 4.0;
+    pa.blk = c->blk;
+    dim3 grid((D.F + kPairThreads - 1) / kPairThreads, (D.F + kTestPerCta - 1) / kTestPerCta);
+    if (precision == MOM_PREC_MIXED) {
+      MOM_TRY(launch_pair<float>(c, c->nq, grid, pa));
+    } else {
+      MOM_TRY(launch_pair<double>(c, c->nq, grid, pa));
+    }
+    if (D.nnear > 0) {
+      NearArgs na;
+      na.nnear = D.nnear;
+      na.F = D.F;
+      na.near_m = D.near_m;
+      na.near_n = D.near_n;
+      na.qrel = D.qrel;
+      na.cp = D.cp;
+      na.mu = D.mu;
+      na.sl = D.sl;
+      na.stat = D.near_static;
+      na.kr = kr;
+      na.ki = ki;
+      na.c1 = c1;
+      na.c2 = c2;
+      na.k2 = {kr * kr - ki * ki, 2 * kr * ki};
+      na.blk = c->blk;
+      const unsigned blocks = (unsigned)((D.nnear + 127) / 128);
+      switch (c->nq) {
+        case 1: near_kernel<1><<<blocks, 128, 0, c->stream>>>(na); break;
+        case 3: near_kernel<3><<<blocks, 128, 0, c->stream>>>(na); break;
+        case 4: near_kernel<4><<<blocks, 128, 0, c->stream>>>(na); break;
+        case 7: near_kernel<7><<<blocks, 128, 0, c->stream>>>(na); break;
+        case 13: near_kernel<13><<<blocks, 128, 0, c->stream>>>(na); break;
+        default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+      }
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+    }
+    GatherArgs ga;
+    ga.F = D.F;
+    ga.Nd = D.Nd;
+    ga.N = c->N;
+    ga.eh = D.eh;
+    ga.epar = D.epar;
+    ga.blk = c->blk;
+    ga.Zsi = Zsi;
+    ga.A = c->A;
+    ga.lda = lda;
+    dim3 gg((D.Nd + 255) / 256, D.Nd);
+    gather_kernel<<<gg, 256, 0, c->stream>>>(ga);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  if (precision == MOM_PREC_MIXED) {
+    convert_to_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, (int64_t)lda * n);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  c->assembled = 1;
+  c->factored = -1;
+  return MOM_OK;
+}
+
+}  // namespace mom

@@ -1,0 +1,142 @@
+// Internal declarations of the B200 PMCHWT library (not part of the C ABI).
+#pragma once
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mom_gpu.h"
+
+namespace mom {
+
+// Physical constants as the reference defines them (constants.f90:8-14):
+// pi is the single-precision literal 3.141592653589 widened to double, and
+// it leaks into mu0, 1/(4 pi) and every angle conversion.
+constexpr double kPi = (double)3.141592653589f;
+constexpr double kEps0 = 8.8541878176e-12;
+constexpr double kMu0 = 4 * kPi * 1e-7;
+constexpr double kC0 = 2.997924580003e8;
+constexpr double kEta0 = 3.767303134622e2;
+
+constexpr int kMaxQ = 13;
+
+// Per-domain device data (structure of arrays).  "Half-edge" h = 3*face +
+// local edge identifies one RWG half (one face of an edge).
+struct DomDev {
+  int F = 0, Nd = 0;
+  double avelen = 0;
+  double *qrel = nullptr;  // [F][nq][3] quadrature points minus the face centroid
+  double *qabs = nullptr;  // [F][nq][3] absolute quadrature points
+  double *cp = nullptr;    // [F][3] centroid
+  double *area = nullptr;  // [F]
+  double *nrm = nullptr;   // [F][3] unit normal
+  double *mu = nullptr;    // [F][3][3] free vertex of local edge e minus centroid
+  double *sl = nullptr;    // [F][3] sign * edge length of local edge e
+  int *hpar = nullptr;     // [F][3] global (parent) edge index of local edge e
+  int *eh = nullptr;       // [Nd][2] half-edges (+, -) of domain edge e, -1 if none
+  int *epar = nullptr;     // [Nd] global edge index of domain edge e
+  // Near pairs (sysmat.f90:233-260), wavelength independent.
+  int64_t nnear = 0;
+  int *near_m = nullptr;   // [nnear] test face
+  int *near_n = nullptr;   // [nnear] source face
+  double *near_static = nullptr;  // [nnear][6][9] contracted closed-form terms
+  // Host mirrors used at set-up.
+  std::vector<double> h_cp, h_qrel, h_qabs, h_area, h_nrm, h_mu, h_sl;
+  std::vector<double> h_fv, h_fs, h_fm, h_bn;  // [F][3][3]: vertices, s(:,e), m(:,e), free vertex of e
+  std::vector<int> h_hpar, h_eh, h_epar;
+};
+
+struct Ctx {
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  std::mutex mu;
+  std::string last_error;
+  int64_t launches = 0;
+
+  // Problem
+  int N = 0;  // master edges; 2N unknowns
+  int ndom = 0;
+  int nq = 0;
+  double qw[kMaxQ] = {0};
+  double qn[kMaxQ][3] = {{0}};
+  std::vector<DomDev> dom;
+  bool have_problem = false;
+
+  // System matrix and factors
+  int64_t n = 0, lda = 0;  // n = 2N
+  double2 *A = nullptr;    // FP64 matrix (LU in place in FP64 mode)
+  float2 *A32 = nullptr;   // FP32 copy (LU in place in mixed mode)
+  size_t A_bytes = 0, A32_bytes = 0;
+  double2 *blk = nullptr;  // face-pair blocks, [F][F][9][2] of the largest domain
+  size_t blk_bytes = 0;
+  int *ipiv = nullptr;     // [n]
+  double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
+  size_t invd_bytes = 0;
+  int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout, [2..] barrier counters
+  void *ws = nullptr;      // general device workspace
+  size_t ws_bytes = 0;
+  int assembled = 0;       // 0 none, 1 FP64 matrix present
+  int factored = -1;       // precision of the factors in place, -1 none
+  int nb = 64;             // panel width
+
+  // Right-hand sides / solutions
+  int nsrc = 0;
+  double2 *B = nullptr;    // [nsrc][n] right-hand sides
+  double2 *X = nullptr;    // [nsrc][n] solutions
+  size_t BX_cap = 0;
+  double2 *Xh = nullptr;   // solutions uploaded from the host for post-processing
+  size_t Xh_cap = 0;
+  std::vector<mom_src> srcs;
+  double omega_rhs = 0;
+  double ri1[2] = {1, 0};
+
+  // Host-side staging (pinned)
+  double *pinned = nullptr;
+  size_t pinned_bytes = 0;
+};
+
+// Error helpers
+int fail(Ctx *c, int code, const std::string &msg);
+int cuda_fail(Ctx *c, cudaError_t e, const char *where);
+#define MOM_CUDA(c, expr)                                      \
+  do {                                                         \
+    cudaError_t _e = (expr);                                   \
+    if (_e != cudaSuccess) return ::mom::cuda_fail(c, _e, #expr); \
+  } while (0)
+#define MOM_BLAS(c, expr)                                                              \
+  do {                                                                                 \
+    cublasStatus_t _s = (expr);                                                        \
+    if (_s != CUBLAS_STATUS_SUCCESS)                                                   \
+      return ::mom::fail(c, MOM_ERR_CUDA, std::string("cuBLAS error ") + std::to_string((int)_s) + " in " #expr); \
+  } while (0)
+#define MOM_TRY(expr)        \
+  do {                       \
+    int _r = (expr);         \
+    if (_r != MOM_OK) return _r; \
+  } while (0)
+
+int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes);
+
+// assemble.cu
+int upload_quadrature(Ctx *c);
+int near_precompute(Ctx *c, int d);
+int assemble(Ctx *c, double omega, const double *ri, int precision);
+
+// lu.cu
+int lu_factor(Ctx *c, int precision);
+int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
+
+// post.cu
+int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src);
+int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src,
+                   const double2 *xdev, int64_t ldx, double *csca, double *cabs);
+int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
+              double *rcs);
+
+}  // namespace mom

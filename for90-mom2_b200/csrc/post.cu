@@ -1,0 +1,481 @@
+// Excitation and post-processing reductions on sm_100a (FP64):
+//   rhs      -> srcvec / src_field_frags / pw_fields(_elliptic)
+//               (source.f90:84-125, 136-315) for identity symmetry;
+//   cs       -> cs_prtsrf (cs.f90:14-104);
+//   farfield -> far_fields / rcs_ext / rcs (ffields.f90:16-122, 203-266).
+// Each edge receives contributions from its two faces; those are computed
+// per half-edge and summed per edge in a second pass, so results are
+// deterministic (the reference adds them in face order).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "mom_internal.h"
+
+namespace mom {
+
+namespace {
+
+struct SrcDev {
+  double dir[3], pol[3];
+  double ph_re, ph_im;  // pw_elliptic phase
+  int type;
+};
+
+struct Z {
+  double re, im;
+};
+__device__ __forceinline__ Z zmul(Z a, Z b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ Z zadd(Z a, Z b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ Z zsub(Z a, Z b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ Z zscale(Z a, double s) { return {a.re * s, a.im * s}; }
+__device__ __forceinline__ Z zconj(Z a) { return {a.re, -a.im}; }
+__device__ __forceinline__ void zcross(const Z *a, const Z *b, Z *r) {
+  r[0] = zsub(zmul(a[1], b[2]), zmul(a[2], b[1]));
+  r[1] = zsub(zmul(a[2], b[0]), zmul(a[0], b[2]));
+  r[2] = zsub(zmul(a[0], b[1]), zmul(a[1], b[0]));
+}
+__device__ __forceinline__ Z zexp_i(Z k, double s) {  // exp(i k s)
+  double sn, cs;
+  sincos(k.re * s, &sn, &cs);
+  const double a = exp(-k.im * s);
+  return {a * cs, a * sn};
+}
+
+// pw_fields / pw_fields_elliptic (source.f90:84-125) at point pt.
+__device__ void src_fields(const SrcDev &S, Z k, double omega, const double *pt, Z *ef, Z *hf) {
+  const double kd = S.dir[0] * pt[0] + S.dir[1] * pt[1] + S.dir[2] * pt[2];
+  const Z ph = zexp_i(k, kd);
+  Z dc[3] = {{S.dir[0], 0}, {S.dir[1], 0}, {S.dir[2], 0}};
+  if (S.type == MOM_SRC_PW) {
+    for (int i = 0; i < 3; i++) ef[i] = zscale(ph, S.pol[i]);
+  } else {
+    Z efx[3], efy[3];
+    for (int i = 0; i < 3; i++) efx[i] = zscale(ph, S.pol[i]);
+    zcross(dc, efx, efy);
+    const Z phase = {S.ph_re, S.ph_im};
+    double nn = 0;
+    for (int i = 0; i < 3; i++) {
+      ef[i] = zadd(efx[i], zmul(phase, efy[i]));
+      nn += ef[i].re * ef[i].re + ef[i].im * ef[i].im;
+    }
+    nn = sqrt(nn);
+    for (int i = 0; i < 3; i++) ef[i] = {ef[i].re / nn, ef[i].im / nn};
+  }
+  Z c[3];
+  zcross(dc, ef, c);
+  const Z kk = {k.re / (omega * kMu0), k.im / (omega * kMu0)};
+  for (int i = 0; i < 3; i++) hf[i] = zmul(kk, c[i]);
+}
+
+struct RhsArgs {
+  double w[kMaxQ];
+  int F, nq;
+  const double *qabs, *area, *sl, *mu, *cp;
+  const SrcDev *src;
+  int nsrc;
+  Z k;
+  double omega;
+  double2 *half;  // [nsrc][F][3][2]  (E part, H part)
+};
+
+// Thread per (face, source): <f_p, E_inc>, <f_p, H_inc> for the three RWG
+// halves of the face (source.f90:214-246).
+__global__ void rhs_half_kernel(RhsArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (f >= a.F) return;
+  const SrcDev S = a.src[s];
+  Z Ie[3] = {{0, 0}, {0, 0}, {0, 0}}, Ih[3] = {{0, 0}, {0, 0}, {0, 0}};
+  const double Am = a.area[f];
+  for (int r = 0; r < a.nq; r++) {
+    const double *pt = a.qabs + ((size_t)f * a.nq + r) * 3;
+    Z ef[3], hf[3];
+    src_fields(S, a.k, a.omega, pt, ef, hf);
+    const double w = a.w[r];
+    for (int p = 0; p < 3; p++) {
+      // f_p(r) = sl_p / (2 Am) (r - v_p),  v_p = cp + mu_p
+      const double cc = a.sl[3 * f + p] / (2.0 * Am);
+      double fm[3];
+      for (int i = 0; i < 3; i++) fm[i] = cc * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * p + i]));
+      Z de = {0, 0}, dh = {0, 0};
+      for (int i = 0; i < 3; i++) {
+        de = zadd(de, zscale(ef[i], fm[i]));
+        dh = zadd(dh, zscale(hf[i], fm[i]));
+      }
+      Ie[p] = zadd(Ie[p], zscale(de, w));
+      Ih[p] = zadd(Ih[p], zscale(dh, w));
+    }
+  }
+  double2 *o = a.half + (((size_t)s * a.F + f) * 3) * 2;
+  for (int p = 0; p < 3; p++) {
+    o[2 * p] = make_double2(Ie[p].re * Am, Ie[p].im * Am);
+    o[2 * p + 1] = make_double2(Ih[p].re * Am, Ih[p].im * Am);
+  }
+}
+
+// Per domain edge: q[J] = sum of the halves' E parts, q[M] = H parts.
+__global__ void rhs_edge_kernel(int Nd, int F, int N, int64_t ldb, const int *eh, const int *epar,
+                                const double2 *half, double2 *B) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (e >= Nd) return;
+  double2 qe = make_double2(0, 0), qh = make_double2(0, 0);
+  int h[2] = {eh[2 * e], eh[2 * e + 1]};
+  if (h[0] >= 0 && h[1] >= 0 && h[1] < h[0]) {  // face order, as the reference accumulates
+    int t = h[0];
+    h[0] = h[1];
+    h[1] = t;
+  }
+  for (int i = 0; i < 2; i++) {
+    if (h[i] < 0) continue;
+    const double2 *v = half + (((size_t)s * F) * 3 + h[i]) * 2;
+    qe.x += v[0].x;
+    qe.y += v[0].y;
+    qh.x += v[1].x;
+    qh.y += v[1].y;
+  }
+  const int64_t r = epar[e];
+  B[(size_t)s * ldb + r] = qe;
+  B[(size_t)s * ldb + r + N] = qh;
+}
+
+struct CsArgs {
+  double w[kMaxQ];
+  int F, nq, N;
+  const double *qabs, *area, *sl, *mu, *cp, *nrm;
+  const int *hpar;
+  const SrcDev *src;
+  const double2 *x;
+  int64_t ldx;
+  Z k;
+  double omega;
+  double *part;  // [nsrc][gridDim.x][2]
+};
+
+// cs_prtsrf: per face the Poynting flux of total and scattered tangential
+// fields at the quadrature points; block partial sums.
+__global__ void __launch_bounds__(256) cs_kernel(CsArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  double i1 = 0, i2 = 0;
+  if (f < a.F) {
+    const SrcDev S = a.src[s];
+    const double2 *x = a.x + (size_t)s * a.ldx;
+    const double An = a.area[f];
+    const double *nor = a.nrm + 3 * f;
+    const Z nc[3] = {{nor[0], 0}, {nor[1], 0}, {nor[2], 0}};
+    Z al[3], be[3];
+    for (int p = 0; p < 3; p++) {
+      const int idx = a.hpar[3 * f + p];
+      al[p] = {x[idx].x, x[idx].y};
+      be[p] = {x[idx + a.N].x, x[idx + a.N].y};
+    }
+    double int1 = 0, int2 = 0;
+    for (int t = 0; t < a.nq; t++) {
+      const double *pt = a.qabs + ((size_t)f * a.nq + t) * 3;
+      Z Et[3] = {{0, 0}, {0, 0}, {0, 0}}, Ht[3] = {{0, 0}, {0, 0}, {0, 0}};
+      for (int p = 0; p < 3; p++) {
+        const double cc = a.sl[3 * f + p] / (2.0 * An);
+        double fr[3], fn[3];
+        for (int i = 0; i < 3; i++) fr[i] = cc * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * p + i]));
+        fn[0] = nor[1] * fr[2] - nor[2] * fr[1];
+        fn[1] = nor[2] * fr[0] - nor[0] * fr[2];
+        fn[2] = nor[0] * fr[1] - nor[1] * fr[0];
+        for (int i = 0; i < 3; i++) {
+          Ht[i] = zsub(Ht[i], zscale(al[p], fn[i]));
+          Et[i] = zadd(Et[i], zscale(be[p], fn[i]));
+        }
+      }
+      Z einc[3], hinc[3], t1[3], Eti[3], Hti[3], Ets[3], Hts[3], cr[3], cj[3];
+      src_fields(S, a.k, a.omega, pt, einc, hinc);
+      zcross(nc, hinc, t1);
+      zcross(t1, nc, Hti);
+      zcross(nc, einc, t1);
+      zcross(t1, nc, Eti);
+      for (int i = 0; i < 3; i++) {
+        Hts[i] = zsub(Ht[i], Hti[i]);
+        Ets[i] = zsub(Et[i], Eti[i]);
+        cj[i] = zconj(Ht[i]);
+      }
+      zcross(Et, cj, cr);
+      double Sn = 0.5 * (cr[0].re * nor[0] + cr[1].re * nor[1] + cr[2].re * nor[2]);
+      const double w = a.w[t];
+      int1 += w * Sn;
+      for (int i = 0; i < 3; i++) cj[i] = zconj(Hts[i]);
+      zcross(Ets, cj, cr);
+      Sn = 0.5 * (cr[0].re * nor[0] + cr[1].re * nor[1] + cr[2].re * nor[2]);
+      int2 += w * Sn;
+    }
+    i1 = int1 * An;
+    i2 = int2 * An;
+  }
+  // deterministic block reduction
+  __shared__ double r1[256], r2[256];
+  r1[threadIdx.x] = i1;
+  r2[threadIdx.x] = i2;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      r1[threadIdx.x] += r1[threadIdx.x + w];
+      r2[threadIdx.x] += r2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.part[((size_t)s * gridDim.x + blockIdx.x) * 2] = r1[0];
+    a.part[((size_t)s * gridDim.x + blockIdx.x) * 2 + 1] = r2[0];
+  }
+}
+
+struct FfArgs {
+  double w[kMaxQ];
+  int F, nq, N;
+  const double *qabs, *area, *sl, *mu, *cp;
+  const int *hpar;
+  const double2 *x;
+  double4 *cur;  // [F*nq][3]: (J re, J im, M re, M im) per component, weighted by w A
+  double *pos;   // [F*nq][3]
+};
+
+// Weighted surface currents at every quadrature point (ffields.f90:70-80):
+// J = sum_q alpha_q f_q, M = sum_q beta_q f_q, times w_t A_n.
+__global__ void ff_current_kernel(FfArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.F * a.nq) return;
+  const int f = j / a.nq, t = j % a.nq;
+  const double *pt = a.qabs + (size_t)j * 3;
+  const double An = a.area[f];
+  const double w = a.w[t] * An;
+  double J[3][2] = {{0, 0}, {0, 0}, {0, 0}}, M[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  for (int q = 0; q < 3; q++) {
+    const int idx = a.hpar[3 * f + q];
+    const double2 al = a.x[idx], be = a.x[idx + a.N];
+    const double cc = a.sl[3 * f + q] / (2.0 * An);
+    for (int i = 0; i < 3; i++) {
+      const double fi = cc * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * q + i]));
+      J[i][0] += fi * al.x;
+      J[i][1] += fi * al.y;
+      M[i][0] += fi * be.x;
+      M[i][1] += fi * be.y;
+    }
+  }
+  for (int i = 0; i < 3; i++) {
+    a.cur[(size_t)j * 3 + i] = make_double4(w * J[i][0], w * J[i][1], w * M[i][0], w * M[i][1]);
+    a.pos[(size_t)j * 3 + i] = pt[i];
+  }
+}
+
+constexpr int kFfThreads = 128;
+constexpr int kFfTile = 128;
+
+// One thread per direction: N and L radiation vectors by the phasor sum over
+// all weighted quadrature points, then E_theta, E_phi at r = 1 m.
+__global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const double4 *cur, const double *pos,
+                                                            int ntheta, int nphi, Z k, Z ri, double *rcs) {
+  __shared__ double4 s_cur[kFfTile][3];
+  __shared__ double s_pos[kFfTile][3];
+  const int dirx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nd = ntheta * nphi;
+  const int it = dirx % ntheta, ip = dirx / ntheta;
+  const double theta = kPi * (double)it / (double)(ntheta - 1);
+  const double phi = 2.0 * kPi * (double)ip / (double)(nphi - 1);
+  double st, ct, sp, cp;
+  sincos(theta, &st, &ct);
+  sincos(phi, &sp, &cp);
+  const double ux = st * cp, uy = st * sp, uz = ct;
+  Z Nt = {0, 0}, Np = {0, 0}, Lt = {0, 0}, Lp = {0, 0};
+  for (int base = 0; base < npts; base += kFfTile) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kFfTile; i += blockDim.x) {
+      const int j = base + i;
+      for (int c = 0; c < 3; c++) {
+        s_cur[i][c] = (j < npts) ? cur[(size_t)j * 3 + c] : make_double4(0, 0, 0, 0);
+        s_pos[i][c] = (j < npts) ? pos[(size_t)j * 3 + c] : 0.0;
+      }
+    }
+    __syncthreads();
+    const int cnt = min(kFfTile, npts - base);
+    for (int i = 0; i < cnt; i++) {
+      const double s = s_pos[i][0] * ux + s_pos[i][1] * uy + s_pos[i][2] * uz;
+      // phasor = exp(-i k s)
+      double sn, cs;
+      sincos(-k.re * s, &sn, &cs);
+      const double am = exp(k.im * s);
+      const Z ph = {am * cs, am * sn};
+      const double4 jx = s_cur[i][0], jy = s_cur[i][1], jz = s_cur[i][2];
+      // theta and phi projections
+      const Z jt = {ct * cp * jx.x + ct * sp * jy.x - st * jz.x, ct * cp * jx.y + ct * sp * jy.y - st * jz.y};
+      const Z jp = {-sp * jx.x + cp * jy.x, -sp * jx.y + cp * jy.y};
+      const Z mt = {ct * cp * jx.z + ct * sp * jy.z - st * jz.z, ct * cp * jx.w + ct * sp * jy.w - st * jz.w};
+      const Z mp = {-sp * jx.z + cp * jy.z, -sp * jx.w + cp * jy.w};
+      Nt = zadd(Nt, zmul(jt, ph));
+      Np = zadd(Np, zmul(jp, ph));
+      Lt = zadd(Lt, zmul(mt, ph));
+      Lp = zadd(Lp, zmul(mp, ph));
+    }
+  }
+  if (dirx >= nd) return;
+  // prefix = i k exp(i k r) / (4 pi r), r = 1
+  const Z e = zexp_i(k, 1.0);
+  const Z ik = {-k.im, k.re};
+  Z prefix = zmul(ik, e);
+  prefix = zscale(prefix, 1.0 / (4.0 * kPi * 1.0));
+  // eta0 / ri
+  const double rr = ri.re * ri.re + ri.im * ri.im;
+  const Z er = {kEta0 * ri.re / rr, -kEta0 * ri.im / rr};
+  const Z et = zmul(prefix, zadd(Lp, zmul(er, Nt)));
+  const Z ep = zscale(zmul(prefix, zsub(Lt, zmul(er, Np))), -1.0);
+  const double a = hypot(et.re, et.im), b = hypot(ep.re, ep.im);
+  rcs[(size_t)it + (size_t)ip * ntheta] = a * a + b * b;
+}
+
+void make_src(const mom_src &s, SrcDev &d) {
+  // get_dir / get_pol (aux.f90:245-261), evaluated on the host in FP64.
+  const double th = s.theta, ph = s.phi, ps = (s.type == MOM_SRC_PW) ? s.psi : 0.0;
+  d.dir[0] = sin(th) * cos(ph);
+  d.dir[1] = sin(th) * sin(ph);
+  d.dir[2] = cos(th);
+  d.pol[0] = cos(ps) * sin(ph) - sin(ps) * cos(th) * cos(ph);
+  d.pol[1] = -cos(ps) * cos(ph) - sin(ps) * cos(th) * sin(ph);
+  d.pol[2] = sin(ps) * sin(th);
+  d.ph_re = s.phase_re;
+  d.ph_im = s.phase_im;
+  d.type = s.type;
+}
+
+int upload_sources(Ctx *c, int nsrc, const mom_src *src, SrcDev **out) {
+  std::vector<SrcDev> h(nsrc);
+  for (int i = 0; i < nsrc; i++) {
+    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC)
+      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+    make_src(src[i], h[i]);
+  }
+  const size_t bytes = sizeof(SrcDev) * nsrc;
+  char *ws = (char *)c->ws;
+  *out = reinterpret_cast<SrcDev *>(ws);
+  MOM_CUDA(c, cudaMemcpyAsync(*out, h.data(), bytes, cudaMemcpyHostToDevice, c->stream));
+  return MOM_OK;
+}
+
+}  // namespace
+
+// srcvec for all sources on domain 1's mesh: B[:, s] (2N each, ld = n).
+int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src) {
+  const DomDev &D = c->dom[0];
+  const size_t src_bytes = ((sizeof(SrcDev) * nsrc + 255) / 256) * 256;
+  const size_t half_bytes = sizeof(double2) * 6 * (size_t)D.F * nsrc;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, src_bytes + half_bytes));
+  SrcDev *dsrc = nullptr;
+  MOM_TRY(upload_sources(c, nsrc, src, &dsrc));
+  RhsArgs a;
+  for (int i = 0; i < kMaxQ; i++) a.w[i] = c->qw[i];
+  a.F = D.F;
+  a.nq = c->nq;
+  a.qabs = D.qabs;
+  a.area = D.area;
+  a.sl = D.sl;
+  a.mu = D.mu;
+  a.cp = D.cp;
+  a.src = dsrc;
+  a.nsrc = nsrc;
+  a.k = {ri1[0] * omega / kC0, ri1[1] * omega / kC0};
+  a.omega = omega;
+  a.half = reinterpret_cast<double2 *>((char *)c->ws + src_bytes);
+  MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * c->n * nsrc, c->stream));
+  rhs_half_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(a);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  rhs_edge_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(D.Nd, D.F, c->N, c->n, D.eh, D.epar, a.half,
+                                                                           c->B);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src,
+                   const double2 *xdev, int64_t ldx, double *csca, double *cabs) {
+  const DomDev &D = c->dom[dom];
+  const int blocks = (D.F + 255) / 256;
+  const size_t src_bytes = ((sizeof(SrcDev) * nsrc + 255) / 256) * 256;
+  const size_t part_bytes = sizeof(double) * 2 * (size_t)blocks * nsrc;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, src_bytes + part_bytes));
+  SrcDev *dsrc = nullptr;
+  MOM_TRY(upload_sources(c, nsrc, src, &dsrc));
+  CsArgs a;
+  for (int i = 0; i < kMaxQ; i++) a.w[i] = c->qw[i];
+  a.F = D.F;
+  a.nq = c->nq;
+  a.N = c->N;
+  a.qabs = D.qabs;
+  a.area = D.area;
+  a.sl = D.sl;
+  a.mu = D.mu;
+  a.cp = D.cp;
+  a.nrm = D.nrm;
+  a.hpar = D.hpar;
+  a.src = dsrc;
+  a.x = xdev;
+  a.ldx = ldx;
+  a.k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
+  a.omega = omega;
+  a.part = reinterpret_cast<double *>((char *)c->ws + src_bytes);
+  cs_kernel<<<dim3(blocks, nsrc), 256, 0, c->stream>>>(a);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  std::vector<double> part(2 * (size_t)blocks * nsrc);
+  MOM_CUDA(c, cudaMemcpyAsync(part.data(), a.part, part_bytes, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  const double cc = 2.0 / (kEps0 * kC0 * ri[0]);  // cs.f90:38
+  for (int s = 0; s < nsrc; s++) {
+    double ab = 0, sc = 0;
+    for (int b = 0; b < blocks; b++) {
+      ab += part[((size_t)s * blocks + b) * 2];
+      sc += part[((size_t)s * blocks + b) * 2 + 1];
+    }
+    cabs[s] = -cc * ab;
+    csca[s] = cc * sc;
+  }
+  return MOM_OK;
+}
+
+int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
+              double *rcs) {
+  const DomDev &D = c->dom[dom];
+  const int npts = D.F * c->nq;
+  const int nd = ntheta * nphi;
+  const size_t cur_bytes = sizeof(double4) * 3 * (size_t)npts;
+  const size_t pos_bytes = sizeof(double) * 3 * (size_t)npts;
+  const size_t out_bytes = sizeof(double) * (size_t)nd;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, cur_bytes + pos_bytes + out_bytes + 512));
+  FfArgs a;
+  for (int i = 0; i < kMaxQ; i++) a.w[i] = c->qw[i];
+  a.F = D.F;
+  a.nq = c->nq;
+  a.N = c->N;
+  a.qabs = D.qabs;
+  a.area = D.area;
+  a.sl = D.sl;
+  a.mu = D.mu;
+  a.cp = D.cp;
+  a.hpar = D.hpar;
+  a.x = xdev;
+  a.cur = reinterpret_cast<double4 *>(c->ws);
+  a.pos = reinterpret_cast<double *>((char *)c->ws + cur_bytes);
+  double *dout = reinterpret_cast<double *>((char *)c->ws + cur_bytes + pos_bytes);
+  ff_current_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  const Z k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
+  const Z rz = {ri[0], ri[1]};
+  ff_dir_kernel<<<(nd + kFfThreads - 1) / kFfThreads, kFfThreads, 0, c->stream>>>(npts, a.cur, a.pos, ntheta, nphi,
+                                                                                 k, rz, dout);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+}  // namespace mom

@@ -1,0 +1,367 @@
+"""Python front end of the B200 PMCHWT library (``lib/libmomgpu.so``).
+
+A thin ctypes layer over the C ABI in ``include/mom_gpu.h``, with names that
+mirror the reference's Fortran entry points for the linear scattering path:
+
+    sysmat_pmchwt  (sysmat.f90:18)      -> Solver.sysmat
+    srcvec         (source.f90:136)     -> Solver.srcvec
+    solve_systems  (solver.f90:325)     -> Solver.solve
+    cs_prtsrf      (cs.f90:14)          -> Solver.cross_sections
+    rcs            (ffields.f90:252)    -> Solver.rcs
+    solve_batch    (solver.f90:17)      -> Solver.solve_wavelength (one wavelength)
+
+and the problem set-up commands ``mesh`` / ``ndom`` / ``sdom`` / ``fdom``
+(interface.f90:32-123, 357-366) -> Problem.  All computation runs in the
+CUDA library; there is no CPU fallback: importing this module on a machine
+where the library cannot be loaded raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmomgpu.so")
+
+MOM_OK = 0
+MOM_ERR_ARG, MOM_ERR_ALLOC, MOM_ERR_CUDA, MOM_ERR_SINGULAR, MOM_ERR_TIMEOUT = 1, 2, 3, 4, 5
+MOM_ERR_STATE, MOM_ERR_MESH, MOM_ERR_NOCONV, MOM_ERR_IO = 6, 7, 8, 9
+FP64, MIXED = 0, 1
+SRC_PW, SRC_PW_ELLIPTIC = 1, 10
+
+# constants.f90:8-14 (pi is a single-precision literal in the reference)
+PI_F = float(np.float32(3.141592653589))
+C0 = 2.997924580003e8
+DEGTORAD = PI_F / 180.0
+
+# Every entry point the C ABI header declares (checked by the tests).
+EXPORTS = [
+    "mom_gpu_create", "mom_gpu_destroy", "mom_gpu_strerror", "mom_gpu_last_error", "mom_gpu_set_problem",
+    "mom_gpu_sysmat", "mom_gpu_srcvec", "mom_gpu_solve", "mom_gpu_solve_wavelength", "mom_gpu_cross_sections",
+    "mom_gpu_rcs", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
+    "mom_gpu_launch_count", "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
+    "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
+    "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
+]
+
+
+class MomError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d)" % (msg, status))
+        self.status = status
+
+
+class MomMesh(C.Structure):
+    _fields_ = [("nnodes", C.c_int32), ("nfaces", C.c_int32), ("nedges", C.c_int32),
+                ("nodes", C.POINTER(C.c_double)), ("face_nodes", C.POINTER(C.c_int32)),
+                ("face_edges", C.POINTER(C.c_int32)), ("edge_nodes", C.POINTER(C.c_int32)),
+                ("edge_faces", C.POINTER(C.c_int32)), ("edge_bnodes", C.POINTER(C.c_int32)),
+                ("edge_parent", C.POINTER(C.c_int32))]
+
+
+class MomSrc(C.Structure):
+    _fields_ = [("type", C.c_int32), ("theta", C.c_double), ("phi", C.c_double), ("psi", C.c_double),
+                ("phase_re", C.c_double), ("phase_im", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it is missing: no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libmomgpu.so not built; run __graft_entry__.build() (for90-mom2_b200/mom_build.py)")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    L.mom_gpu_create.argtypes = [C.c_int32, C.POINTER(vp)]
+    L.mom_gpu_destroy.argtypes = [vp]
+    L.mom_gpu_destroy.restype = None
+    L.mom_gpu_strerror.argtypes = [C.c_int32]
+    L.mom_gpu_strerror.restype = C.c_char_p
+    L.mom_gpu_last_error.argtypes = [vp]
+    L.mom_gpu_last_error.restype = C.c_char_p
+    L.mom_gpu_set_problem.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(MomMesh), C.c_int32, dp, dp]
+    L.mom_gpu_sysmat.argtypes = [vp, C.c_double, dp, C.c_int32, vp, C.c_int64]
+    L.mom_gpu_srcvec.argtypes = [vp, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp, C.c_int64]
+    L.mom_gpu_solve.argtypes = [vp, C.c_int32, C.c_double, C.c_int32, vp, C.c_int64, ip]
+    L.mom_gpu_solve_wavelength.argtypes = [vp, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32, C.c_double,
+                                           C.c_int32, vp, C.c_int64, ip]
+    L.mom_gpu_cross_sections.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp, C.c_int64,
+                                         dp, dp]
+    L.mom_gpu_rcs.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, C.c_int32, C.c_int32, dp]
+    L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
+    L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
+    L.mom_gpu_synchronize.argtypes = [vp]
+    L.mom_gpu_launch_count.argtypes = [vp]
+    L.mom_gpu_launch_count.restype = C.c_int64
+    L.mom_problem_create.argtypes = [C.POINTER(vp)]
+    L.mom_problem_destroy.argtypes = [vp]
+    L.mom_problem_destroy.restype = None
+    L.mom_problem_load_gmsh.argtypes = [vp, C.c_char_p, C.c_double]
+    L.mom_problem_set_mesh.argtypes = [vp, C.c_int32, dp, C.c_int32, ip, ip, C.c_double]
+    L.mom_problem_set_ndom.argtypes = [vp, C.c_int32]
+    L.mom_problem_set_domain.argtypes = [vp, C.c_int32, C.c_int32, ip]
+    L.mom_problem_finalize.argtypes = [vp]
+    L.mom_problem_nedges.argtypes = [vp]
+    L.mom_problem_ndom.argtypes = [vp]
+    L.mom_problem_domain.argtypes = [vp, C.c_int32, C.POINTER(MomMesh)]
+    L.mom_tri_rule.argtypes = [C.c_char_p, dp, dp]
+    L.mom_problem_upload.argtypes = [vp, vp, C.c_char_p]
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _check(status, ctx=None, what=""):
+    if status != MOM_OK:
+        msg = lib().mom_gpu_strerror(status).decode()
+        if ctx is not None:
+            detail = lib().mom_gpu_last_error(ctx).decode()
+            if detail:
+                msg = detail
+        raise MomError(status, (what + ": " if what else "") + msg)
+
+
+def tri_rule(name: str = "tri_gl13"):
+    """Triangle quadrature of quad.f90 (weights[nq], nodes[nq, 3])."""
+    w = np.zeros(13)
+    nd = np.zeros((13, 3))
+    nq = lib().mom_tri_rule(name.encode(), _dp(w), _dp(nd))
+    if nq < 0:
+        raise MomError(MOM_ERR_ARG, "Unrecognized quadrature type " + name)
+    return w[:nq].copy(), nd[:nq].copy()
+
+
+def omega_of(wl: float) -> float:
+    """omega = 2 pi c0 / wl with the reference's float-rounded pi (solver.f90:77)."""
+    return 2.0 * PI_F * C0 / wl
+
+
+def src_pw(theta_deg: float, phi_deg: float, psi_deg: float) -> dict:
+    """``ssrc i 'pw' theta phi psi`` (interface.f90:500-505): degrees -> radians."""
+    return dict(type="pw", theta=theta_deg * DEGTORAD, phi=phi_deg * DEGTORAD, psi=psi_deg * DEGTORAD)
+
+
+def src_pw_elliptic(theta_deg: float, phi_deg: float, phase: complex) -> dict:
+    return dict(type="pw_elliptic", theta=theta_deg * DEGTORAD, phi=phi_deg * DEGTORAD, phase=complex(phase))
+
+
+def _srcs(srcs):
+    if isinstance(srcs, dict):
+        srcs = [srcs]
+    arr = (MomSrc * len(srcs))()
+    for i, s in enumerate(srcs):
+        if s["type"] == "pw":
+            arr[i] = MomSrc(SRC_PW, s["theta"], s["phi"], s["psi"], 0.0, 0.0)
+        else:
+            ph = complex(s["phase"])
+            arr[i] = MomSrc(SRC_PW_ELLIPTIC, s["theta"], s["phi"], 0.0, ph.real, ph.imag)
+    return arr, len(srcs)
+
+
+def _ri(ri):
+    vals = [complex(v) for v in (ri if np.ndim(ri) else [ri])]
+    return np.array([[v.real, v.imag] for v in vals], dtype=np.float64).ravel()
+
+
+class Problem:
+    """Master mesh and domain submeshes (mesh / ndom / sdom / fdom commands)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(lib().mom_problem_create(C.byref(h)), what="mom_problem_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().mom_problem_destroy(self.h)
+            self.h = None
+
+    @classmethod
+    def from_gmsh(cls, path, scale, domains):
+        p = cls()
+        _check(lib().mom_problem_load_gmsh(p.h, path.encode(), scale), what="load " + path)
+        p.set_domains(domains)
+        return p
+
+    @classmethod
+    def from_arrays(cls, nodes, faces, face_ids, scale, domains):
+        p = cls()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        faces = np.ascontiguousarray(faces, dtype=np.int32)
+        ids = np.ascontiguousarray(face_ids, dtype=np.int32)
+        _check(lib().mom_problem_set_mesh(p.h, len(nodes), _dp(nodes), len(faces), _ip(faces), _ip(ids), scale),
+               what="mesh")
+        p.set_domains(domains)
+        return p
+
+    def set_domains(self, domains):
+        L = lib()
+        _check(L.mom_problem_set_ndom(self.h, len(domains)), what="ndom")
+        for d, ids in enumerate(domains):
+            a = np.ascontiguousarray(ids, dtype=np.int32)
+            _check(L.mom_problem_set_domain(self.h, d, len(a), _ip(a)), what="sdom %d" % (d + 1))
+        _check(L.mom_problem_finalize(self.h), what="fdom")
+
+    @property
+    def nedges(self):
+        return lib().mom_problem_nedges(self.h)
+
+    @property
+    def ndom(self):
+        return lib().mom_problem_ndom(self.h)
+
+    def domain(self, d):
+        """Copy of the flattened topology of domain d (d = -1: master mesh)."""
+        m = MomMesh()
+        _check(lib().mom_problem_domain(self.h, d, C.byref(m)), what="domain")
+
+        def arr(ptr, n, k, dt):
+            return np.ctypeslib.as_array(ptr, shape=(n * k,)).reshape(n, k).astype(dt).copy() if n else None
+
+        return dict(nodes=arr(m.nodes, m.nnodes, 3, np.float64), face_node=arr(m.face_nodes, m.nfaces, 3, np.int32),
+                    face_edge=arr(m.face_edges, m.nfaces, 3, np.int32),
+                    edge_node=arr(m.edge_nodes, m.nedges, 2, np.int32),
+                    edge_face=arr(m.edge_faces, m.nedges, 2, np.int32),
+                    edge_bnode=arr(m.edge_bnodes, m.nedges, 2, np.int32),
+                    edge_parent=arr(m.edge_parent, m.nedges, 1, np.int32).ravel())
+
+
+class Solver:
+    """One CUDA context of the PMCHWT library on ``device``."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib().mom_gpu_create(device, C.byref(h))
+        if st != MOM_OK:
+            raise MomError(st, "mom_gpu_create failed: " + lib().mom_gpu_strerror(st).decode())
+        self.h = h
+        self.N = None
+        self.ndom = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mom_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, st, what):
+        _check(st, self.h, what)
+
+    def set_problem(self, problem: Problem, quad: str = "tri_gl13"):
+        self._ck(lib().mom_problem_upload(problem.h, self.h, quad.encode()), "set_problem")
+        self.N = problem.nedges
+        self.ndom = problem.ndom
+
+    def sysmat(self, omega, ri, precision=FP64, want_host=False):
+        """sysmat_pmchwt: build the 2N x 2N matrix on the device (optionally copy it back)."""
+        r = _ri(ri)
+        if len(r) != 2 * self.ndom:
+            raise ValueError("one refractive index per domain")
+        A = np.zeros((2 * self.N, 2 * self.N), dtype=np.complex128, order="F") if want_host else None
+        self._ck(lib().mom_gpu_sysmat(self.h, omega, _dp(r), precision, A.ctypes.data if A is not None else None,
+                                      2 * self.N), "sysmat")
+        return A
+
+    def srcvec(self, omega, ri1, srcs, want_host=False):
+        arr, ns = _srcs(srcs)
+        r = _ri(ri1)
+        q = np.zeros((2 * self.N, ns), dtype=np.complex128, order="F") if want_host else None
+        self._ck(lib().mom_gpu_srcvec(self.h, omega, _dp(r), ns, arr, q.ctypes.data if q is not None else None,
+                                      2 * self.N), "srcvec")
+        self.nsrc = ns
+        return q
+
+    def solve(self, precision=FP64, tol=1e-12, maxit=30, want_host=True):
+        x = np.zeros((2 * self.N, self.nsrc), dtype=np.complex128, order="F") if want_host else None
+        it = C.c_int32()
+        self._ck(lib().mom_gpu_solve(self.h, precision, tol, maxit, x.ctypes.data if x is not None else None,
+                                     2 * self.N, C.byref(it)), "solve")
+        self.iters = it.value
+        return x
+
+    def solve_wavelength(self, omega, ri, srcs, precision=FP64, tol=1e-12, maxit=30, want_host=True):
+        arr, ns = _srcs(srcs)
+        r = _ri(ri)
+        x = np.zeros((2 * self.N, ns), dtype=np.complex128, order="F") if want_host else None
+        it = C.c_int32()
+        self._ck(lib().mom_gpu_solve_wavelength(self.h, omega, _dp(r), ns, arr, precision, tol, maxit,
+                                                x.ctypes.data if x is not None else None, 2 * self.N, C.byref(it)),
+                 "solve_wavelength")
+        self.nsrc = ns
+        self.iters = it.value
+        return x
+
+    def cross_sections(self, omega, ri, srcs, x=None, dom=0):
+        """cs_prtsrf: (csca[nsrc], cabs[nsrc]) from x (2N x nsrc) or the device solutions."""
+        arr, ns = _srcs(srcs)
+        r = _ri(ri)
+        csca = np.zeros(ns)
+        cabs = np.zeros(ns)
+        xp = None
+        if x is not None:
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            xp = x.ctypes.data
+        self._ck(lib().mom_gpu_cross_sections(self.h, dom, omega, _dp(r), ns, arr, xp, 2 * self.N, _dp(csca),
+                                              _dp(cabs)), "cross_sections")
+        return csca, cabs
+
+    def rcs(self, omega, ri, ntheta, nphi, isrc=0, x=None, dom=0):
+        r = _ri(ri)
+        out = np.zeros((ntheta, nphi), order="F")
+        xp = None
+        if x is not None:
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            xp = x.ctypes.data
+        self._ck(lib().mom_gpu_rcs(self.h, dom, omega, _dp(r), isrc, xp, 2 * self.N, ntheta, nphi, _dp(out)), "rcs")
+        return out
+
+    def synchronize(self):
+        self._ck(lib().mom_gpu_synchronize(self.h), "synchronize")
+
+    @property
+    def launch_count(self):
+        return lib().mom_gpu_launch_count(self.h)
+
+    def device_matrix(self):
+        p = C.c_void_p()
+        ld = C.c_int64()
+        self._ck(lib().mom_gpu_device_matrix(self.h, C.byref(p), C.byref(ld)), "device_matrix")
+        return p.value, ld.value
+
+
+# Reference-named wrappers ----------------------------------------------------
+
+def sysmat_pmchwt(solver: Solver, omega, ri, precision=FP64):
+    return solver.sysmat(omega, ri, precision, want_host=True)
+
+
+def srcvec(solver: Solver, omega, ri1, srcs):
+    return solver.srcvec(omega, ri1, srcs, want_host=True)
+
+
+def solve_systems(solver: Solver, precision=FP64, tol=1e-12, maxit=30):
+    return solver.solve(precision, tol, maxit)
+
+
+def cs_prtsrf(solver: Solver, omega, ri, x, src, dom=0):
+    csca, cabs = solver.cross_sections(omega, ri, [src], x=x, dom=dom)
+    return float(csca[0]), float(cabs[0])
+
+
+def rcs(solver: Solver, omega, ri, x, ntheta, nphi, dom=0):
+    return solver.rcs(omega, ri, ntheta, nphi, x=x, dom=dom)

@@ -1,0 +1,167 @@
+/*
+ * mom_gpu.h -- C ABI of the B200 PMCHWT solver (drop-in for the linear
+ * scattering hot path of for90-mom2).
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (MOM_OK on success) and is thread safe per context (an internal mutex
+ * serialises calls on one context; the reference calls cs_prtsrf from
+ * OpenMP threads, interface.f90:1411-1432).  Matrices and vectors are
+ * column-major complex(dp) with interleaved re/im, exactly the Fortran
+ * COMPLEX(KIND=dp) layout; "double *" arguments that hold complex data point
+ * at 2*count doubles.  Indices in the mesh structures are 0-based.
+ *
+ * The reference's Fortran caller would bind these through ISO_C_BINDING;
+ * each declaration names the reference routine it replaces.
+ */
+#ifndef MOM_GPU_H
+#define MOM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference prints and STOPs on these conditions. */
+#define MOM_OK 0
+#define MOM_ERR_ARG 1      /* invalid argument (size, index, pointer) */
+#define MOM_ERR_ALLOC 2    /* device or host allocation failed */
+#define MOM_ERR_CUDA 3     /* CUDA runtime / cuBLAS error */
+#define MOM_ERR_SINGULAR 4 /* zero pivot: ZGETRF INFO > 0 (linalg.f90:170-173) */
+#define MOM_ERR_TIMEOUT 5  /* a bounded device wait ran out */
+#define MOM_ERR_STATE 6    /* call order violated (e.g. solve before sysmat) */
+#define MOM_ERR_MESH 7     /* inconsistent mesh (mesh.f90:415-418, 1366-1367) */
+#define MOM_ERR_NOCONV 8   /* iterative refinement did not reach the tolerance */
+#define MOM_ERR_IO 9       /* mesh file could not be read (mesh.f90:622-626) */
+
+/* Arithmetic of sysmat / solve. */
+#define MOM_PREC_FP64 0  /* FP64 assembly and FP64 LU (the reference's arithmetic) */
+#define MOM_PREC_MIXED 1 /* FP32 far pairs + FP64 near pairs; FP32 LU with TF32
+                            tensor-core trailing updates; FP64 refinement */
+
+/* Source types (source.f90:20-30). */
+#define MOM_SRC_PW 1
+#define MOM_SRC_PW_ELLIPTIC 10
+
+typedef struct mom_ctx mom_ctx;
+
+/* One domain's boundary submesh after the reference's sdom/fdom commands
+ * (mesh_container, mesh.f90:27-83, flattened to structure-of-arrays).
+ * Orientation (orient_basis, mesh.f90:454-558) is already applied:
+ * edge_faces[2e] is the "+" face and edge_bnodes[2e] its free vertex. */
+typedef struct mom_mesh {
+  int32_t nnodes, nfaces, nedges;
+  const double *nodes;        /* [nnodes][3], metres */
+  const int32_t *face_nodes;  /* [nfaces][3] */
+  const int32_t *face_edges;  /* [nfaces][3]: local edge k = (node k, node k+1) */
+  const int32_t *edge_nodes;  /* [nedges][2] */
+  const int32_t *edge_faces;  /* [nedges][2]: (+face, -face) */
+  const int32_t *edge_bnodes; /* [nedges][2]: free vertex of the + / - face */
+  const int32_t *edge_parent; /* [nedges]: global (master) edge index */
+} mom_mesh;
+
+/* Excitation (srcdata, source.f90:36-58); angles in radians. */
+typedef struct mom_src {
+  int32_t type;           /* MOM_SRC_PW or MOM_SRC_PW_ELLIPTIC */
+  double theta, phi, psi; /* psi unused for pw_elliptic */
+  double phase_re, phase_im; /* pw_elliptic Ex/Ey phase factor */
+} mom_src;
+
+/* Context on one CUDA device.  Owns a stream, cuBLAS handle and the device
+ * copies of the problem, the system matrix, its LU factors and solutions. */
+int mom_gpu_create(int32_t device, mom_ctx **out);
+void mom_gpu_destroy(mom_ctx *ctx);
+const char *mom_gpu_strerror(int32_t status);
+/* Text of the last error on this context (empty if none). */
+const char *mom_gpu_last_error(mom_ctx *ctx);
+
+/* Upload the domain submeshes and the triangle rule (b%domains(:)%mesh and
+ * b%qd_tri of the batch type, common.f90:71-108).  nedges_total is the
+ * master mesh edge count N (2N unknowns).  qw[nq], qnodes[nq][3] follow
+ * quad_data (quad.f90:269-274): point = qn[2] p1 + qn[0] p2 + qn[1] p3.
+ * Geometry (normals, areas, edge lengths, average edge length) is derived
+ * as compute_basis_data does (mesh.f90:1265-1322).  nq <= 13. */
+int mom_gpu_set_problem(mom_ctx *ctx, int32_t nedges_total, int32_t ndom, const mom_mesh *doms, int32_t nq,
+                        const double *qw, const double *qnodes);
+
+/* Replaces sysmat_pmchwt (sysmat.f90:18-105) for the identity group: builds
+ * the 2N x 2N PMCHWT matrix for angular frequency omega and one refractive
+ * index per domain (ri[2*ndom], re/im).  The matrix stays on the device; if
+ * A_host is not NULL it is also copied there (leading dimension lda >= 2N). */
+int mom_gpu_sysmat(mom_ctx *ctx, double omega, const double *ri, int32_t precision, double *A_host, int64_t lda);
+
+/* Replaces srcvec (source.f90:136-247) for nsrc sources on domain 1's
+ * boundary with refractive index ri1 (re/im): the right-hand sides are kept
+ * on the device; if q_host is not NULL they are also copied there as a
+ * 2N x nsrc column-major block (leading dimension ldq >= 2N). */
+int mom_gpu_srcvec(mom_ctx *ctx, double omega, const double *ri1, int32_t nsrc, const mom_src *src, double *q_host,
+                   int64_t ldq);
+
+/* Replaces solve_systems / solve_multi_linsys (solver.f90:325-357,
+ * linalg.f90:159-180): LU-factors the device matrix with partial pivoting
+ * and solves for the device right-hand sides.  MOM_PREC_MIXED factors in
+ * FP32 and refines in FP64 until ||b - A x|| <= tol ||b|| (at most maxit
+ * steps; iters_out may be NULL).  x_host (2N x nsrc, ldx) may be NULL. */
+int mom_gpu_solve(mom_ctx *ctx, int32_t precision, double tol, int32_t maxit, double *x_host, int64_t ldx,
+                  int32_t *iters_out);
+
+/* One wavelength of solve_batch (solver.f90:76-142): sysmat + srcvec +
+ * solve.  x_host (2N x nsrc, ldx) receives the solutions if not NULL. */
+int mom_gpu_solve_wavelength(mom_ctx *ctx, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                             int32_t precision, double tol, int32_t maxit, double *x_host, int64_t ldx,
+                             int32_t *iters_out);
+
+/* Replaces cs_prtsrf (cs.f90:14-104) for nsrc sources: scattering and
+ * absorption cross sections from the surface currents on domain dom
+ * (0-based; the reference uses domain 1) with refractive index ri (re/im).
+ * x_host (2N x nsrc, ldx) or, if NULL, the device solutions. */
+int mom_gpu_cross_sections(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t nsrc,
+                           const mom_src *src, const double *x_host, int64_t ldx, double *csca, double *cabs);
+
+/* Replaces rcs / rcs_ext (ffields.f90:203-266, far_fields 16-122): the
+ * bistatic |E_theta|^2 + |E_phi|^2 at r = 1 m on the endpoint-inclusive
+ * ntheta x nphi grid (column-major, as rcsdata(1:ntheta,1:nphi)) for
+ * source column isrc of x_host (2N x ?, ldx) or, if NULL, of the device
+ * solutions. */
+int mom_gpu_rcs(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
+                int64_t ldx, int32_t ntheta, int32_t nphi, double *rcs);
+
+/* Device views for callers that keep data resident (bench, tests). */
+int mom_gpu_device_matrix(mom_ctx *ctx, void **A_dev, int64_t *lda);
+int mom_gpu_device_solution(mom_ctx *ctx, void **x_dev, int64_t *ldx, int32_t *nsrc);
+int mom_gpu_synchronize(mom_ctx *ctx);
+/* Kernel launches issued by this context since creation (instrumentation). */
+int64_t mom_gpu_launch_count(mom_ctx *ctx);
+
+/* ---- Host-side problem set-up (the reference's mesh/sdom/fdom commands) ---- */
+
+typedef struct mom_problem mom_problem;
+
+int mom_problem_create(mom_problem **out);
+void mom_problem_destroy(mom_problem *p);
+/* read_mesh (interface.f90:357-366): load_mesh_gmsh + build_mesh(scale). */
+int mom_problem_load_gmsh(mom_problem *p, const char *path, double scale);
+/* The same from arrays: faces[nfaces][3] 0-based, face_ids[nfaces]. */
+int mom_problem_set_mesh(mom_problem *p, int32_t nnodes, const double *nodes, int32_t nfaces, const int32_t *faces,
+                         const int32_t *face_ids, double scale);
+/* read_ndom / read_sdom (interface.f90:32-105): signed surface ids; a
+ * negative id inverts those faces (invert_faces, mesh.f90:278-288). */
+int mom_problem_set_ndom(mom_problem *p, int32_t ndom);
+int mom_problem_set_domain(mom_problem *p, int32_t dom, int32_t nsurf, const int32_t *surf_ids);
+/* read_fdom (interface.f90:107-123): submesh_edge_connectivity +
+ * orient_basis. */
+int mom_problem_finalize(mom_problem *p);
+int32_t mom_problem_nedges(const mom_problem *p);
+int32_t mom_problem_ndom(const mom_problem *p);
+/* Flattened view of domain dom (valid until the problem is destroyed). */
+int mom_problem_domain(const mom_problem *p, int32_t dom, mom_mesh *out);
+/* Named triangle rule of quad.f90 ("tri_gl1", "tri_gl3", "tri_gl4",
+ * "tri_gl7", "tri_gl13"): qw[13], qnodes[13][3]; returns nq or < 0. */
+int32_t mom_tri_rule(const char *name, double *qw, double *qnodes);
+/* Convenience: mom_gpu_set_problem with all domains of p and a named rule. */
+int mom_problem_upload(const mom_problem *p, mom_ctx *ctx, const char *quad_name);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

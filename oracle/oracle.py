@@ -1,0 +1,221 @@
+"""Python front end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU legs of bench.py use
+this module, and only as the checker.  It loads ``_build/libmomoracle.so``
+(a plain-C FP64 restatement of the reference's hot path, see mom_oracle.c)
+and adds the LAPACK step of ``solve_multi_linsys`` (linalg.f90:159-180):
+ZGETRF + ZGETRS, here from the OpenBLAS that ships with scipy.  The
+reference links Intel MKL (CMakeLists.txt:27) with no version pinned, so the
+LU step is pinned by backward error instead of bitwise factors.
+
+Parity status: unpinned against reference outputs (no Fortran compiler
+exists to run the reference, and it ships no golden vectors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+PI_F = float(np.float32(3.141592653589))  # constants.f90:10 (single-precision literal)
+EPS0 = 8.8541878176e-12
+MU0 = 4 * PI_F * 1e-7
+C0 = 2.997924580003e8
+ETA0 = 3.767303134622e2
+DEGTORAD = PI_F / 180.0
+
+
+def omega_of(wl: float) -> float:
+    """Angular frequency as solve_batch computes it (solver.f90:77)."""
+    return 2.0 * PI_F * C0 / wl
+
+
+def build() -> str:
+    path = os.path.join(_HERE, "_build", "libmomoracle.so")
+    src = os.path.join(_HERE, "mom_oracle.c")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return path
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(build())
+        L = _LIB
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        L.oracle_problem_create.argtypes = [C.c_int, dp, C.c_int, ip, ip, C.c_double, C.c_int, ip, ip,
+                                            C.c_char_p, C.POINTER(C.c_void_p)]
+        L.oracle_problem_free.argtypes = [C.c_void_p]
+        L.oracle_problem_sizes.argtypes = [C.c_void_p, ip]
+        L.oracle_problem_export.argtypes = [C.c_void_p, C.c_int, dp, ip, ip, ip, ip, ip, ip, dp]
+        L.oracle_sysmat.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int]
+        L.oracle_operator.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, dp, C.c_void_p]
+        L.oracle_srcvec.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p]
+        L.oracle_cs.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p, dp, dp]
+        L.oracle_rcs.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_int, C.c_int, dp, C.c_int]
+        L.oracle_srcint.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_int, C.c_int, dp, C.c_int, C.c_void_p]
+        L.oracle_static_integrals.argtypes = [C.c_void_p, C.c_int, dp, C.c_int, C.c_int, dp]
+        L.oracle_face_geometry.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, dp, ip, dp, dp]
+        L.oracle_tri_rule.argtypes = [C.c_char_p, ip, dp, dp]
+        L.oracle_pi.restype = C.c_double
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class OSrc(C.Structure):
+    _fields_ = [("type", C.c_int), ("theta", C.c_double), ("phi", C.c_double), ("psi", C.c_double),
+                ("phase_re", C.c_double), ("phase_im", C.c_double)]
+
+
+def make_src(src: dict) -> OSrc:
+    """src: {'type': 'pw', 'theta', 'phi', 'psi'} or {'type': 'pw_elliptic', 'theta', 'phi', 'phase'},
+    angles in radians (``ssrc`` converts degrees with the float-rounded pi, interface.f90:486-515)."""
+    if src["type"] == "pw":
+        return OSrc(1, src["theta"], src["phi"], src["psi"], 0.0, 0.0)
+    ph = complex(src["phase"])
+    return OSrc(10, src["theta"], src["phi"], 0.0, ph.real, ph.imag)
+
+
+def tri_rule(name: str = "tri_gl13"):
+    nq = C.c_int()
+    w = np.zeros(13)
+    nd = np.zeros((13, 3))
+    if lib().oracle_tri_rule(name.encode(), C.byref(nq), _dp(w), _dp(nd)):
+        raise ValueError("Unrecognized quadrature type " + name)
+    return w[: nq.value].copy(), nd[: nq.value].copy()
+
+
+class OracleProblem:
+    """Master mesh + domain submeshes after ``mesh``/``sdom``/``fdom``."""
+
+    def __init__(self, nodes, faces, face_ids, scale, domains, quad="tri_gl13"):
+        L = lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        faces = np.ascontiguousarray(faces, dtype=np.int32)
+        ids = np.ascontiguousarray(face_ids, dtype=np.int32)
+        nsurf = np.array([len(d) for d in domains], dtype=np.int32)
+        dids = np.array([i for d in domains for i in d], dtype=np.int32)
+        h = C.c_void_p()
+        rc = L.oracle_problem_create(len(nodes), _dp(nodes), len(faces), _ip(faces), _ip(ids), scale,
+                                     len(domains), _ip(nsurf), _ip(dids), quad.encode(), C.byref(h))
+        if rc:
+            raise RuntimeError("oracle problem setup failed (%d)" % rc)
+        self.h = h
+        self.ndom = len(domains)
+        sz = np.zeros(3 + 3 * self.ndom, dtype=np.int32)
+        L.oracle_problem_sizes(h, _ip(sz))
+        self.N = int(sz[0])
+        self.master_sizes = (int(sz[1]), int(sz[2]), int(sz[0]))
+        self.dom_sizes = [tuple(int(v) for v in sz[3 + 3 * d: 6 + 3 * d]) for d in range(self.ndom)]
+
+    @classmethod
+    def from_msh(cls, path, scale, domains, quad="tri_gl13"):
+        import sys
+        sys.path.insert(0, os.path.join(os.path.dirname(_HERE), "for90-mom2_b200"))
+        from mom_b200.meshgen import read_gmsh
+        nodes, faces, ids = read_gmsh(path)
+        return cls(nodes, faces, ids, scale, domains, quad)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_problem_free(self.h)
+            self.h = None
+
+    def export(self, d: int) -> dict:
+        nn, nf, ne = self.master_sizes if d < 0 else self.dom_sizes[d]
+        out = dict(nodes=np.zeros((nn, 3)), face_node=np.zeros((nf, 3), np.int32),
+                   face_edge=np.zeros((nf, 3), np.int32), edge_node=np.zeros((ne, 2), np.int32),
+                   edge_face=np.zeros((ne, 2), np.int32), edge_bnode=np.zeros((ne, 2), np.int32),
+                   edge_parent=np.zeros(ne, np.int32))
+        av = C.c_double()
+        lib().oracle_problem_export(self.h, d, _dp(out["nodes"]), _ip(out["face_node"]), _ip(out["face_edge"]),
+                                    _ip(out["edge_node"]), _ip(out["edge_face"]), _ip(out["edge_bnode"]),
+                                    _ip(out["edge_parent"]), C.byref(av))
+        out["avelen"] = av.value
+        return out
+
+    def sysmat(self, omega, ri, mlo=0, mhi=-1, nthreads=0):
+        """sysmat_pmchwt (sysmat.f90:18-105): the 2N x 2N PMCHWT matrix, Fortran order."""
+        A = np.zeros((2 * self.N, 2 * self.N), dtype=np.complex128, order="F")
+        rr = np.array([[complex(v).real, complex(v).imag] for v in ri], dtype=np.float64)
+        lib().oracle_sysmat(self.h, omega, _dp(rr), A.ctypes.data, 2 * self.N, mlo, mhi, nthreads)
+        return A
+
+    def operator(self, d, op, omega, ri):
+        """One domain operator: op 0 = D, 1 = H, 2 = K (computeD/H/K)."""
+        nd = self.dom_sizes[d][2]
+        M = np.zeros((nd, nd), dtype=np.complex128, order="F")
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        lib().oracle_operator(self.h, d, op, omega, _dp(rr), M.ctypes.data)
+        return M
+
+    def srcvec(self, omega, ri, src, d=0):
+        q = np.zeros(2 * self.N, dtype=np.complex128)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        s = make_src(src)
+        lib().oracle_srcvec(self.h, d, omega, _dp(rr), C.byref(s), q.ctypes.data)
+        return q
+
+    def cs(self, omega, ri, x, src, d=0):
+        """cs_prtsrf (cs.f90:14-104): returns (csca, cabs)."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        s = make_src(src)
+        a, b = C.c_double(), C.c_double()
+        lib().oracle_cs(self.h, d, omega, _dp(rr), x.ctypes.data, C.byref(s), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def rcs(self, omega, ri, x, ntheta, nphi, d=0, nthreads=0):
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        out = np.zeros((ntheta, nphi), order="F")
+        lib().oracle_rcs(self.h, d, omega, _dp(rr), x.ctypes.data, ntheta, nphi, _dp(out), nthreads)
+        return out
+
+    def srcint(self, d, which, r, f, tface, k, near):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        kk = np.array([complex(k).real, complex(k).imag])
+        res = np.zeros(3 if which == 1 else 9, dtype=np.complex128)
+        lib().oracle_srcint(self.h, d, which, _dp(r), f, tface, _dp(kk), int(near), res.ctypes.data)
+        return res if which == 1 else res.reshape(3, 3)
+
+    def static_integrals(self, d, r, f, e):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        out = np.zeros(14)
+        lib().oracle_static_integrals(self.h, d, _dp(r), f, e, _dp(out))
+        return dict(K2m1=out[0:3], K21=out[3:6], K4m1=out[6:9], K41=out[9:12], K1m1=out[12], K11=out[13])
+
+    def face_geometry(self, d, f):
+        nodes = np.zeros((3, 3))
+        area = C.c_double()
+        sign = np.zeros(3, np.int32)
+        ln = np.zeros(3)
+        bn = np.zeros((3, 3))
+        lib().oracle_face_geometry(self.h, d, f, _dp(nodes), C.byref(area), _ip(sign), _dp(ln), _dp(bn))
+        return dict(nodes=nodes, area=area.value, sign=sign, length=ln, bnode=bn)
+
+
+def solve(A, q):
+    """solve_multi_linsys (linalg.f90:159-180): ZGETRF + ZGETRS('N'), STOP on INFO /= 0."""
+    from scipy.linalg import lapack
+    lu, piv, info = lapack.zgetrf(A, overwrite_a=False)
+    if info != 0:
+        raise RuntimeError("Matrix factorization failed!")
+    x, info = lapack.zgetrs(lu, piv, q)
+    if info != 0:
+        raise RuntimeError("Solving of system failed!")
+    return x
