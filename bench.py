@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the linear PMCHWT solve on B200: solves/s (assemble + LU + solve).
+
+Workload (N=1): the mixed-precision solve at scale -- an icosphere of radius
+50 nm subdivided 4 times (5120 triangles, 7680 RWG edges, 15360 PMCHWT
+unknowns, complex128), interior eps = -9 + 1.3i, vacuum outside, vacuum
+wavelength 600 nm, x-polarised plane wave along +z.  One step = one solve:
+system-matrix assembly + right-hand side + LU factorisation + solve with FP64
+iterative refinement to a relative residual <= 1e-12.  The FP64 path is timed
+beside it ("fp64"), and sigma_ext of the mixed solve is compared with the FP64
+solve (which matches the CPU oracle to 1e-9 in the test suite).
+
+Data are synthetic (a seeded icosphere; no dataset exists for this path).  The
+3.8 GB FP64 matrix exceeds the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun) every rank solves its own replica (the path has no data
+exchange: "replicas only"); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "for90-mom2_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "solves/s (assemble+LU+solve), mixed vs FP64 on 1 B200 at sigma_ext rel err <=1e-6"
+WL = 600e-9
+EPS_IN = complex(-9.0, 1.3)
+SUBDIV = 4
+RADIUS_NM = 50.0
+TOL = 1e-12
+MAXIT = 60
+
+
+def workload_name(subdiv):
+    F = 20 * 4 ** subdiv
+    return "icosphere r=50nm s=%d (%d triangles, %d unknowns), eps=-9+1.3i, 600 nm, x-pol pw +z" % (
+        subdiv, F, 3 * F)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_problem(M, subdiv):
+    import numpy as np
+    from mom_b200 import meshgen
+    nodes, faces = meshgen.icosphere(subdiv, RADIUS_NM)
+    ids = np.ones(len(faces), dtype=np.int32)
+    return nodes, faces, ids, [[1], [-1]]
+
+
+def cpu_sample(subdiv, threads, budget_s=20.0):
+    """Time the CPU oracle (C restatement of the reference + OpenBLAS LAPACK) on a
+    bounded sample of the workload and extrapolate to one full solve."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    import oracle as O
+    from mom_b200 import meshgen
+    nodes, faces = meshgen.icosphere(subdiv, RADIUS_NM)
+    ids = np.ones(len(faces), int)
+    P = O.OracleProblem(nodes, faces, ids, 1e-9, [[1], [-1]])
+    F = len(faces)
+    n = 2 * P.N
+    om = O.omega_of(WL)
+    ri = [1.0, np.sqrt(EPS_IN)]
+    src = dict(type="pw", theta=0.0, phi=90 * O.DEGTORAD, psi=0.0)
+    # assembly: rows of m_s test faces per domain, extrapolated by F / m_s
+    m_s = max(2, min(F, 64))
+    t0 = time.perf_counter()
+    P.sysmat_sample(om, ri, 0, m_s, threads)
+    t_asm = (time.perf_counter() - t0) * F / m_s
+    # RHS and sigma: full
+    t0 = time.perf_counter()
+    q = P.srcvec(om, ri[0], src)
+    t_rhs = time.perf_counter() - t0
+    # LU + getrs: scipy zgetrf/zgetrs on an n_s x n_s matrix, scaled by n^3 and n^2
+    from scipy.linalg import lapack
+    n_s = min(n, 4096)
+    rng = np.random.default_rng(0)
+    As = rng.standard_normal((n_s, n_s)) + 1j * rng.standard_normal((n_s, n_s)) + n_s * np.eye(n_s)
+    As = np.asfortranarray(As)
+    t0 = time.perf_counter()
+    lu, piv, info = lapack.zgetrf(As, overwrite_a=True)
+    t_lu = (time.perf_counter() - t0) * (n / n_s) ** 3
+    b = rng.standard_normal(n_s) + 0j
+    t0 = time.perf_counter()
+    lapack.zgetrs(lu, piv, b)
+    t_rs = (time.perf_counter() - t0) * (n / n_s) ** 2
+    total = t_asm + t_rhs + t_lu + t_rs
+    sample = ("sysmat rows of %d/%d test faces per domain (x%d), srcvec full, zgetrf/zgetrs on n=%d (x(n/%d)^3, "
+              "x(n/%d)^2); OpenMP + OpenBLAS" % (m_s, F, F // m_s, n_s, n_s, n_s))
+    return dict(total_s=total, phases_s=dict(assembly=t_asm, rhs=t_rhs, lu=t_lu, getrs=t_rs), sample=sample)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU restatement of the reference's path (the Fortran
+    reference cannot be compiled here: no Fortran compiler), all host threads."""
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    for _ in range(max(0, args.warmup if args.warmup < 1 else 1)):
+        pass
+    vals = []
+    info = None
+    for _ in range(args.steps):
+        info = cpu_sample(args.subdiv, cores)
+        vals.append(1.0 / info["total_s"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+            "config": {"workload": workload_name(args.subdiv), "precision": "FP64 (CPU)"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": info["sample"],
+                             "phases_s": info["phases_s"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, local_rank, world):
+    import numpy as np
+    import torch
+    import mom_b200 as M
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    nodes, faces, ids, doms = make_problem(M, args.subdiv)
+    S = M.Solver(local_rank)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(EPS_IN)]
+    src = [M.src_pw(0, 90, 0)]
+    stream = torch.cuda.ExternalStream(S.stream)
+
+    def step(prec):
+        S.sysmat(om, ri, prec)
+        S.srcvec(om, ri[0], src)
+        S.solve(prec, tol=TOL, maxit=MAXIT, want_host=False)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(prec, steps, warm):
+        for _ in range(warm):
+            step(prec)
+        barrier()
+        l0, b0 = S.launch_count, S.library_calls
+        S.profile(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        iters = []
+        for _ in range(steps):
+            step(prec)
+            iters.append(S.iters)
+        e1.record(stream)
+        e1.synchronize()
+        prof = S.profile_read()
+        S.profile(False)
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms), prof, S.launch_count - l0, S.library_calls - b0, iters
+
+    # ---- mixed precision (the headline) ----
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ms_mixed, prof, launches, libcalls, iters = timed(M.MIXED, args.steps, args.warmup)
+    clocks = sampler.stop()
+    csca, cabs = S.cross_sections(om, ri[0], src)
+    ext_mixed = float(csca[0] + cabs[0])
+    # ---- FP64 path, same workload ----
+    ms_fp64, prof64, _, _, _ = timed(M.FP64, args.fp64_steps, 1)
+    csca64, cabs64 = S.cross_sections(om, ri[0], src)
+    ext_fp64 = float(csca64[0] + cabs64[0])
+    sig_err = abs(ext_mixed - ext_fp64) / abs(ext_fp64)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    pin_x = torch.empty((1, 2 * S.N * 2), dtype=torch.float64, pin_memory=True).numpy()
+    xh = pin_x.view(np.complex128).reshape(2 * S.N, 1, order="F")
+    for _ in range(1):
+        S.solve_wavelength(om, ri, src, M.MIXED, TOL, MAXIT, want_host=True)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x = S.solve_wavelength(om, ri, src, M.MIXED, TOL, MAXIT, want_host=True)
+        xh[:, 0] = x[:, 0]
+        cs = S.cross_sections(om, ri[0], src)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    h2d = 48 * len(src) + 16 * len(ri)  # mom_src structs + refractive indices
+    d2h = 16 * 2 * S.N * len(src) + 16 * len(src)  # solution + (csca, cabs)
+
+    # ---- roofline of the dominant kernel category (timed live above) ----
+    hbm_gbs, bf16_tf, peak_src = load_peaks()
+    cat, (cat_ms, cat_n) = max(prof.items(), key=lambda kv: kv[1][0])
+    F = len(faces)
+    n = 2 * S.N
+    roof = None
+    if cat == "pair":
+        # 17,914 FLOP per face pair (169 point pairs x 88 + 3042 contraction); one launch = F^2 pairs of a domain
+        flop = 17914.0 * F * F
+        ach = flop / (cat_ms / cat_n * 1e-3) / 1e12
+        roof = {"kernel": "pair_kernel<float,13> (far-pair assembly, FP32 pipe)", "bound": "fp32", "achieved": ach,
+                "unit": "TFLOP/s", "traffic": None}
+    elif cat == "gemm":
+        # trailing updates + TRSM products: 8 real FLOP per complex MAC
+        nb = 64
+        flop = sum(8.0 * (n - (k + 1) * nb) ** 2 * nb + 8.0 * nb * nb * (n - (k + 1) * nb) for k in range(n // nb))
+        ach = flop / (cat_ms * 1e-3) / 1e12 / args.steps
+        roof = {"kernel": "LU trailing CGEMM (TF32 tensor cores)", "bound": "tensor", "achieved": ach,
+                "unit": "TFLOP/s", "peak": bf16_tf / 2.0, "frac": ach / (bf16_tf / 2.0), "traffic": None,
+                "peak_note": "TF32 dense = half of the %s bf16 peak" % peak_src}
+    elif cat in ("trsv", "residual"):
+        bytes_ = (8.0 if cat == "trsv" else 16.0) * n * n
+        ach = bytes_ / (cat_ms / cat_n * 1e-3) / 1e9
+        roof = {"kernel": cat, "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": hbm_gbs,
+                "frac": ach / hbm_gbs, "traffic": None, "peak_note": peak_src}
+    if roof is None:
+        roof = {"kernel": cat, "bound": "n/a", "achieved": None, "unit": None, "peak": None, "frac": None,
+                "traffic": None}
+    if roof.get("bound") == "fp32":
+        # FP32 non-tensor peak: 148 SMs x 128 FP32 lanes x 2 FLOP x SM clock (no measured figure exists)
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+        roof.update(peak=peak, frac=roof["achieved"] / peak,
+                    peak_note="nominal FP32 SIMT at the sampled median SM clock (%.0f MHz)" % sm_mhz)
+
+    phases = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps} for k, v in prof.items()}
+    phases64 = {k: {"ms_per_step": v[0] / args.fp64_steps} for k, v in prof64.items()}
+
+    value = world * 1000.0 / ms_mixed
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32/tf32 far pairs + LU, fp64 near pairs + refinement (complex)",
+            "data": "synthetic",
+            "config": {"workload": workload_name(args.subdiv), "precision": "mixed", "refine_tol": TOL,
+                       "l2": "matrix 3.8 GB > 126 MB L2, no flush", "parallelism": "replicas x%d" % world},
+            "fp64": {"value": world * 1000.0 / ms_fp64, "unit": "solves/s", "ms_per_step": ms_fp64,
+                     "phases": phases64},
+            "mixed_over_fp64": ms_fp64 / ms_mixed,
+            "sigma_ext": {"mixed": ext_mixed, "fp64": ext_fp64, "rel_err": sig_err},
+            "refine_iters": iters,
+            "phases": phases,
+            "clocks": clocks,
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches / args.steps * args.steps),
+            "library_gemm_calls": libcalls,
+            "roofline": roof}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = host_cores()
+        info = cpu_sample(args.subdiv, cores)
+        line["cpu_baseline"] = {"value": 1.0 / info["total_s"], "unit": "solves/s", "cores": cores, "kind": "port",
+                                "sample": info["sample"], "phases_s": info["phases_s"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    S.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--subdiv", type=int, default=SUBDIV)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, local_rank, world)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

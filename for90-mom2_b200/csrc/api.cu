@@ -22,6 +22,23 @@ int cuda_fail(Ctx *c, cudaError_t e, const char *where) {
   return fail(c, MOM_ERR_CUDA, std::string(cudaGetErrorString(e)) + " in " + where);
 }
 
+ProfScope::ProfScope(Ctx *c_, int cat_) : c(c_), cat(cat_) {
+  if (!c->prof) return;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    cudaGetLastError();
+    a = b = nullptr;
+    return;
+  }
+  cudaEventRecord(a, c->stream);
+}
+
+ProfScope::~ProfScope() {
+  if (!a) return;
+  cudaEventRecord(b, c->stream);
+  c->prof_ev[cat].push_back({a, b});
+  c->prof_launch[cat]++;
+}
+
 int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes) {
   if (*p && *cap >= bytes) return MOM_OK;
   if (*p) {
@@ -66,6 +83,7 @@ void free_problem(Ctx *c) {
   cudaFree(c->A32);
   cudaFree(c->blk);
   cudaFree(c->ipiv);
+  cudaFree(c->perm);
   cudaFree(c->invd);
   cudaFree(c->B);
   cudaFree(c->X);
@@ -73,6 +91,7 @@ void free_problem(Ctx *c) {
   c->A32 = nullptr;
   c->blk = nullptr;
   c->ipiv = nullptr;
+  c->perm = nullptr;
   c->invd = nullptr;
   c->B = c->X = nullptr;
   c->BX_cap = 0;
@@ -370,7 +389,7 @@ int mom_gpu_set_problem(mom_ctx *c, int32_t nedges_total, int32_t ndom, const mo
   c->A_bytes = sizeof(double2) * (size_t)c->lda * c->n;
   c->blk_bytes = sizeof(double2) * 18 * maxF * maxF;
   if (cudaMalloc(&c->A, c->A_bytes) != cudaSuccess || cudaMalloc(&c->blk, c->blk_bytes) != cudaSuccess ||
-      cudaMalloc(&c->ipiv, sizeof(int) * c->n) != cudaSuccess ||
+      cudaMalloc(&c->ipiv, sizeof(int) * c->n) != cudaSuccess || cudaMalloc(&c->perm, sizeof(int) * c->n) != cudaSuccess ||
       cudaMalloc(&c->invd, sizeof(double2) * 2 * (size_t)c->nb * c->n) != cudaSuccess) {
     cudaGetLastError();
     free_problem(c);
@@ -512,5 +531,39 @@ int mom_gpu_synchronize(mom_ctx *c) {
 }
 
 int64_t mom_gpu_launch_count(mom_ctx *c) { return c ? c->launches : 0; }
+
+void *mom_gpu_stream(mom_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int64_t mom_gpu_library_calls(mom_ctx *c) { return c ? c->blas_calls : 0; }
+
+int mom_gpu_profile(mom_ctx *c, int32_t enable) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  cudaStreamSynchronize(c->stream);
+  for (auto &v : c->prof_ev) {
+    for (auto &e : v) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    v.clear();
+  }
+  for (auto &n : c->prof_launch) n = 0;
+  c->prof = enable != 0;
+  return MOM_OK;
+}
+
+int mom_gpu_profile_read(mom_ctx *c, int32_t category, double *ms_total, int64_t *launches) {
+  if (!c || category < 0 || category >= 8 || !ms_total || !launches) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  double t = 0;
+  for (auto &e : c->prof_ev[category]) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) t += ms;
+  }
+  *ms_total = t;
+  *launches = c->prof_launch[category];
+  return MOM_OK;
+}
 
 }  // extern "C"

@@ -753,10 +753,13 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
     pa.fK = L0 * L0 * kOofpi / 4.0;
     pa.blk = c->blk;
     dim3 grid((D.F + kPairThreads - 1) / kPairThreads, (D.F + kTestPerCta - 1) / kTestPerCta);
-    if (precision == MOM_PREC_MIXED) {
-      MOM_TRY(launch_pair<float>(c, c->nq, grid, pa));
-    } else {
-      MOM_TRY(launch_pair<double>(c, c->nq, grid, pa));
+    {
+      ProfScope ps(c, kProfPair);
+      if (precision == MOM_PREC_MIXED) {
+        MOM_TRY(launch_pair<float>(c, c->nq, grid, pa));
+      } else {
+        MOM_TRY(launch_pair<double>(c, c->nq, grid, pa));
+      }
     }
     if (D.nnear > 0) {
       NearArgs na;
@@ -776,6 +779,7 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
       na.k2 = {kr * kr - ki * ki, 2 * kr * ki};
       na.blk = c->blk;
       const unsigned blocks = (unsigned)((D.nnear + 127) / 128);
+      ProfScope ps(c, kProfNear);
       switch (c->nq) {
         case 1: near_kernel<1><<<blocks, 128, 0, c->stream>>>(na); break;
         case 3: near_kernel<3><<<blocks, 128, 0, c->stream>>>(na); break;
@@ -798,6 +802,7 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
     ga.A = c->A;
     ga.lda = lda;
     dim3 gg((D.Nd + 255) / 256, D.Nd);
+    ProfScope ps(c, kProfGather);
     gather_kernel<<<gg, 256, 0, c->stream>>>(ga);
     c->launches++;
     MOM_CUDA(c, cudaGetLastError());

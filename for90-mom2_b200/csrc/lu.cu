@@ -37,7 +37,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 
 constexpr int kPanelThreads = 256;
-constexpr long long kSpinLimit = 1LL << 24;  // bounded barrier wait (~seconds)
+constexpr long long kSpinLimit = 1LL << 26;  // bounded barrier wait (a few seconds)
 
 struct PanelArgs {
   void *A;
@@ -53,26 +53,34 @@ struct PanelArgs {
   double2 *col_data;  // [2][nb]
 };
 
+// Grid-wide barrier of a cooperative launch: one release-add per CTA on a
+// counter zeroed before the launch, acquire-polling until it reaches
+// target.  The wait is bounded: after kSpinLimit polls the CTA sets *timeout
+// and every CTA leaves (the host reports MOM_ERR_TIMEOUT).
 __device__ bool grid_barrier(unsigned *bar, unsigned target, int *timeout) {
   __syncthreads();
   bool ok = true;
   if (threadIdx.x == 0) {
     __threadfence();
-    atomicAdd(bar, 1u);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     long long it = 0;
     while (true) {
       unsigned v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
       if (v >= target) break;
-      if (*(volatile int *)timeout) { ok = false; break; }
-      if (++it > kSpinLimit) {
-        atomicExch(timeout, 1);
-        ok = false;
-        break;
+      if ((++it & 255) == 0) {
+        if (*(volatile int *)timeout) {
+          ok = false;
+          break;
+        }
+        if (it > kSpinLimit) {
+          atomicExch(timeout, 1);
+          ok = false;
+          break;
+        }
+        __nanosleep(32);
       }
-      __nanosleep(64);
     }
-    __threadfence();
   }
   __shared__ int s_ok;
   if (threadIdx.x == 0) s_ok = ok;
@@ -85,6 +93,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   extern __shared__ double2 slab[];  // [nb][rpc] column-major within the CTA
   __shared__ double red_abs[kPanelThreads];
   __shared__ int red_row[kPanelThreads];
+  __shared__ int red_cta[kPanelThreads];
+  __shared__ double2 s_prow_data[64];
   __shared__ int s_prow, s_pcta;
   const int tid = threadIdx.x, cta = blockIdx.x;
   const int nb = a.nb, rpc = a.rpc;
@@ -140,24 +150,39 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       for (int j = tid; j < nb; j += kPanelThreads) a.col_data[(size_t)par * nb + j] = slab[j * rpc + li];
     }
     if (!grid_barrier(a.bar, (unsigned)(c + 1) * a.P, a.timeout)) return;
-    // global pivot: largest cabs1, first row on ties (izamax)
-    if (tid == 0) {
-      double gb = -1.0;
-      int gr = 0x7fffffff, gc = -1;
-      for (int p = 0; p < a.P; p++) {
-        const double v = __ldcg(a.cand_abs + par * a.P + p);
-        const int r = __ldcg(a.cand_row + par * a.P + p);
-        if (v > gb || (v == gb && r < gr)) {
-          gb = v;
-          gr = r;
-          gc = p;
-        }
+    // global pivot: largest cabs1, first row on ties (izamax); the P
+    // candidates are reduced in parallel by the CTA.
+    {
+      double v = -1.0;
+      int r = 0x7fffffff, w = -1;
+      if (tid < a.P) {
+        v = __ldcg(a.cand_abs + par * a.P + tid);
+        r = __ldcg(a.cand_row + par * a.P + tid);
+        w = tid;
       }
-      s_prow = gr;
-      s_pcta = gc;
-      if (cta == 0) {
-        a.ipiv[col] = gr;
-        if (gb == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+      red_abs[tid] = v;
+      red_row[tid] = r;
+      red_cta[tid] = w;
+      __syncthreads();
+      for (int h = kPanelThreads / 2; h > 0; h >>= 1) {
+        if (tid < h) {
+          const double ov = red_abs[tid + h];
+          const int orow = red_row[tid + h];
+          if (ov > red_abs[tid] || (ov == red_abs[tid] && orow < red_row[tid])) {
+            red_abs[tid] = ov;
+            red_row[tid] = orow;
+            red_cta[tid] = red_cta[tid + h];
+          }
+        }
+        __syncthreads();
+      }
+      if (tid == 0) {
+        s_prow = red_row[0];
+        s_pcta = red_cta[0];
+        if (cta == 0) {
+          a.ipiv[col] = red_row[0];
+          if (red_abs[0] == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+        }
       }
     }
     __syncthreads();
@@ -173,8 +198,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       const int li = (int)(col - row0);
       for (int j = tid; j < nb; j += kPanelThreads) slab[j * rpc + li] = __ldcg(pdat + j);
     }
+    for (int j = tid; j < nb; j += kPanelThreads) s_prow_data[j] = __ldcg(pdat + j);
     __syncthreads();
-    const double2 piv = __ldcg(pdat + c);
+    const double2 piv = s_prow_data[c];
     const double pa = piv.x * piv.x + piv.y * piv.y;
     if (pa != 0.0) {
       const double2 rp = make_double2(piv.x / pa, -piv.y / pa);  // 1 / pivot
@@ -184,7 +210,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         const double2 l = cmul(slab[c * rpc + i], rp);
         slab[c * rpc + i] = l;
         for (int j = c + 1; j < nb; j++) {
-          const double2 u = __ldcg(pdat + j);
+          const double2 u = s_prow_data[j];
           double2 v = slab[j * rpc + i];
           v.x -= l.x * u.x - l.y * u.y;
           v.y -= l.x * u.y + l.y * u.x;
@@ -265,96 +291,215 @@ __global__ void diag_inv_kernel(const T *A, int64_t lda, int64_t j0, int nb, dou
   }
 }
 
-// Forward / backward block substitution step (one launch per block):
-//   y_k = Inv_k x_k   (every CTA recomputes it; CTA 0 stores it in Y)
-//   x_i -= M[i, k-block] y_k for the rows i of the remaining range.
-// lower: rows i >= (k+1) nb ; upper: rows i < k nb.  nrhs <= 8 per launch.
-template <typename T>
-__global__ void __launch_bounds__(256) trsv_step_kernel(const T *M, int64_t lda, int64_t n, int64_t k0, int nb,
-                                                        const double2 *inv, double2 *X, double2 *Y, int64_t ldx,
-                                                        int nrhs, int lower) {
-  extern __shared__ double2 yk[];  // [nrhs][nb]
-  for (int idx = threadIdx.x; idx < nb * nrhs; idx += blockDim.x) {
-    const int r = idx % nb, s = idx / nb;
-    double2 acc = make_double2(0, 0);
-    for (int j = 0; j < nb; j++) {
-      const double2 iv = inv[r + j * nb];
-      const double2 xv = X[(size_t)s * ldx + k0 + j];
-      acc.x += iv.x * xv.x - iv.y * xv.y;
-      acc.y += iv.x * xv.y + iv.y * xv.x;
-    }
-    yk[s * nb + r] = acc;
-  }
+// The row interchanges of the whole factorisation, in order, composed into
+// one permutation: perm[i] = source row of row i of P*B.  One thread walks
+// the swaps in shared memory (once per factorisation).
+__global__ void compose_pivots_kernel(const int *ipiv, int n, int *perm) {
+  extern __shared__ int p[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = i;
   __syncthreads();
-  if (blockIdx.x == 0)
-    for (int idx = threadIdx.x; idx < nb * nrhs; idx += blockDim.x) {
-      const int r = idx % nb, s = idx / nb;
-      Y[(size_t)s * ldx + k0 + r] = yk[s * nb + r];
-    }
-  const int64_t lo = lower ? k0 + nb : 0, hi = lower ? n : k0;
-  for (int64_t i = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
-    double2 acc[8];
-    for (int s = 0; s < nrhs; s++) acc[s] = make_double2(0, 0);
-    for (int j = 0; j < nb; j++) {
-      const double2 m = ld2(M + i + (k0 + j) * lda);
-      for (int s = 0; s < nrhs; s++) {
-        const double2 y = yk[s * nb + j];
-        acc[s].x += m.x * y.x - m.y * y.y;
-        acc[s].y += m.x * y.y + m.y * y.x;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; i++) {
+      const int r = ipiv[i];
+      if (r != i) {
+        const int t = p[i];
+        p[i] = p[r];
+        p[r] = t;
       }
     }
-    for (int s = 0; s < nrhs; s++) {
-      double2 v = X[(size_t)s * ldx + i];
-      v.x -= acc[s].x;
-      v.y -= acc[s].y;
-      X[(size_t)s * ldx + i] = v;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = p[i];
+}
+
+
+struct TrsvArgs {
+  const void *M;     // LU factors (T)
+  int64_t lda, n;
+  int nb, P, rpc, ns;
+  const double2 *inv;  // [nblk][2][nb][nb]: inv(L_kk), inv(U_kk)
+  const int *perm;
+  double2 *X, *Y;      // [ns][n]: right-hand sides in X, scratch Y; solution returned in X
+  unsigned *bar;
+  int *timeout;
+};
+
+// y = Inv * x for an nb x nb block and ns vectors held in shared memory;
+// several threads share one output and reduce through shared memory.
+__device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *xs, double2 *ys, double2 *red) {
+  const int O = nb * ns;
+  int parts = 1;
+  while (parts * 2 * O <= (int)blockDim.x && parts < 16) parts *= 2;
+  const int tid = threadIdx.x;
+  for (int base = 0; base < O * parts; base += blockDim.x) {
+    const int g = base + tid;
+    double2 acc = make_double2(0, 0);
+    if (g < O * parts) {
+      const int o = g / parts, part = g % parts;
+      const int r = o % nb, sv = o / nb;
+#pragma unroll 4
+      for (int j = part; j < nb; j += parts) {
+        const double2 iv = __ldg(inv + r + (size_t)j * nb);
+        const double2 xv = xs[sv * nb + j];
+        acc.x += iv.x * xv.x - iv.y * xv.y;
+        acc.y += iv.x * xv.y + iv.y * xv.x;
+      }
     }
+    red[tid] = acc;
+    __syncthreads();
+    if (g < O * parts && (g % parts) == 0) {
+      double2 t = red[tid];
+      for (int q = 1; q < parts; q++) {
+        t.x += red[tid + q].x;
+        t.y += red[tid + q].y;
+      }
+      ys[g / parts] = t;
+    }
+    __syncthreads();
   }
 }
 
-// X = P B (row interchanges of the whole factorisation, in order).
-__global__ void apply_pivots_kernel(double2 *X, int64_t ldx, int64_t n, const int *ipiv, int nrhs) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nrhs) return;
-  double2 *x = X + (size_t)s * ldx;
-  for (int64_t i = 0; i < n; i++) {
-    const int64_t r = ipiv[i];
-    if (r != i) {
-      double2 t = x[i];
-      x[i] = x[r];
-      x[r] = t;
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes_is_16) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes_is_16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Row range of CTA-owned rows that block kb updates in pass 0 (below the
+// block) or pass 1 (above it).
+__device__ __forceinline__ void upd_range(int pass, int64_t k0, int nb, int64_t r0, int64_t r1, int64_t *lo,
+                                          int64_t *hi) {
+  *lo = pass == 0 ? max(r0, k0 + nb) : r0;
+  *hi = pass == 0 ? r1 : min(r1, k0);
+}
+
+// Forward (unit lower) and backward (upper) substitution of P A = L U for
+// NS right-hand sides in one cooperative launch: per diagonal block one
+// bounded grid barrier.  CTA c owns rows [c rpc, (c+1) rpc) for the updates;
+// the factor tile of the next block is fetched into shared memory with
+// cp.async while the CTA waits at the barrier.
+template <typename T, int NS>
+__global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
+  __shared__ double2 xs[8 * 64], ys[8 * 64], red[256];
+  extern __shared__ __align__(16) unsigned char tile_raw[];  // [nb][rpc] of T
+  T *tile = reinterpret_cast<T *>(tile_raw);
+  const T *M = reinterpret_cast<const T *>(a.M);
+  const int64_t n = a.n, lda = a.lda;
+  const int nb = a.nb, nblk = (int)(n / nb), rpc = a.rpc;
+  constexpr int ns = NS;
+  const int64_t r0 = (int64_t)blockIdx.x * rpc;
+  const int64_t r1 = min(n, r0 + rpc);
+  unsigned step = 0;
+  auto prefetch = [&](int pass, int kk) {
+    if (kk >= nblk) return;
+    const int kb = pass == 0 ? kk : nblk - 1 - kk;
+    const int64_t k0 = (int64_t)kb * nb;
+    int64_t lo, hi;
+    upd_range(pass, k0, nb, r0, r1, &lo, &hi);
+    const int cnt = (int)(hi > lo ? hi - lo : 0);
+    for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
+      const int i = idx % cnt, j = idx / cnt;
+      cp_async(tile + (size_t)j * rpc + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // Y = P X
+  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+    for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + a.perm[i]];
+  prefetch(0, 0);
+  if (!grid_barrier(a.bar, ++step * a.P, a.timeout)) return;
+  for (int pass = 0; pass < 2; pass++) {
+    double2 *src = pass == 0 ? a.Y : a.X;  // vector being reduced
+    double2 *dst = pass == 0 ? a.X : a.Y;  // solved blocks
+    for (int kk = 0; kk < nblk; kk++) {
+      const int kb = pass == 0 ? kk : nblk - 1 - kk;
+      const int64_t k0 = (int64_t)kb * nb;
+      for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
+        const int j = idx % nb, sv = idx / nb;
+        xs[sv * nb + j] = __ldcg(src + (size_t)sv * n + k0 + j);
+      }
+      __syncthreads();
+      block_apply(a.inv + ((size_t)kb * 2 + pass) * nb * nb, nb, ns, xs, ys, red);
+      // owners of block kb's rows store the solved block
+      for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
+        const int j = idx % nb, sv = idx / nb;
+        const int64_t i = k0 + j;
+        if (i >= r0 && i < r1) dst[(size_t)sv * n + i] = ys[sv * nb + j];
+      }
+      int64_t lo, hi;
+      upd_range(pass, k0, nb, r0, r1, &lo, &hi);
+      cp_async_wait_all();
+      __syncthreads();
+      for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        double2 acc[NS];
+#pragma unroll
+        for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
+        const T *mp = tile + (i - lo);
+#pragma unroll 8
+        for (int j = 0; j < nb; j++) {
+          const double2 m = ld2(mp + (size_t)j * rpc);
+#pragma unroll
+          for (int sv = 0; sv < ns; sv++) {
+            const double2 y = ys[sv * nb + j];
+            acc[sv].x += m.x * y.x - m.y * y.y;
+            acc[sv].y += m.x * y.y + m.y * y.x;
+          }
+        }
+#pragma unroll
+        for (int sv = 0; sv < ns; sv++) {
+          double2 v = src[(size_t)sv * n + i];
+          v.x -= acc[sv].x;
+          v.y -= acc[sv].y;
+          src[(size_t)sv * n + i] = v;
+        }
+      }
+      __syncthreads();
+      // next tile: the following block of this pass, or the first of the next pass
+      if (kk + 1 < nblk) prefetch(pass, kk + 1);
+      else if (pass == 0) prefetch(1, 0);
+      if (!grid_barrier(a.bar, ++step * a.P, a.timeout)) return;
     }
   }
+  cp_async_wait_all();
+  // the solution is in Y; return it in X
+  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + i] = a.Y[(size_t)s * n + i];
 }
 
 constexpr int kGemvRows = 256;
 constexpr int kGemvCols = 256;
 
 // partial[chunk][s][i] = sum_{j in chunk} A[i, j] x_s[j]  (FP64 matrix)
+template <int NS>
 __global__ void __launch_bounds__(kGemvRows) gemv_partial_kernel(const double2 *A, int64_t lda, int64_t n,
-                                                                 const double2 *X, int64_t ldx, int nrhs,
-                                                                 double2 *partial) {
-  __shared__ double2 xs[8][kGemvCols];
+                                                                 const double2 *X, int64_t ldx, double2 *partial) {
+  __shared__ double2 xs[NS][kGemvCols];
   const int64_t i = (int64_t)blockIdx.x * kGemvRows + threadIdx.x;
   const int64_t j0 = (int64_t)blockIdx.y * kGemvCols;
   const int cnt = (n - j0) < kGemvCols ? (int)(n - j0) : kGemvCols;
-  for (int idx = threadIdx.x; idx < cnt * nrhs; idx += kGemvRows) {
+  for (int idx = threadIdx.x; idx < cnt * NS; idx += kGemvRows) {
     const int j = idx % cnt, s = idx / cnt;
     xs[s][j] = X[(size_t)s * ldx + j0 + j];
   }
   __syncthreads();
   if (i >= n) return;
-  double2 acc[8];
-  for (int s = 0; s < nrhs; s++) acc[s] = make_double2(0, 0);
+  double2 acc[NS];
+#pragma unroll
+  for (int s = 0; s < NS; s++) acc[s] = make_double2(0, 0);
+#pragma unroll 8
   for (int j = 0; j < cnt; j++) {
     const double2 m = A[i + (j0 + j) * lda];
-    for (int s = 0; s < nrhs; s++) {
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
       const double2 x = xs[s][j];
       acc[s].x += m.x * x.x - m.y * x.y;
       acc[s].y += m.x * x.y + m.y * x.x;
     }
   }
-  for (int s = 0; s < nrhs; s++) partial[((size_t)blockIdx.y * nrhs + s) * n + i] = acc[s];
+#pragma unroll
+  for (int s = 0; s < NS; s++) partial[((size_t)blockIdx.y * NS + s) * n + i] = acc[s];
 }
 
 // R = B - sum of partials; per-column squared norms of R into rn (block partials).
@@ -417,7 +562,7 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   const size_t o_cd = take(sizeof(double2) * 2 * P * nb);
   const size_t o_cl = take(sizeof(double2) * 2 * nb);
   const size_t o_w = take(esz * (size_t)nb * c->n);
-  const size_t o_i32 = take(sizeof(float2) * nb * nb);
+  const size_t o_i32 = take(sizeof(float2) * (size_t)nb * c->n);
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off));
   char *b = (char *)c->ws;
   w.bar = (unsigned *)(b + o_bar);
@@ -442,77 +587,110 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
   MOM_CUDA(c, cudaMemsetAsync(c->dinfo, 0, sizeof(int) * 4, c->stream));
   const bool mixed = precision == MOM_PREC_MIXED;
   MOM_BLAS(c, cublasSetMathMode(c->blas, mixed ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_DEFAULT_MATH));
-  const int nblk = (int)(n / nb);
-  for (int kb = 0; kb < nblk; kb++) {
-    const int64_t j0 = (int64_t)kb * nb;
-    const int64_t m = n - j0;
-    int P = (int)std::min<int64_t>(c->nsm, (m + 31) / 32);
-    int rpc = (int)((m + P - 1) / P);
-    P = (int)((m + rpc - 1) / rpc);
-    const size_t smem = sizeof(double2) * (size_t)nb * rpc;
-    if (smem > 227 * 1024) return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory");
-    PanelArgs pa;
-    pa.A = A;
-    pa.lda = lda;
-    pa.n = n;
-    pa.j0 = j0;
-    pa.nb = nb;
-    pa.rpc = rpc;
-    pa.P = P;
-    pa.ipiv = c->ipiv;
-    pa.info = w.info;
-    pa.timeout = w.timeout;
-    pa.bar = w.bar;
-    pa.cand_abs = w.cand_abs;
-    pa.cand_row = w.cand_row;
-    pa.cand_data = w.cand_data;
-    pa.col_data = w.col_data;
-    MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned), c->stream));
-    MOM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    void *args[] = {&pa};
-    MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
-                                            c->stream));
-    c->launches++;
-    if (n > nb) {
-      laswp_kernel<T><<<(unsigned)((n - nb + 255) / 256), 256, 0, c->stream>>>(A, lda, n, j0, nb, c->ipiv);
-      c->launches++;
+  // C <- alpha * A(m x k) * B(k x nc) + beta * C, column-major with lda
+  auto gemm = [&](int64_t m, int64_t ncol, int64_t k, double alpha, const T *Am, int64_t la, const T *Bm, int64_t lb,
+                  double beta, T *Cm, int64_t lc) -> int {
+    if (m <= 0 || ncol <= 0 || k <= 0) return MOM_OK;
+    c->blas_calls++;
+    if (!mixed) {
+      const cuDoubleComplex al = make_cuDoubleComplex(alpha, 0), be = make_cuDoubleComplex(beta, 0);
+      MOM_BLAS(c, cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)ncol, (int)k, &al,
+                              (const cuDoubleComplex *)Am, (int)la, (const cuDoubleComplex *)Bm, (int)lb, &be,
+                              (cuDoubleComplex *)Cm, (int)lc));
+    } else {
+      const cuComplex al = make_cuComplex((float)alpha, 0), be = make_cuComplex((float)beta, 0);
+      MOM_BLAS(c, cublasCgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)ncol, (int)k, &al,
+                              (const cuComplex *)Am, (int)la, (const cuComplex *)Bm, (int)lb, &be, (cuComplex *)Cm,
+                              (int)lc));
     }
-    double2 *invL = c->invd + (size_t)kb * 2 * nb * nb, *invU = invL + (size_t)nb * nb;
-    MOM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(double2) * nb * nb)));
-    diag_inv_kernel<T><<<1, std::max(nb, 64), sizeof(double2) * nb * nb, c->stream>>>(A, lda, j0, nb, invL, invU,
-                                                                                     mixed ? w.invL32 : nullptr);
-    c->launches++;
-    MOM_CUDA(c, cudaGetLastError());
-    const int64_t nc = n - j0 - nb;  // trailing columns
-    if (nc > 0) {
-      T *A12 = A + j0 + (j0 + nb) * lda;
-      T *L21 = A + (j0 + nb) + j0 * lda;
-      T *A22 = A + (j0 + nb) + (j0 + nb) * lda;
-      if (!mixed) {
-        const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0),
-                              mone = make_cuDoubleComplex(-1, 0);
-        MOM_BLAS(c, cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, (int)nc, nb, &one, (cuDoubleComplex *)invL, nb,
-                                (cuDoubleComplex *)A12, (int)lda, &zero, (cuDoubleComplex *)w.W, nb));
-        MOM_CUDA(c, cudaMemcpy2DAsync(A12, sizeof(T) * lda, w.W, sizeof(T) * nb, sizeof(T) * nb, nc,
-                                      cudaMemcpyDeviceToDevice, c->stream));
-        MOM_BLAS(c, cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)(m - nb), (int)nc, nb, &mone,
-                                (cuDoubleComplex *)L21, (int)lda, (cuDoubleComplex *)A12, (int)lda, &one,
-                                (cuDoubleComplex *)A22, (int)lda));
-      } else {
-        const cuComplex one = make_cuComplex(1, 0), zero = make_cuComplex(0, 0), mone = make_cuComplex(-1, 0);
-        MOM_BLAS(c, cublasCgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, (int)nc, nb, &one, (cuComplex *)w.invL32, nb,
-                                (cuComplex *)A12, (int)lda, &zero, (cuComplex *)w.W, nb));
-        MOM_CUDA(c, cudaMemcpy2DAsync(A12, sizeof(T) * lda, w.W, sizeof(T) * nb, sizeof(T) * nb, nc,
-                                      cudaMemcpyDeviceToDevice, c->stream));
-        MOM_BLAS(c, cublasCgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)(m - nb), (int)nc, nb, &mone,
-                                (cuComplex *)L21, (int)lda, (cuComplex *)A12, (int)lda, &one, (cuComplex *)A22,
-                                (int)lda));
+    return MOM_OK;
+  };
+  // B(nb x ncol, at A + j0 + col*lda) <- inv(L_jj) B, through the workspace
+  auto trsm_l = [&](int64_t j0, int64_t col, int64_t ncol, int kb) -> int {
+    if (ncol <= 0) return MOM_OK;
+    const T *inv = mixed ? (const T *)(w.invL32 + (size_t)kb * nb * nb) : (const T *)(c->invd + (size_t)kb * 2 * nb * nb);
+    T *B = A + j0 + col * lda;
+    MOM_TRY(gemm(nb, ncol, nb, 1.0, inv, nb, B, lda, 0.0, (T *)w.W, nb));
+    MOM_CUDA(c, cudaMemcpy2DAsync(B, sizeof(T) * lda, w.W, sizeof(T) * nb, sizeof(T) * nb, ncol,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    return MOM_OK;
+  };
+  const int NB = 4 * nb;  // outer block: trailing updates run with K = NB
+  for (int64_t J0 = 0; J0 < n; J0 += NB) {
+    const int64_t NBc = std::min<int64_t>(NB, n - J0);
+    for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
+      const int kb = (int)(j0 / nb);
+      const int64_t m = n - j0;
+      int P = (int)std::min<int64_t>(c->nsm, (m + 31) / 32);
+      int rpc = (int)((m + P - 1) / P);
+      P = (int)((m + rpc - 1) / rpc);
+      const size_t smem = sizeof(double2) * (size_t)nb * rpc;
+      if (smem > 227 * 1024) return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory");
+      PanelArgs pa;
+      pa.A = A;
+      pa.lda = lda;
+      pa.n = n;
+      pa.j0 = j0;
+      pa.nb = nb;
+      pa.rpc = rpc;
+      pa.P = P;
+      pa.ipiv = c->ipiv;
+      pa.info = w.info;
+      pa.timeout = w.timeout;
+      pa.bar = w.bar;
+      pa.cand_abs = w.cand_abs;
+      pa.cand_row = w.cand_row;
+      pa.cand_data = w.cand_data;
+      pa.col_data = w.col_data;
+      {
+        ProfScope ps(c, kProfPanel);
+        MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned), c->stream));
+        MOM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        void *args[] = {&pa};
+        MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
+                                                c->stream));
+        c->launches++;
+        if (n > nb) {
+          laswp_kernel<T><<<(unsigned)((n - nb + 255) / 256), 256, 0, c->stream>>>(A, lda, n, j0, nb, c->ipiv);
+          c->launches++;
+        }
+        double2 *invL = c->invd + (size_t)kb * 2 * nb * nb, *invU = invL + (size_t)nb * nb;
+        MOM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(double2) * nb * nb)));
+        diag_inv_kernel<T><<<1, std::max(nb, 64), sizeof(double2) * nb * nb, c->stream>>>(
+            A, lda, j0, nb, invL, invU, mixed ? w.invL32 + (size_t)kb * nb * nb : nullptr);
+        c->launches++;
+        MOM_CUDA(c, cudaGetLastError());
       }
-      c->launches += 3;
+      // update the rest of the outer block: U = inv(L_jj) A_j,rest ; A_below,rest -= L_below,j U
+      const int64_t rest = J0 + NBc - (j0 + nb);
+      if (rest > 0) {
+        ProfScope pg(c, kProfGemm);
+        MOM_TRY(trsm_l(j0, j0 + nb, rest, kb));
+        MOM_TRY(gemm(n - j0 - nb, rest, nb, -1.0, A + (j0 + nb) + j0 * lda, lda, A + j0 + (j0 + nb) * lda, lda, 1.0,
+                     A + (j0 + nb) + (j0 + nb) * lda, lda));
+      }
+    }
+    // trailing columns: block-row TRSM with L_JJ, then A22 -= L21 U12 with K = NBc
+    const int64_t t0 = J0 + NBc, nc = n - t0;
+    if (nc > 0) {
+      ProfScope pg(c, kProfGemm);
+      for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
+        MOM_TRY(trsm_l(j0, t0, nc, (int)(j0 / nb)));
+        const int64_t below = J0 + NBc - (j0 + nb);
+        MOM_TRY(gemm(below, nc, nb, -1.0, A + (j0 + nb) + j0 * lda, lda, A + j0 + t0 * lda, lda, 1.0,
+                     A + (j0 + nb) + t0 * lda, lda));
+      }
+      MOM_TRY(gemm(n - t0, nc, NBc, -1.0, A + t0 + J0 * lda, lda, A + J0 + t0 * lda, lda, 1.0, A + t0 + t0 * lda,
+                   lda));
     }
   }
   MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+  MOM_CUDA(c, cudaFuncSetAttribute(compose_pivots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(int) * n)));
+  compose_pivots_kernel<<<1, 256, sizeof(int) * n, c->stream>>>(c->ipiv, (int)n, c->perm);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
   int hinfo[2] = {0, 0};
   MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 2, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -528,32 +706,41 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
 // X (n x nrhs, ld n) <- A^{-1} X with the factors in place; Y is scratch.
 template <typename T>
 int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
-  const int64_t n = c->n, lda = c->lda;
-  const int nb = c->nb, nblk = (int)(n / nb);
-  apply_pivots_kernel<<<(nrhs + 31) / 32, 32, 0, c->stream>>>(X, n, n, c->ipiv, nrhs);
-  c->launches++;
-  for (int s0 = 0; s0 < nrhs; s0 += 8) {
-    const int ns = std::min(8, nrhs - s0);
-    double2 *x = X + (size_t)s0 * n, *y = Y + (size_t)s0 * n;
-    const size_t smem = sizeof(double2) * nb * ns;
-    for (int kb = 0; kb < nblk; kb++) {
-      const int64_t k0 = (int64_t)kb * nb;
-      const int64_t rows = n - k0 - nb;
-      const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, 2 * c->nsm));
-      trsv_step_kernel<T><<<g, 256, smem, c->stream>>>(A, lda, n, k0, nb, c->invd + (size_t)kb * 2 * nb * nb, x, y, n,
-                                                       ns, 1);
-      c->launches++;
-    }
-    for (int kb = nblk - 1; kb >= 0; kb--) {
-      const int64_t k0 = (int64_t)kb * nb;
-      const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((k0 + 255) / 256, 2 * c->nsm));
-      trsv_step_kernel<T><<<g, 256, smem, c->stream>>>(A, lda, n, k0, nb,
-                                                       c->invd + (size_t)kb * 2 * nb * nb + (size_t)nb * nb, y, x, n,
-                                                       ns, 0);
-      c->launches++;
-    }
+  const int64_t n = c->n;
+  const int nb = c->nb;
+  ProfScope ps(c, kProfTrsv);
+  int P = c->nsm;
+  int rpc = (int)((n + P - 1) / P);
+  P = (int)((n + rpc - 1) / rpc);
+  for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
+    ns = 8;
+    while (ns > nrhs - s0) ns >>= 1;  // chunks of 8, 4, 2, 1 vectors
+    TrsvArgs ta;
+    ta.M = A;
+    ta.lda = c->lda;
+    ta.n = n;
+    ta.nb = nb;
+    ta.P = P;
+    ta.rpc = rpc;
+    ta.ns = ns;
+    ta.inv = c->invd;
+    ta.perm = c->perm;
+    ta.X = X + (size_t)s0 * n;
+    ta.Y = Y + (size_t)s0 * n;
+    ta.bar = reinterpret_cast<unsigned *>(c->dinfo + 4);
+    ta.timeout = c->dinfo + 1;
+    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned), c->stream));
+    void *args[] = {&ta};
+    void *fn = ns == 1 ? (void *)trsv_coop_kernel<T, 1>
+               : ns == 2 ? (void *)trsv_coop_kernel<T, 2>
+               : ns == 4 ? (void *)trsv_coop_kernel<T, 4>
+                         : (void *)trsv_coop_kernel<T, 8>;
+    const size_t tile = sizeof(T) * (size_t)nb * rpc;
+    if (tile > 200 * 1024) return fail(c, MOM_ERR_ARG, "triangular-solve tile does not fit in shared memory");
+    MOM_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile));
+    MOM_CUDA(c, cudaLaunchCooperativeKernel(fn, dim3(P), dim3(256), args, tile, c->stream));
+    c->launches++;
   }
-  MOM_CUDA(c, cudaGetLastError());
   return MOM_OK;
 }
 
@@ -575,6 +762,10 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
     MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, vec));
     MOM_TRY(getrs_t<double2>(c, c->A, c->X, (double2 *)c->ws, nrhs));
     if (iters) *iters = 0;
+    int tmo = 0;
+    MOM_CUDA(c, cudaMemcpyAsync(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (tmo) return fail(c, MOM_ERR_TIMEOUT, "triangular solve barrier timed out");
     return MOM_OK;
   }
   // Mixed: x = 0, r = b; repeat d = LU32^{-1} r, x += d, r = b - A x.
@@ -608,17 +799,26 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
     MOM_TRY(getrs_t<float2>(c, c->A32, Dv, Yv, nrhs));
     axpy_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(c->X, Dv, (int64_t)n * nrhs);
     c->launches++;
-    for (int s0 = 0; s0 < nrhs; s0 += 8) {
-      const int ns = std::min(8, nrhs - s0);
-      gemv_partial_kernel<<<dim3(rblocks, nchunk), kGemvRows, 0, c->stream>>>(c->A, c->lda, n, c->X + (size_t)s0 * n,
-                                                                               n, ns, Pp);
+    ProfScope pr(c, kProfResidual);
+    for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
+      ns = 8;
+      while (ns > nrhs - s0) ns >>= 1;
+      const dim3 gg(rblocks, nchunk);
+      const double2 *xs0 = c->X + (size_t)s0 * n;
+      if (ns == 1) gemv_partial_kernel<1><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+      else if (ns == 2) gemv_partial_kernel<2><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+      else if (ns == 4) gemv_partial_kernel<4><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+      else gemv_partial_kernel<8><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
       residual_kernel<<<dim3(rblocks, ns), 256, 0, c->stream>>>(c->B + (size_t)s0 * n, n, Pp, nchunk, n, ns,
                                                                 R + (size_t)s0 * n, n, rn2 + (size_t)s0 * rblocks);
       c->launches += 2;
     }
     MOM_CUDA(c, cudaGetLastError());
     MOM_CUDA(c, cudaMemcpyAsync(h.data(), rn2, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    int tmo = 0;
+    MOM_CUDA(c, cudaMemcpyAsync(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (tmo) return fail(c, MOM_ERR_TIMEOUT, "triangular solve barrier timed out");
     worst = 0;
     for (int s = 0; s < nrhs; s++) {
       double t = 0;

@@ -76,6 +76,7 @@ struct Ctx {
   double2 *blk = nullptr;  // face-pair blocks, [F][F][9][2] of the largest domain
   size_t blk_bytes = 0;
   int *ipiv = nullptr;     // [n]
+  int *perm = nullptr;     // [n] composed row permutation of the factorisation
   double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
   size_t invd_bytes = 0;
   int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout, [2..] barrier counters
@@ -96,9 +97,27 @@ struct Ctx {
   double omega_rhs = 0;
   double ri1[2] = {1, 0};
 
+  // Optional per-category kernel timers (CUDA events on the context stream).
+  bool prof = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[8];
+  int64_t prof_launch[8] = {0};
+  int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)
+
   // Host-side staging (pinned)
   double *pinned = nullptr;
   size_t pinned_bytes = 0;
+};
+
+// Kernel categories for the optional timers.
+enum ProfCat { kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost };
+
+// Records start/end events around a launch when profiling is on.
+struct ProfScope {
+  struct Ctx *c;
+  int cat;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(struct Ctx *c_, int cat_);
+  ~ProfScope();
 };
 
 // Error helpers

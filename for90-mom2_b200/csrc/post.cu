@@ -384,6 +384,7 @@ int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *
   a.omega = omega;
   a.half = reinterpret_cast<double2 *>((char *)c->ws + src_bytes);
   MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * c->n * nsrc, c->stream));
+  ProfScope ps(c, kProfPost);
   rhs_half_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
@@ -421,9 +422,12 @@ int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, co
   a.k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
   a.omega = omega;
   a.part = reinterpret_cast<double *>((char *)c->ws + src_bytes);
+  {
+  ProfScope ps(c, kProfPost);
   cs_kernel<<<dim3(blocks, nsrc), 256, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
+  }
   std::vector<double> part(2 * (size_t)blocks * nsrc);
   MOM_CUDA(c, cudaMemcpyAsync(part.data(), a.part, part_bytes, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -464,6 +468,8 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   a.cur = reinterpret_cast<double4 *>(c->ws);
   a.pos = reinterpret_cast<double *>((char *)c->ws + cur_bytes);
   double *dout = reinterpret_cast<double *>((char *)c->ws + cur_bytes + pos_bytes);
+  {
+  ProfScope ps(c, kProfPost);
   ff_current_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
@@ -473,6 +479,7 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
                                                                                  k, rz, dout);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
+  }
   MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
   return MOM_OK;

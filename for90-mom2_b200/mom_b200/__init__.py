@@ -41,7 +41,8 @@ EXPORTS = [
     "mom_gpu_create", "mom_gpu_destroy", "mom_gpu_strerror", "mom_gpu_last_error", "mom_gpu_set_problem",
     "mom_gpu_sysmat", "mom_gpu_srcvec", "mom_gpu_solve", "mom_gpu_solve_wavelength", "mom_gpu_cross_sections",
     "mom_gpu_rcs", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
-    "mom_gpu_launch_count", "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
+    "mom_gpu_launch_count", "mom_gpu_stream", "mom_gpu_library_calls", "mom_gpu_profile", "mom_gpu_profile_read",
+    "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
 ]
@@ -99,6 +100,12 @@ def lib():
     L.mom_gpu_synchronize.argtypes = [vp]
     L.mom_gpu_launch_count.argtypes = [vp]
     L.mom_gpu_launch_count.restype = C.c_int64
+    L.mom_gpu_stream.argtypes = [vp]
+    L.mom_gpu_stream.restype = C.c_void_p
+    L.mom_gpu_library_calls.argtypes = [vp]
+    L.mom_gpu_library_calls.restype = C.c_int64
+    L.mom_gpu_profile.argtypes = [vp, C.c_int32]
+    L.mom_gpu_profile_read.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.mom_problem_create.argtypes = [C.POINTER(vp)]
     L.mom_problem_destroy.argtypes = [vp]
     L.mom_problem_destroy.restype = None
@@ -334,8 +341,35 @@ class Solver:
         self._ck(lib().mom_gpu_synchronize(self.h), "synchronize")
 
     @property
+    def stream(self):
+        """The library's cudaStream_t as an integer handle."""
+        return lib().mom_gpu_stream(self.h)
+
+    @property
     def launch_count(self):
+        """Kernel launches of this library (its own kernels) since creation."""
         return lib().mom_gpu_launch_count(self.h)
+
+    @property
+    def library_calls(self):
+        """cuBLAS GEMM calls since creation."""
+        return lib().mom_gpu_library_calls(self.h)
+
+    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post")
+
+    def profile(self, enable=True):
+        """Turn the per-category kernel timers on (and reset them) or off."""
+        self._ck(lib().mom_gpu_profile(self.h, 1 if enable else 0), "profile")
+
+    def profile_read(self):
+        """{category: (ms_total, launches)} of the kernel timers."""
+        out = {}
+        for i, name in enumerate(self.PROF_CATEGORIES):
+            ms = C.c_double()
+            n = C.c_int64()
+            self._ck(lib().mom_gpu_profile_read(self.h, i, C.byref(ms), C.byref(n)), "profile_read")
+            out[name] = (ms.value, n.value)
+        return out
 
     def device_matrix(self):
         p = C.c_void_p()

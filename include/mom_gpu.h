@@ -132,6 +132,17 @@ int mom_gpu_device_solution(mom_ctx *ctx, void **x_dev, int64_t *ldx, int32_t *n
 int mom_gpu_synchronize(mom_ctx *ctx);
 /* Kernel launches issued by this context since creation (instrumentation). */
 int64_t mom_gpu_launch_count(mom_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+ * order their own work against the library's. */
+void *mom_gpu_stream(mom_ctx *ctx);
+/* cuBLAS GEMM calls issued by this context (library kernels). */
+int64_t mom_gpu_library_calls(mom_ctx *ctx);
+/* Optional kernel timers: enable (1) / disable (0) and reset; then read the
+ * summed device time and launch count of a category: 0 pair (far-pair
+ * assembly), 1 near pairs, 2 gather, 3 LU panel, 4 LU GEMMs, 5 triangular
+ * solves, 6 refinement residual, 7 post-processing. */
+int mom_gpu_profile(mom_ctx *ctx, int32_t enable);
+int mom_gpu_profile_read(mom_ctx *ctx, int32_t category, double *ms_total, int64_t *launches);
 
 /* ---- Host-side problem set-up (the reference's mesh/sdom/fdom commands) ---- */
 

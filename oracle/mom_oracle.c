@@ -936,6 +936,62 @@ void oracle_sysmat(void *p, double omega, const double *ri_ri, cplx *A, int64_t 
   }
 }
 
+/* Bounded CPU sample for timing: the D, H and K rows of test faces
+ * [mlo, mhi) of every domain (the same per-pair work as oracle_sysmat, with
+ * the rows kept per test face so no 2N x 2N matrix is allocated).  Returns a
+ * checksum so the work cannot be elided. */
+double oracle_sysmat_sample(void *p, double omega, const double *ri_ri, int mlo, int mhi, int nthreads) {
+  oproblem *P = p;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  double chk = 0;
+  for (int d = 0; d < P->ndom; d++) {
+    omesh *m = P->dom + d;
+    cplx ri = ri_ri[2 * d] + I * ri_ri[2 * d + 1];
+    int hi = mhi > m->nfaces ? m->nfaces : mhi, lo = mlo < 0 ? 0 : mlo;
+    if (lo >= hi) continue;
+    /* rows-only variant of compute_op: a face-local row per (test face, p) */
+    int Nd = m->nedges, F = m->nfaces, nq = P->qd.nq;
+    cplx k = ri * omega / O_C0;
+    cplx *rows = calloc((size_t)3 * (hi - lo) * Nd, sizeof(cplx));
+    cplx *intaux = malloc(sizeof(cplx) * 9 * nq * (size_t)F);
+    if (!rows || !intaux) abort();
+    for (int op = 0; op < 3; op++) {
+      size_t per = (op == 1) ? 3 : 9;
+      for (int mm = lo; mm < hi; mm++) {
+        double qpm[13 * 3], fmv[3][13][3];
+        quad_tri_points(&P->qd, m, mm, qpm);
+        for (int pp = 0; pp < 3; pp++)
+          for (int r = 0; r < nq; r++) rwg(m, qpm + 3 * r, mm, pp, fmv[pp][r]);
+#pragma omp parallel for schedule(static)
+        for (int n = 0; n < F; n++) {
+          int near = near_faces(m, n, mm);
+          for (int r = 0; r < nq; r++) {
+            cplx *dst = intaux + ((size_t)n * nq + r) * per;
+            if (op == 0) intK2(qpm + 3 * r, n, m, k, near, &P->qd, dst);
+            else if (op == 1) intK1(qpm + 3 * r, n, m, k, near, &P->qd, dst);
+            else intK4(qpm + 3 * r, n, m, k, mm, near, &P->qd, dst);
+          }
+        }
+        for (int n = 0; n < F; n++)
+          for (int pp = 0; pp < 3; pp++)
+            for (int q = 0; q < 3; q++) {
+              cplx int1 = 0;
+              for (int r = 0; r < nq; r++) {
+                const cplx *a = intaux + ((size_t)n * nq + r) * per;
+                if (op == 1) int1 += P->qd.w[r] * a[q];
+                else int1 += P->qd.w[r] * (fmv[pp][r][0] * a[3 * q] + fmv[pp][r][1] * a[3 * q + 1] + fmv[pp][r][2] * a[3 * q + 2]);
+              }
+              rows[(size_t)(3 * (mm - lo) + pp) + (size_t)m->face_edge[3 * n + q] * 3 * (hi - lo)] += int1;
+            }
+      }
+    }
+    for (size_t i = 0; i < (size_t)3 * (hi - lo) * Nd; i++) chk += cabs(rows[i]);
+    free(rows);
+    free(intaux);
+  }
+  return chk;
+}
+
 /* One domain operator (D, H or K) for tests: M is N_d x N_d. */
 void oracle_operator(void *p, int d, int op, double omega, const double *ri_ri, cplx *M) {
   oproblem *P = p;

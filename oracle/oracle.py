@@ -56,6 +56,8 @@ def lib():
         L.oracle_problem_sizes.argtypes = [C.c_void_p, ip]
         L.oracle_problem_export.argtypes = [C.c_void_p, C.c_int, dp, ip, ip, ip, ip, ip, ip, dp]
         L.oracle_sysmat.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int]
+        L.oracle_sysmat_sample.argtypes = [C.c_void_p, C.c_double, dp, C.c_int, C.c_int, C.c_int]
+        L.oracle_sysmat_sample.restype = C.c_double
         L.oracle_operator.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, dp, C.c_void_p]
         L.oracle_srcvec.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p]
         L.oracle_cs.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p, dp, dp]
@@ -154,6 +156,11 @@ class OracleProblem:
         rr = np.array([[complex(v).real, complex(v).imag] for v in ri], dtype=np.float64)
         lib().oracle_sysmat(self.h, omega, _dp(rr), A.ctypes.data, 2 * self.N, mlo, mhi, nthreads)
         return A
+
+    def sysmat_sample(self, omega, ri, mlo, mhi, nthreads=0):
+        """Timing sample: the sysmat work of test faces [mlo, mhi) of every domain (no matrix)."""
+        rr = np.array([[complex(v).real, complex(v).imag] for v in ri], dtype=np.float64)
+        return lib().oracle_sysmat_sample(self.h, omega, _dp(rr), mlo, mhi, nthreads)
 
     def operator(self, d, op, omega, ri):
         """One domain operator: op 0 = D, 1 = H, 2 = K (computeD/H/K)."""
