@@ -40,7 +40,7 @@ DEGTORAD = PI_F / 180.0
 EXPORTS = [
     "mom_gpu_create", "mom_gpu_destroy", "mom_gpu_strerror", "mom_gpu_last_error", "mom_gpu_set_problem",
     "mom_gpu_sysmat", "mom_gpu_srcvec", "mom_gpu_solve", "mom_gpu_solve_wavelength", "mom_gpu_cross_sections",
-    "mom_gpu_rcs", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
+    "mom_gpu_rcs", "mom_gpu_cross_sections_noalloc", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
     "mom_gpu_launch_count", "mom_gpu_stream", "mom_gpu_library_calls", "mom_gpu_profile", "mom_gpu_profile_read",
     "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
@@ -95,6 +95,8 @@ def lib():
     L.mom_gpu_cross_sections.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp, C.c_int64,
                                          dp, dp]
     L.mom_gpu_rcs.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, C.c_int32, C.c_int32, dp]
+    L.mom_gpu_cross_sections_noalloc.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp,
+                                                 C.c_int64, dp, dp]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
@@ -326,6 +328,25 @@ class Solver:
         self._ck(lib().mom_gpu_cross_sections(self.h, dom, omega, _dp(r), ns, arr, xp, 2 * self.N, _dp(csca),
                                               _dp(cabs)), "cross_sections")
         return csca, cabs
+
+    def cross_sections_noalloc(self, omega, ri, srcs, x_dev, ldx, dom=0):
+        """Cross sections through the allocation-free entry point: x_dev is a device
+        pointer (int) to the 2N x nsrc solutions with leading dimension ldx."""
+        arr, ns = _srcs(srcs)
+        r = _ri(ri)
+        csca = np.zeros(ns)
+        cabs = np.zeros(ns)
+        self._ck(lib().mom_gpu_cross_sections_noalloc(self.h, dom, omega, _dp(r), ns, arr, C.c_void_p(x_dev), ldx,
+                                                      _dp(csca), _dp(cabs)), "cross_sections_noalloc")
+        return csca, cabs
+
+    def device_solution(self):
+        """(device pointer, leading dimension, number of sources) of the solutions."""
+        p = C.c_void_p()
+        ld = C.c_int64()
+        ns = C.c_int32()
+        self._ck(lib().mom_gpu_device_solution(self.h, C.byref(p), C.byref(ld), C.byref(ns)), "device_solution")
+        return p.value, ld.value, ns.value
 
     def rcs(self, omega, ri, ntheta, nphi, isrc=0, x=None, dom=0):
         r = _ri(ri)

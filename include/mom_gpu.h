@@ -126,6 +126,23 @@ int mom_gpu_cross_sections(mom_ctx *ctx, int32_t dom, double omega, const double
 int mom_gpu_rcs(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
                 int64_t ldx, int32_t ntheta, int32_t nphi, double *rcs);
 
+/* Allocation-free cross sections.  No counterpart in the reference.  For
+ * callers that cannot allocate device memory at call time (their device
+ * memory is reserved up front by another allocator, or they cannot accept
+ * the implicit device-wide synchronisation of cudaMalloc / cudaFree): the
+ * same results as mom_gpu_cross_sections, computed with a fixed scratch
+ * array compiled into the library instead of allocated buffers.  x_dev is a
+ * device pointer to the 2N x nsrc solutions (leading dimension ldx >= 2N,
+ * e.g. from mom_gpu_device_solution); csca / cabs are host arrays.
+ * Limits: 1 <= nsrc <= 64 and at most 65536 faces in domain dom; larger
+ * requests return MOM_ERR_ARG.  The first call on a device looks up the
+ * scratch array's device address, so make it before any stream capture.
+ * All calls on a device share the scratch array: calls that overlap on the
+ * GPU (from different contexts) race. */
+int mom_gpu_cross_sections_noalloc(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t nsrc,
+                                   const mom_src *src, const void *x_dev, int64_t ldx, double *csca,
+                                   double *cabs);
+
 /* Device views for callers that keep data resident (bench, tests). */
 int mom_gpu_device_matrix(mom_ctx *ctx, void **A_dev, int64_t *lda);
 int mom_gpu_device_solution(mom_ctx *ctx, void **x_dev, int64_t *ldx, int32_t *nsrc);
