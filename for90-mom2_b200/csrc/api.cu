@@ -310,7 +310,8 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   c->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess) {
+      cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess ||
+      cudaMalloc(&c->flags, sizeof(unsigned) * 256) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return MOM_ERR_CUDA;
@@ -332,6 +333,7 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->ws);
   cudaFree(c->Xh);
   cudaFree(c->dinfo);
+  cudaFree(c->flags);
   if (c->pinned) cudaFreeHost(c->pinned);
   cublasDestroy(c->blas);
   cudaStreamDestroy(c->stream);
@@ -553,7 +555,7 @@ int mom_gpu_profile(mom_ctx *c, int32_t enable) {
 }
 
 int mom_gpu_profile_read(mom_ctx *c, int32_t category, double *ms_total, int64_t *launches) {
-  if (!c || category < 0 || category >= 8 || !ms_total || !launches) return MOM_ERR_ARG;
+  if (!c || category < 0 || category >= kProfCount || !ms_total || !launches) return MOM_ERR_ARG;
   std::lock_guard<std::mutex> g(c->mu);
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
   double t = 0;

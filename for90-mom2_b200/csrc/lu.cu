@@ -53,241 +53,329 @@ struct PanelArgs {
   double2 *col_data;  // [2][nb]
 };
 
-// Grid-wide barrier of a cooperative launch: one release-add per CTA on a
-// counter zeroed before the launch, acquire-polling until it reaches
-// target.  The wait is bounded: after kSpinLimit polls the CTA sets *timeout
-// and every CTA leaves (the host reports MOM_ERR_TIMEOUT).
-__device__ bool grid_barrier(unsigned *bar, unsigned target, int *timeout) {
-  __syncthreads();
-  bool ok = true;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-    long long it = 0;
-    while (true) {
-      unsigned v;
-      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
-      if (v >= target) break;
-      if ((++it & 255) == 0) {
-        if (*(volatile int *)timeout) {
-          ok = false;
-          break;
-        }
-        if (it > kSpinLimit) {
-          atomicExch(timeout, 1);
-          ok = false;
-          break;
-        }
-        __nanosleep(32);
-      }
+// (value, row) pair reduction: larger |re|+|im| wins, the first row on ties.
+__device__ __forceinline__ void argmax_warp(double &v, int &r, int &w) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffffu, v, o);
+    const int orow = __shfl_down_sync(0xffffffffu, r, o);
+    const int ow = __shfl_down_sync(0xffffffffu, w, o);
+    if (ov > v || (ov == v && orow < r)) {
+      v = ov;
+      r = orow;
+      w = ow;
     }
   }
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) s_ok = ok;
+}
+
+// Grid barrier for warp 0 of each CTA: CTA c publishes its arrival epoch in
+// flags[c] with a release store (no same-address atomics), then the warp
+// polls all P flags with acquire loads until every CTA has reached epoch.
+// Bounded: after kSpinLimit polling rounds *timeout is set and the warp
+// returns false.  flags[] is zeroed before the launch.
+__device__ __forceinline__ bool flag_barrier_warp0(unsigned *flags, int P, unsigned epoch, int *timeout) {
+  const int lane = threadIdx.x & 31;
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flags + blockIdx.x), "r"(epoch) : "memory");
+  long long it = 0;
+  int ok = 1;
+  while (true) {
+    bool done = true;
+    for (int p = lane; p < P; p += 32) {
+      unsigned f;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flags + p) : "memory");
+      done = done && (f >= epoch);
+    }
+    if (__all_sync(0xffffffffu, done)) {
+      __threadfence();  // acquire: order the later reads after the observed flags
+      break;
+    }
+    if ((++it & 255) == 0) {
+      int stop = 0;
+      if (lane == 0) {
+        if (*(volatile int *)timeout) stop = 1;
+        else if (it > kSpinLimit) {
+          atomicExch(timeout, 1);
+          stop = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, stop, 0)) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  return ok != 0;
+}
+
+// Block-wide form: warp 0 crosses the barrier, the rest of the CTA waits.
+__device__ bool flag_barrier(unsigned *flags, int P, unsigned epoch, int *timeout) {
   __syncthreads();
-  return s_ok != 0;
+  __shared__ int s_fok;
+  if (threadIdx.x < 32) {
+    const bool ok = flag_barrier_warp0(flags, P, epoch, timeout);
+    if (threadIdx.x == 0) s_fok = ok;
+  }
+  __syncthreads();
+  return s_fok != 0;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   extern __shared__ double2 slab[];  // [nb][rpc] column-major within the CTA
-  __shared__ double red_abs[kPanelThreads];
-  __shared__ int red_row[kPanelThreads];
-  __shared__ int red_cta[kPanelThreads];
+  __shared__ double w_abs[kPanelThreads / 32];
+  __shared__ int w_row[kPanelThreads / 32];
   __shared__ double2 s_prow_data[64];
-  __shared__ int s_prow, s_pcta;
-  const int tid = threadIdx.x, cta = blockIdx.x;
+  __shared__ int s_prow, s_ok;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;
   const int nb = a.nb, rpc = a.rpc;
   T *A = reinterpret_cast<T *>(a.A);
   const int64_t row0 = a.j0 + (int64_t)cta * rpc;
   const int64_t rem = a.n - row0;
   const int nrow = rem <= 0 ? 0 : (rem < rpc ? (int)rem : rpc);
-  for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
-    const int c = idx / rpc, i = idx % rpc;
-    slab[idx] = (i < nrow) ? ld2(A + (row0 + i) + (a.j0 + c) * a.lda) : make_double2(0, 0);
+  for (int base = tid; base < nb * rpc; base += 8 * kPanelThreads) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * kPanelThreads;
+      const int c = idx / rpc, i = idx % rpc;
+      v[u] = (idx < nb * rpc && i < nrow) ? ld2(A + (row0 + i) + (a.j0 + c) * a.lda) : make_double2(0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * kPanelThreads;
+      if (idx < nb * rpc) slab[idx] = v[u];
+    }
   }
   __syncthreads();
+  const bool mine = tid < nrow;
+  const int64_t g = row0 + tid;  // global row owned by this thread
+  double cv = (mine && g >= a.j0) ? cabs1(slab[tid]) : -1.0;  // candidate for column 0
   for (int c = 0; c < nb; c++) {
     const int64_t col = a.j0 + c;
     const int par = c & 1;
-    // local pivot candidate in column c over owned rows >= col
-    double best = -1.0;
-    int brow = 0x7fffffff;
-    for (int i = tid; i < nrow; i += kPanelThreads) {
-      const int64_t g = row0 + i;
-      if (g < col) continue;
-      const double v = cabs1(slab[c * rpc + i]);
-      if (v > best || (v == best && g < brow)) {
-        best = v;
-        brow = (int)g;
-      }
+    // 1. CTA candidate
+    double v = cv;
+    int r = (v >= 0.0) ? (int)g : 0x7fffffff, wdummy = 0;
+    argmax_warp(v, r, wdummy);
+    if (lane == 0) {
+      w_abs[wid] = v;
+      w_row[wid] = r;
     }
-    red_abs[tid] = best;
-    red_row[tid] = brow;
     __syncthreads();
-    for (int w = kPanelThreads / 2; w > 0; w >>= 1) {
-      if (tid < w) {
-        const double ov = red_abs[tid + w];
-        const int orow = red_row[tid + w];
-        if (ov > red_abs[tid] || (ov == red_abs[tid] && orow < red_row[tid])) {
-          red_abs[tid] = ov;
-          red_row[tid] = orow;
-        }
+    if (wid == 0) {
+      double bv = lane < kPanelThreads / 32 ? w_abs[lane] : -1.0;
+      int br = lane < kPanelThreads / 32 ? w_row[lane] : 0x7fffffff;
+      argmax_warp(bv, br, wdummy);
+      bv = __shfl_sync(0xffffffffu, bv, 0);
+      br = __shfl_sync(0xffffffffu, br, 0);
+      // 2. publish candidate (value, row, row data) and, if owned, row col
+      if (lane == 0) {
+        a.cand_abs[par * a.P + cta] = bv;
+        a.cand_row[par * a.P + cta] = br;
       }
-      __syncthreads();
-    }
-    const int my_row = red_row[0];
-    if (tid == 0) {
-      a.cand_abs[par * a.P + cta] = red_abs[0];
-      a.cand_row[par * a.P + cta] = my_row;
-    }
-    if (red_abs[0] >= 0.0) {
-      const int li = my_row - (int)row0;
-      for (int j = tid; j < nb; j += kPanelThreads) a.cand_data[((size_t)par * a.P + cta) * nb + j] = slab[j * rpc + li];
-    }
-    if (col >= row0 && col < row0 + nrow) {
-      const int li = (int)(col - row0);
-      for (int j = tid; j < nb; j += kPanelThreads) a.col_data[(size_t)par * nb + j] = slab[j * rpc + li];
-    }
-    if (!grid_barrier(a.bar, (unsigned)(c + 1) * a.P, a.timeout)) return;
-    // global pivot: largest cabs1, first row on ties (izamax); the P
-    // candidates are reduced in parallel by the CTA.
-    {
-      double v = -1.0;
-      int r = 0x7fffffff, w = -1;
-      if (tid < a.P) {
-        v = __ldcg(a.cand_abs + par * a.P + tid);
-        r = __ldcg(a.cand_row + par * a.P + tid);
-        w = tid;
+      if (bv >= 0.0) {
+        const int li = br - (int)row0;
+        for (int j = lane; j < nb; j += 32) a.cand_data[((size_t)par * a.P + cta) * nb + j] = slab[j * rpc + li];
       }
-      red_abs[tid] = v;
-      red_row[tid] = r;
-      red_cta[tid] = w;
-      __syncthreads();
-      for (int h = kPanelThreads / 2; h > 0; h >>= 1) {
-        if (tid < h) {
-          const double ov = red_abs[tid + h];
-          const int orow = red_row[tid + h];
-          if (ov > red_abs[tid] || (ov == red_abs[tid] && orow < red_row[tid])) {
-            red_abs[tid] = ov;
-            red_row[tid] = orow;
-            red_cta[tid] = red_cta[tid + h];
+      if (col >= row0 && col < row0 + nrow) {
+        const int li = (int)(col - row0);
+        for (int j = lane; j < nb; j += 32) a.col_data[(size_t)par * nb + j] = slab[j * rpc + li];
+      }
+      int ok = flag_barrier_warp0(a.bar, a.P, (unsigned)(c + 1), a.timeout) ? 1 : 0;
+      if (ok) {
+        // 3. global pivot from the P candidates
+        double gv = -1.0;
+        int gr = 0x7fffffff, gw = -1;
+        for (int p = lane; p < a.P; p += 32) {
+          const double pv = __ldcg(a.cand_abs + par * a.P + p);
+          const int pr = __ldcg(a.cand_row + par * a.P + p);
+          if (pv > gv || (pv == gv && pr < gr)) {
+            gv = pv;
+            gr = pr;
+            gw = p;
           }
         }
-        __syncthreads();
-      }
-      if (tid == 0) {
-        s_prow = red_row[0];
-        s_pcta = red_cta[0];
-        if (cta == 0) {
-          a.ipiv[col] = red_row[0];
-          if (red_abs[0] == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+        argmax_warp(gv, gr, gw);
+        gv = __shfl_sync(0xffffffffu, gv, 0);
+        gr = __shfl_sync(0xffffffffu, gr, 0);
+        gw = __shfl_sync(0xffffffffu, gw, 0);
+        const double2 *pdat = a.cand_data + ((size_t)par * a.P + gw) * nb;
+        const double2 *cdat = a.col_data + (size_t)par * nb;
+        const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
+        const bool own_c = col >= row0 && col < row0 + nrow;
+        for (int j = lane; j < nb; j += 32) {
+          const double2 pv = __ldcg(pdat + j), cvv = __ldcg(cdat + j);
+          s_prow_data[j] = pv;
+          if (own_p) slab[j * rpc + (gr - (int)row0)] = cvv;  // row prow <- old row col
+          if (own_c) slab[j * rpc + (int)(col - row0)] = pv;  // row col  <- pivot row
+        }
+        if (lane == 0) {
+          s_prow = gr;
+          if (cta == 0) {
+            a.ipiv[col] = gr;
+            if (gv == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+          }
         }
       }
+      if (lane == 0) s_ok = ok;
     }
     __syncthreads();
-    const int prow = s_prow, pcta = s_pcta;
-    const double2 *pdat = a.cand_data + ((size_t)par * a.P + pcta) * nb;
-    const double2 *cdat = a.col_data + (size_t)par * nb;
-    // swap rows col <-> prow inside the panel
-    if (prow != col && prow >= row0 && prow < row0 + nrow) {
-      const int li = prow - (int)row0;
-      for (int j = tid; j < nb; j += kPanelThreads) slab[j * rpc + li] = __ldcg(cdat + j);
-    }
-    if (col >= row0 && col < row0 + nrow) {
-      const int li = (int)(col - row0);
-      for (int j = tid; j < nb; j += kPanelThreads) slab[j * rpc + li] = __ldcg(pdat + j);
-    }
-    for (int j = tid; j < nb; j += kPanelThreads) s_prow_data[j] = __ldcg(pdat + j);
-    __syncthreads();
-    const double2 piv = s_prow_data[c];
-    const double pa = piv.x * piv.x + piv.y * piv.y;
-    if (pa != 0.0) {
-      const double2 rp = make_double2(piv.x / pa, -piv.y / pa);  // 1 / pivot
-      for (int i = tid; i < nrow; i += kPanelThreads) {
-        const int64_t g = row0 + i;
-        if (g <= col) continue;
-        const double2 l = cmul(slab[c * rpc + i], rp);
-        slab[c * rpc + i] = l;
-        for (int j = c + 1; j < nb; j++) {
-          const double2 u = s_prow_data[j];
-          double2 v = slab[j * rpc + i];
-          v.x -= l.x * u.x - l.y * u.y;
-          v.y -= l.x * u.y + l.y * u.x;
-          slab[j * rpc + i] = v;
+    if (!s_ok) return;
+    // 4. swap, scale, rank-1 update of the owned row; next candidate
+    cv = -1.0;
+    if (mine) {
+      if (g > col) {
+        const double2 piv = s_prow_data[c];
+        const double pa = piv.x * piv.x + piv.y * piv.y;
+        if (pa != 0.0) {
+          const double2 rp = make_double2(piv.x / pa, -piv.y / pa);  // 1 / pivot
+          const double2 l = cmul(slab[c * rpc + tid], rp);
+          slab[c * rpc + tid] = l;
+          for (int j = c + 1; j < nb; j++) {
+            const double2 u = s_prow_data[j];
+            double2 x = slab[j * rpc + tid];
+            x.x -= l.x * u.x - l.y * u.y;
+            x.y -= l.x * u.y + l.y * u.x;
+            slab[j * rpc + tid] = x;
+          }
         }
+        if (c + 1 < nb) cv = cabs1(slab[(c + 1) * rpc + tid]);
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
     const int c = idx / rpc, i = idx % rpc;
     if (i < nrow) st2(A + (row0 + i) + (a.j0 + c) * a.lda, slab[idx]);
   }
 }
 
-// Row interchanges ipiv[j0 .. j0+nb) applied, in order, to the columns
-// outside the panel.
+// The nb row interchanges of a panel (ipiv[j0 .. j0+nb), applied in order)
+// composed into one permutation of the at most 2 nb rows they touch:
+// after the swaps, row dst[i] holds the old row src[i], i < *count.
+__global__ void pivot_map_kernel(const int *ipiv, int64_t j0, int nb, int *dst, int *src, int *count) {
+  __shared__ int rows[128], orig[128];
+  __shared__ int cnt;
+  if (threadIdx.x != 0) return;
+  cnt = 0;
+  auto slot = [&](int r) {
+    for (int i = 0; i < cnt; i++)
+      if (rows[i] == r) return i;
+    rows[cnt] = r;
+    orig[cnt] = r;
+    return cnt++;
+  };
+  for (int c = 0; c < nb; c++) {
+    const int a = (int)(j0 + c), b = ipiv[j0 + c];
+    if (a == b) continue;
+    const int ia = slot(a), ib = slot(b);
+    const int t = orig[ia];
+    orig[ia] = orig[ib];
+    orig[ib] = t;
+  }
+  int k = 0;
+  for (int i = 0; i < cnt; i++)
+    if (orig[i] != rows[i]) {
+      dst[k] = rows[i];
+      src[k] = orig[i];
+      k++;
+    }
+  *count = k;
+}
+
+// Apply the composed panel permutation to every column outside the panel:
+// one warp per column, all source rows loaded before any store.
 template <typename T>
-__global__ void laswp_kernel(T *A, int64_t lda, int64_t n, int64_t j0, int nb, const int *ipiv) {
-  int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void laswp_kernel(T *A, int64_t lda, int64_t n, int64_t j0, int nb, const int *dst, const int *src,
+                             const int *count) {
+  const int lane = threadIdx.x & 31;
+  int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (col >= n - nb) return;
   if (col >= j0) col += nb;
+  const int k = *count;
   T *a = A + col * lda;
-  for (int c = 0; c < nb; c++) {
-    const int64_t r = ipiv[j0 + c];
-    if (r != j0 + c) {
-      T t = a[j0 + c];
-      a[j0 + c] = a[r];
-      a[r] = t;
-    }
+  T v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = lane + 32 * q;
+    if (i < k) v[q] = a[src[i]];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = lane + 32 * q;
+    if (i < k) a[dst[i]] = v[q];
   }
 }
 
 // Inverses of the unit-lower L11 and upper U11 diagonal blocks of the panel
-// (FP64), stored as inv[0] = inv(L11), inv[1] = inv(U11), column-major nb x nb.
-// One CTA, thread j computes column j.
+// (FP64), stored as inv[0] = inv(L11), inv[1] = inv(U11), column-major
+// nb x nb.  One CTA; thread j < nb builds column j of inv(L11) and thread
+// nb + j column j of inv(U11), entirely in shared memory.
 template <typename T>
 __global__ void diag_inv_kernel(const T *A, int64_t lda, int64_t j0, int nb, double2 *invL, double2 *invU,
                                 float2 *invL32) {
-  extern __shared__ double2 D[];  // nb x nb
-  const int j = threadIdx.x;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;
-    D[idx] = ld2(A + (j0 + r) + (j0 + c) * lda);
+  extern __shared__ double2 sm[];
+  double2 *D = sm, *XL = sm + nb * nb, *XU = sm + 2 * nb * nb;
+  // eight independent loads in flight per thread before the shared stores
+  for (int base = threadIdx.x; base < nb * nb; base += 8 * blockDim.x) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * blockDim.x;
+      if (idx < nb * nb) v[u] = ld2(A + (j0 + idx % nb) + (j0 + idx / nb) * lda);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * blockDim.x;
+      if (idx < nb * nb) D[idx] = v[u];
+    }
   }
   __syncthreads();
-  if (j >= nb) return;
-  // inv(L): solve L x = e_j (unit diagonal)
-  for (int i = 0; i < nb; i++) {
-    double2 v = make_double2(i == j ? 1.0 : 0.0, 0.0);
-    if (i > j) {
-      for (int k = j; k < i; k++) {
-        const double2 l = D[i + k * nb], x = invL[k + j * nb];
+  // XL / XU are stored transposed ([k][j], thread j contiguous) so the
+  // threads of a warp hit distinct banks.
+  const int t = threadIdx.x;
+  if (t < nb) {
+    const int j = t;  // unit lower: x_i = -sum_{k=j}^{i-1} L_ik x_k
+    for (int i = 0; i < nb; i++) {
+      double2 v = make_double2(i == j ? 1.0 : 0.0, 0.0);
+      // k runs over the same values in every thread (D[i + k nb] is then a
+      // broadcast); entries with k < j are zero by construction of XL.
+      for (int k = 0; k < i; k++) {
+        const double2 l = D[i + k * nb], x = XL[j + k * nb];
         v.x -= l.x * x.x - l.y * x.y;
         v.y -= l.x * x.y + l.y * x.x;
       }
-    } else if (i < j) {
-      v = make_double2(0, 0);
+      XL[j + i * nb] = v;
     }
-    invL[i + j * nb] = v;
-    if (invL32) invL32[i + j * nb] = make_float2((float)v.x, (float)v.y);
-  }
-  // inv(U): solve U x = e_j, i from j down to 0
-  for (int i = nb - 1; i >= 0; i--) {
-    double2 v = make_double2(0, 0);
-    if (i <= j) {
-      v = make_double2(i == j ? 1.0 : 0.0, 0.0);
-      for (int k = i + 1; k <= j; k++) {
-        const double2 u = D[i + k * nb], x = invU[k + j * nb];
-        v.x -= u.x * x.x - u.y * x.y;
-        v.y -= u.x * x.y + u.y * x.x;
+  } else if (t < 2 * nb) {
+    const int j = t - nb;  // upper: x_i = (delta_ij - sum_{k=i+1}^{j} U_ik x_k) / U_ii
+    for (int i = nb - 1; i >= 0; i--) {
+      double2 v = make_double2(0, 0);
+      if (i <= j) {
+        v = make_double2(i == j ? 1.0 : 0.0, 0.0);
+        for (int k = i + 1; k <= j; k++) {
+          const double2 u = D[i + k * nb], x = XU[j + k * nb];
+          v.x -= u.x * x.x - u.y * x.y;
+          v.y -= u.x * x.y + u.y * x.x;
+        }
+        const double2 d = D[i + i * nb];
+        const double dd = d.x * d.x + d.y * d.y;
+        v = (dd != 0.0) ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd) : make_double2(0, 0);
       }
-      const double2 d = D[i + i * nb];
-      const double dd = d.x * d.x + d.y * d.y;
-      v = (dd != 0.0) ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd) : make_double2(0, 0);
+      XU[j + i * nb] = v;
     }
-    invU[i + j * nb] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+    const int r = idx % nb, c = idx / nb;  // inv(r, c) is held at X[c + r * nb]
+    const double2 l = XL[c + r * nb], u = XU[c + r * nb];
+    invL[idx] = l;
+    invU[idx] = u;
+    if (invL32) invL32[idx] = make_float2((float)l.x, (float)l.y);
   }
 }
 
@@ -311,7 +399,6 @@ __global__ void compose_pivots_kernel(const int *ipiv, int n, int *perm) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = p[i];
 }
 
-
 struct TrsvArgs {
   const void *M;     // LU factors (T)
   int64_t lda, n;
@@ -321,6 +408,7 @@ struct TrsvArgs {
   double2 *X, *Y;      // [ns][n]: right-hand sides in X, scratch Y; solution returned in X
   unsigned *bar;
   int *timeout;
+  int direct;  // 1: factor tiles do not fit in shared memory; read them from global memory
 };
 
 // y = Inv * x for an nb x nb block and ns vectors held in shared memory;
@@ -338,7 +426,7 @@ __device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *x
       const int r = o % nb, sv = o / nb;
 #pragma unroll 4
       for (int j = part; j < nb; j += parts) {
-        const double2 iv = __ldg(inv + r + (size_t)j * nb);
+        const double2 iv = inv[r + (size_t)j * nb];
         const double2 xv = xs[sv * nb + j];
         acc.x += iv.x * xv.x - iv.y * xv.y;
         acc.y += iv.x * xv.y + iv.y * xv.x;
@@ -383,8 +471,10 @@ __device__ __forceinline__ void upd_range(int pass, int64_t k0, int nb, int64_t 
 template <typename T, int NS>
 __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
   __shared__ double2 xs[8 * 64], ys[8 * 64], red[256];
-  extern __shared__ __align__(16) unsigned char tile_raw[];  // [nb][rpc] of T
+  extern __shared__ __align__(16) unsigned char tile_raw[];  // [nb][rpc] of T, then [nb][nb] double2
   T *tile = reinterpret_cast<T *>(tile_raw);
+  double2 *sinv = reinterpret_cast<double2 *>(
+      tile_raw + (a.direct ? 0 : ((sizeof(T) * (size_t)a.nb * a.rpc + 15) / 16) * 16));
   const T *M = reinterpret_cast<const T *>(a.M);
   const int64_t n = a.n, lda = a.lda;
   const int nb = a.nb, nblk = (int)(n / nb), rpc = a.rpc;
@@ -398,18 +488,20 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
     const int64_t k0 = (int64_t)kb * nb;
     int64_t lo, hi;
     upd_range(pass, k0, nb, r0, r1, &lo, &hi);
-    const int cnt = (int)(hi > lo ? hi - lo : 0);
+    const int cnt = (a.direct || hi <= lo) ? 0 : (int)(hi - lo);
     for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
       const int i = idx % cnt, j = idx / cnt;
       cp_async(tile + (size_t)j * rpc + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
     }
+    const double2 *ib = a.inv + ((size_t)kb * 2 + pass) * nb * nb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) cp_async(sinv + idx, ib + idx, 1);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   // Y = P X
   for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
     for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + a.perm[i]];
   prefetch(0, 0);
-  if (!grid_barrier(a.bar, ++step * a.P, a.timeout)) return;
+  if (!flag_barrier(a.bar, a.P, ++step, a.timeout)) return;
   for (int pass = 0; pass < 2; pass++) {
     double2 *src = pass == 0 ? a.Y : a.X;  // vector being reduced
     double2 *dst = pass == 0 ? a.X : a.Y;  // solved blocks
@@ -420,8 +512,9 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
         const int j = idx % nb, sv = idx / nb;
         xs[sv * nb + j] = __ldcg(src + (size_t)sv * n + k0 + j);
       }
+      cp_async_wait_all();
       __syncthreads();
-      block_apply(a.inv + ((size_t)kb * 2 + pass) * nb * nb, nb, ns, xs, ys, red);
+      block_apply(sinv, nb, ns, xs, ys, red);
       // owners of block kb's rows store the solved block
       for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
         const int j = idx % nb, sv = idx / nb;
@@ -430,16 +523,15 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
       }
       int64_t lo, hi;
       upd_range(pass, k0, nb, r0, r1, &lo, &hi);
-      cp_async_wait_all();
-      __syncthreads();
       for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         double2 acc[NS];
 #pragma unroll
         for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
-        const T *mp = tile + (i - lo);
+        const T *mp = a.direct ? M + i + k0 * lda : tile + (i - lo);
+        const int64_t mstride = a.direct ? lda : rpc;
 #pragma unroll 8
         for (int j = 0; j < nb; j++) {
-          const double2 m = ld2(mp + (size_t)j * rpc);
+          const double2 m = ld2(mp + (size_t)j * mstride);
 #pragma unroll
           for (int sv = 0; sv < ns; sv++) {
             const double2 y = ys[sv * nb + j];
@@ -459,7 +551,7 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
       // next tile: the following block of this pass, or the first of the next pass
       if (kk + 1 < nblk) prefetch(pass, kk + 1);
       else if (pass == 0) prefetch(1, 0);
-      if (!grid_barrier(a.bar, ++step * a.P, a.timeout)) return;
+      if (!flag_barrier(a.bar, a.P, ++step, a.timeout)) return;
     }
   }
   cp_async_wait_all();
@@ -545,6 +637,8 @@ struct LuWork {
   double2 *cand_data, *col_data;
   double2 *W;      // nb x n workspace for the TRSM product
   float2 *invL32;  // nb x nb
+  float *tcw;      // tensor-core GEMM operands (mixed path)
+  int *pmap;       // [257]: composed panel permutation (dst[128], src[128], count)
 };
 
 int lu_workspace(Ctx *c, int precision, LuWork &w) {
@@ -556,13 +650,15 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
     off += (bytes + 255) / 256 * 256;
     return o;
   };
-  const size_t o_bar = take(sizeof(unsigned) * 4);
+  const size_t o_bar = take(sizeof(unsigned) * 256);
   const size_t o_ca = take(sizeof(double) * 2 * P);
   const size_t o_cr = take(sizeof(int) * 2 * P);
   const size_t o_cd = take(sizeof(double2) * 2 * P * nb);
   const size_t o_cl = take(sizeof(double2) * 2 * nb);
   const size_t o_w = take(esz * (size_t)nb * c->n);
   const size_t o_i32 = take(sizeof(float2) * (size_t)nb * c->n);
+  const size_t o_pm = take(sizeof(int) * 260);
+  const size_t o_tc = take(precision == MOM_PREC_MIXED ? tc_cgemm_work_bytes((int)c->n, (int)c->n, 4 * nb) : 0);
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off));
   char *b = (char *)c->ws;
   w.bar = (unsigned *)(b + o_bar);
@@ -574,6 +670,8 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   w.col_data = (double2 *)(b + o_cl);
   w.W = (double2 *)(b + o_w);
   w.invL32 = (float2 *)(b + o_i32);
+  w.tcw = (float *)(b + o_tc);
+  w.pmap = (int *)(b + o_pm);
   return MOM_OK;
 }
 
@@ -586,7 +684,8 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
   MOM_TRY(lu_workspace(c, precision, w));
   MOM_CUDA(c, cudaMemsetAsync(c->dinfo, 0, sizeof(int) * 4, c->stream));
   const bool mixed = precision == MOM_PREC_MIXED;
-  MOM_BLAS(c, cublasSetMathMode(c->blas, mixed ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_DEFAULT_MATH));
+  // The small GEMMs (block TRSM, updates inside an outer block) stay in full FP32 / FP64.
+  MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
   // C <- alpha * A(m x k) * B(k x nc) + beta * C, column-major with lda
   auto gemm = [&](int64_t m, int64_t ncol, int64_t k, double alpha, const T *Am, int64_t la, const T *Bm, int64_t lb,
                   double beta, T *Cm, int64_t lc) -> int {
@@ -625,7 +724,8 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
       int rpc = (int)((m + P - 1) / P);
       P = (int)((m + rpc - 1) / rpc);
       const size_t smem = sizeof(double2) * (size_t)nb * rpc;
-      if (smem > 227 * 1024) return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory");
+      if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64)
+        return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory (matrix order too large)");
       PanelArgs pa;
       pa.A = A;
       pa.lda = lda;
@@ -644,20 +744,25 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
       pa.col_data = w.col_data;
       {
         ProfScope ps(c, kProfPanel);
-        MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned), c->stream));
+        MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned) * 256, c->stream));
         MOM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         void *args[] = {&pa};
         MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
                                                 c->stream));
         c->launches++;
+      }
+      {
+        ProfScope pz(c, kProfPivotAux);
         if (n > nb) {
-          laswp_kernel<T><<<(unsigned)((n - nb + 255) / 256), 256, 0, c->stream>>>(A, lda, n, j0, nb, c->ipiv);
-          c->launches++;
+          pivot_map_kernel<<<1, 32, 0, c->stream>>>(c->ipiv, j0, nb, w.pmap, w.pmap + 128, w.pmap + 256);
+          laswp_kernel<T><<<(unsigned)(((n - nb) * 32 + 255) / 256), 256, 0, c->stream>>>(A, lda, n, j0, nb, w.pmap,
+                                                                                          w.pmap + 128, w.pmap + 256);
+          c->launches += 2;
         }
         double2 *invL = c->invd + (size_t)kb * 2 * nb * nb, *invU = invL + (size_t)nb * nb;
         MOM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(double2) * nb * nb)));
-        diag_inv_kernel<T><<<1, std::max(nb, 64), sizeof(double2) * nb * nb, c->stream>>>(
+                                         (int)(sizeof(double2) * 3 * nb * nb)));
+        diag_inv_kernel<T><<<1, 2 * nb, sizeof(double2) * 3 * nb * nb, c->stream>>>(
             A, lda, j0, nb, invL, invU, mixed ? w.invL32 + (size_t)kb * nb * nb : nullptr);
         c->launches++;
         MOM_CUDA(c, cudaGetLastError());
@@ -681,8 +786,16 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
         MOM_TRY(gemm(below, nc, nb, -1.0, A + (j0 + nb) + j0 * lda, lda, A + j0 + t0 * lda, lda, 1.0,
                      A + (j0 + nb) + t0 * lda, lda));
       }
-      MOM_TRY(gemm(n - t0, nc, NBc, -1.0, A + t0 + J0 * lda, lda, A + J0 + t0 * lda, lda, 1.0, A + t0 + t0 * lda,
-                   lda));
+      if (mixed) {
+        // the large update on the tensor cores (3xTF32, FP32-accurate)
+        MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(A + t0 + t0 * lda), lda,
+                                reinterpret_cast<const float2 *>(A + t0 + J0 * lda), lda,
+                                reinterpret_cast<const float2 *>(A + J0 + t0 * lda), lda, (int)(n - t0), (int)nc,
+                                (int)NBc, w.tcw, c->dinfo + 2));
+      } else {
+        MOM_TRY(gemm(n - t0, nc, NBc, -1.0, A + t0 + J0 * lda, lda, A + J0 + t0 * lda, lda, 1.0, A + t0 + t0 * lda,
+                     lda));
+      }
     }
   }
   MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
@@ -691,10 +804,11 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
   compose_pivots_kernel<<<1, 256, sizeof(int) * n, c->stream>>>(c->ipiv, (int)n, c->perm);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
-  int hinfo[2] = {0, 0};
-  MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 2, cudaMemcpyDeviceToHost, c->stream));
+  int hinfo[3] = {0, 0, 0};
+  MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (hinfo[1]) return fail(c, MOM_ERR_TIMEOUT, "panel factorisation barrier timed out");
+  if (hinfo[2]) return fail(c, MOM_ERR_TIMEOUT, "tensor-core GEMM wait timed out");
   if (hinfo[0]) {
     c->factored = -1;
     return fail(c, MOM_ERR_SINGULAR, "Matrix factorization failed! (zero pivot at column " + std::to_string(hinfo[0]) + ")");
@@ -727,16 +841,20 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
     ta.perm = c->perm;
     ta.X = X + (size_t)s0 * n;
     ta.Y = Y + (size_t)s0 * n;
-    ta.bar = reinterpret_cast<unsigned *>(c->dinfo + 4);
+    ta.bar = c->flags;
     ta.timeout = c->dinfo + 1;
-    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned), c->stream));
+    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned) * 256, c->stream));
     void *args[] = {&ta};
     void *fn = ns == 1 ? (void *)trsv_coop_kernel<T, 1>
                : ns == 2 ? (void *)trsv_coop_kernel<T, 2>
                : ns == 4 ? (void *)trsv_coop_kernel<T, 4>
                          : (void *)trsv_coop_kernel<T, 8>;
-    const size_t tile = sizeof(T) * (size_t)nb * rpc;
-    if (tile > 200 * 1024) return fail(c, MOM_ERR_ARG, "triangular-solve tile does not fit in shared memory");
+    size_t tile = ((sizeof(T) * (size_t)nb * rpc + 15) / 16) * 16 + sizeof(double2) * nb * nb;
+    ta.direct = 0;
+    if (tile > 200 * 1024) {
+      ta.direct = 1;
+      tile = sizeof(double2) * nb * nb;
+    }
     MOM_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile));
     MOM_CUDA(c, cudaLaunchCooperativeKernel(fn, dim3(P), dim3(256), args, tile, c->stream));
     c->launches++;

@@ -79,7 +79,8 @@ struct Ctx {
   int *perm = nullptr;     // [n] composed row permutation of the factorisation
   double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
   size_t invd_bytes = 0;
-  int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout, [2..] barrier counters
+  int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout
+  unsigned *flags = nullptr;  // [256] per-CTA barrier epochs of the cooperative solve kernel
   void *ws = nullptr;      // general device workspace
   size_t ws_bytes = 0;
   int assembled = 0;       // 0 none, 1 FP64 matrix present
@@ -99,8 +100,8 @@ struct Ctx {
 
   // Optional per-category kernel timers (CUDA events on the context stream).
   bool prof = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[8];
-  int64_t prof_launch[8] = {0};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[12];
+  int64_t prof_launch[12] = {0};
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)
 
   // Host-side staging (pinned)
@@ -109,7 +110,10 @@ struct Ctx {
 };
 
 // Kernel categories for the optional timers.
-enum ProfCat { kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost };
+enum ProfCat {
+  kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost, kProfPivotAux,
+  kProfCount
+};
 
 // Records start/end events around a launch when profiling is on.
 struct ProfScope {
@@ -150,6 +154,11 @@ int assemble(Ctx *c, double omega, const double *ri, int precision);
 // lu.cu
 int lu_factor(Ctx *c, int precision);
 int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
+
+// tc_gemm.cu: C -= L U (complex FP32) on the tensor cores, 3xTF32
+int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
+                    int nc, int k, float *work, int *err);
+size_t tc_cgemm_work_bytes(int m, int nc, int k);
 
 // post.cu
 int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src);

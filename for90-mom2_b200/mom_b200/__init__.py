@@ -42,7 +42,7 @@ EXPORTS = [
     "mom_gpu_sysmat", "mom_gpu_srcvec", "mom_gpu_solve", "mom_gpu_solve_wavelength", "mom_gpu_cross_sections",
     "mom_gpu_rcs", "mom_gpu_cross_sections_noalloc", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
     "mom_gpu_launch_count", "mom_gpu_stream", "mom_gpu_library_calls", "mom_gpu_profile", "mom_gpu_profile_read",
-    "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
+    "mom_gpu_selftest_cgemm", "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
 ]
@@ -108,6 +108,8 @@ def lib():
     L.mom_gpu_library_calls.restype = C.c_int64
     L.mom_gpu_profile.argtypes = [vp, C.c_int32]
     L.mom_gpu_profile_read.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    fp = C.POINTER(C.c_float)
+    L.mom_gpu_selftest_cgemm.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, fp, fp, fp]
     L.mom_problem_create.argtypes = [C.POINTER(vp)]
     L.mom_problem_destroy.argtypes = [vp]
     L.mom_problem_destroy.restype = None
@@ -340,6 +342,18 @@ class Solver:
                                                       _dp(csca), _dp(cabs)), "cross_sections_noalloc")
         return csca, cabs
 
+    def selftest_cgemm(self, L, U, Cmat):
+        """Cmat - L U (complex64) computed by the library's tensor-core LU-update kernel."""
+        L = np.asfortranarray(L, dtype=np.complex64)
+        U = np.asfortranarray(U, dtype=np.complex64)
+        Cc = np.asfortranarray(Cmat, dtype=np.complex64).copy(order="F")
+        m, k = L.shape
+        nc = U.shape[1]
+        fp = C.POINTER(C.c_float)
+        self._ck(lib().mom_gpu_selftest_cgemm(self.h, m, nc, k, L.ctypes.data_as(fp), U.ctypes.data_as(fp),
+                                              Cc.ctypes.data_as(fp)), "selftest_cgemm")
+        return Cc
+
     def device_solution(self):
         """(device pointer, leading dimension, number of sources) of the solutions."""
         p = C.c_void_p()
@@ -376,7 +390,7 @@ class Solver:
         """cuBLAS GEMM calls since creation."""
         return lib().mom_gpu_library_calls(self.h)
 
-    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post")
+    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux")
 
     def profile(self, enable=True):
         """Turn the per-category kernel timers on (and reset them) or off."""

@@ -143,6 +143,11 @@ int mom_gpu_cross_sections_noalloc(mom_ctx *ctx, int32_t dom, double omega, cons
                                    const mom_src *src, const void *x_dev, int64_t ldx, double *csca,
                                    double *cabs);
 
+/* Diagnostics: C -= L U for host complex64 arrays (column-major; L m x k,
+ * U k x nc, C m x nc; m a multiple of 64, k of 16) through the tensor-core
+ * kernel that performs the trailing updates of the mixed-precision LU. */
+int mom_gpu_selftest_cgemm(mom_ctx *ctx, int32_t m, int32_t nc, int32_t k, const float *L, const float *U, float *C);
+
 /* Device views for callers that keep data resident (bench, tests). */
 int mom_gpu_device_matrix(mom_ctx *ctx, void **A_dev, int64_t *lda);
 int mom_gpu_device_solution(mom_ctx *ctx, void **x_dev, int64_t *ldx, int32_t *nsrc);
@@ -157,7 +162,8 @@ int64_t mom_gpu_library_calls(mom_ctx *ctx);
 /* Optional kernel timers: enable (1) / disable (0) and reset; then read the
  * summed device time and launch count of a category: 0 pair (far-pair
  * assembly), 1 near pairs, 2 gather, 3 LU panel, 4 LU GEMMs, 5 triangular
- * solves, 6 refinement residual, 7 post-processing. */
+ * solves, 6 refinement residual, 7 post-processing, 8 row interchanges and
+ * diagonal-block inverses of the LU. */
 int mom_gpu_profile(mom_ctx *ctx, int32_t enable);
 int mom_gpu_profile_read(mom_ctx *ctx, int32_t category, double *ms_total, int64_t *launches);
 
