@@ -154,6 +154,22 @@ def cpu_sample(subdiv, threads, budget_s=20.0):
     return dict(total_s=total, phases_s=dict(assembly=t_asm, rhs=t_rhs, lu=t_lu, getrs=t_rs), sample=sample)
 
 
+def reduce_max(x, world, device):
+    """Max of a per-rank scalar over the process group (step times are taken as the max over ranks)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ms_per_step_max, world):
+    """Whole-job solves/s of N independent replicas: every rank completes one solve per step."""
+    return world * 1000.0 / ms_per_step_max
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -213,17 +229,13 @@ def run_ours(args, rank, local_rank, world):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, "cuda")
 
     def timed(prec, steps, warm):
         for _ in range(warm):
             step(prec)
         barrier()
-        l0, b0 = S.launch_count, S.library_calls
+        l0, b0, f0 = S.launch_count, S.library_calls, S.tensor_flops
         S.profile(True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -238,19 +250,19 @@ def run_ours(args, rank, local_rank, world):
         S.profile(False)
         barrier()
         ms = e0.elapsed_time(e1) / steps
-        return max_over_ranks(ms), prof, S.launch_count - l0, S.library_calls - b0, iters
+        return max_over_ranks(ms), prof, S.launch_count - l0, S.library_calls - b0, iters, S.tensor_flops - f0
 
     # ---- mixed precision (the headline) ----
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ms_mixed, prof, launches, libcalls, iters = timed(M.MIXED, args.steps, args.warmup)
+    ms_mixed, prof, launches, libcalls, iters, tc_flops = timed(M.MIXED, args.steps, args.warmup)
     clocks = sampler.stop()
     csca, cabs = S.cross_sections(om, ri[0], src)
     ext_mixed = float(csca[0] + cabs[0])
     # ---- FP64 path, same workload ----
     ms_fp64, prof64, ext_fp64, sig_err = None, {}, None, None
     if args.fp64_steps > 0:
-        ms_fp64, prof64, _, _, _ = timed(M.FP64, args.fp64_steps, 1)
+        ms_fp64, prof64, _, _, _, _ = timed(M.FP64, args.fp64_steps, 1)
         csca64, cabs64 = S.cross_sections(om, ri[0], src)
         ext_fp64 = float(csca64[0] + cabs64[0])
         sig_err = abs(ext_mixed - ext_fp64) / abs(ext_fp64)
@@ -272,45 +284,56 @@ def run_ours(args, rank, local_rank, world):
     h2d = 48 * len(src) + 16 * len(ri)  # mom_src structs + refractive indices
     d2h = 16 * 2 * S.N * len(src) + 16 * len(src)  # solution + (csca, cabs)
 
-    # ---- roofline of the dominant kernel category (timed live above) ----
+    # ---- rooflines of the timed kernels (device time from events around each launch) ----
     hbm_gbs, bf16_tf, peak_src = load_peaks()
-    cat, (cat_ms, cat_n) = max(prof.items(), key=lambda kv: kv[1][0])
     F = len(faces)
     n = 2 * S.N
-    roof = None
-    if cat == "pair":
-        # 17,914 FLOP per face pair (169 point pairs x 88 + 3042 contraction); one launch = F^2 pairs of a domain
-        flop = 17914.0 * F * F
-        ach = flop / (cat_ms / cat_n * 1e-3) / 1e12
-        roof = {"kernel": "pair_kernel<float,13> (far-pair assembly, FP32 pipe)", "bound": "fp32", "achieved": ach,
-                "unit": "TFLOP/s", "traffic": None}
-    elif cat == "gemm":
-        # trailing updates + TRSM products: 8 real FLOP per complex MAC
-        nb = 64
-        flop = sum(8.0 * (n - (k + 1) * nb) ** 2 * nb + 8.0 * nb * nb * (n - (k + 1) * nb) for k in range(n // nb))
-        ach = flop / (cat_ms * 1e-3) / 1e12 / args.steps
-        roof = {"kernel": "LU trailing CGEMM (TF32 tensor cores)", "bound": "tensor", "achieved": ach,
-                "unit": "TFLOP/s", "peak": bf16_tf / 2.0, "frac": ach / (bf16_tf / 2.0), "traffic": None,
-                "peak_note": "TF32 dense = half of the %s bf16 peak" % peak_src}
-    elif cat in ("trsv", "residual"):
-        bytes_ = (8.0 if cat == "trsv" else 16.0) * n * n
-        ach = bytes_ / (cat_ms / cat_n * 1e-3) / 1e9
-        roof = {"kernel": cat, "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": hbm_gbs,
-                "frac": ach / hbm_gbs, "traffic": None, "peak_note": peak_src}
-    if roof is None:
-        roof = {"kernel": cat, "bound": "n/a", "achieved": None, "unit": None, "peak": None, "frac": None,
-                "traffic": None}
-    if roof.get("bound") == "fp32":
-        # FP32 non-tensor peak: 148 SMs x 128 FP32 lanes x 2 FLOP x SM clock (no measured figure exists)
-        sm_mhz = clocks.get("sm_mhz") or 1965.0
+    nb = 64
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    roofs = {}
+    ms, cnt = prof["tc_gemm"]
+    if cnt:
+        ach = tc_flops / (ms * 1e-3) / 1e12
+        roofs["tc_gemm"] = {"kernel": "tc_gemm_kernel (tcgen05 kind::tf32, 3 passes, LU trailing update)",
+                            "bound": "tensor", "achieved": ach, "unit": "TFLOP/s", "peak": bf16_tf / 2.0,
+                            "frac": ach / (bf16_tf / 2.0), "traffic": None,
+                            "peak_note": "dense TF32 = half of the %s bf16 burst peak; FLOP = 3 passes executed" % peak_src}
+    ms, cnt = prof["panel"]
+    if cnt:
+        bytes_ = sum(2.0 * 8 * (n - k * nb) * nb for k in range(n // nb)) * args.steps  # FP32 panel read + write
+        ach = bytes_ / (ms * 1e-3) / 1e9
+        roofs["panel"] = {"kernel": "panel_kernel<float2> (pivoted panel, grid barrier per column)", "bound": "hbm",
+                          "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs, "traffic": None,
+                          "peak_note": "%s; latency-bound: one device-wide pivot exchange per column" % peak_src}
+    ms, cnt = prof["pair"]
+    if cnt:
+        flop = 17914.0 * F * F * cnt  # 17,914 FLOP per face pair, F^2 pairs per launch (one domain)
+        ach = flop / (ms * 1e-3) / 1e12
         peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
-        roof.update(peak=peak, frac=roof["achieved"] / peak,
-                    peak_note="nominal FP32 SIMT at the sampled median SM clock (%.0f MHz)" % sm_mhz)
+        roofs["pair"] = {"kernel": "pair_kernel<float,13> (far-pair assembly, FP32 pipe)", "bound": "fp32",
+                         "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak, "traffic": None,
+                         "peak_note": "nominal FP32 SIMT at the sampled SM clock %.0f MHz" % sm_mhz}
+    ms, cnt = prof["trsv"]
+    if cnt:
+        bytes_ = 8.0 * n * n * cnt  # FP32 L and U factors read once per solve
+        ach = bytes_ / (ms * 1e-3) / 1e9
+        roofs["trsv"] = {"kernel": "trsv_coop_kernel<float2> (forward+backward substitution)", "bound": "hbm",
+                         "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs, "traffic": None,
+                         "peak_note": peak_src}
+    ms, cnt = prof["residual"]
+    if cnt:
+        bytes_ = 16.0 * n * n * cnt  # FP64 matrix read once per residual
+        ach = bytes_ / (ms * 1e-3) / 1e9
+        roofs["residual"] = {"kernel": "gemv_partial_kernel (FP64 refinement residual)", "bound": "hbm",
+                             "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs,
+                             "traffic": None, "peak_note": peak_src}
+    top = max(roofs, key=lambda k: prof[k][0])  # the kernel with the most device time per step
+    roof = dict(roofs[top])
 
     phases = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps} for k, v in prof.items()}
     phases64 = {k: {"ms_per_step": v[0] / args.fp64_steps} for k, v in prof64.items()}
 
-    value = world * 1000.0 / ms_mixed
+    value = replica_value(ms_mixed, world)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32/tf32 far pairs + LU, fp64 near pairs + refinement (complex)",
@@ -326,9 +349,10 @@ def run_ours(args, rank, local_rank, world):
             "clocks": clocks,
             "e2e": ({"value": world * 1000.0 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                      "d2h_bytes_per_step": d2h} if e2e_ms else None),
-            "gpu_launches": int(launches / args.steps * args.steps),
+            "gpu_launches": int(launches),
             "library_gemm_calls": libcalls,
-            "roofline": roof}
+            "roofline": roof,
+            "rooflines": roofs}
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
         info = cpu_sample(args.subdiv, cores)

@@ -538,6 +538,8 @@ void *mom_gpu_stream(mom_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 int64_t mom_gpu_library_calls(mom_ctx *c) { return c ? c->blas_calls : 0; }
 
+double mom_gpu_tensor_flops(mom_ctx *c) { return c ? c->tc_flops : 0.0; }
+
 int mom_gpu_profile(mom_ctx *c, int32_t enable) {
   if (!c) return MOM_ERR_ARG;
   std::lock_guard<std::mutex> g(c->mu);

@@ -743,9 +743,9 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
       pa.cand_data = w.cand_data;
       pa.col_data = w.col_data;
       {
-        ProfScope ps(c, kProfPanel);
         MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned) * 256, c->stream));
         MOM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ProfScope ps(c, kProfPanel);
         void *args[] = {&pa};
         MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
                                                 c->stream));

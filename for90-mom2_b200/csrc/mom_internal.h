@@ -103,6 +103,7 @@ struct Ctx {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[12];
   int64_t prof_launch[12] = {0};
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)
+  double tc_flops = 0;     // FLOP executed by the tensor-core LU updates since creation
 
   // Host-side staging (pinned)
   double *pinned = nullptr;
@@ -112,6 +113,7 @@ struct Ctx {
 // Kernel categories for the optional timers.
 enum ProfCat {
   kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost, kProfPivotAux,
+  kProfTc,
   kProfCount
 };
 

@@ -372,8 +372,12 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   const int grid = ntiles < c->nsm ? ntiles : c->nsm;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;
   MOM_CUDA(c, cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  tc_gemm_kernel<<<grid, kTcThreads, smem, c->stream>>>(mAhi, mAlo, mBhi, mBlo, ta);
+  {
+    ProfScope ps(c, kProfTc);
+    tc_gemm_kernel<<<grid, kTcThreads, smem, c->stream>>>(mAhi, mAlo, mBhi, mBlo, ta);
+  }
   c->launches++;
+  c->tc_flops += 6.0 * Mr * (double)nc * Kr;  // three TF32 passes, 2 FLOP per real MAC
   MOM_CUDA(c, cudaGetLastError());
   return MOM_OK;
 }

@@ -41,7 +41,7 @@ EXPORTS = [
     "mom_gpu_create", "mom_gpu_destroy", "mom_gpu_strerror", "mom_gpu_last_error", "mom_gpu_set_problem",
     "mom_gpu_sysmat", "mom_gpu_srcvec", "mom_gpu_solve", "mom_gpu_solve_wavelength", "mom_gpu_cross_sections",
     "mom_gpu_rcs", "mom_gpu_cross_sections_noalloc", "mom_gpu_device_matrix", "mom_gpu_device_solution", "mom_gpu_synchronize",
-    "mom_gpu_launch_count", "mom_gpu_stream", "mom_gpu_library_calls", "mom_gpu_profile", "mom_gpu_profile_read",
+    "mom_gpu_launch_count", "mom_gpu_stream", "mom_gpu_library_calls", "mom_gpu_tensor_flops", "mom_gpu_profile", "mom_gpu_profile_read",
     "mom_gpu_selftest_cgemm", "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
@@ -106,6 +106,8 @@ def lib():
     L.mom_gpu_stream.restype = C.c_void_p
     L.mom_gpu_library_calls.argtypes = [vp]
     L.mom_gpu_library_calls.restype = C.c_int64
+    L.mom_gpu_tensor_flops.argtypes = [vp]
+    L.mom_gpu_tensor_flops.restype = C.c_double
     L.mom_gpu_profile.argtypes = [vp, C.c_int32]
     L.mom_gpu_profile_read.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     fp = C.POINTER(C.c_float)
@@ -390,7 +392,12 @@ class Solver:
         """cuBLAS GEMM calls since creation."""
         return lib().mom_gpu_library_calls(self.h)
 
-    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux")
+    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux", "tc_gemm")
+
+    @property
+    def tensor_flops(self):
+        """FLOP executed by the tensor-core LU update kernel since creation."""
+        return lib().mom_gpu_tensor_flops(self.h)
 
     def profile(self, enable=True):
         """Turn the per-category kernel timers on (and reset them) or off."""
