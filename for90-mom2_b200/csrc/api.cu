@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -29,14 +30,34 @@ ProfScope::ProfScope(Ctx *c_, int cat_) : c(c_), cat(cat_) {
     a = b = nullptr;
     return;
   }
-  cudaEventRecord(a, c->stream);
+  // Inside a capture the records become event nodes of the graph.
+  if (c->capturing) cudaEventRecordWithFlags(a, c->stream, cudaEventRecordExternal);
+  else cudaEventRecord(a, c->stream);
 }
 
 ProfScope::~ProfScope() {
   if (!a) return;
+  if (c->capturing) {
+    cudaEventRecordWithFlags(b, c->stream, cudaEventRecordExternal);
+    c->cap_ev.emplace_back(cat, a, b);
+    return;
+  }
   cudaEventRecord(b, c->stream);
   c->prof_ev[cat].push_back({a, b});
   c->prof_launch[cat]++;
+}
+
+void Ctx::LuGraph::reset() {
+  if (exec) cudaGraphExecDestroy(exec);
+  exec = nullptr;
+  for (auto &e : ev) {
+    cudaEventDestroy(std::get<1>(e));
+    cudaEventDestroy(std::get<2>(e));
+  }
+  ev.clear();
+  key.clear();
+  launches = blas_calls = 0;
+  tc_flops = 0;
 }
 
 int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes) {
@@ -321,6 +342,19 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
     delete c;
     return MOM_ERR_CUDA;
   }
+  // A fixed cuBLAS workspace (no allocation inside the captured LU graph).
+  if (cudaMalloc(&c->blas_ws, kBlasWorkspace) != cudaSuccess ||
+      cublasSetWorkspace(c->blas, c->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS || lu_init_kernels(c) != MOM_OK ||
+      tc_init_kernels(c) != MOM_OK) {
+    cudaGetLastError();
+    cublasDestroy(c->blas);
+    cudaFree(c->blas_ws);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return MOM_ERR_CUDA;
+  }
+  const char *eg = std::getenv("MOM_LU_GRAPH");
+  c->use_graph = !(eg && eg[0] == '0');
   *out = c;
   return MOM_OK;
 }
@@ -335,7 +369,9 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->dinfo);
   cudaFree(c->flags);
   if (c->pinned) cudaFreeHost(c->pinned);
+  for (auto &g : c->lu_graph) g.reset();
   cublasDestroy(c->blas);
+  cudaFree(c->blas_ws);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -552,6 +588,7 @@ int mom_gpu_profile(mom_ctx *c, int32_t enable) {
     v.clear();
   }
   for (auto &n : c->prof_launch) n = 0;
+  for (auto &t : c->prof_ms) t = 0;
   c->prof = enable != 0;
   return MOM_OK;
 }
@@ -565,7 +602,7 @@ int mom_gpu_profile_read(mom_ctx *c, int32_t category, double *ms_total, int64_t
     float ms = 0;
     if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) t += ms;
   }
-  *ms_total = t;
+  *ms_total = t + c->prof_ms[category];
   *launches = c->prof_launch[category];
   return MOM_OK;
 }

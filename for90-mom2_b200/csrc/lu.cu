@@ -256,34 +256,69 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
 // The nb row interchanges of a panel (ipiv[j0 .. j0+nb), applied in order)
 // composed into one permutation of the at most 2 nb rows they touch:
 // after the swaps, row dst[i] holds the old row src[i], i < *count.
+// One warp: rows inside the panel are tracked in a direct array, rows below
+// it (at most nb distinct) in a list searched by the whole warp at once, so
+// each interchange costs a few warp-wide steps.  Requires nb <= 64.
 __global__ void pivot_map_kernel(const int *ipiv, int64_t j0, int nb, int *dst, int *src, int *count) {
-  __shared__ int rows[128], orig[128];
-  __shared__ int cnt;
-  if (threadIdx.x != 0) return;
-  cnt = 0;
-  auto slot = [&](int r) {
-    for (int i = 0; i < cnt; i++)
-      if (rows[i] == r) return i;
-    rows[cnt] = r;
-    orig[cnt] = r;
-    return cnt++;
-  };
-  for (int c = 0; c < nb; c++) {
-    const int a = (int)(j0 + c), b = ipiv[j0 + c];
-    if (a == b) continue;
-    const int ia = slot(a), ib = slot(b);
-    const int t = orig[ia];
-    orig[ia] = orig[ib];
-    orig[ib] = t;
+  __shared__ int piv[64], in_orig[64], out_row[64], out_orig[64];
+  const int lane = threadIdx.x;
+  for (int i = lane; i < nb; i += 32) {
+    piv[i] = ipiv[j0 + i];
+    in_orig[i] = (int)j0 + i;
   }
-  int k = 0;
-  for (int i = 0; i < cnt; i++)
-    if (orig[i] != rows[i]) {
-      dst[k] = rows[i];
-      src[k] = orig[i];
-      k++;
+  __syncwarp();
+  int nout = 0;  // warp-uniform
+  for (int c = 0; c < nb; c++) {
+    const int b = piv[c];
+    const int a = (int)j0 + c;
+    if (b == a) continue;
+    int *slot;
+    if (b < j0 + nb) {
+      slot = &in_orig[b - j0];
+    } else {
+      const unsigned m0 = __ballot_sync(0xffffffffu, lane < nout && out_row[lane] == b);
+      const unsigned m1 = __ballot_sync(0xffffffffu, lane + 32 < nout && out_row[lane + 32] == b);
+      int s;
+      if (m0) s = __ffs(m0) - 1;
+      else if (m1) s = 32 + __ffs(m1) - 1;
+      else {
+        s = nout++;
+        if (lane == 0) {
+          out_row[s] = b;
+          out_orig[s] = b;
+        }
+      }
+      slot = &out_orig[s];
     }
-  *count = k;
+    if (lane == 0) {
+      const int t = in_orig[c];
+      in_orig[c] = *slot;
+      *slot = t;
+    }
+    __syncwarp();
+  }
+  // compact the rows whose content changed: inside rows first, then the list
+  int k = 0;
+  for (int base = 0; base < nb + nout; base += 32) {
+    const int i = base + lane;
+    int r = -1, o = -1;
+    if (i < nb) {
+      r = (int)j0 + i;
+      o = in_orig[i];
+    } else if (i < nb + nout) {
+      r = out_row[i - nb];
+      o = out_orig[i - nb];
+    }
+    const bool moved = r >= 0 && o != r;
+    const unsigned m = __ballot_sync(0xffffffffu, moved);
+    if (moved) {
+      const int at = k + __popc(m & ((1u << lane) - 1u));
+      dst[at] = r;
+      src[at] = o;
+    }
+    k += __popc(m);
+  }
+  if (lane == 0) *count = k;
 }
 
 // Apply the composed panel permutation to every column outside the panel:
@@ -311,68 +346,134 @@ __global__ void laswp_kernel(T *A, int64_t lda, int64_t n, int64_t j0, int nb, c
   }
 }
 
-// Inverses of the unit-lower L11 and upper U11 diagonal blocks of the panel
+// Inverses of the unit-lower L11 and upper U11 diagonal blocks of a panel
 // (FP64), stored as inv[0] = inv(L11), inv[1] = inv(U11), column-major
-// nb x nb.  One CTA; thread j < nb builds column j of inv(L11) and thread
-// nb + j column j of inv(U11), entirely in shared memory.
+// 64 x 64.  One CTA of 512 threads (256 per triangle), all in shared memory,
+// by recursive doubling: the sixteen 8 x 8 diagonal blocks are inverted by
+// substitution, then neighbouring inverses are joined for block sizes 8, 16
+// and 32,
+//   inv([L11 0; L21 L22]) = [X11 0; -X22 L21 X11, X22],
+//   inv([U11 U12; 0 U22]) = [Y11, -Y11 U12 Y22; 0 Y22],
+// each join as two small triangular-times-dense products.  The dependent
+// chain is 8 substitution steps and six products instead of 64 substitution
+// steps.  Product temporaries sit in the half of each inverse that is zero
+// (above the diagonal of inv(L), below it for inv(U)); the triangular k
+// ranges below never read those halves, and the final store masks them.
+constexpr int kDiagNb = 64;
+constexpr int kDiagThreads = 512;
+
+__device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+
+// For the 32 / B joins of one triangle (join p works on rows and columns
+// from o = 2 B p): C(o+cr.., o+cc..) = s * A(o+ar.., o+ac..) * B(o+br.., o+bc..),
+// B x B blocks of 64 x 64 column-major shared arrays, with k restricted to
+// the non-zero part of the triangular factor: MODE 0 k >= col, 1 k <= row,
+// 2 k <= col, 3 k >= row.  Thread u < 256 makes B / 8 outputs.
+template <int B, int MODE>
+__device__ __forceinline__ void join_product(int u, double s, const double2 *Am, int ar, int ac, const double2 *Bm,
+                                             int br, int bc, double2 *Cm, int cr, int cc) {
+#pragma unroll
+  for (int i = 0; i < B / 8; i++) {
+    const int e = u + 256 * i;
+    const int p = e / (B * B), rem = e % (B * B);
+    const int col = rem / B, row = rem % B;
+    const int o = 2 * B * p;
+    const double2 *a = Am + (o + ar + row) + (o + ac) * kDiagNb;
+    const double2 *b = Bm + (o + br) + (o + bc + col) * kDiagNb;
+    const int k0 = MODE == 0 ? col : (MODE == 3 ? row : 0);
+    const int k1 = MODE == 1 ? row + 1 : (MODE == 2 ? col + 1 : B);
+    double2 acc = make_double2(0, 0);
+    for (int k = k0; k < k1; k++) cfma(acc, a[k * kDiagNb], b[k]);
+    Cm[(o + cr + row) + (o + cc + col) * kDiagNb] = make_double2(s * acc.x, s * acc.y);
+  }
+}
+
+// L: T = L21 X11 into the upper slot, then X21 = -X22 T;
+// U: T = U12 Y22 into the lower slot, then Y12 = -Y11 T.
+template <int B>
+__device__ __forceinline__ void join_level(int t, const double2 *D, double2 *XL, double2 *XU) {
+  if (t < 256) join_product<B, 0>(t, 1.0, D, B, 0, XL, 0, 0, XL, 0, B);
+  else join_product<B, 2>(t - 256, 1.0, D, 0, B, XU, B, B, XU, B, 0);
+  __syncthreads();
+  if (t < 256) join_product<B, 1>(t, -1.0, XL, B, B, XL, 0, B, XL, B, 0);
+  else join_product<B, 3>(t - 256, -1.0, XU, 0, 0, XU, B, 0, XU, 0, B);
+  __syncthreads();
+}
+
 template <typename T>
-__global__ void diag_inv_kernel(const T *A, int64_t lda, int64_t j0, int nb, double2 *invL, double2 *invU,
-                                float2 *invL32) {
+__global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int64_t lda, int64_t j0, double2 *invL,
+                                                                double2 *invU, float2 *invL32) {
   extern __shared__ double2 sm[];
-  double2 *D = sm, *XL = sm + nb * nb, *XU = sm + 2 * nb * nb;
-  // eight independent loads in flight per thread before the shared stores
-  for (int base = threadIdx.x; base < nb * nb; base += 8 * blockDim.x) {
-    double2 v[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int idx = base + u * blockDim.x;
-      if (idx < nb * nb) v[u] = ld2(A + (j0 + idx % nb) + (j0 + idx / nb) * lda);
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int idx = base + u * blockDim.x;
-      if (idx < nb * nb) D[idx] = v[u];
-    }
-  }
-  __syncthreads();
-  // XL / XU are stored transposed ([k][j], thread j contiguous) so the
-  // threads of a warp hit distinct banks.
+  constexpr int nb = kDiagNb, nn = kDiagNb * kDiagNb;
+  double2 *D = sm, *XL = sm + nn, *XU = sm + 2 * nn, *rinv = sm + 3 * nn;
   const int t = threadIdx.x;
-  if (t < nb) {
-    const int j = t;  // unit lower: x_i = -sum_{k=j}^{i-1} L_ik x_k
-    for (int i = 0; i < nb; i++) {
-      double2 v = make_double2(i == j ? 1.0 : 0.0, 0.0);
-      // k runs over the same values in every thread (D[i + k nb] is then a
-      // broadcast); entries with k < j are zero by construction of XL.
-      for (int k = 0; k < i; k++) {
-        const double2 l = D[i + k * nb], x = XL[j + k * nb];
-        v.x -= l.x * x.x - l.y * x.y;
-        v.y -= l.x * x.y + l.y * x.x;
-      }
-      XL[j + i * nb] = v;
+  // eight independent loads in flight per thread before the shared stores
+  {
+    double2 v[nn / kDiagThreads];
+#pragma unroll
+    for (int u = 0; u < nn / kDiagThreads; u++) {
+      const int idx = t + u * kDiagThreads;
+      v[u] = ld2(A + (j0 + idx % nb) + (j0 + idx / nb) * lda);
     }
-  } else if (t < 2 * nb) {
-    const int j = t - nb;  // upper: x_i = (delta_ij - sum_{k=i+1}^{j} U_ik x_k) / U_ii
-    for (int i = nb - 1; i >= 0; i--) {
-      double2 v = make_double2(0, 0);
-      if (i <= j) {
-        v = make_double2(i == j ? 1.0 : 0.0, 0.0);
-        for (int k = i + 1; k <= j; k++) {
-          const double2 u = D[i + k * nb], x = XU[j + k * nb];
-          v.x -= u.x * x.x - u.y * x.y;
-          v.y -= u.x * x.y + u.y * x.x;
-        }
-        const double2 d = D[i + i * nb];
-        const double dd = d.x * d.x + d.y * d.y;
-        v = (dd != 0.0) ? make_double2((v.x * d.x + v.y * d.y) / dd, (v.y * d.x - v.x * d.y) / dd) : make_double2(0, 0);
-      }
-      XU[j + i * nb] = v;
-    }
+#pragma unroll
+    for (int u = 0; u < nn / kDiagThreads; u++) D[t + u * kDiagThreads] = v[u];
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int r = idx % nb, c = idx / nb;  // inv(r, c) is held at X[c + r * nb]
-    const double2 l = XL[c + r * nb], u = XU[c + r * nb];
+  if (t < nb) {  // 1 / U_ii (0 for a zero pivot; the panel reports it)
+    const double2 d = D[t + t * nb];
+    const double dd = d.x * d.x + d.y * d.y;
+    rinv[t] = dd != 0.0 ? make_double2(d.x / dd, -d.y / dd) : make_double2(0, 0);
+  }
+  __syncthreads();
+  // the 8 x 8 diagonal blocks: thread (block q, column c) by substitution
+  if (t < 64) {
+    const int q = t >> 3, c = t & 7, o = 8 * q;
+    double2 x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      double2 v = make_double2(i == c ? 1.0 : 0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < i; k++)
+        if (k >= c) {
+          const double2 l = D[(o + i) + (o + k) * nb];
+          v.x -= l.x * x[k].x - l.y * x[k].y;
+          v.y -= l.x * x[k].y + l.y * x[k].x;
+        }
+      x[i] = i >= c ? v : make_double2(0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) XL[(o + i) + (o + c) * nb] = x[i];
+  } else if (t >= 256 && t < 256 + 64) {
+    const int q = (t - 256) >> 3, c = t & 7, o = 8 * q;
+    double2 y[8];
+#pragma unroll
+    for (int i = 7; i >= 0; i--) {
+      double2 v = make_double2(i == c ? 1.0 : 0.0, 0.0);
+#pragma unroll
+      for (int k = i + 1; k < 8; k++)
+        if (k <= c) {
+          const double2 u = D[(o + i) + (o + k) * nb];
+          v.x -= u.x * y[k].x - u.y * y[k].y;
+          v.y -= u.x * y[k].y + u.y * y[k].x;
+        }
+      y[i] = i <= c ? cmul(v, rinv[o + i]) : make_double2(0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) XU[(o + i) + (o + c) * nb] = y[i];
+  }
+  __syncthreads();
+  join_level<8>(t, D, XL, XU);
+  join_level<16>(t, D, XL, XU);
+  join_level<32>(t, D, XL, XU);
+  for (int idx = t; idx < nn; idx += kDiagThreads) {
+    const int r = idx % nb, c = idx / nb;
+    const double2 l = r > c ? XL[idx] : make_double2(r == c ? 1.0 : 0.0, 0.0);
+    const double2 u = r <= c ? XU[idx] : make_double2(0, 0);
     invL[idx] = l;
     invU[idx] = u;
     if (invL32) invL32[idx] = make_float2((float)l.x, (float)l.y);
@@ -675,13 +776,12 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   return MOM_OK;
 }
 
+// Issues every launch of the factorisation on the context stream (eagerly,
+// or into an open capture).
 template <typename T>
-int lu_factor_t(Ctx *c, T *A, int precision) {
+int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
   const int64_t n = c->n, lda = c->lda;
   const int nb = c->nb;
-  if (n % nb != 0) return fail(c, MOM_ERR_ARG, "matrix order must be a multiple of the panel width");
-  LuWork w;
-  MOM_TRY(lu_workspace(c, precision, w));
   MOM_CUDA(c, cudaMemsetAsync(c->dinfo, 0, sizeof(int) * 4, c->stream));
   const bool mixed = precision == MOM_PREC_MIXED;
   // The small GEMMs (block TRSM, updates inside an outer block) stay in full FP32 / FP64.
@@ -744,7 +844,6 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
       pa.col_data = w.col_data;
       {
         MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned) * 256, c->stream));
-        MOM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         ProfScope ps(c, kProfPanel);
         void *args[] = {&pa};
         MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
@@ -759,11 +858,12 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                                                                           w.pmap + 128, w.pmap + 256);
           c->launches += 2;
         }
+      }
+      {
+        ProfScope pd(c, kProfDiagInv);
         double2 *invL = c->invd + (size_t)kb * 2 * nb * nb, *invU = invL + (size_t)nb * nb;
-        MOM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(double2) * 3 * nb * nb)));
-        diag_inv_kernel<T><<<1, 2 * nb, sizeof(double2) * 3 * nb * nb, c->stream>>>(
-            A, lda, j0, nb, invL, invU, mixed ? w.invL32 + (size_t)kb * nb * nb : nullptr);
+        diag_inv_kernel<T><<<1, kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), c->stream>>>(
+            A, lda, j0, invL, invU, mixed ? w.invL32 + (size_t)kb * nb * nb : nullptr);
         c->launches++;
         MOM_CUDA(c, cudaGetLastError());
       }
@@ -799,14 +899,84 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
     }
   }
   MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
-  MOM_CUDA(c, cudaFuncSetAttribute(compose_pivots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(int) * n)));
   compose_pivots_kernel<<<1, 256, sizeof(int) * n, c->stream>>>(c->ipiv, (int)n, c->perm);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+// Captures the factorisation of this precision into g (replacing what g held).
+template <typename T>
+int lu_capture(Ctx *c, T *A, int precision, const LuWork &w, Ctx::LuGraph &g, const std::vector<uintptr_t> &key) {
+  g.reset();
+  const int64_t l0 = c->launches, b0 = c->blas_calls;
+  const double f0 = c->tc_flops;
+  MOM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  c->capturing = true;
+  const int st = lu_enqueue<T>(c, A, precision, w);
+  c->capturing = false;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  g.ev.swap(c->cap_ev);
+  c->cap_ev.clear();
+  g.launches = c->launches - l0;
+  g.blas_calls = c->blas_calls - b0;
+  g.tc_flops = c->tc_flops - f0;
+  c->launches = l0;  // counted again on every replay
+  c->blas_calls = b0;
+  c->tc_flops = f0;
+  if (st != MOM_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    g.reset();
+    return st != MOM_OK ? st : cuda_fail(c, e, "cudaStreamEndCapture (LU factorisation)");
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    g.exec = nullptr;
+    g.reset();
+    return cuda_fail(c, ei, "cudaGraphInstantiate (LU factorisation)");
+  }
+  g.key = key;
+  return MOM_OK;
+}
+
+template <typename T>
+int lu_factor_t(Ctx *c, T *A, int precision) {
+  const int64_t n = c->n;
+  const int nb = c->nb;
+  if (n % nb != 0) return fail(c, MOM_ERR_ARG, "matrix order must be a multiple of the panel width");
+  if (nb != kDiagNb) return fail(c, MOM_ERR_ARG, "panel width must be 64");
+  LuWork w;
+  MOM_TRY(lu_workspace(c, precision, w));
+  Ctx::LuGraph *g = nullptr;
+  if (c->use_graph) {
+    // Everything the captured launches bake in: sizes, buffer addresses, the
+    // SM count (panel grid) and whether timing events are part of the graph.
+    const std::vector<uintptr_t> key = {(uintptr_t)n,         (uintptr_t)c->lda,   (uintptr_t)nb,
+                                        (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
+                                        (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
+                                        (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof};
+    g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
+    if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
+    MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
+    c->launches += g->launches;
+    c->blas_calls += g->blas_calls;
+    c->tc_flops += g->tc_flops;
+  } else {
+    MOM_TRY(lu_enqueue<T>(c, A, precision, w));
+  }
   int hinfo[3] = {0, 0, 0};
   MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (g && c->prof) {
+    for (auto &e : g->ev) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, std::get<1>(e), std::get<2>(e)) == cudaSuccess) c->prof_ms[std::get<0>(e)] += ms;
+      c->prof_launch[std::get<0>(e)]++;
+    }
+  }
   if (hinfo[1]) return fail(c, MOM_ERR_TIMEOUT, "panel factorisation barrier timed out");
   if (hinfo[2]) return fail(c, MOM_ERR_TIMEOUT, "tensor-core GEMM wait timed out");
   if (hinfo[0]) {
@@ -855,13 +1025,48 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
       ta.direct = 1;
       tile = sizeof(double2) * nb * nb;
     }
-    MOM_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile));
     MOM_CUDA(c, cudaLaunchCooperativeKernel(fn, dim3(P), dim3(256), args, tile, c->stream));
     c->launches++;
   }
   return MOM_OK;
 }
 
+
+// Opt a kernel in to all the dynamic shared memory the device allows next to
+// its static shared memory.
+template <typename T>
+cudaError_t set_smem(T *fn) {
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+}  // namespace
+
+// Shared-memory opt-in of the LU kernels, once per context (outside any
+// stream capture and off the factorisation's critical path).
+int lu_init_kernels(Ctx *c) {
+  MOM_CUDA(c, set_smem(panel_kernel<double2>));
+  MOM_CUDA(c, set_smem(panel_kernel<float2>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<double2>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<float2>));
+  MOM_CUDA(c, set_smem(compose_pivots_kernel));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8>));
+  return MOM_OK;
+}
+
+namespace {
 }  // namespace
 
 int lu_factor(Ctx *c, int precision) {

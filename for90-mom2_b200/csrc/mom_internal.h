@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/mom_gpu.h"
@@ -23,6 +24,7 @@ constexpr double kC0 = 2.997924580003e8;
 constexpr double kEta0 = 3.767303134622e2;
 
 constexpr int kMaxQ = 13;
+constexpr size_t kBlasWorkspace = 64u << 20;
 
 // Per-domain device data (structure of arrays).  "Half-edge" h = 3*face +
 // local edge identifies one RWG half (one face of an edge).
@@ -55,6 +57,7 @@ struct Ctx {
   int nsm = 0;
   cudaStream_t stream = nullptr;
   cublasHandle_t blas = nullptr;
+  void *blas_ws = nullptr;  // fixed cuBLAS workspace
   std::mutex mu;
   std::string last_error;
   int64_t launches = 0;
@@ -102,6 +105,21 @@ struct Ctx {
   bool prof = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[12];
   int64_t prof_launch[12] = {0};
+  double prof_ms[12] = {0};  // time of scopes replayed inside graphs, resolved after each replay
+
+  // The LU factorisation of each precision as one CUDA graph, replayed while
+  // the matrix order, buffers and profiling state stay those it was captured with.
+  struct LuGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uintptr_t> key;
+    std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> ev;  // timed scopes inside the graph
+    int64_t launches = 0, blas_calls = 0;  // per replay
+    double tc_flops = 0;
+    void reset();
+  } lu_graph[2];
+  bool use_graph = true;   // MOM_LU_GRAPH=0 turns graph replay off (every launch issued eagerly)
+  bool capturing = false;  // a stream capture is open on the context stream
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> cap_ev;
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)
   double tc_flops = 0;     // FLOP executed by the tensor-core LU updates since creation
 
@@ -113,7 +131,7 @@ struct Ctx {
 // Kernel categories for the optional timers.
 enum ProfCat {
   kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost, kProfPivotAux,
-  kProfTc,
+  kProfTc, kProfDiagInv,
   kProfCount
 };
 
@@ -154,6 +172,7 @@ int near_precompute(Ctx *c, int d);
 int assemble(Ctx *c, double omega, const double *ri, int precision);
 
 // lu.cu
+int lu_init_kernels(Ctx *c);
 int lu_factor(Ctx *c, int precision);
 int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
 
@@ -161,6 +180,7 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
                     int nc, int k, float *work, int *err);
 size_t tc_cgemm_work_bytes(int m, int nc, int k);
+int tc_init_kernels(Ctx *c);
 
 // post.cu
 int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src);

@@ -371,7 +371,6 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   const int ntiles = (Mr / kBM) * ((nc + kBN - 1) / kBN);
   const int grid = ntiles < c->nsm ? ntiles : c->nsm;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;
-  MOM_CUDA(c, cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   {
     ProfScope ps(c, kProfTc);
     tc_gemm_kernel<<<grid, kTcThreads, smem, c->stream>>>(mAhi, mAlo, mBhi, mBlo, ta);
@@ -379,6 +378,12 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   c->launches++;
   c->tc_flops += 6.0 * Mr * (double)nc * Kr;  // three TF32 passes, 2 FLOP per real MAC
   MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+int tc_init_kernels(Ctx *c) {
+  MOM_CUDA(c, cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kStages * kStageBytes + 1024));
   return MOM_OK;
 }
 

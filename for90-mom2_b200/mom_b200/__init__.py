@@ -392,7 +392,8 @@ class Solver:
         """cuBLAS GEMM calls since creation."""
         return lib().mom_gpu_library_calls(self.h)
 
-    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux", "tc_gemm")
+    PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux", "tc_gemm",
+                       "diag_inv")
 
     @property
     def tensor_flops(self):
