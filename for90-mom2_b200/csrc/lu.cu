@@ -46,12 +46,24 @@ struct PanelArgs {
   int *ipiv;
   int *info;      // first zero pivot (1-based), 0 if none
   int *timeout;   // set when a barrier wait ran out
-  unsigned *bar;  // arrival counter, zeroed before launch
-  double *cand_abs;   // [2][P]
-  int *cand_row;      // [2][P]
-  double2 *cand_data; // [2][P][nb]
-  double2 *col_data;  // [2][nb]
+  unsigned long long *rec;  // [2][P] candidate records, zeroed before launch
+  double2 *cand_data;       // [2][P][nb]
+  double2 *col_data;        // [2][nb]
 };
+
+// A CTA's pivot candidate for one column as one 64-bit word, so that seeing
+// the arrival and reading the candidate is a single load:
+//   bits 63..32  float bits of |re|+|im| plus one (0: no candidate),
+//   bits 31..8   0xffffff - (row - j0)  (ties go to the smaller row),
+//   bits  7..0   column epoch c + 1.
+// Comparing words >> 8 as unsigned integers orders candidates by magnitude,
+// then by the smaller row.  Within a CTA the magnitude is compared in FP64;
+// across CTAs in its FP32 rounding.
+__device__ __forceinline__ unsigned long long pack_candidate(double v, int64_t row, int64_t j0, int epoch) {
+  const unsigned long long mag = v >= 0.0 ? (unsigned long long)__float_as_uint((float)v) + 1ull : 0ull;
+  return (mag << 32) | ((unsigned long long)((0xffffffu - (unsigned)(row - j0)) & 0xffffffu) << 8) |
+         (unsigned)epoch;
+}
 
 // (value, row) pair reduction: larger |re|+|im| wins, the first row on ties.
 __device__ __forceinline__ void argmax_warp(double &v, int &r, int &w) {
@@ -122,13 +134,30 @@ __device__ bool flag_barrier(unsigned *flags, int P, unsigned epoch, int *timeou
   return s_fok != 0;
 }
 
+// Largest packed candidate over a warp: the magnitude word first, then the
+// row word among the lanes that hold that magnitude (two warp reductions).
+__device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k) {
+  const unsigned hi = (unsigned)(k >> 32);
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? (unsigned)k : 0u);
+  return ((unsigned long long)mh << 32) | ml;
+}
+
+// Panel factorisation (unblocked, partial pivoting) of columns j0 .. j0+nb
+// over rows j0 .. n, cooperative over P CTAs; CTA p holds rows
+// [j0 + p rpc, j0 + (p+1) rpc) of the panel in shared memory.  Thread t
+// works on row t % rpc and on the columns j = t / rpc (mod S), S = 256 / rpc
+// threads per row, so short panels keep every thread busy.  Per column:
+// CTA argmax, one packed record per CTA exchanged through global memory,
+// row swap, scaling and the rank-1 update of the CTA's rows.
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   extern __shared__ double2 slab[];  // [nb][rpc] column-major within the CTA
-  __shared__ double w_abs[kPanelThreads / 32];
-  __shared__ int w_row[kPanelThreads / 32];
+  __shared__ unsigned long long w_key[kPanelThreads / 32];
   __shared__ double2 s_prow_data[64];
-  __shared__ int s_prow, s_ok;
+  __shared__ double2 s_l[kPanelThreads];
+  __shared__ double2 s_rp;
+  __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;
   const int nb = a.nb, rpc = a.rpc;
   T *A = reinterpret_cast<T *>(a.A);
@@ -150,59 +179,82 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     }
   }
   __syncthreads();
-  const bool mine = tid < nrow;
-  const int64_t g = row0 + tid;  // global row owned by this thread
-  double cv = (mine && g >= a.j0) ? cabs1(slab[tid]) : -1.0;  // candidate for column 0
+  const int S = kPanelThreads / rpc;  // threads per row (rpc <= kPanelThreads)
+  const int i = tid % rpc, sph = tid / rpc;
+  const bool mine = sph < S && i < nrow;
+  const int64_t g = row0 + i;  // global row of this thread
+  double cv = (mine && sph == 0) ? cabs1(slab[i]) : -1.0;  // candidate for column 0
   for (int c = 0; c < nb; c++) {
     const int64_t col = a.j0 + c;
     const int par = c & 1;
-    // 1. CTA candidate
-    double v = cv;
-    int r = (v >= 0.0) ? (int)g : 0x7fffffff, wdummy = 0;
-    argmax_warp(v, r, wdummy);
-    if (lane == 0) {
-      w_abs[wid] = v;
-      w_row[wid] = r;
-    }
+    // 1. CTA candidate (packed: magnitude, then the smaller row)
+    const unsigned long long wk = warp_max_key(cv >= 0.0 ? pack_candidate(cv, g, a.j0, 0) : 0ull);
+    if (lane == 0) w_key[wid] = wk;
     __syncthreads();
     if (wid == 0) {
-      double bv = lane < kPanelThreads / 32 ? w_abs[lane] : -1.0;
-      int br = lane < kPanelThreads / 32 ? w_row[lane] : 0x7fffffff;
-      argmax_warp(bv, br, wdummy);
-      bv = __shfl_sync(0xffffffffu, bv, 0);
-      br = __shfl_sync(0xffffffffu, br, 0);
-      // 2. publish candidate (value, row, row data) and, if owned, row col
-      if (lane == 0) {
-        a.cand_abs[par * a.P + cta] = bv;
-        a.cand_row[par * a.P + cta] = br;
-      }
-      if (bv >= 0.0) {
-        const int li = br - (int)row0;
+      const unsigned long long bkey = warp_max_key(lane < kPanelThreads / 32 ? w_key[lane] : 0ull);
+      // 2. publish the candidate row data (and row col, if owned), then the
+      //    record; the release store orders the whole warp's stores before it
+      if (bkey != 0ull) {
+        const int li = (int)(0xffffffu - (unsigned)((bkey >> 8) & 0xffffffu)) - (int)(row0 - a.j0);
         for (int j = lane; j < nb; j += 32) a.cand_data[((size_t)par * a.P + cta) * nb + j] = slab[j * rpc + li];
       }
       if (col >= row0 && col < row0 + nrow) {
         const int li = (int)(col - row0);
         for (int j = lane; j < nb; j += 32) a.col_data[(size_t)par * nb + j] = slab[j * rpc + li];
       }
-      int ok = flag_barrier_warp0(a.bar, a.P, (unsigned)(c + 1), a.timeout) ? 1 : 0;
-      if (ok) {
-        // 3. global pivot from the P candidates
-        double gv = -1.0;
-        int gr = 0x7fffffff, gw = -1;
-        for (int p = lane; p < a.P; p += 32) {
-          const double pv = __ldcg(a.cand_abs + par * a.P + p);
-          const int pr = __ldcg(a.cand_row + par * a.P + p);
-          if (pv > gv || (pv == gv && pr < gr)) {
-            gv = pv;
-            gr = pr;
-            gw = p;
+      __syncwarp();
+      unsigned long long *rec = a.rec + (size_t)par * a.P;
+      if (lane == 0) {
+        const unsigned long long word = bkey | (unsigned)(c + 1);
+        asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(rec + cta), "l"(word) : "memory");
+      }
+      // 3. wait for all P records of this column (acquire loads); lane l
+      //    keeps the best of records l, l + 32, ...
+      unsigned long long best = 0;
+      int bw = -1;
+      unsigned pending = 0;
+      for (int q = 0; q < 8; q++)
+        if (lane + 32 * q < a.P) pending |= 1u << q;
+      long long it = 0;
+      int ok = 1;
+      while (true) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          if (!(pending >> q & 1u)) continue;
+          unsigned long long wv;
+          asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(wv) : "l"(rec + lane + 32 * q) : "memory");
+          if ((int)(wv & 0xffu) == c + 1) {
+            pending &= ~(1u << q);
+            if (bw < 0 || (wv >> 8) > (best >> 8)) {
+              best = wv;
+              bw = lane + 32 * q;
+            }
           }
         }
-        argmax_warp(gv, gr, gw);
-        gv = __shfl_sync(0xffffffffu, gv, 0);
-        gr = __shfl_sync(0xffffffffu, gr, 0);
-        gw = __shfl_sync(0xffffffffu, gw, 0);
-        const double2 *pdat = a.cand_data + ((size_t)par * a.P + gw) * nb;
+        if (__all_sync(0xffffffffu, pending == 0)) break;
+        if ((++it & 255) == 0) {
+          int stop = 0;
+          if (lane == 0) {
+            if (*(volatile int *)a.timeout) stop = 1;
+            else if (it > kSpinLimit) {
+              atomicExch(a.timeout, 1);
+              stop = 1;
+            }
+          }
+          if (__shfl_sync(0xffffffffu, stop, 0)) {
+            ok = 0;
+            break;
+          }
+        }
+      }
+      if (ok) {
+        // global pivot: the largest record; its CTA index travels with it
+        const unsigned long long gkey = warp_max_key(bw >= 0 ? (best & ~0xffull) : 0ull);
+        const int gw = __ffs(__ballot_sync(0xffffffffu, bw >= 0 && (best & ~0xffull) == gkey)) - 1;
+        const int gcta = gw < 0 ? 0 : __shfl_sync(0xffffffffu, bw, gw);
+        const int gr = (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
+        const double2 *pdat = a.cand_data + ((size_t)par * a.P + gcta) * nb;
         const double2 *cdat = a.col_data + (size_t)par * nb;
         const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
         const bool own_c = col >= row0 && col < row0 + nrow;
@@ -211,45 +263,56 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
           s_prow_data[j] = pv;
           if (own_p) slab[j * rpc + (gr - (int)row0)] = cvv;  // row prow <- old row col
           if (own_c) slab[j * rpc + (int)(col - row0)] = pv;  // row col  <- pivot row
-        }
-        if (lane == 0) {
-          s_prow = gr;
-          if (cta == 0) {
-            a.ipiv[col] = gr;
-            if (gv == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+          if (j == c) {
+            const double pa = pv.x * pv.x + pv.y * pv.y;
+            s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
+            if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
           }
         }
+        if (lane == 0 && cta == 0) a.ipiv[col] = gr;
       }
       if (lane == 0) s_ok = ok;
     }
     __syncthreads();
     if (!s_ok) return;
-    // 4. swap, scale, rank-1 update of the owned row; next candidate
+    // 4. scale column c of the rows below the pivot (one thread per row) ...
+    const double2 rp = s_rp;
+    const bool live = mine && g > col && (rp.x != 0.0 || rp.y != 0.0);
+    if (live && sph == 0) {
+      const double2 l = cmul(slab[c * rpc + i], rp);
+      slab[c * rpc + i] = l;
+      s_l[i] = l;
+    }
+    __syncthreads();
+    // ... and the rank-1 update of columns c+1 .. nb, S threads per row
     cv = -1.0;
-    if (mine) {
-      if (g > col) {
-        const double2 piv = s_prow_data[c];
-        const double pa = piv.x * piv.x + piv.y * piv.y;
-        if (pa != 0.0) {
-          const double2 rp = make_double2(piv.x / pa, -piv.y / pa);  // 1 / pivot
-          const double2 l = cmul(slab[c * rpc + tid], rp);
-          slab[c * rpc + tid] = l;
-          for (int j = c + 1; j < nb; j++) {
-            const double2 u = s_prow_data[j];
-            double2 x = slab[j * rpc + tid];
-            x.x -= l.x * u.x - l.y * u.y;
-            x.y -= l.x * u.y + l.y * u.x;
-            slab[j * rpc + tid] = x;
-          }
+    const int own = (c + 1) % S;  // phase of the thread that holds column c+1
+    if (mine && g > col) {
+      const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
+      if (live) {
+        const double2 l = s_l[i];
+        for (int j = jst; j < nb; j += 4 * S) {
+          double2 x[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j + u * S < nb) x[u] = slab[(j + u * S) * rpc + i];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j + u * S < nb) {
+              const double2 uu = s_prow_data[j + u * S];
+              x[u].x -= l.x * uu.x - l.y * uu.y;
+              x[u].y -= l.x * uu.y + l.y * uu.x;
+              slab[(j + u * S) * rpc + i] = x[u];
+            }
         }
-        if (c + 1 < nb) cv = cabs1(slab[(c + 1) * rpc + tid]);
       }
+      if (sph == own && c + 1 < nb) cv = cabs1(slab[(c + 1) * rpc + i]);
     }
   }
   __syncthreads();
   for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
-    const int c = idx / rpc, i = idx % rpc;
-    if (i < nrow) st2(A + (row0 + i) + (a.j0 + c) * a.lda, slab[idx]);
+    const int c = idx / rpc, ii = idx % rpc;
+    if (ii < nrow) st2(A + (row0 + ii) + (a.j0 + c) * a.lda, slab[idx]);
   }
 }
 
@@ -733,8 +796,7 @@ __global__ void axpy_kernel(double2 *X, const double2 *D, int64_t count) {
 struct LuWork {
   unsigned *bar;
   int *info, *timeout;
-  double *cand_abs;
-  int *cand_row;
+  unsigned long long *rec;
   double2 *cand_data, *col_data;
   double2 *W;      // nb x n workspace for the TRSM product
   float2 *invL32;  // nb x nb
@@ -752,8 +814,7 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
     return o;
   };
   const size_t o_bar = take(sizeof(unsigned) * 256);
-  const size_t o_ca = take(sizeof(double) * 2 * P);
-  const size_t o_cr = take(sizeof(int) * 2 * P);
+  const size_t o_ca = take(sizeof(unsigned long long) * 2 * P);
   const size_t o_cd = take(sizeof(double2) * 2 * P * nb);
   const size_t o_cl = take(sizeof(double2) * 2 * nb);
   const size_t o_w = take(esz * (size_t)nb * c->n);
@@ -765,8 +826,7 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   w.bar = (unsigned *)(b + o_bar);
   w.info = c->dinfo;
   w.timeout = c->dinfo + 1;
-  w.cand_abs = (double *)(b + o_ca);
-  w.cand_row = (int *)(b + o_cr);
+  w.rec = (unsigned long long *)(b + o_ca);
   w.cand_data = (double2 *)(b + o_cd);
   w.col_data = (double2 *)(b + o_cl);
   w.W = (double2 *)(b + o_w);
@@ -824,7 +884,7 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
       int rpc = (int)((m + P - 1) / P);
       P = (int)((m + rpc - 1) / rpc);
       const size_t smem = sizeof(double2) * (size_t)nb * rpc;
-      if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64)
+      if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64 || P > 256)
         return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory (matrix order too large)");
       PanelArgs pa;
       pa.A = A;
@@ -837,13 +897,11 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
       pa.ipiv = c->ipiv;
       pa.info = w.info;
       pa.timeout = w.timeout;
-      pa.bar = w.bar;
-      pa.cand_abs = w.cand_abs;
-      pa.cand_row = w.cand_row;
+      pa.rec = w.rec;
       pa.cand_data = w.cand_data;
       pa.col_data = w.col_data;
       {
-        MOM_CUDA(c, cudaMemsetAsync(w.bar, 0, sizeof(unsigned) * 256, c->stream));
+        MOM_CUDA(c, cudaMemsetAsync(w.rec, 0, sizeof(unsigned long long) * 2 * P, c->stream));
         ProfScope ps(c, kProfPanel);
         void *args[] = {&pa};
         MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
