@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "mom_internal.h"
 
@@ -94,6 +95,15 @@ void free_domain(DomDev &D) {
   cudaFree(D.near_m);
   cudaFree(D.near_n);
   cudaFree(D.near_static);
+  cudaFree(D.nodes);
+  cudaFree(D.fsign);
+  cudaFree(D.fnode);
+  cudaFree(D.fea);
+  cudaFree(D.feb);
+  cudaFree(D.fbn);
+  cudaFree(D.near_bits);
+  cudaFree(D.inc_node);
+  cudaFree(D.inc_face);
   D = DomDev();
 }
 
@@ -157,6 +167,13 @@ int build_domain(Ctx *c, const mom_mesh &m, DomDev &D) {
   D.F = F;
   D.Nd = Nd;
   const double *P = m.nodes;
+  D.nnodes = m.nnodes;
+  D.h_nodes.assign(P, P + 3 * (size_t)m.nnodes);
+  D.h_fnode.assign(m.face_nodes, m.face_nodes + 3 * (size_t)F);
+  D.h_fea.resize(3 * (size_t)F);
+  D.h_feb.resize(3 * (size_t)F);
+  D.h_fbn.resize(3 * (size_t)F);
+  D.h_fsign.resize(3 * (size_t)F);
   D.h_cp.resize(3 * (size_t)F);
   D.h_area.resize(F);
   D.h_nrm.resize(3 * (size_t)F);
@@ -237,6 +254,10 @@ int build_domain(Ctx *c, const mom_mesh &m, DomDev &D) {
                     "Error evaluating mesh face sign (this could imply corrupted mesh connectivity)!");
       }
       D.h_sl[3 * (size_t)f + e] = sign * elen[ge];
+      D.h_fsign[3 * (size_t)f + e] = sign;
+      D.h_fea[3 * (size_t)f + e] = m.edge_nodes[2 * ge];
+      D.h_feb[3 * (size_t)f + e] = m.edge_nodes[2 * ge + 1];
+      D.h_fbn[3 * (size_t)f + e] = bn;
       D.h_hpar[3 * (size_t)f + e] = m.edge_parent[ge];
       for (int i = 0; i < 3; i++) {
         D.h_bn[9 * (size_t)f + 3 * e + i] = P[3 * bn + i];
@@ -366,6 +387,9 @@ void mom_gpu_destroy(mom_ctx *c) {
   free_problem(c);
   cudaFree(c->ws);
   cudaFree(c->Xh);
+  cudaFree(c->adj);
+  cudaFree(c->adj_part);
+  cudaFree(c->adjW);
   cudaFree(c->dinfo);
   cudaFree(c->flags);
   if (c->pinned) cudaFreeHost(c->pinned);
@@ -501,6 +525,100 @@ int mom_gpu_solve_wavelength(mom_ctx *c, double omega, const double *ri, int32_t
   r = mom_gpu_srcvec(c, omega, ri, nsrc, src, nullptr, 0);
   if (r) return r;
   return mom_gpu_solve(c, precision, tol, maxit, x_host, ldx, iters_out);
+}
+
+int32_t mom_gpu_domain_nodes(mom_ctx *c, int32_t dom) {
+  if (!c || !c->have_problem || dom < 0 || dom >= c->ndom) return -1;
+  return c->dom[dom].nnodes;
+}
+
+// Shared set-up of the adjoint entry points: G = d sigma / dx of the solved
+// sources and the adjoint currents A^T lambda = G (2 nsrc columns: ext, abs
+// per source) in c->adj; returns the pointers.
+static int adjoint_currents(mom_ctx *c, int32_t precision, double omega, const double *ri, int32_t nsrc,
+                            const mom_src *src, double tol, int32_t maxit, double2 **G, double2 **lam,
+                            double2 **xo, int32_t *iters) {
+  MOM_TRY(check_prec(c, precision));
+  if (c->factored != precision) return fail(c, MOM_ERR_STATE, "the adjoint needs the factors of a solve in this precision");
+  if (nsrc != c->nsrc || nsrc <= 0 || !src || !ri || !(omega > 0))
+    return fail(c, MOM_ERR_ARG, "the adjoint sources must be those of the last solve");
+  if (precision == MOM_PREC_MIXED && (maxit <= 0 || !(tol > 0))) return fail(c, MOM_ERR_ARG, "mixed adjoint needs tol > 0, maxit > 0");
+  const size_t col = sizeof(double2) * (size_t)c->n, R = 2 * (size_t)nsrc;
+  MOM_TRY(ensure_buffer(c, &c->adj, &c->adj_bytes, 3 * R * col));
+  *G = (double2 *)c->adj;
+  *lam = (double2 *)((char *)c->adj + R * col);
+  *xo = (double2 *)((char *)c->adj + 2 * R * col);
+  MOM_TRY(cs_gradient(c, 0, omega, ri, nsrc, src, c->X, c->n, *G));
+  int it = 0;
+  MOM_TRY(lu_solve_ex(c, precision, 1, *G, *lam, (int)R, tol, maxit, &it));
+  if (iters) *iters = it;
+  for (int s = 0; s < nsrc; s++)
+    for (int k = 0; k < 2; k++)
+      MOM_CUDA(c, cudaMemcpyAsync((char *)*xo + (2 * s + k) * col, c->X + (size_t)s * c->n, col,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+  return MOM_OK;
+}
+
+int mom_gpu_adjoint(mom_ctx *c, int32_t precision, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                    int32_t eps_dom, double tol, int32_t maxit, double *deps, double *dnodes, int32_t *iters_out) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (nsrc < 1 || nsrc > 4) return fail(c, MOM_ERR_ARG, "per-source adjoint gradients take 1 to 4 sources");
+  if (deps && (eps_dom < 1 || eps_dom >= c->ndom)) return fail(c, MOM_ERR_ARG, "eps_dom must be an interior domain");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  double2 *G = nullptr, *lam = nullptr, *xo = nullptr;
+  MOM_TRY(adjoint_currents(c, precision, omega, ri, nsrc, src, tol, maxit, &G, &lam, &xo, iters_out));
+  const int R = 2 * nsrc;
+  if (deps) {
+    std::vector<double> t(2 * R);
+    MOM_TRY(adjoint_eps(c, omega, ri, eps_dom, R, lam, xo, nullptr, t.data()));
+    // d sigma = -Re(lambda^T A' x d eps): d/dRe eps = -Re t', d/dIm eps = Im t'
+    for (int o = 0; o < R; o++) {
+      deps[2 * o] = -t[2 * o];
+      deps[2 * o + 1] = t[2 * o + 1];
+    }
+  }
+  if (dnodes) {
+    std::vector<int> osrc(R), okind(R);
+    for (int o = 0; o < R; o++) {
+      osrc[o] = o / 2;
+      okind[o] = o % 2;
+    }
+    MOM_TRY(adjoint_nodes(c, omega, ri, R, lam, xo, osrc.data(), okind.data(), nsrc, src, dnodes));
+  }
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int mom_gpu_adjoint_mean_eps(mom_ctx *c, int32_t precision, double omega, const double *ri, int32_t nsrc,
+                             const mom_src *src, int32_t eps_dom, double tol, int32_t maxit, double *dmean,
+                             int32_t *iters_out) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (!dmean || eps_dom < 1 || eps_dom >= c->ndom) return fail(c, MOM_ERR_ARG, "eps_dom must be an interior domain");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  double2 *G = nullptr, *lam = nullptr, *xo = nullptr;
+  MOM_TRY(adjoint_currents(c, precision, omega, ri, nsrc, src, tol, maxit, &G, &lam, &xo, iters_out));
+  const int64_t n = c->n;
+  MOM_TRY(ensure_buffer(c, &c->adjW, &c->adjW_bytes, sizeof(double2) * (size_t)n * n));
+  double2 *W = (double2 *)c->adjW;
+  for (int k = 0; k < 2; k++) {
+    // W = (1/nsrc) sum_s lambda_{2s+k} x_s^T (a plain library GEMM, K = nsrc)
+    const cuDoubleComplex al = make_cuDoubleComplex(1.0 / nsrc, 0.0), be = make_cuDoubleComplex(0.0, 0.0);
+    MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+    MOM_BLAS(c, cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, (int)n, nsrc, &al,
+                            (const cuDoubleComplex *)(lam + (size_t)k * n), (int)(2 * n),
+                            (const cuDoubleComplex *)c->X, (int)n, &be, (cuDoubleComplex *)W, (int)n));
+    c->blas_calls++;
+    double t[2];
+    MOM_TRY(adjoint_eps(c, omega, ri, eps_dom, 0, nullptr, nullptr, W, t));
+    dmean[2 * k] = -t[0];
+    dmean[2 * k + 1] = t[1];
+  }
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
 }
 
 int mom_gpu_cross_sections(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t nsrc,

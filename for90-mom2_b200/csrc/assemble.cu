@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <vector>
 
 #include "mom_internal.h"
 
@@ -323,60 +324,166 @@ __global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
 
 // ---- closed-form static integrals (int.f90), FP64 ------------------------
 
-struct FaceGeo {
-  double v[3][3];   // vertices
-  double s[3][3];   // edge unit vectors s(:,e)
-  double mm[3][3];  // in-plane edge normals m(:,e)
-  double n[3];      // unit normal
+// The closed-form integrals below are templates on the scalar type S: double
+// for the matrix, and a forward-mode dual number for the adjoint gradients.
+template <typename S>
+struct FaceGeoT {
+  S v[3][3];   // vertices
+  S s[3][3];   // edge unit vectors s(:,e)
+  S mm[3][3];  // in-plane edge normals m(:,e)
+  S n[3];      // unit normal
 };
+using FaceGeo = FaceGeoT<double>;
 
-__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-__device__ __forceinline__ double norm3(const double *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+template <typename S>
+__device__ __forceinline__ S dot3(const S *a, const S *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+template <typename S>
+__device__ __forceinline__ S norm3(const S *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
 
 // int.f90:15-53 intLm1
-__device__ double d_intLm1(const double *r, const FaceGeo &g, int e) {
-  const double *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
-  double a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
-  double Rp = norm3(a), Rm = norm3(b);
-  double sp = -dot3(a, s), sm = -dot3(b, s);
-  double div1 = Rp - sp, div2 = Rm + sm;
+template <typename S>
+__device__ S d_intLm1(const S *r, const FaceGeoT<S> &g, int e) {
+  const S *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
+  S a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
+  S Rp = norm3(a), Rm = norm3(b);
+  S sp = -dot3(a, s), sm = -dot3(b, s);
+  S div1 = Rp - sp, div2 = Rm + sm;
   if (fabs(div1) > fabs(div2)) return log((Rm - sm) / div1);
   return log((Rp + sp) / div2);
 }
 
 // int.f90:55-96 intL1 and 98-135 intL3 together (they share R02, Rp, Rm).
-__device__ void d_intL13(const double *r, const FaceGeo &g, int e, const double *n, double lm1, double *L1, double *L3) {
-  const double *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
-  double rp[3];
+template <typename S>
+__device__ void d_intL13(const S *r, const FaceGeoT<S> &g, int e, const S *n, S lm1, S *L1, S *L3) {
+  const S *p1 = g.v[e], *p2 = g.v[(e + 1) % 3], *s = g.s[e];
+  S rp[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) rp[i] = r[i] - 0.5 * (p1[i] + p2[i]);
-  double h = dot3(n, rp), t = dot3(g.mm[e], rp);
-  double R02 = t * t + h * h;
-  double a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
-  double Rp = norm3(a), Rm = norm3(b);
-  double sp = -dot3(a, s), sm = -dot3(b, s);
-  double l1 = (R02 == 0) ? 0.5 * (sp * Rp - sm * Rm) : 0.5 * R02 * lm1 + 0.5 * (sp * Rp - sm * Rm);
+  S h = dot3(n, rp), t = dot3(g.mm[e], rp);
+  S R02 = t * t + h * h;
+  S a[3] = {r[0] - p2[0], r[1] - p2[1], r[2] - p2[2]}, b[3] = {r[0] - p1[0], r[1] - p1[1], r[2] - p1[2]};
+  S Rp = norm3(a), Rm = norm3(b);
+  S sp = -dot3(a, s), sm = -dot3(b, s);
+  S l1 = (R02 == 0) ? 0.5 * (sp * Rp - sm * Rm) : 0.5 * R02 * lm1 + 0.5 * (sp * Rp - sm * Rm);
   *L1 = l1;
   *L3 = 0.75 * R02 * l1 + 0.25 * (sp * (Rp * Rp * Rp) - sm * (Rm * Rm * Rm));
 }
 
 // int.f90:137-162 intSm3h
-__device__ double d_intSm3h(const double *r, const FaceGeo &g) {
-  double a[3][3];
+template <typename S>
+__device__ S d_intSm3h(const S *r, const FaceGeoT<S> &g) {
+  S a[3][3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    double v[3] = {g.v[k][0] - r[0], g.v[k][1] - r[1], g.v[k][2] - r[2]};
-    double l = norm3(v);
+    S v[3] = {g.v[k][0] - r[0], g.v[k][1] - r[1], g.v[k][2] - r[2]};
+    S l = norm3(v);
 #pragma unroll
     for (int i = 0; i < 3; i++) a[k][i] = v[i] / l;
   }
-  double x = 1.0 + dot3(a[0], a[1]) + dot3(a[0], a[2]) + dot3(a[1], a[2]);
-  double c[3] = {a[1][1] * a[2][2] - a[1][2] * a[2][1], a[1][2] * a[2][0] - a[1][0] * a[2][2],
-                 a[1][0] * a[2][1] - a[1][1] * a[2][0]};
-  double y = fabs(dot3(a[0], c));
-  double om = 2.0 * atan2(y, x);
-  double rp1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
+  S x = 1.0 + dot3(a[0], a[1]) + dot3(a[0], a[2]) + dot3(a[1], a[2]);
+  S c[3] = {a[1][1] * a[2][2] - a[1][2] * a[2][1], a[1][2] * a[2][0] - a[1][0] * a[2][2],
+            a[1][0] * a[2][1] - a[1][1] * a[2][0]};
+  S y = fabs(dot3(a[0], c));
+  S om = 2.0 * atan2(y, x);
+  S rp1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
   return dot3(g.n, rp1) > 0.0 ? fabs(om) : -fabs(om);
+}
+
+// The k-independent closed-form integrals of source face n (geometry g,
+// area An, RWG sl and free vertices bnn) at the NQ test points qm of face m
+// (area Am, sl slm, free vertices bnm), contracted with the test RWG
+// functions: out[0..5] = Dm1, D1, Hm1, H1, Km1, K1 (each 3x3, row p = test
+// edge; K terms zero for the self pair).
+template <typename S, int NQ>
+__device__ void static_terms(const S (*qm)[3], S Am, const S *slm, const S (*bnm)[3], const FaceGeoT<S> &g, S An,
+                             const S *sln, const S (*bnn)[3], bool self, S out[6][9]) {
+  S acc[6][9];
+#pragma unroll
+  for (int o = 0; o < 6; o++)
+#pragma unroll
+    for (int i = 0; i < 9; i++) acc[o][i] = 0.0;
+  for (int t = 0; t < NQ; t++) {
+    const S *r = qm[t];
+    const double wt = c_qw[t];
+    S Lm1[3], L1[3], L3[3];
+    // intSm1 (int.f90:181-226) decides per edge whether intLm1 is needed
+    // when h == 0; intL1 always calls intLm1 unless R02 == 0.
+    S r1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
+    S h = dot3(g.n, r1);
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      Lm1[e] = d_intLm1(r, g, e);
+      d_intL13(r, g, e, g.n, Lm1[e], &L1[e], &L3[e]);
+    }
+    S tt[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      S re[3] = {r[0] - g.v[e][0], r[1] - g.v[e][1], r[2] - g.v[e][2]};
+      tt[e] = dot3(g.mm[e], re);
+    }
+    S Sm3h = d_intSm3h(r, g);
+    S Sm1;
+    if (h == 0) {
+      S e1 = tt[0] == 0 ? S(0.0) : Lm1[0], e2 = tt[1] == 0 ? S(0.0) : Lm1[1], e3 = tt[2] == 0 ? S(0.0) : Lm1[2];
+      Sm1 = -(tt[0] * e1 + tt[1] * e2 + tt[2] * e3);
+    } else {
+      Sm1 = -h * Sm3h - (tt[0] * Lm1[0] + tt[1] * Lm1[1] + tt[2] * Lm1[2]);
+    }
+    S S1 = (h * h) / 3.0 * Sm1 - 1.0 / 3.0 * (tt[0] * L1[0] + tt[1] * L1[1] + tt[2] * L1[2]);
+    S rho[3], K3m1[3], K31[3], mL1[3], mL3[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      rho[i] = r[i] - h * g.n[i];
+      mL1[i] = g.mm[0][i] * L1[0] + g.mm[1][i] * L1[1] + g.mm[2][i] * L1[2];
+      mL3[i] = g.mm[0][i] * L3[0] + g.mm[1][i] * L3[1] + g.mm[2][i] * L3[2];
+      K3m1[i] = g.mm[0][i] * Lm1[0] + g.mm[1][i] * Lm1[1] + g.mm[2][i] * Lm1[2] + g.n[i] * Sm3h;
+      K31[i] = (h == 0) ? mL1[i] : mL1[i] - h * g.n[i] * Sm1;
+    }
+    // test functions at r: f_p = sl_p/(2 Am) (r - u_p), div f_p = sl_p / Am
+    S fp[3][3], dvp[3];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const S slp = slm[p];
+      const S *u = bnm[p];
+#pragma unroll
+      for (int i = 0; i < 3; i++) fp[p][i] = slp / (2.0 * Am) * (r[i] - u[i]);
+      dvp[p] = slp / Am;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const S slq = sln[q];
+      const S cq = slq / (2.0 * An);
+      const S *pq = bnn[q];
+      S K2m1[3], K21[3], K4m1[3], K41[3], rpq[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        K2m1[i] = cq * (mL1[i] + (rho[i] - pq[i]) * Sm1);
+        K21[i] = cq * (1.0 / 3.0 * mL3[i] + (rho[i] - pq[i]) * S1);
+        rpq[i] = r[i] - pq[i];
+      }
+      K4m1[0] = -cq * (rpq[1] * K3m1[2] - rpq[2] * K3m1[1]);
+      K4m1[1] = -cq * (rpq[2] * K3m1[0] - rpq[0] * K3m1[2]);
+      K4m1[2] = -cq * (rpq[0] * K3m1[1] - rpq[1] * K3m1[0]);
+      K41[0] = -cq * (rpq[1] * K31[2] - rpq[2] * K31[1]);
+      K41[1] = -cq * (rpq[2] * K31[0] - rpq[0] * K31[2]);
+      K41[2] = -cq * (rpq[0] * K31[1] - rpq[1] * K31[0]);
+      const S K1m1 = slq / An * Sm1, K11 = slq / An * S1;
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+        const int pq_ = 3 * p + q;
+        acc[0][pq_] += wt * dot3(fp[p], K2m1);
+        acc[1][pq_] += wt * dot3(fp[p], K21);
+        acc[2][pq_] += wt * dvp[p] * K1m1;
+        acc[3][pq_] += wt * dvp[p] * K11;
+        acc[4][pq_] += wt * dot3(fp[p], K4m1);
+        acc[5][pq_] += wt * dot3(fp[p], K41);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; k++)
+#pragma unroll
+    for (int i = 0; i < 9; i++) out[k][i] = (self && k >= 4) ? S(0.0) : acc[k][i] * Am;
 }
 
 struct StaticArgs {
@@ -399,96 +506,16 @@ __global__ void __launch_bounds__(128) near_static_kernel(StaticArgs a) {
   if (j >= a.nnear) return;
   const int m = a.near_m[j], n = a.near_n[j];
   const FaceGeo g = a.geo[n];
-  const double An = a.area[n], Am = a.area[m];
-  double acc[6][9];
-#pragma unroll
-  for (int o = 0; o < 6; o++)
-#pragma unroll
-    for (int i = 0; i < 9; i++) acc[o][i] = 0.0;
-  for (int t = 0; t < NQ; t++) {
-    const double *r = a.qabs + ((size_t)m * NQ + t) * 3;
-    const double wt = c_qw[t];
-    double Lm1[3], L1[3], L3[3];
-    // intSm1 (int.f90:181-226) decides per edge whether intLm1 is needed
-    // when h == 0; intL1 always calls intLm1 unless R02 == 0.
-    double r1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
-    double h = dot3(g.n, r1);
-#pragma unroll
-    for (int e = 0; e < 3; e++) {
-      Lm1[e] = d_intLm1(r, g, e);
-      d_intL13(r, g, e, g.n, Lm1[e], &L1[e], &L3[e]);
-    }
-    double tt[3];
-#pragma unroll
-    for (int e = 0; e < 3; e++) {
-      double re[3] = {r[0] - g.v[e][0], r[1] - g.v[e][1], r[2] - g.v[e][2]};
-      tt[e] = dot3(g.mm[e], re);
-    }
-    double Sm3h = d_intSm3h(r, g);
-    double Sm1;
-    if (h == 0) {
-      double e1 = tt[0] == 0 ? 0.0 : Lm1[0], e2 = tt[1] == 0 ? 0.0 : Lm1[1], e3 = tt[2] == 0 ? 0.0 : Lm1[2];
-      Sm1 = -(tt[0] * e1 + tt[1] * e2 + tt[2] * e3);
-    } else {
-      Sm1 = -h * Sm3h - (tt[0] * Lm1[0] + tt[1] * Lm1[1] + tt[2] * Lm1[2]);
-    }
-    double S1 = (h * h) / 3.0 * Sm1 - 1.0 / 3.0 * (tt[0] * L1[0] + tt[1] * L1[1] + tt[2] * L1[2]);
-    double rho[3], K3m1[3], K31[3], mL1[3], mL3[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-      rho[i] = r[i] - h * g.n[i];
-      mL1[i] = g.mm[0][i] * L1[0] + g.mm[1][i] * L1[1] + g.mm[2][i] * L1[2];
-      mL3[i] = g.mm[0][i] * L3[0] + g.mm[1][i] * L3[1] + g.mm[2][i] * L3[2];
-      K3m1[i] = g.mm[0][i] * Lm1[0] + g.mm[1][i] * Lm1[1] + g.mm[2][i] * Lm1[2] + g.n[i] * Sm3h;
-      K31[i] = (h == 0) ? mL1[i] : mL1[i] - h * g.n[i] * Sm1;
-    }
-    // test functions at r: f_p = sl_p/(2 Am) (r - u_p), div f_p = sl_p / Am
-    double fp[3][3], dvp[3];
-#pragma unroll
-    for (int p = 0; p < 3; p++) {
-      const double slp = a.sl[3 * m + p];
-      const double *u = a.bn + 9 * m + 3 * p;
-#pragma unroll
-      for (int i = 0; i < 3; i++) fp[p][i] = slp / (2.0 * Am) * (r[i] - u[i]);
-      dvp[p] = slp / Am;
-    }
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const double slq = a.sl[3 * n + q];
-      const double cq = slq / (2.0 * An);
-      const double *pq = a.bn + 9 * n + 3 * q;
-      double K2m1[3], K21[3], K4m1[3], K41[3], rpq[3];
-#pragma unroll
-      for (int i = 0; i < 3; i++) {
-        K2m1[i] = cq * (mL1[i] + (rho[i] - pq[i]) * Sm1);
-        K21[i] = cq * (1.0 / 3.0 * mL3[i] + (rho[i] - pq[i]) * S1);
-        rpq[i] = r[i] - pq[i];
-      }
-      K4m1[0] = -cq * (rpq[1] * K3m1[2] - rpq[2] * K3m1[1]);
-      K4m1[1] = -cq * (rpq[2] * K3m1[0] - rpq[0] * K3m1[2]);
-      K4m1[2] = -cq * (rpq[0] * K3m1[1] - rpq[1] * K3m1[0]);
-      K41[0] = -cq * (rpq[1] * K31[2] - rpq[2] * K31[1]);
-      K41[1] = -cq * (rpq[2] * K31[0] - rpq[0] * K31[2]);
-      K41[2] = -cq * (rpq[0] * K31[1] - rpq[1] * K31[0]);
-      const double K1m1 = slq / An * Sm1, K11 = slq / An * S1;
-#pragma unroll
-      for (int p = 0; p < 3; p++) {
-        const int pq_ = 3 * p + q;
-        acc[0][pq_] += wt * dot3(fp[p], K2m1);
-        acc[1][pq_] += wt * dot3(fp[p], K21);
-        acc[2][pq_] += wt * dvp[p] * K1m1;
-        acc[3][pq_] += wt * dvp[p] * K11;
-        acc[4][pq_] += wt * dot3(fp[p], K4m1);
-        acc[5][pq_] += wt * dot3(fp[p], K41);
-      }
-    }
-  }
+  const double(*qm)[3] = reinterpret_cast<const double(*)[3]>(a.qabs + (size_t)m * NQ * 3);
+  const double(*bnm)[3] = reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)m);
+  const double(*bnn)[3] = reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)n);
+  double out[6][9];
+  static_terms<double, NQ>(qm, a.area[m], a.sl + 3 * m, bnm, g, a.area[n], a.sl + 3 * n, bnn, m == n, out);
   double *o = a.out + j * 54;
-  const bool self = (m == n);
 #pragma unroll
   for (int k = 0; k < 6; k++)
 #pragma unroll
-    for (int i = 0; i < 9; i++) o[9 * k + i] = (self && k >= 4) ? 0.0 : acc[k][i] * Am;
+    for (int i = 0; i < 9; i++) o[9 * k + i] = out[k][i];
 }
 
 struct NearArgs {
@@ -814,6 +841,253 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
   }
   c->assembled = 1;
   c->factored = -1;
+  return MOM_OK;
+}
+
+#include "adjoint_impl.cuh"
+
+namespace {
+
+template <typename V>
+int upload_vec(Ctx *c, V **dst, const std::vector<V> &src) {
+  MOM_CUDA(c, cudaMalloc(dst, sizeof(V) * std::max<size_t>(1, src.size())));
+  if (!src.empty())
+    MOM_CUDA(c, cudaMemcpyAsync(*dst, src.data(), sizeof(V) * src.size(), cudaMemcpyHostToDevice, c->stream));
+  return MOM_OK;
+}
+
+// Topology of domain d for the geometry derivatives: nodes, face and edge
+// node indices, the near-pair bitmap and the (vertex, face) incidences.
+int adjoint_setup(Ctx *c, int d) {
+  DomDev &D = c->dom[d];
+  if (D.adj_ready) return MOM_OK;
+  const int F = D.F;
+  MOM_TRY(upload_vec(c, &D.nodes, D.h_nodes));
+  MOM_TRY(upload_vec(c, &D.fsign, D.h_fsign));
+  MOM_TRY(upload_vec(c, &D.fnode, D.h_fnode));
+  MOM_TRY(upload_vec(c, &D.fea, D.h_fea));
+  MOM_TRY(upload_vec(c, &D.feb, D.h_feb));
+  MOM_TRY(upload_vec(c, &D.fbn, D.h_fbn));
+  const size_t words = ((size_t)F * F + 31) / 32;
+  MOM_CUDA(c, cudaMalloc(&D.near_bits, sizeof(unsigned) * words));
+  MOM_CUDA(c, cudaMemsetAsync(D.near_bits, 0, sizeof(unsigned) * words, c->stream));
+  if (D.nnear > 0) {
+    near_bits_kernel<<<(unsigned)((D.nnear + 255) / 256), 256, 0, c->stream>>>(D.nnear, F, D.near_m, D.near_n,
+                                                                                D.near_bits);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  std::vector<int> inode, iface;
+  std::vector<std::vector<int>> byn(D.nnodes);
+  for (int f = 0; f < F; f++)
+    for (int k = 0; k < 3; k++) byn[D.h_fnode[3 * (size_t)f + k]].push_back(f);
+  for (int v = 0; v < D.nnodes; v++)
+    for (int f : byn[v]) {
+      inode.push_back(v);
+      iface.push_back(f);
+    }
+  D.ninc = (int)inode.size();
+  MOM_TRY(upload_vec(c, &D.inc_node, inode));
+  MOM_TRY(upload_vec(c, &D.inc_face, iface));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  D.adj_ready = true;
+  return MOM_OK;
+}
+
+AdjTopo topo_of(const Ctx *c, const DomDev &D) {
+  AdjTopo t;
+  t.F = D.F;
+  t.N = c->N;
+  t.nodes = D.nodes;
+  t.fnode = D.fnode;
+  t.fea = D.fea;
+  t.feb = D.feb;
+  t.fbn = D.fbn;
+  t.fsign = D.fsign;
+  t.hpar = D.hpar;
+  t.near_bits = D.near_bits;
+  return t;
+}
+
+Cd cdiv(Cd a, Cd b) {
+  const double d = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+Cd cmulh(Cd a, Cd b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+// Medium constants of domain d (sysmat.f90:40-60) as dual numbers, with the
+// derivative along Re(eps) when seed is set.
+void medium_duals(double omega, const double *ri, int d, bool seed, AdjPairArgs &a) {
+  const Cd n = {ri[2 * d], ri[2 * d + 1]};
+  const double k0 = omega / kC0;
+  const Cd eps = cmulh(n, n);
+  const Cd dk = seed ? cdiv({k0, 0.0}, {2.0 * n.re, 2.0 * n.im}) : Cd{0.0, 0.0};  // dk/deps = k0 / (2 n)
+  a.kr = Dual(n.re * k0, dk.re);
+  a.ki = Dual(n.im * k0, dk.im);
+  a.c1 = {Dual(0.0), Dual(-omega * kMu0)};
+  const Cd den = {-omega * kEps0 * eps.im, omega * kEps0 * eps.re};  // i omega eps0 eps
+  const Cd c2 = cdiv({-1.0, 0.0}, den);
+  const Cd dc2 = seed ? cdiv({-c2.re, -c2.im}, eps) : Cd{0.0, 0.0};  // dc2/deps = -c2 / eps
+  a.c2 = {Dual(c2.re, dc2.re), Dual(c2.im, dc2.im)};
+  const double ie2 = 1.0 / (kEta0 * kEta0);
+  a.Zsi = {Dual(eps.re * ie2, seed ? ie2 : 0.0), Dual(eps.im * ie2, 0.0)};
+}
+
+int adj_launch_pair(Ctx *c, const dim3 &grid, const AdjPairArgs &a) {
+  switch (c->nq) {
+    case 1: launch_adj_pair<1>(grid, c->stream, a); break;
+    case 3: launch_adj_pair<3>(grid, c->stream, a); break;
+    case 4: launch_adj_pair<4>(grid, c->stream, a); break;
+    case 7: launch_adj_pair<7>(grid, c->stream, a); break;
+    case 13: launch_adj_pair<13>(grid, c->stream, a); break;
+    default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+  }
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+}  // namespace
+
+int adjoint_eps(Ctx *c, double omega, const double *ri, int d, int R, const double2 *lam, const double2 *xv,
+                const double2 *W, double *out) {
+  if (R < 0 || R > kAdjMaxObj) return fail(c, MOM_ERR_ARG, "too many adjoint objectives");
+  MOM_TRY(adjoint_setup(c, d));
+  DomDev &D = c->dom[d];
+  AdjPairArgs a;
+  a.t = topo_of(c, D);
+  a.n = c->n;
+  medium_duals(omega, ri, d, true, a);
+  a.mode = 0;
+  a.inc_node = a.inc_face = nullptr;
+  a.R = R;
+  a.lam = lam;
+  a.xv = xv;
+  a.W = W;
+  const int nobj = R == 0 ? 1 : R;
+  const dim3 grid((D.F + kAdjThreads - 1) / kAdjThreads, D.F);
+  const size_t nvals = (size_t)grid.x * grid.y * nobj * 2;
+  MOM_TRY(ensure_buffer(c, &c->adj_part, &c->adj_part_bytes, sizeof(double) * nvals));
+  a.part = (double *)c->adj_part;
+  MOM_TRY(adj_launch_pair(c, grid, a));
+  std::vector<double> h(nvals);
+  MOM_CUDA(c, cudaMemcpyAsync(h.data(), a.part, sizeof(double) * nvals, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int o = 0; o < nobj; o++) {
+    double re = 0, im = 0;
+    for (size_t b = 0; b < (size_t)grid.x * grid.y; b++) {
+      re += h[(b * nobj + o) * 2];
+      im += h[(b * nobj + o) * 2 + 1];
+    }
+    out[2 * o] = re;
+    out[2 * o + 1] = im;
+  }
+  return MOM_OK;
+}
+
+int adjoint_nodes(Ctx *c, double omega, const double *ri, int R, const double2 *lam, const double2 *xv,
+                  const int *obj_src, const int *obj_kind, int nsrc, const mom_src *src, double *out) {
+  if (R < 1 || R > kAdjMaxObj) return fail(c, MOM_ERR_ARG, "1 to 8 adjoint objectives");
+  int total = 0;
+  std::vector<int> off(c->ndom);
+  for (int d = 0; d < c->ndom; d++) {
+    off[d] = total;
+    total += c->dom[d].nnodes;
+  }
+  std::fill(out, out + (size_t)R * total * 3, 0.0);
+  // - Re(lambda^T dA x) of every domain's blocks
+  for (int d = 0; d < c->ndom; d++) {
+    MOM_TRY(adjoint_setup(c, d));
+    DomDev &D = c->dom[d];
+    if (D.ninc == 0) continue;
+    AdjPairArgs a;
+    a.t = topo_of(c, D);
+    a.n = c->n;
+    medium_duals(omega, ri, d, false, a);
+    a.mode = 1;
+    a.inc_node = D.inc_node;
+    a.inc_face = D.inc_face;
+    a.R = R;
+    a.lam = lam;
+    a.xv = xv;
+    a.W = nullptr;
+    const dim3 grid((D.F + kAdjThreads - 1) / kAdjThreads, 3 * D.ninc);
+    const size_t nvals = (size_t)grid.x * grid.y * R * 2;
+    MOM_TRY(ensure_buffer(c, &c->adj_part, &c->adj_part_bytes, sizeof(double) * nvals));
+    a.part = (double *)c->adj_part;
+    MOM_TRY(adj_launch_pair(c, grid, a));
+    std::vector<double> h(nvals);
+    std::vector<int> inode(D.ninc);
+    MOM_CUDA(c, cudaMemcpyAsync(h.data(), a.part, sizeof(double) * nvals, cudaMemcpyDeviceToHost, c->stream));
+    MOM_CUDA(c, cudaMemcpyAsync(inode.data(), D.inc_node, sizeof(int) * D.ninc, cudaMemcpyDeviceToHost, c->stream));
+    MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int item = 0; item < 3 * D.ninc; item++) {
+      const int v = inode[item / 3], k = item % 3;
+      for (int o = 0; o < R; o++) {
+        double re = 0;
+        for (unsigned b = 0; b < grid.x; b++) re += h[(((size_t)item * grid.x + b) * R + o) * 2];
+        out[((size_t)o * total + off[d] + v) * 3 + k] -= re;
+      }
+    }
+  }
+  // Re(lambda^T dq) and the explicit term of sigma on the exterior surface
+  {
+    MOM_TRY(adjoint_setup(c, 0));
+    DomDev &D = c->dom[0];
+    std::vector<AdjSrc> hs(nsrc);
+    for (int s = 0; s < nsrc; s++) {
+      if (src[s].type != MOM_SRC_PW && src[s].type != MOM_SRC_PW_ELLIPTIC)
+        return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+      src_geometry(src[s], hs[s].dir, hs[s].pol);
+      hs[s].ph_re = src[s].phase_re;
+      hs[s].ph_im = src[s].phase_im;
+      hs[s].type = src[s].type;
+    }
+    const size_t items = 3 * (size_t)D.ninc;
+    const size_t b_src = ((sizeof(AdjSrc) * nsrc + 255) / 256) * 256, b_obj = 512,
+                 b_out = sizeof(double) * items * R;
+    MOM_TRY(ensure_buffer(c, &c->adj_part, &c->adj_part_bytes, b_src + 2 * b_obj + b_out));
+    char *base = (char *)c->adj_part;
+    AdjFaceArgs f;
+    f.t = topo_of(c, D);
+    f.n = c->n;
+    f.ninc = D.ninc;
+    f.inc_node = D.inc_node;
+    f.inc_face = D.inc_face;
+    f.R = R;
+    f.src = (const AdjSrc *)base;
+    f.obj_src = (const int *)(base + b_src);
+    f.obj_kind = (const int *)(base + b_src + b_obj);
+    f.lam = lam;
+    f.xv = xv;
+    f.k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
+    f.omega = omega;
+    f.cc = 2.0 / (kEps0 * kC0 * ri[0]);  // cs.f90:38
+    f.out = (double *)(base + b_src + 2 * b_obj);
+    MOM_CUDA(c, cudaMemcpyAsync((void *)f.src, hs.data(), sizeof(AdjSrc) * nsrc, cudaMemcpyHostToDevice, c->stream));
+    MOM_CUDA(c, cudaMemcpyAsync((void *)f.obj_src, obj_src, sizeof(int) * R, cudaMemcpyHostToDevice, c->stream));
+    MOM_CUDA(c, cudaMemcpyAsync((void *)f.obj_kind, obj_kind, sizeof(int) * R, cudaMemcpyHostToDevice, c->stream));
+    const int blocks = (int)((items + 63) / 64);
+    switch (c->nq) {
+      case 1: launch_adj_face<1>(blocks, c->stream, f); break;
+      case 3: launch_adj_face<3>(blocks, c->stream, f); break;
+      case 4: launch_adj_face<4>(blocks, c->stream, f); break;
+      case 7: launch_adj_face<7>(blocks, c->stream, f); break;
+      case 13: launch_adj_face<13>(blocks, c->stream, f); break;
+      default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+    }
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+    std::vector<double> h(items * R);
+    std::vector<int> inode(D.ninc);
+    MOM_CUDA(c, cudaMemcpyAsync(h.data(), f.out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    MOM_CUDA(c, cudaMemcpyAsync(inode.data(), D.inc_node, sizeof(int) * D.ninc, cudaMemcpyDeviceToHost, c->stream));
+    MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t item = 0; item < items; item++) {
+      const int v = inode[item / 3], k = (int)(item % 3);
+      for (int o = 0; o < R; o++) out[((size_t)o * total + off[0] + v) * 3 + k] += h[item * R + o];
+    }
+  }
   return MOM_OK;
 }
 

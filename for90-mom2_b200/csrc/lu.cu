@@ -577,7 +577,9 @@ struct TrsvArgs {
 
 // y = Inv * x for an nb x nb block and ns vectors held in shared memory;
 // several threads share one output and reduce through shared memory.
-__device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *xs, double2 *ys, double2 *red) {
+// tr: apply the transpose of the block.
+__device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *xs, double2 *ys, double2 *red,
+                            bool tr = false) {
   const int O = nb * ns;
   int parts = 1;
   while (parts * 2 * O <= (int)blockDim.x && parts < 16) parts *= 2;
@@ -590,7 +592,7 @@ __device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *x
       const int r = o % nb, sv = o / nb;
 #pragma unroll 4
       for (int j = part; j < nb; j += parts) {
-        const double2 iv = inv[r + (size_t)j * nb];
+        const double2 iv = tr ? inv[j + (size_t)r * nb] : inv[r + (size_t)j * nb];
         const double2 xv = xs[sv * nb + j];
         acc.x += iv.x * xv.x - iv.y * xv.y;
         acc.y += iv.x * xv.y + iv.y * xv.x;
@@ -631,14 +633,18 @@ __device__ __forceinline__ void upd_range(int pass, int64_t k0, int nb, int64_t 
 // NS right-hand sides in one cooperative launch: per diagonal block one
 // bounded grid barrier.  CTA c owns rows [c rpc, (c+1) rpc) for the updates;
 // the factor tile of the next block is fetched into shared memory with
-// cp.async while the CTA waits at the barrier.
-template <typename T, int NS>
+// cp.async while the CTA waits at the barrier.  TR solves A^T x = b instead:
+// forward with U^T, backward with L^T (unit), then x = P^T z; the factor
+// tile of block kb is then the block row kb of U (or L) to the right (left)
+// of the diagonal, stored row by row with a padded stride.
+template <typename T, int NS, bool TR>
 __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
   __shared__ double2 xs[8 * 64], ys[8 * 64], red[256];
-  extern __shared__ __align__(16) unsigned char tile_raw[];  // [nb][rpc] of T, then [nb][nb] double2
+  extern __shared__ __align__(16) unsigned char tile_raw[];  // tile of T, then [nb][nb] double2
   T *tile = reinterpret_cast<T *>(tile_raw);
-  double2 *sinv = reinterpret_cast<double2 *>(
-      tile_raw + (a.direct ? 0 : ((sizeof(T) * (size_t)a.nb * a.rpc + 15) / 16) * 16));
+  // tile element (row i, column j of the block): TR i * (nb + 1) + j, else j * rpc + i
+  const size_t tile_elems = TR ? (size_t)a.rpc * (a.nb + 1) : (size_t)a.nb * a.rpc;
+  double2 *sinv = reinterpret_cast<double2 *>(tile_raw + (a.direct ? 0 : ((sizeof(T) * tile_elems + 15) / 16) * 16));
   const T *M = reinterpret_cast<const T *>(a.M);
   const int64_t n = a.n, lda = a.lda;
   const int nb = a.nb, nblk = (int)(n / nb), rpc = a.rpc;
@@ -653,17 +659,26 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
     int64_t lo, hi;
     upd_range(pass, k0, nb, r0, r1, &lo, &hi);
     const int cnt = (a.direct || hi <= lo) ? 0 : (int)(hi - lo);
-    for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
-      const int i = idx % cnt, j = idx / cnt;
-      cp_async(tile + (size_t)j * rpc + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
+    if (TR) {
+      // block row: factor entries (k0 + j, lo + i), contiguous in j
+      for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
+        const int j = idx % nb, i = idx / nb;
+        cp_async(tile + (size_t)i * (nb + 1) + j, M + (k0 + j) + (lo + i) * lda, sizeof(T) == 16);
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
+        const int i = idx % cnt, j = idx / cnt;
+        cp_async(tile + (size_t)j * rpc + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
+      }
     }
-    const double2 *ib = a.inv + ((size_t)kb * 2 + pass) * nb * nb;
+    // pass 0 applies inv(L) (or inv(U)^T), pass 1 inv(U) (or inv(L)^T)
+    const double2 *ib = a.inv + ((size_t)kb * 2 + (TR ? 1 - pass : pass)) * nb * nb;
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) cp_async(sinv + idx, ib + idx, 1);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  // Y = P X
+  // Y = P X (TR: Y = X)
   for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-    for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + a.perm[i]];
+    for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + (TR ? i : a.perm[i])];
   prefetch(0, 0);
   if (!flag_barrier(a.bar, a.P, ++step, a.timeout)) return;
   for (int pass = 0; pass < 2; pass++) {
@@ -678,7 +693,7 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
       }
       cp_async_wait_all();
       __syncthreads();
-      block_apply(sinv, nb, ns, xs, ys, red);
+      block_apply(sinv, nb, ns, xs, ys, red, TR);
       // owners of block kb's rows store the solved block
       for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
         const int j = idx % nb, sv = idx / nb;
@@ -691,8 +706,9 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
         double2 acc[NS];
 #pragma unroll
         for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
-        const T *mp = a.direct ? M + i + k0 * lda : tile + (i - lo);
-        const int64_t mstride = a.direct ? lda : rpc;
+        const T *mp = TR ? (a.direct ? M + k0 + i * lda : tile + (size_t)(i - lo) * (nb + 1))
+                         : (a.direct ? M + i + k0 * lda : tile + (i - lo));
+        const int64_t mstride = TR ? 1 : (a.direct ? lda : rpc);
 #pragma unroll 8
         for (int j = 0; j < nb; j++) {
           const double2 m = ld2(mp + (size_t)j * mstride);
@@ -719,9 +735,9 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
     }
   }
   cp_async_wait_all();
-  // the solution is in Y; return it in X
+  // the solution is in Y; return it in X (TR: X = P^T Y)
   for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + i] = a.Y[(size_t)s * n + i];
+    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + (TR ? a.perm[i] : i)] = a.Y[(size_t)s * n + i];
 }
 
 constexpr int kGemvRows = 256;
@@ -756,6 +772,38 @@ __global__ void __launch_bounds__(kGemvRows) gemv_partial_kernel(const double2 *
   }
 #pragma unroll
   for (int s = 0; s < NS; s++) partial[((size_t)blockIdx.y * NS + s) * n + i] = acc[s];
+}
+
+// Y[s][j] = sum_i A[i, j] x_s[i] (FP64 matrix, transposed product): one
+// warp per column, lanes stride down the column.
+template <int NS>
+__global__ void __launch_bounds__(256) gemv_t_kernel(const double2 *A, int64_t lda, int64_t n, const double2 *X,
+                                                     int64_t ldx, double2 *Y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const double2 *col = A + j * lda;
+  double2 acc[NS];
+#pragma unroll
+  for (int s = 0; s < NS; s++) acc[s] = make_double2(0, 0);
+  for (int64_t i = lane; i < n; i += 32) {
+    const double2 m = __ldcs(col + i);
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+      const double2 x = X[(size_t)s * ldx + i];
+      acc[s].x += m.x * x.x - m.y * x.y;
+      acc[s].y += m.x * x.y + m.y * x.x;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      acc[s].x += __shfl_xor_sync(0xffffffffu, acc[s].x, o);
+      acc[s].y += __shfl_xor_sync(0xffffffffu, acc[s].y, o);
+    }
+    if (lane == 0) Y[(size_t)s * n + j] = acc[s];
+  }
 }
 
 // R = B - sum of partials; per-column squared norms of R into rn (block partials).
@@ -1045,8 +1093,9 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
   return MOM_OK;
 }
 
-// X (n x nrhs, ld n) <- A^{-1} X with the factors in place; Y is scratch.
-template <typename T>
+// X (n x nrhs, ld n) <- A^{-1} X (TR: A^{-T} X) with the factors in place;
+// Y is scratch.
+template <typename T, bool TR = false>
 int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
   const int64_t n = c->n;
   const int nb = c->nb;
@@ -1073,11 +1122,12 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
     ta.timeout = c->dinfo + 1;
     MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned) * 256, c->stream));
     void *args[] = {&ta};
-    void *fn = ns == 1 ? (void *)trsv_coop_kernel<T, 1>
-               : ns == 2 ? (void *)trsv_coop_kernel<T, 2>
-               : ns == 4 ? (void *)trsv_coop_kernel<T, 4>
-                         : (void *)trsv_coop_kernel<T, 8>;
-    size_t tile = ((sizeof(T) * (size_t)nb * rpc + 15) / 16) * 16 + sizeof(double2) * nb * nb;
+    void *fn = ns == 1 ? (void *)trsv_coop_kernel<T, 1, TR>
+               : ns == 2 ? (void *)trsv_coop_kernel<T, 2, TR>
+               : ns == 4 ? (void *)trsv_coop_kernel<T, 4, TR>
+                         : (void *)trsv_coop_kernel<T, 8, TR>;
+    const size_t elems = TR ? (size_t)rpc * (nb + 1) : (size_t)nb * rpc;
+    size_t tile = ((sizeof(T) * elems + 15) / 16) * 16 + sizeof(double2) * nb * nb;
     ta.direct = 0;
     if (tile > 200 * 1024) {
       ta.direct = 1;
@@ -1113,14 +1163,22 @@ int lu_init_kernels(Ctx *c) {
   MOM_CUDA(c, set_smem(diag_inv_kernel<double2>));
   MOM_CUDA(c, set_smem(diag_inv_kernel<float2>));
   MOM_CUDA(c, set_smem(compose_pivots_kernel));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8, false>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4, true>));
+  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8, true>));
   return MOM_OK;
 }
 
@@ -1132,16 +1190,20 @@ int lu_factor(Ctx *c, int precision) {
   return lu_factor_t<double2>(c, c->A, precision);
 }
 
-// Solve for the nsrc right-hand sides in c->B into c->X.
-int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
+// Solve A X = B (trans: A^T X = B) for nrhs columns (ld n) with the factors
+// of `precision` in place.  FP64: one triangular solve.  Mixed: x = 0,
+// r = b; repeat d = LU32^{-1} r, x += d, r = b - A x with the FP64 matrix
+// until max_s ||r_s|| / ||b_s|| <= tol.
+int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, int nrhs, double tol, int maxit,
+                int *iters) {
   const int64_t n = c->n;
-  const int nrhs = c->nsrc;
   if (c->factored != precision) return fail(c, MOM_ERR_STATE, "matrix not factored in this precision");
   const size_t vec = sizeof(double2) * (size_t)n * nrhs;
   if (precision == MOM_PREC_FP64) {
-    MOM_CUDA(c, cudaMemcpyAsync(c->X, c->B, vec, cudaMemcpyDeviceToDevice, c->stream));
+    if (X != B) MOM_CUDA(c, cudaMemcpyAsync(X, B, vec, cudaMemcpyDeviceToDevice, c->stream));
     MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, vec));
-    MOM_TRY(getrs_t<double2>(c, c->A, c->X, (double2 *)c->ws, nrhs));
+    if (trans) MOM_TRY((getrs_t<double2, true>(c, c->A, X, (double2 *)c->ws, nrhs)));
+    else MOM_TRY((getrs_t<double2, false>(c, c->A, X, (double2 *)c->ws, nrhs)));
     if (iters) *iters = 0;
     int tmo = 0;
     MOM_CUDA(c, cudaMemcpyAsync(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1149,7 +1211,6 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
     if (tmo) return fail(c, MOM_ERR_TIMEOUT, "triangular solve barrier timed out");
     return MOM_OK;
   }
-  // Mixed: x = 0, r = b; repeat d = LU32^{-1} r, x += d, r = b - A x.
   const int nchunk = (int)((n + kGemvCols - 1) / kGemvCols);
   const int rblocks = (int)((n + 255) / 256);
   const size_t off_r = 0, off_d = vec, off_y = 2 * vec, off_p = 3 * vec;
@@ -1162,9 +1223,9 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
   double *rn2 = (double *)(ws + off_n);
   // ||b|| per column
   std::vector<double> bn(nrhs), h(rblocks * (size_t)nrhs);
-  MOM_CUDA(c, cudaMemsetAsync(c->X, 0, vec, c->stream));
-  MOM_CUDA(c, cudaMemcpyAsync(R, c->B, vec, cudaMemcpyDeviceToDevice, c->stream));
-  residual_kernel<<<dim3(rblocks, nrhs), 256, 0, c->stream>>>(c->B, n, Pp, 0, n, nrhs, R, n, rn2);
+  MOM_CUDA(c, cudaMemsetAsync(X, 0, vec, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(R, B, vec, cudaMemcpyDeviceToDevice, c->stream));
+  residual_kernel<<<dim3(rblocks, nrhs), 256, 0, c->stream>>>(B, n, Pp, 0, n, nrhs, R, n, rn2);
   c->launches++;
   MOM_CUDA(c, cudaMemcpyAsync(h.data(), rn2, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1177,20 +1238,31 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
   double worst = 1.0;
   for (it = 1; it <= maxit; it++) {
     MOM_CUDA(c, cudaMemcpyAsync(Dv, R, vec, cudaMemcpyDeviceToDevice, c->stream));
-    MOM_TRY(getrs_t<float2>(c, c->A32, Dv, Yv, nrhs));
-    axpy_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(c->X, Dv, (int64_t)n * nrhs);
+    if (trans) MOM_TRY((getrs_t<float2, true>(c, c->A32, Dv, Yv, nrhs)));
+    else MOM_TRY((getrs_t<float2, false>(c, c->A32, Dv, Yv, nrhs)));
+    axpy_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(X, Dv, (int64_t)n * nrhs);
     c->launches++;
     ProfScope pr(c, kProfResidual);
     for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
       ns = 8;
       while (ns > nrhs - s0) ns >>= 1;
-      const dim3 gg(rblocks, nchunk);
-      const double2 *xs0 = c->X + (size_t)s0 * n;
-      if (ns == 1) gemv_partial_kernel<1><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
-      else if (ns == 2) gemv_partial_kernel<2><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
-      else if (ns == 4) gemv_partial_kernel<4><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
-      else gemv_partial_kernel<8><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
-      residual_kernel<<<dim3(rblocks, ns), 256, 0, c->stream>>>(c->B + (size_t)s0 * n, n, Pp, nchunk, n, ns,
+      const double2 *xs0 = X + (size_t)s0 * n;
+      int nch = nchunk;
+      if (trans) {
+        const unsigned gb = (unsigned)((n + 7) / 8);
+        if (ns == 1) gemv_t_kernel<1><<<gb, 256, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else if (ns == 2) gemv_t_kernel<2><<<gb, 256, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else if (ns == 4) gemv_t_kernel<4><<<gb, 256, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else gemv_t_kernel<8><<<gb, 256, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        nch = 1;
+      } else {
+        const dim3 gg(rblocks, nchunk);
+        if (ns == 1) gemv_partial_kernel<1><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else if (ns == 2) gemv_partial_kernel<2><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else if (ns == 4) gemv_partial_kernel<4><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+        else gemv_partial_kernel<8><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+      }
+      residual_kernel<<<dim3(rblocks, ns), 256, 0, c->stream>>>(B + (size_t)s0 * n, n, Pp, nch, n, ns,
                                                                 R + (size_t)s0 * n, n, rn2 + (size_t)s0 * rblocks);
       c->launches += 2;
     }
@@ -1215,6 +1287,11 @@ int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
     return fail(c, MOM_ERR_NOCONV, buf);
   }
   return MOM_OK;
+}
+
+// Solve for the nsrc right-hand sides in c->B into c->X.
+int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters) {
+  return lu_solve_ex(c, precision, 0, c->B, c->X, c->nsrc, tol, maxit, iters);
 }
 
 }  // namespace mom

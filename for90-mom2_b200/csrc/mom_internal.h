@@ -50,6 +50,17 @@ struct DomDev {
   std::vector<double> h_cp, h_qrel, h_qabs, h_area, h_nrm, h_mu, h_sl;
   std::vector<double> h_fv, h_fs, h_fm, h_bn;  // [F][3][3]: vertices, s(:,e), m(:,e), free vertex of e
   std::vector<int> h_hpar, h_eh, h_epar;
+  // Topology for the geometry derivatives of the adjoint (uploaded on first use).
+  int nnodes = 0;
+  std::vector<double> h_nodes;                   // [nnodes][3]
+  std::vector<int> h_fnode, h_fea, h_feb, h_fbn;  // [F][3] face vertices; ends and free vertex of local edge e
+  std::vector<double> h_fsign;                   // [F][3] +1 / -1
+  bool adj_ready = false;
+  double *nodes = nullptr, *fsign = nullptr;
+  int *fnode = nullptr, *fea = nullptr, *feb = nullptr, *fbn = nullptr;
+  unsigned *near_bits = nullptr;                 // [F*F] bits
+  int ninc = 0;                                  // (vertex, face) incidences, by vertex
+  int *inc_node = nullptr, *inc_face = nullptr;
 };
 
 struct Ctx {
@@ -123,6 +134,15 @@ struct Ctx {
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)
   double tc_flops = 0;     // FLOP executed by the tensor-core LU updates since creation
 
+  // Adjoint buffers: objective gradients, adjoint currents, forward currents,
+  // block partial sums, and the dense objective matrix of the mean gradient.
+  void *adj = nullptr;
+  size_t adj_bytes = 0;
+  void *adj_part = nullptr;
+  size_t adj_part_bytes = 0;
+  void *adjW = nullptr;
+  size_t adjW_bytes = 0;
+
   // Host-side staging (pinned)
   double *pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -175,6 +195,8 @@ int assemble(Ctx *c, double omega, const double *ri, int precision);
 int lu_init_kernels(Ctx *c);
 int lu_factor(Ctx *c, int precision);
 int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
+int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, int nrhs, double tol, int maxit,
+                int *iters);
 
 // tc_gemm.cu: C -= L U (complex FP32) on the tensor cores, 3xTF32
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
@@ -188,5 +210,20 @@ int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, co
                    const double2 *xdev, int64_t ldx, double *csca, double *cabs);
 int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
               double *rcs);
+int cs_gradient(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src, const double2 *xdev,
+                int64_t ldx, double2 *G);
+void src_geometry(const mom_src &s, double dir[3], double pol[3]);
+
+// adjoint (assemble.cu): derivative contractions.  Objective o pairs the
+// adjoint currents lam[o] with the forward currents xv[o] (n each); R = 0
+// uses the dense W(r, c) = sum lam[r] x[c] instead.
+// adjoint_eps: t'_o = lam_o^T (dA / d eps_d) x_o (complex) into out[o][2].
+int adjoint_eps(Ctx *c, double omega, const double *ri, int d, int R, const double2 *lam, const double2 *xv,
+                const double2 *W, double *out);
+// adjoint_nodes: d sigma_o / d(node coordinates) of every domain, out
+// [R][sum of the domains' nodes][3]; obj_src / obj_kind give the source and
+// the cross section (0 ext, 1 abs) of each objective.
+int adjoint_nodes(Ctx *c, double omega, const double *ri, int R, const double2 *lam, const double2 *xv,
+                  const int *obj_src, const int *obj_kind, int nsrc, const mom_src *src, double *out);
 
 }  // namespace mom

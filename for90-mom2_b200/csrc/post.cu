@@ -17,6 +17,21 @@ namespace mom {
 
 namespace {
 
+}  // namespace
+
+// get_dir / get_pol (aux.f90:245-261), evaluated on the host in FP64.
+void src_geometry(const mom_src &s, double dir[3], double pol[3]) {
+  const double th = s.theta, ph = s.phi, ps = (s.type == MOM_SRC_PW) ? s.psi : 0.0;
+  dir[0] = sin(th) * cos(ph);
+  dir[1] = sin(th) * sin(ph);
+  dir[2] = cos(th);
+  pol[0] = cos(ps) * sin(ph) - sin(ps) * cos(th) * cos(ph);
+  pol[1] = -cos(ps) * cos(ph) - sin(ps) * cos(th) * sin(ph);
+  pol[2] = sin(ps) * sin(th);
+}
+
+namespace {
+
 struct SrcDev {
   double dir[3], pol[3];
   double ph_re, ph_im;  // pw_elliptic phase
@@ -229,6 +244,114 @@ __global__ void __launch_bounds__(256) cs_kernel(CsArgs a) {
   }
 }
 
+// d sigma / dx of cs_prtsrf, d sigma = Re(G^T dx), per face and source:
+// with E = sum_p beta_p (n x f_p) and H = -sum_p alpha_p (n x f_p),
+// d/dbeta_p 0.5 Re[(E x H*).n] = 0.5 (n x f_p) x H* . n and
+// d/dalpha_p = -0.5 E* x (n x f_p) . n; sigma_abs uses the total fields,
+// sigma_sca the scattered ones.  Output per half: [s][F][3][ext alpha,
+// ext beta, abs alpha, abs beta].
+__global__ void __launch_bounds__(128) cs_grad_half_kernel(CsArgs a, double cc, double2 *half) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (f >= a.F) return;
+  const SrcDev S = a.src[s];
+  const double2 *x = a.x + (size_t)s * a.ldx;
+  const double An = a.area[f];
+  const double *nor = a.nrm + 3 * f;
+  const Z nc[3] = {{nor[0], 0}, {nor[1], 0}, {nor[2], 0}};
+  Z al[3], be[3];
+  for (int p = 0; p < 3; p++) {
+    const int idx = a.hpar[3 * f + p];
+    al[p] = {x[idx].x, x[idx].y};
+    be[p] = {x[idx + a.N].x, x[idx + a.N].y};
+  }
+  Z g[3][4];
+  for (int p = 0; p < 3; p++)
+    for (int k = 0; k < 4; k++) g[p][k] = {0, 0};
+  for (int t = 0; t < a.nq; t++) {
+    const double *pt = a.qabs + ((size_t)f * a.nq + t) * 3;
+    double fn[3][3];
+    Z Et[3] = {{0, 0}, {0, 0}, {0, 0}}, Ht[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int p = 0; p < 3; p++) {
+      const double c0 = a.sl[3 * f + p] / (2.0 * An);
+      double fr[3];
+      for (int i = 0; i < 3; i++) fr[i] = c0 * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * p + i]));
+      fn[p][0] = nor[1] * fr[2] - nor[2] * fr[1];
+      fn[p][1] = nor[2] * fr[0] - nor[0] * fr[2];
+      fn[p][2] = nor[0] * fr[1] - nor[1] * fr[0];
+      for (int i = 0; i < 3; i++) {
+        Ht[i] = zsub(Ht[i], zscale(al[p], fn[p][i]));
+        Et[i] = zadd(Et[i], zscale(be[p], fn[p][i]));
+      }
+    }
+    Z einc[3], hinc[3], t1[3], Eti[3], Hti[3], Es[3], Hs[3];
+    src_fields(S, a.k, a.omega, pt, einc, hinc);
+    zcross(nc, hinc, t1);
+    zcross(t1, nc, Hti);
+    zcross(nc, einc, t1);
+    zcross(t1, nc, Eti);
+    for (int i = 0; i < 3; i++) {
+      Hs[i] = zsub(Ht[i], Hti[i]);
+      Es[i] = zsub(Et[i], Eti[i]);
+    }
+    const double w = 0.5 * a.w[t] * An;
+    for (int p = 0; p < 3; p++) {
+      const Z fz[3] = {{fn[p][0], 0}, {fn[p][1], 0}, {fn[p][2], 0}};
+      Z hc[3], ec[3], cr[3];
+      // total fields
+      for (int i = 0; i < 3; i++) {
+        hc[i] = zconj(Ht[i]);
+        ec[i] = zconj(Et[i]);
+      }
+      zcross(fz, hc, cr);
+      const Z gbt = zadd(zadd(zscale(cr[0], nor[0]), zscale(cr[1], nor[1])), zscale(cr[2], nor[2]));
+      zcross(ec, fz, cr);
+      const Z gat = zscale(zadd(zadd(zscale(cr[0], nor[0]), zscale(cr[1], nor[1])), zscale(cr[2], nor[2])), -1.0);
+      // scattered fields
+      for (int i = 0; i < 3; i++) {
+        hc[i] = zconj(Hs[i]);
+        ec[i] = zconj(Es[i]);
+      }
+      zcross(fz, hc, cr);
+      const Z gbs = zadd(zadd(zscale(cr[0], nor[0]), zscale(cr[1], nor[1])), zscale(cr[2], nor[2]));
+      zcross(ec, fz, cr);
+      const Z gas = zscale(zadd(zadd(zscale(cr[0], nor[0]), zscale(cr[1], nor[1])), zscale(cr[2], nor[2])), -1.0);
+      // sigma_ext = cc (I_sca - I_tot), sigma_abs = -cc I_tot
+      g[p][0] = zadd(g[p][0], zscale(zsub(gas, gat), cc * w));
+      g[p][1] = zadd(g[p][1], zscale(zsub(gbs, gbt), cc * w));
+      g[p][2] = zadd(g[p][2], zscale(gat, -cc * w));
+      g[p][3] = zadd(g[p][3], zscale(gbt, -cc * w));
+    }
+  }
+  double2 *o = half + (((size_t)s * a.F + f) * 3) * 4;
+  for (int p = 0; p < 3; p++)
+    for (int k = 0; k < 4; k++) o[4 * p + k] = make_double2(g[p][k].re, g[p][k].im);
+}
+
+// G[2 s] (ext) and G[2 s + 1] (abs): sums of the halves of each edge.
+__global__ void cs_grad_edge_kernel(int Nd, int F, int N, int64_t n, const int *eh, const int *epar,
+                                    const double2 *half, double2 *G) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (e >= Nd) return;
+  double2 v[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  for (int i = 0; i < 2; i++) {
+    const int h = eh[2 * e + i];
+    if (h < 0) continue;
+    const double2 *src = half + (((size_t)s * F) * 3 + h) * 4;
+    for (int k = 0; k < 4; k++) {
+      v[k].x += src[k].x;
+      v[k].y += src[k].y;
+    }
+  }
+  const int64_t r = epar[e];
+  double2 *ge = G + (size_t)(2 * s) * n, *ga = G + (size_t)(2 * s + 1) * n;
+  ge[r] = v[0];
+  ge[r + N] = v[1];
+  ga[r] = v[2];
+  ga[r + N] = v[3];
+}
+
 struct FfArgs {
   double w[kMaxQ];
   int F, nq, N;
@@ -332,14 +455,7 @@ __global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const doub
 }
 
 void make_src(const mom_src &s, SrcDev &d) {
-  // get_dir / get_pol (aux.f90:245-261), evaluated on the host in FP64.
-  const double th = s.theta, ph = s.phi, ps = (s.type == MOM_SRC_PW) ? s.psi : 0.0;
-  d.dir[0] = sin(th) * cos(ph);
-  d.dir[1] = sin(th) * sin(ph);
-  d.dir[2] = cos(th);
-  d.pol[0] = cos(ps) * sin(ph) - sin(ps) * cos(th) * cos(ph);
-  d.pol[1] = -cos(ps) * cos(ph) - sin(ps) * cos(th) * sin(ph);
-  d.pol[2] = sin(ps) * sin(th);
+  src_geometry(s, d.dir, d.pol);
   d.ph_re = s.phase_re;
   d.ph_im = s.phase_im;
   d.type = s.type;
@@ -441,6 +557,45 @@ int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, co
     cabs[s] = -cc * ab;
     csca[s] = cc * sc;
   }
+  return MOM_OK;
+}
+
+// d sigma_ext / dx and d sigma_abs / dx on domain dom for nsrc sources into
+// G (2 nsrc columns of length n, zero outside the domain's unknowns).
+int cs_gradient(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src, const double2 *xdev,
+                int64_t ldx, double2 *G) {
+  const DomDev &D = c->dom[dom];
+  const size_t src_bytes = ((sizeof(SrcDev) * nsrc + 255) / 256) * 256;
+  const size_t half_bytes = sizeof(double2) * 12 * (size_t)D.F * nsrc;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, src_bytes + half_bytes));
+  SrcDev *dsrc = nullptr;
+  MOM_TRY(upload_sources(c, nsrc, src, &dsrc));
+  CsArgs a;
+  for (int i = 0; i < kMaxQ; i++) a.w[i] = c->qw[i];
+  a.F = D.F;
+  a.nq = c->nq;
+  a.N = c->N;
+  a.qabs = D.qabs;
+  a.area = D.area;
+  a.sl = D.sl;
+  a.mu = D.mu;
+  a.cp = D.cp;
+  a.nrm = D.nrm;
+  a.hpar = D.hpar;
+  a.src = dsrc;
+  a.x = xdev;
+  a.ldx = ldx;
+  a.k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
+  a.omega = omega;
+  a.part = nullptr;
+  double2 *half = reinterpret_cast<double2 *>((char *)c->ws + src_bytes);
+  const double cc = 2.0 / (kEps0 * kC0 * ri[0]);  // cs.f90:38
+  MOM_CUDA(c, cudaMemsetAsync(G, 0, sizeof(double2) * (size_t)c->n * 2 * nsrc, c->stream));
+  cs_grad_half_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(a, cc, half);
+  cs_grad_edge_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(D.Nd, D.F, c->N, c->n, D.eh, D.epar,
+                                                                             half, G);
+  c->launches += 2;
+  MOM_CUDA(c, cudaGetLastError());
   return MOM_OK;
 }
 

@@ -333,6 +333,15 @@ int mom_problem_domain(const mom_problem *p, int32_t dom, mom_mesh *out) {
   return MOM_OK;
 }
 
+int mom_problem_node_parent(const mom_problem *p, int32_t dom, int32_t *parent) {
+  if (!p || !parent) return MOM_ERR_ARG;
+  if (!p->finalized) return MOM_ERR_STATE;
+  if (dom < 0 || dom >= (int)p->dom.size()) return MOM_ERR_ARG;
+  const Mesh &m = p->dom[dom];
+  for (int i = 0; i < m.nnodes; i++) parent[i] = m.node_parent[i];
+  return MOM_OK;
+}
+
 // Triangle rules of quad.f90 (tri_quad_data, quad.f90:277-315).  tri_gl13
 // (quad.f90:115-171) and the tri_gl3 nodes (102-113) are default-real
 // literals in the reference, i.e. rounded to single precision; the others

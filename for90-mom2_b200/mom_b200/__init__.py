@@ -45,6 +45,7 @@ EXPORTS = [
     "mom_gpu_selftest_cgemm", "mom_problem_create", "mom_problem_destroy", "mom_problem_load_gmsh",
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
+    "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
 ]
 
 
@@ -97,6 +98,12 @@ def lib():
     L.mom_gpu_rcs.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, C.c_int32, C.c_int32, dp]
     L.mom_gpu_cross_sections_noalloc.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp,
                                                  C.c_int64, dp, dp]
+    L.mom_gpu_adjoint.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32, C.c_double,
+                                  C.c_int32, vp, vp, ip]
+    L.mom_gpu_adjoint_mean_eps.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32,
+                                           C.c_double, C.c_int32, dp, ip]
+    L.mom_gpu_domain_nodes.argtypes = [vp, C.c_int32]
+    L.mom_problem_node_parent.argtypes = [vp, C.c_int32, ip]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
@@ -252,6 +259,18 @@ class Problem:
                     edge_parent=arr(m.edge_parent, m.nedges, 1, np.int32).ravel())
 
 
+    def node_parent(self, d):
+        """Master-mesh node index of each submesh node of domain d."""
+        n = self.domain(d)["nodes"].shape[0]
+        out = np.zeros(n, dtype=np.int32)
+        _check(lib().mom_problem_node_parent(self.h, d, out.ctypes.data_as(C.POINTER(C.c_int32))),
+               what="node_parent")
+        return out
+
+    def master_nodes(self):
+        return self.domain(-1)["nodes"].shape[0]
+
+
 class Solver:
     """One CUDA context of the PMCHWT library on ``device``."""
 
@@ -332,6 +351,41 @@ class Solver:
         self._ck(lib().mom_gpu_cross_sections(self.h, dom, omega, _dp(r), ns, arr, xp, 2 * self.N, _dp(csca),
                                               _dp(cabs)), "cross_sections")
         return csca, cabs
+
+    def adjoint(self, omega, ri, srcs, precision, eps_dom=None, nodes=False, tol=1e-12, maxit=30):
+        """Adjoint gradients of sigma_ext and sigma_abs for the sources of the last solve.
+
+        Returns a dict: ``deps`` [nsrc][2 (ext, abs)][2 (d/dRe eps, d/dIm eps)] of interior
+        domain eps_dom, and with nodes=True ``dnodes``: a list over domains of
+        [nsrc][2][nnodes_d][3] arrays (d sigma / d node coordinates, per metre)."""
+        arr, ns = _srcs(srcs)
+        r = _ri(ri)
+        deps = np.zeros((ns, 2, 2)) if eps_dom is not None else None
+        counts = [lib().mom_gpu_domain_nodes(self.h, d) for d in range(self.ndom)]
+        total = sum(counts)
+        dn = np.zeros((ns, 2, total, 3)) if nodes else None
+        it = C.c_int32()
+        self._ck(lib().mom_gpu_adjoint(self.h, precision, omega, _dp(r), ns, arr,
+                                       -1 if eps_dom is None else eps_dom, 1e-12 if tol is None else tol, maxit,
+                                       deps.ctypes.data if deps is not None else None,
+                                       dn.ctypes.data if dn is not None else None, C.byref(it)), "adjoint")
+        out = {"iters": it.value}
+        if deps is not None:
+            out["deps"] = deps
+        if dn is not None:
+            offs = np.cumsum([0] + counts)
+            out["dnodes"] = [dn[:, :, offs[d]:offs[d + 1], :] for d in range(self.ndom)]
+        return out
+
+    def adjoint_mean_eps(self, omega, ri, srcs, precision, eps_dom, tol=1e-12, maxit=30):
+        """d(mean sigma_ext, mean sigma_abs) / d(Re eps, Im eps) of domain eps_dom: [2][2]."""
+        arr, ns = _srcs(srcs)
+        r = _ri(ri)
+        out = np.zeros((2, 2))
+        it = C.c_int32()
+        self._ck(lib().mom_gpu_adjoint_mean_eps(self.h, precision, omega, _dp(r), ns, arr, eps_dom, tol, maxit,
+                                                _dp(out), C.byref(it)), "adjoint_mean_eps")
+        return out
 
     def cross_sections_noalloc(self, omega, ri, srcs, x_dev, ldx, dom=0):
         """Cross sections through the allocation-free entry point: x_dev is a device

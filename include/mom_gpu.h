@@ -143,6 +143,33 @@ int mom_gpu_cross_sections_noalloc(mom_ctx *ctx, int32_t dom, double omega, cons
                                    const mom_src *src, const void *x_dev, int64_t ldx, double *csca,
                                    double *cabs);
 
+/* ---- Adjoint gradients (no counterpart in the reference) ----
+ * After mom_gpu_solve for the same sources (and the same omega and ri), the
+ * factors of `precision` are reused for one transposed solve A^T lambda = G
+ * per objective, G = d sigma / dx of cs_prtsrf on domain 0 (cs.f90:14-104).
+ * Derivatives of the system matrix are recomputed face pair by face pair in
+ * dual arithmetic and contracted with lambda and x (never stored).
+ * Objectives per source s: o = 2 s (sigma_ext), 2 s + 1 (sigma_abs).
+ *   deps   (or NULL) [2 nsrc][2]: d sigma_o / d Re(eps), d / d Im(eps) of the
+ *          permittivity eps = ri[eps_dom]^2 of interior domain eps_dom;
+ *   dnodes (or NULL) [2 nsrc][sum_d nnodes_d][3]: d sigma_o / d(node
+ *          coordinates, metres) of each domain's submesh nodes, domains
+ *          concatenated in order (mom_gpu_domain_nodes); a master-mesh
+ *          vertex shared by several domains sums its entries
+ *          (mom_problem_node_parent).
+ * The near-pair classification stays that of the unperturbed mesh.  1 to 4
+ * sources; tol / maxit drive the refinement of a mixed transposed solve. */
+int mom_gpu_adjoint(mom_ctx *ctx, int32_t precision, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                    int32_t eps_dom, double tol, int32_t maxit, double *deps, double *dnodes, int32_t *iters);
+/* d(mean over the nsrc sources of sigma_ext, sigma_abs) / d(Re eps, Im eps)
+ * of interior domain eps_dom: dmean[2][2]; any nsrc.  Uses an n x n complex
+ * FP64 work matrix W = (1/nsrc) sum_s lambda_s x_s^T. */
+int mom_gpu_adjoint_mean_eps(mom_ctx *ctx, int32_t precision, double omega, const double *ri, int32_t nsrc,
+                             const mom_src *src, int32_t eps_dom, double tol, int32_t maxit, double *dmean,
+                             int32_t *iters);
+/* Number of submesh nodes of domain dom, -1 without a problem. */
+int32_t mom_gpu_domain_nodes(mom_ctx *ctx, int32_t dom);
+
 /* Diagnostics: C -= L U for host complex64 arrays (column-major; L m x k,
  * U k x nc, C m x nc; m a multiple of 64, k of 16) through the tensor-core
  * kernel that performs the trailing updates of the mixed-precision LU. */
@@ -192,6 +219,8 @@ int32_t mom_problem_nedges(const mom_problem *p);
 int32_t mom_problem_ndom(const mom_problem *p);
 /* Flattened view of domain dom (valid until the problem is destroyed). */
 int mom_problem_domain(const mom_problem *p, int32_t dom, mom_mesh *out);
+/* Master-mesh node of each submesh node of domain dom: parent[nnodes]. */
+int mom_problem_node_parent(const mom_problem *p, int32_t dom, int32_t *parent);
 /* Named triangle rule of quad.f90 ("tri_gl1", "tri_gl3", "tri_gl4",
  * "tri_gl7", "tri_gl13"): qw[13], qnodes[13][3]; returns nq or < 0. */
 int32_t mom_tri_rule(const char *name, double *qw, double *qnodes);
