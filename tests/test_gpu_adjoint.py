@@ -122,3 +122,33 @@ def test_vertex_gradient_matches_fd(solver, prec):
         fd = (sp - sm) / (2 * h)
         for o in range(2):
             assert abs(gm[o, v, k] - fd[o]) <= 1e-5 * scale[o], (prec, v, k, o, gm[o, v, k], fd[o])
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.MIXED])
+def test_matches_oracle_finite_differences(solver, prec):
+    """Against central differences of the oracle's own cross sections
+    (tests/golden/adjoint_fd_s1.json, made by make_adjoint_fd.py)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "adjoint_fd_s1.json")) as fh:
+        ref = json.load(fh)
+    geo = sphere(1, perturbed=True)
+    nodes, faces, ids, doms = geo
+    eps = complex(*ref["eps"])
+    ri = ri_of([eps])
+    s = sigmas(solver, geo, ri, prec)[0]
+    assert np.allclose(s, ref["sigma"], rtol=1e-9 if prec == M.FP64 else 1e-6)
+    out = solver.adjoint(M.omega_of(WL), ri, SRC, prec, eps_dom=1, nodes=True)
+    g = out["deps"][0]
+    for j in range(2):
+        for k in range(2):
+            fd = ref["deps"][j][k]
+            assert abs(g[k, j] - fd) <= 1e-5 * abs(fd), (j, k, g[k, j], fd)
+    prob = M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms)
+    gm = np.zeros((2, len(nodes), 3))
+    for d, gd in enumerate(out["dnodes"]):
+        np.add.at(gm, (slice(None), prob.node_parent(d)), gd[0] * 1e-9)
+    scale = np.abs(gm).max(axis=(1, 2))
+    for v, k, fd in ref["dverts"]:
+        for o in range(2):
+            assert abs(gm[o, v, k] - fd[o]) <= 1e-5 * scale[o], (v, k, o, gm[o, v, k], fd[o])

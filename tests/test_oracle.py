@@ -155,3 +155,27 @@ def test_oracle_regression_fixture(p1):
     sca, ab = p1.cs(om, ri[0], x, src)
     assert abs(sca - g["csca"]) <= 1e-10 * abs(g["csca"])
     assert abs(ab - g["cabs"]) <= 1e-10 * abs(g["cabs"])
+
+
+def test_adjoint_fd_fixture_is_the_oracles():
+    """tests/golden/adjoint_fd_s1.json holds central differences of this oracle's
+    cross sections: recompute sigma and the d/dRe(eps) entry."""
+    with open(os.path.join(HERE, "golden", "adjoint_fd_s1.json")) as fh:
+        g = json.load(fh)
+    nodes, faces = meshgen.perturbed_sphere(1, 50.0, lmax=4, sigma=0.03, seed=4)
+    ids = np.ones(len(faces), int)
+    src = dict(type="pw", theta=0.0, phi=90 * O.DEGTORAD, psi=0.0)
+    om = O.omega_of(g["wavelength"])
+    eps = complex(*g["eps"])
+
+    def sig(e):
+        P = O.OracleProblem(nodes, faces, ids, 1e-9, [[1], [-1]])
+        ri = [1.0 + 0j, complex(np.sqrt(e))]
+        x = O.solve(P.sysmat(om, ri), P.srcvec(om, ri[0], src))
+        sca, ab = P.cs(om, ri[0], x, src)
+        return np.array([sca + ab, ab])
+
+    assert np.allclose(sig(eps), g["sigma"], rtol=1e-10)
+    h = g["deps_step"]
+    fd = (sig(eps + h) - sig(eps - h)) / (2 * h)
+    assert np.allclose(fd, g["deps"][0], rtol=1e-8)
