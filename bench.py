@@ -352,10 +352,15 @@ def run_ours(args, rank, local_rank, world):
             "clocks": clocks,
             "e2e": ({"value": world * 1000.0 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                      "d2h_bytes_per_step": d2h} if e2e_ms else None),
+            "autotune_panel_ctas": {"mixed": S.autotune_result(M.MIXED)[0],
+                                    "fp64": S.autotune_result(M.FP64)[0] if ms_fp64 else None},
             "gpu_launches": int(launches),
             "library_gemm_calls": libcalls,
             "roofline": roof,
             "rooflines": roofs}
+    if not args.no_extras and world == 1:
+        line["sweep"] = bench_sweep(M, args.sweep_workers, local_rank)
+        line["adjoint"] = bench_adjoint(M, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
         info = cpu_sample(args.subdiv, cores)
@@ -369,6 +374,81 @@ def run_ours(args, rank, local_rank, world):
     return 0
 
 
+def bench_sweep(M, workers, dev):
+    """Uneven wavelength sweep: the s=3 sphere and three seeded ellipsoids, 64 wavelengths
+    on 400-900 nm with a Drude permittivity, mixed precision refined to 1e-12; every mesh's
+    wavelengths split over `workers` contexts that run concurrently (mom_gpu_sweep_many)."""
+    import numpy as np
+    from mom_b200 import workloads as W
+    meshes = W.sweep_meshes()
+    wls = W.sweep_wavelengths(64)
+    oms = np.array([M.omega_of(w) for w in wls])
+    ri = np.stack([np.ones(len(wls)), np.sqrt(W.drude_eps(wls))], axis=1)
+    src = [M.src_pw(0, 90, 0)]
+    solvers, parts = [], []
+    for _, (nodes, faces, ids, doms) in meshes:
+        prob = M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms)
+        for w in range(workers):
+            s = M.Solver(dev)
+            s.set_problem(prob)
+            solvers.append(s)
+            parts.append(np.arange(w, len(wls), workers))
+    out = {"workload": "sweep: sphere s=3 + 3 ellipsoids (%s unknowns), 64 wavelengths 400-900 nm, Drude eps"
+                       % "/".join(str(2 * solvers[i * workers].N) for i in range(len(meshes))),
+           "contexts": len(solvers)}
+    for prec, name in ((M.MIXED, "mixed"), (M.FP64, "fp64")):
+        # warm-up: autotuning and graph capture of every context
+        M.sweep_many(solvers, [oms[p[:1]] for p in parts], [ri[p[:1]] for p in parts], src, prec)
+        t0 = time.perf_counter()
+        res = M.sweep_many(solvers, [oms[p] for p in parts], [ri[p] for p in parts], src, prec)
+        dt = time.perf_counter() - t0
+        out[name] = {"solves_per_s": len(meshes) * len(wls) / dt, "seconds": dt,
+                     "panel_ctas": [solvers[i * workers].autotune_result(prec)[0] for i in range(len(meshes))]}
+        out[name + "_sigma_ext_first"] = float(res[0][0][0, 0] + res[0][1][0, 0])
+    for s in solvers:
+        s.close()
+    return out
+
+
+def bench_adjoint(M, dev):
+    """Adjoint gradients on the perturbed s=3 sphere (3840 unknowns, 642 vertices):
+    time of d sigma / d eps and of d sigma / d(all vertex coordinates), and the eps
+    gradient against central differences (step 1e-6) of the FP64 cross sections."""
+    import numpy as np
+    from mom_b200 import workloads as W
+    nodes, faces, ids, doms = W.perturbed(3)
+    S = M.Solver(dev)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    om = M.omega_of(WL)
+    src = [M.src_pw(0, 90, 0)]
+
+    def sig(eps, prec=M.FP64):
+        ri = [1.0, np.sqrt(eps)]
+        S.solve_wavelength(om, ri, src, prec, 1e-12, 30)
+        a, b = S.cross_sections(om, ri[0], src)
+        return np.array([a[0] + b[0], b[0]])
+
+    out = {"workload": "perturbed sphere s=3 (3840 unknowns, %d vertices)" % len(nodes)}
+    fd = []
+    for dz in (1e-6, 1e-6j):
+        fd.append((sig(EPS_IN + dz) - sig(EPS_IN - dz)) / 2e-6)
+    fd = np.array(fd)
+    for prec, name in ((M.FP64, "fp64"), (M.MIXED, "mixed")):
+        ri = [1.0, np.sqrt(EPS_IN)]
+        sig(EPS_IN, prec)
+        t0 = time.perf_counter()
+        g = S.adjoint(om, ri, src, prec, eps_dom=1)["deps"][0]
+        t1 = time.perf_counter()
+        sig(EPS_IN, prec)
+        t2 = time.perf_counter()
+        S.adjoint(om, ri, src, prec, nodes=True)
+        t3 = time.perf_counter()
+        out[name] = {"eps_grad_ms": (t1 - t0) * 1e3, "vertex_grad_ms": (t3 - t2) * 1e3,
+                     "eps_grad_vs_fd_max_rel": float(np.max(np.abs(g.T - fd) / np.abs(fd)))}
+    S.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -379,6 +459,8 @@ def main():
     ap.add_argument("--subdiv", type=int, default=SUBDIV)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
+    ap.add_argument("--no-extras", action="store_true", help="skip the sweep and adjoint side measurements")
+    ap.add_argument("--sweep-workers", type=int, default=3, help="concurrent contexts per sweep mesh")
     args = ap.parse_args()
     rank, local_rank, world = dist_env()
     if args.impl == "reference":

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "mom_internal.h"
@@ -376,6 +377,10 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   }
   const char *eg = std::getenv("MOM_LU_GRAPH");
   c->use_graph = !(eg && eg[0] == '0');
+  const char *ea = std::getenv("MOM_AUTOTUNE");
+  c->autotune = !(ea && ea[0] == '0');
+  const char *ep = std::getenv("MOM_PANEL_CTAS");
+  if (ep) c->panel_cap_env = std::max(0, std::atoi(ep));
   *out = c;
   return MOM_OK;
 }
@@ -525,6 +530,60 @@ int mom_gpu_solve_wavelength(mom_ctx *c, double omega, const double *ri, int32_t
   r = mom_gpu_srcvec(c, omega, ri, nsrc, src, nullptr, 0);
   if (r) return r;
   return mom_gpu_solve(c, precision, tol, maxit, x_host, ldx, iters_out);
+}
+
+int mom_gpu_sweep(mom_ctx *c, int32_t nwl, const double *omega, const double *ri, int32_t nsrc, const mom_src *src,
+                  int32_t precision, double tol, int32_t maxit, double *csca, double *cabs, int32_t *iters) {
+  if (!c) return MOM_ERR_ARG;
+  if (nwl <= 0 || !omega || !ri || nsrc <= 0 || !src || !csca || !cabs) return fail(c, MOM_ERR_ARG, "invalid sweep arguments");
+  int ndom = 0;
+  {
+    std::lock_guard<std::mutex> g(c->mu);
+    if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+    ndom = c->ndom;
+  }
+  for (int w = 0; w < nwl; w++) {
+    const double *r = ri + (size_t)w * 2 * ndom;
+    int it = 0;
+    MOM_TRY(mom_gpu_solve_wavelength(c, omega[w], r, nsrc, src, precision, tol, maxit, nullptr, 0, &it));
+    MOM_TRY(mom_gpu_cross_sections(c, 0, omega[w], r, nsrc, src, nullptr, 0, csca + (size_t)w * nsrc,
+                                   cabs + (size_t)w * nsrc));
+    if (iters) iters[w] = it;
+  }
+  return MOM_OK;
+}
+
+int mom_gpu_sweep_many(int32_t nctx, mom_ctx **ctx, const int32_t *nwl, const double *const *omega,
+                       const double *const *ri, int32_t nsrc, const mom_src *src, int32_t precision, double tol,
+                       int32_t maxit, double *const *csca, double *const *cabs, int32_t *status) {
+  if (nctx <= 0 || !ctx || !nwl || !omega || !ri || !csca || !cabs) return MOM_ERR_ARG;
+  std::vector<int> st(nctx, MOM_OK);
+  std::vector<std::thread> th;
+  th.reserve(nctx);
+  for (int i = 0; i < nctx; i++)
+    th.emplace_back([&, i]() {
+      st[i] = mom_gpu_sweep(ctx[i], nwl[i], omega[i], ri[i], nsrc, src, precision, tol, maxit, csca[i], cabs[i],
+                            nullptr);
+    });
+  for (auto &t : th) t.join();
+  int rc = MOM_OK;
+  for (int i = 0; i < nctx; i++) {
+    if (status) status[i] = st[i];
+    if (rc == MOM_OK && st[i] != MOM_OK) rc = st[i];
+  }
+  return rc;
+}
+
+int mom_gpu_autotune_result(mom_ctx *c, int32_t precision, int32_t *panel_ctas, double *ms) {
+  if (!c || !panel_ctas) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  for (const auto &t : c->tuned)
+    if (t.n == c->n && t.precision == precision) {
+      *panel_ctas = t.cap == 0 ? c->nsm : t.cap;
+      if (ms) *ms = t.ms;
+      return MOM_OK;
+    }
+  return fail(c, MOM_ERR_STATE, "no autotuning result for this matrix order and precision");
 }
 
 int32_t mom_gpu_domain_nodes(mom_ctx *c, int32_t dom) {

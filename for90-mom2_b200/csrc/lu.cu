@@ -928,7 +928,10 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
     for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
       const int kb = (int)(j0 / nb);
       const int64_t m = n - j0;
-      int P = (int)std::min<int64_t>(c->nsm, (m + 31) / 32);
+      // CTAs: at most the cap, at least enough for rpc <= 208 rows
+      const int cap = c->panel_cap > 0 ? std::min(c->panel_cap, c->nsm) : c->nsm;
+      int P = (int)std::min<int64_t>(cap, (m + 31) / 32);
+      P = (int)std::min<int64_t>(c->nsm, std::max<int64_t>(P, (m + 207) / 208));
       int rpc = (int)((m + P - 1) / P);
       P = (int)((m + rpc - 1) / rpc);
       const size_t smem = sizeof(double2) * (size_t)nb * rpc;
@@ -1063,7 +1066,8 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
     const std::vector<uintptr_t> key = {(uintptr_t)n,         (uintptr_t)c->lda,   (uintptr_t)nb,
                                         (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
-                                        (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof};
+                                        (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
+                                        (uintptr_t)c->panel_cap};
     g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
     if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
@@ -1185,7 +1189,98 @@ int lu_init_kernels(Ctx *c) {
 namespace {
 }  // namespace
 
+namespace {
+
+__global__ void widen_copy_fp32(const double2 *__restrict__ A, float2 *__restrict__ B, int64_t count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = A[i];
+    B[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// Autotuner of the panel parallelism: factor the matrix once per candidate
+// CTA cap (eagerly, timed with events) and keep the fastest for this
+// (order, precision).  The matrix is restored before each trial: the FP32
+// copy from the FP64 matrix (mixed), or the FP64 matrix from a backup when
+// it takes at most 8 GB (otherwise the FP64 path keeps one CTA per SM).
+int lu_autotune(Ctx *c, int precision) {
+  if (c->panel_cap_env > 0) {
+    c->panel_cap = c->panel_cap_env;
+    return MOM_OK;
+  }
+  for (const auto &t : c->tuned)
+    if (t.n == c->n && t.precision == precision) {
+      c->panel_cap = t.cap;
+      return MOM_OK;
+    }
+  if (!c->autotune) {
+    c->panel_cap = 0;
+    return MOM_OK;
+  }
+  const int64_t n = c->n, count = c->lda * n;
+  const bool mixed = precision == MOM_PREC_MIXED;
+  const size_t bytes = sizeof(double2) * (size_t)count;
+  double2 *backup = nullptr;
+  if (!mixed) {
+    if (bytes > (size_t)8 << 30 || cudaMalloc(&backup, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      c->tuned.push_back({n, precision, 0, 0.0});
+      c->panel_cap = 0;
+      return MOM_OK;
+    }
+    MOM_CUDA(c, cudaMemcpyAsync(backup, c->A, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  const bool prof = c->prof;
+  c->prof = false;
+  const int64_t l0 = c->launches, b0 = c->blas_calls;
+  const double f0 = c->tc_flops;
+  cudaEvent_t e0, e1;
+  MOM_CUDA(c, cudaEventCreate(&e0));
+  MOM_CUDA(c, cudaEventCreate(&e1));
+  int best = 0;
+  double best_ms = 1e30;
+  int rc = MOM_OK;
+  const int cands[] = {0, 96, 64, 48, 32, 24, 16};
+  LuWork w;
+  rc = lu_workspace(c, precision, w);
+  for (int cand : cands) {
+    if (rc != MOM_OK) break;
+    if (cand >= c->nsm) continue;
+    if (mixed) widen_copy_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, count);
+    else cudaMemcpyAsync(c->A, backup, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    c->panel_cap = cand;
+    cudaEventRecord(e0, c->stream);
+    rc = mixed ? lu_enqueue<float2>(c, c->A32, precision, w) : lu_enqueue<double2>(c, c->A, precision, w);
+    cudaEventRecord(e1, c->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "autotune trial");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rc == MOM_OK && ms < best_ms) {
+      best_ms = ms;
+      best = cand;
+    }
+  }
+  // leave the matrix as it was
+  if (mixed) widen_copy_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, count);
+  else cudaMemcpyAsync(c->A, backup, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(backup);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->prof = prof;
+  c->launches = l0;
+  c->blas_calls = b0;
+  c->tc_flops = f0;
+  if (rc != MOM_OK) return rc;
+  c->tuned.push_back({n, precision, best, best_ms});
+  c->panel_cap = best;
+  return MOM_OK;
+}
+
+}  // namespace
+
 int lu_factor(Ctx *c, int precision) {
+  MOM_TRY(lu_autotune(c, precision));
   if (precision == MOM_PREC_MIXED) return lu_factor_t<float2>(c, c->A32, precision);
   return lu_factor_t<double2>(c, c->A, precision);
 }

@@ -129,6 +129,18 @@ struct Ctx {
     void reset();
   } lu_graph[2];
   bool use_graph = true;   // MOM_LU_GRAPH=0 turns graph replay off (every launch issued eagerly)
+  // Panel parallelism: at most panel_cap CTAs per panel (0: one per SM).
+  // Autotuned per (matrix order, precision) at the first factorisation
+  // unless MOM_AUTOTUNE=0; MOM_PANEL_CTAS fixes it.
+  int panel_cap = 0;
+  int panel_cap_env = 0;
+  bool autotune = true;
+  struct Tuned {
+    int64_t n;
+    int precision, cap;
+    double ms;
+  };
+  std::vector<Tuned> tuned;
   bool capturing = false;  // a stream capture is open on the context stream
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> cap_ev;
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)

@@ -46,6 +46,7 @@ EXPORTS = [
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
     "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
+    "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result",
 ]
 
 
@@ -103,6 +104,12 @@ def lib():
     L.mom_gpu_adjoint_mean_eps.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32,
                                            C.c_double, C.c_int32, dp, ip]
     L.mom_gpu_domain_nodes.argtypes = [vp, C.c_int32]
+    L.mom_gpu_sweep.argtypes = [vp, C.c_int32, dp, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32, C.c_double,
+                                C.c_int32, dp, dp, ip]
+    L.mom_gpu_sweep_many.argtypes = [C.c_int32, C.POINTER(vp), ip, C.POINTER(dp), C.POINTER(dp), C.c_int32,
+                                     C.POINTER(MomSrc), C.c_int32, C.c_double, C.c_int32, C.POINTER(dp),
+                                     C.POINTER(dp), ip]
+    L.mom_gpu_autotune_result.argtypes = [vp, C.c_int32, ip, dp]
     L.mom_problem_node_parent.argtypes = [vp, C.c_int32, ip]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
@@ -271,6 +278,32 @@ class Problem:
         return self.domain(-1)["nodes"].shape[0]
 
 
+def sweep_many(solvers, omegas, ri_per_wl, srcs, precision=MIXED, tol=1e-12, maxit=30):
+    """Sweeps of several problems concurrently (one host thread per solver inside
+    the library).  omegas[i], ri_per_wl[i]: wavelengths of solver i.  Returns a list
+    of (csca, cabs)."""
+    arr, ns = _srcs(srcs)
+    k = len(solvers)
+    hs = (C.c_void_p * k)(*[s.h for s in solvers])
+    oms = [np.ascontiguousarray(o, dtype=np.float64) for o in omegas]
+    ris = [np.ascontiguousarray(np.asarray(r, dtype=np.complex128).reshape(len(o), s.ndom)).view(np.float64).ravel()
+           for r, o, s in zip(ri_per_wl, oms, solvers)]
+    outs = [(np.zeros((len(o), ns)), np.zeros((len(o), ns))) for o in oms]
+    nwl = np.array([len(o) for o in oms], dtype=np.int32)
+    dpp = C.POINTER(C.c_double)
+    po = (dpp * k)(*[_dp(o) for o in oms])
+    pr = (dpp * k)(*[_dp(r) for r in ris])
+    pa = (dpp * k)(*[_dp(o[0]) for o in outs])
+    pb = (dpp * k)(*[_dp(o[1]) for o in outs])
+    st = np.zeros(k, dtype=np.int32)
+    rc = lib().mom_gpu_sweep_many(k, hs, nwl.ctypes.data_as(C.POINTER(C.c_int32)), po, pr, ns, arr, precision, tol,
+                                  maxit, pa, pb, st.ctypes.data_as(C.POINTER(C.c_int32)))
+    if rc != MOM_OK:
+        bad = int(np.nonzero(st)[0][0]) if np.any(st) else 0
+        _check(rc, solvers[bad].h, "sweep_many")
+    return outs
+
+
 class Solver:
     """One CUDA context of the PMCHWT library on ``device``."""
 
@@ -376,6 +409,26 @@ class Solver:
             offs = np.cumsum([0] + counts)
             out["dnodes"] = [dn[:, :, offs[d]:offs[d + 1], :] for d in range(self.ndom)]
         return out
+
+    def sweep(self, omegas, ri_per_wl, srcs, precision=MIXED, tol=1e-12, maxit=30):
+        """solve_batch over wavelengths: (csca[nwl][nsrc], cabs[nwl][nsrc], iters[nwl])."""
+        arr, ns = _srcs(srcs)
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        nwl = len(om)
+        r = np.ascontiguousarray(np.asarray(ri_per_wl, dtype=np.complex128).reshape(nwl, self.ndom)).view(np.float64)
+        csca = np.zeros((nwl, ns))
+        cabs = np.zeros((nwl, ns))
+        it = np.zeros(nwl, dtype=np.int32)
+        self._ck(lib().mom_gpu_sweep(self.h, nwl, _dp(om), _dp(r.ravel()), ns, arr, precision, tol, maxit, _dp(csca),
+                                     _dp(cabs), it.ctypes.data_as(C.POINTER(C.c_int32))), "sweep")
+        return csca, cabs, it
+
+    def autotune_result(self, precision):
+        """(panel CTAs, best trial ms) chosen by the LU autotuner for the current order."""
+        p = C.c_int32()
+        ms = C.c_double()
+        self._ck(lib().mom_gpu_autotune_result(self.h, precision, C.byref(p), C.byref(ms)), "autotune_result")
+        return p.value, ms.value
 
     def adjoint_mean_eps(self, omega, ri, srcs, precision, eps_dom, tol=1e-12, maxit=30):
         """d(mean sigma_ext, mean sigma_abs) / d(Re eps, Im eps) of domain eps_dom: [2][2]."""

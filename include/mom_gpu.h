@@ -143,6 +143,23 @@ int mom_gpu_cross_sections_noalloc(mom_ctx *ctx, int32_t dom, double omega, cons
                                    const mom_src *src, const void *x_dev, int64_t ldx, double *csca,
                                    double *cabs);
 
+/* ---- Wavelength sweeps ----
+ * solve_batch (solver.f90:17-142) over nwl wavelengths of one problem:
+ * sysmat, srcvec, LU and solve, then cs_prtsrf on domain 0 for every
+ * wavelength; ri is [nwl][ndom] complex (interleaved), csca / cabs
+ * [nwl][nsrc], iters [nwl] or NULL. */
+int mom_gpu_sweep(mom_ctx *ctx, int32_t nwl, const double *omega, const double *ri, int32_t nsrc, const mom_src *src,
+                  int32_t precision, double tol, int32_t maxit, double *csca, double *cabs, int32_t *iters);
+/* Sweeps of several problems at once (no counterpart in the reference): one
+ * host thread per context, each context on its own stream, so that the GPU
+ * overlaps the problems' launches.  status[nctx] (or NULL) per context. */
+int mom_gpu_sweep_many(int32_t nctx, mom_ctx **ctx, const int32_t *nwl, const double *const *omega,
+                       const double *const *ri, int32_t nsrc, const mom_src *src, int32_t precision, double tol,
+                       int32_t maxit, double *const *csca, double *const *cabs, int32_t *status);
+/* Result of the LU autotuner (panel CTAs, best trial time in ms) for the
+ * current matrix order; MOM_ERR_STATE before the first factorisation. */
+int mom_gpu_autotune_result(mom_ctx *ctx, int32_t precision, int32_t *panel_ctas, double *ms);
+
 /* ---- Adjoint gradients (no counterpart in the reference) ----
  * After mom_gpu_solve for the same sources (and the same omega and ri), the
  * factors of `precision` are reused for one transposed solve A^T lambda = G

@@ -1,0 +1,85 @@
+"""Wavelength sweeps (solve_batch over wavelengths) through the C ABI:
+the sweep entry points reproduce the single-wavelength path exactly, the
+concurrent multi-problem sweep reproduces the sequential one, and the FP64
+sweep matches the oracle's cross sections (<= 1e-9 relative)."""
+import numpy as np
+import pytest
+
+import mom_b200 as M
+import oracle as O
+from mom_b200 import meshgen, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def meshes():
+    n1, f1 = meshgen.icosphere(1, 50.0)
+    n2, f2 = meshgen.ellipsoid(1, (35.0, 50.0, 65.0))
+    return [(n1, f1, np.ones(len(f1), int), [[1], [-1]]), (n2, f2, np.ones(len(f2), int), [[1], [-1]])]
+
+
+WLS = np.array([420e-9, 550e-9, 700e-9, 880e-9])
+SRC = [M.src_pw(0, 90, 0), M.src_pw(60, 30, 45)]
+
+
+@pytest.fixture(scope="module")
+def solvers(built):
+    out = []
+    for nodes, faces, ids, doms in meshes():
+        s = M.Solver(0)
+        s.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+        out.append(s)
+    yield out
+    for s in out:
+        s.close()
+
+
+def ri_table():
+    eps = W.drude_eps(WLS)
+    return np.stack([np.ones(len(WLS)), np.sqrt(eps)], axis=1)
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.MIXED])
+def test_sweep_equals_single_wavelength_path(solvers, prec):
+    S = solvers[0]
+    oms = np.array([M.omega_of(w) for w in WLS])
+    ri = ri_table()
+    csca, cabs, it = S.sweep(oms, ri, SRC, prec)
+    for w in range(len(WLS)):
+        S.solve_wavelength(oms[w], ri[w], SRC, prec, 1e-12, 30)
+        a, b = S.cross_sections(oms[w], ri[w][0], SRC)
+        assert np.array_equal(a, csca[w]) and np.array_equal(b, cabs[w])
+    if prec == M.MIXED:
+        assert np.all(it >= 1)
+
+
+def test_sweep_many_equals_sequential(solvers):
+    oms = np.array([M.omega_of(w) for w in WLS])
+    ri = ri_table()
+    seq = [s.sweep(oms, ri, SRC, M.MIXED)[:2] for s in solvers]
+    par = M.sweep_many(solvers, [oms, oms], [ri, ri], SRC, M.MIXED)
+    for (a, b), (c, d) in zip(seq, par):
+        assert np.array_equal(a, c) and np.array_equal(b, d)
+
+
+def test_fp64_sweep_matches_oracle(solvers):
+    nodes, faces, ids, doms = meshes()[1]
+    P = O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+    oms = np.array([M.omega_of(w) for w in WLS])
+    ri = ri_table()
+    csca, cabs, _ = solvers[1].sweep(oms, ri, SRC, M.FP64)
+    w = 2
+    r = [complex(ri[w][0]), complex(ri[w][1])]
+    src = [dict(type="pw", theta=s["theta"], phi=s["phi"], psi=s["psi"]) for s in SRC]
+    A = P.sysmat(oms[w], r)
+    for k, s in enumerate(src):
+        x = O.solve(A, P.srcvec(oms[w], r[0], s))
+        sca, ab = P.cs(oms[w], r[0], x, s)
+        assert abs(csca[w, k] - sca) <= 1e-9 * abs(sca)
+        assert abs(cabs[w, k] - ab) <= 1e-9 * abs(ab)
+
+
+def test_autotuner_records_a_choice(solvers):
+    S = solvers[0]
+    p, ms = S.autotune_result(M.MIXED)
+    assert 1 <= p <= 148 and ms > 0
