@@ -352,8 +352,8 @@ def run_ours(args, rank, local_rank, world):
             "clocks": clocks,
             "e2e": ({"value": world * 1000.0 / e2e_ms, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                      "d2h_bytes_per_step": d2h} if e2e_ms else None),
-            "autotune_panel_ctas": {"mixed": S.autotune_result(M.MIXED)[0],
-                                    "fp64": S.autotune_result(M.FP64)[0] if ms_fp64 else None},
+            "autotune_panel": {"mixed": S.autotune_result(M.MIXED),
+                               "fp64": S.autotune_result(M.FP64) if ms_fp64 else None},
             "gpu_launches": int(launches),
             "library_gemm_calls": libcalls,
             "roofline": roof,
@@ -403,7 +403,8 @@ def bench_sweep(M, workers, dev):
         res = M.sweep_many(solvers, [oms[p] for p in parts], [ri[p] for p in parts], src, prec)
         dt = time.perf_counter() - t0
         out[name] = {"solves_per_s": len(meshes) * len(wls) / dt, "seconds": dt,
-                     "panel_ctas": [solvers[i * workers].autotune_result(prec)[0] for i in range(len(meshes))]}
+                     "panel_ctas_by_height": [dict(zip(*(lambda t: (t["heights"], t["ctas"]))(
+                         solvers[i * workers].autotune_result(prec)))) for i in range(len(meshes))]}
         out[name + "_sigma_ext_first"] = float(res[0][0][0, 0] + res[0][1][0, 0])
     for s in solvers:
         s.close()

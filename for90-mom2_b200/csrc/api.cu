@@ -391,6 +391,7 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaStreamSynchronize(c->stream);
   free_problem(c);
   cudaFree(c->ws);
+  cudaFree(c->ws2);
   cudaFree(c->Xh);
   cudaFree(c->adj);
   cudaFree(c->adj_part);
@@ -574,13 +575,20 @@ int mom_gpu_sweep_many(int32_t nctx, mom_ctx **ctx, const int32_t *nwl, const do
   return rc;
 }
 
-int mom_gpu_autotune_result(mom_ctx *c, int32_t precision, int32_t *panel_ctas, double *ms) {
-  if (!c || !panel_ctas) return MOM_ERR_ARG;
+int mom_gpu_autotune_result(mom_ctx *c, int32_t precision, int32_t max_entries, int32_t *nent, int64_t *heights,
+                            int32_t *ctas, double *us_per_column, double *tune_ms) {
+  if (!c || !nent) return MOM_ERR_ARG;
   std::lock_guard<std::mutex> g(c->mu);
   for (const auto &t : c->tuned)
     if (t.n == c->n && t.precision == precision) {
-      *panel_ctas = t.cap == 0 ? c->nsm : t.cap;
-      if (ms) *ms = t.ms;
+      const int k = std::min<int>(max_entries, (int)t.m.size());
+      for (int i = 0; i < k; i++) {
+        if (heights) heights[i] = t.m[i];
+        if (ctas) ctas[i] = t.P[i];
+        if (us_per_column) us_per_column[i] = t.us[i];
+      }
+      *nent = (int32_t)t.m.size();
+      if (tune_ms) *tune_ms = t.ms;
       return MOM_OK;
     }
   return fail(c, MOM_ERR_STATE, "no autotuning result for this matrix order and precision");

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -884,6 +885,67 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   return MOM_OK;
 }
 
+// Identity of the panel table in use (part of the LU graph key).
+uint64_t tune_hash(const Ctx *c) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)c->panel_cap_env;
+  if (c->tune)
+    for (size_t i = 0; i < c->tune->m.size(); i++) h = (h ^ (uint64_t)(c->tune->m[i] * 1000 + c->tune->P[i])) * 1099511628211ull;
+  return h;
+}
+
+// CTAs for a panel of m rows: the autotuned table's entry at the nearest
+// probed height (log scale), else a cap, else one CTA per SM; never fewer
+// than needed for rpc <= 208 rows.
+int panel_ctas(const Ctx *c, int64_t m) {
+  int P = c->nsm;
+  if (c->panel_cap_env > 0) {
+    P = std::min(c->panel_cap_env, c->nsm);
+  } else if (c->tune && !c->tune->m.empty()) {
+    double bd = 1e30;
+    for (size_t i = 0; i < c->tune->m.size(); i++) {
+      const double d = std::fabs(std::log((double)m / (double)c->tune->m[i]));
+      if (d < bd) {
+        bd = d;
+        P = c->tune->P[i];
+      }
+    }
+  }
+  P = (int)std::min<int64_t>(P, (m + 7) / 8);
+  return (int)std::min<int64_t>(c->nsm, std::max<int64_t>(P, (m + 207) / 208));
+}
+
+// One panel (rows j0 .. n of columns j0 .. j0+nb) on P CTAs.
+template <typename T>
+int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *ipiv, int *info, const LuWork &w) {
+  const int nb = c->nb;
+  const int64_t m = n - j0;
+  const int rpc = (int)((m + P - 1) / P);
+  P = (int)((m + rpc - 1) / rpc);
+  const size_t smem = sizeof(double2) * (size_t)nb * rpc;
+  if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64 || P > 256)
+    return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory (matrix order too large)");
+  PanelArgs pa;
+  pa.A = A;
+  pa.lda = lda;
+  pa.n = n;
+  pa.j0 = j0;
+  pa.nb = nb;
+  pa.rpc = rpc;
+  pa.P = P;
+  pa.ipiv = ipiv;
+  pa.info = info;
+  pa.timeout = w.timeout;
+  pa.rec = w.rec;
+  pa.cand_data = w.cand_data;
+  pa.col_data = w.col_data;
+  MOM_CUDA(c, cudaMemsetAsync(w.rec, 0, sizeof(unsigned long long) * 2 * P, c->stream));
+  void *args[] = {&pa};
+  MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
+                                          c->stream));
+  c->launches++;
+  return MOM_OK;
+}
+
 // Issues every launch of the factorisation on the context stream (eagerly,
 // or into an open capture).
 template <typename T>
@@ -928,36 +990,9 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
     for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
       const int kb = (int)(j0 / nb);
       const int64_t m = n - j0;
-      // CTAs: at most the cap, at least enough for rpc <= 208 rows
-      const int cap = c->panel_cap > 0 ? std::min(c->panel_cap, c->nsm) : c->nsm;
-      int P = (int)std::min<int64_t>(cap, (m + 31) / 32);
-      P = (int)std::min<int64_t>(c->nsm, std::max<int64_t>(P, (m + 207) / 208));
-      int rpc = (int)((m + P - 1) / P);
-      P = (int)((m + rpc - 1) / rpc);
-      const size_t smem = sizeof(double2) * (size_t)nb * rpc;
-      if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64 || P > 256)
-        return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory (matrix order too large)");
-      PanelArgs pa;
-      pa.A = A;
-      pa.lda = lda;
-      pa.n = n;
-      pa.j0 = j0;
-      pa.nb = nb;
-      pa.rpc = rpc;
-      pa.P = P;
-      pa.ipiv = c->ipiv;
-      pa.info = w.info;
-      pa.timeout = w.timeout;
-      pa.rec = w.rec;
-      pa.cand_data = w.cand_data;
-      pa.col_data = w.col_data;
       {
-        MOM_CUDA(c, cudaMemsetAsync(w.rec, 0, sizeof(unsigned long long) * 2 * P, c->stream));
         ProfScope ps(c, kProfPanel);
-        void *args[] = {&pa};
-        MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
-                                                c->stream));
-        c->launches++;
+        MOM_TRY(launch_panel<T>(c, A, lda, n, j0, panel_ctas(c, m), c->ipiv, w.info, w));
       }
       {
         ProfScope pz(c, kProfPivotAux);
@@ -1067,7 +1102,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
-                                        (uintptr_t)c->panel_cap};
+                                        (uintptr_t)tune_hash(c)};
     g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
     if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
@@ -1191,89 +1226,95 @@ namespace {
 
 namespace {
 
-__global__ void widen_copy_fp32(const double2 *__restrict__ A, float2 *__restrict__ B, int64_t count) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
-    const double2 v = A[i];
-    B[i] = make_float2((float)v.x, (float)v.y);
-  }
-}
 
-// Autotuner of the panel parallelism: factor the matrix once per candidate
-// CTA cap (eagerly, timed with events) and keep the fastest for this
-// (order, precision).  The matrix is restored before each trial: the FP32
-// copy from the FP64 matrix (mixed), or the FP64 matrix from a backup when
-// it takes at most 8 GB (otherwise the FP64 path keeps one CTA per SM).
-int lu_autotune(Ctx *c, int precision) {
-  if (c->panel_cap_env > 0) {
-    c->panel_cap = c->panel_cap_env;
-    return MOM_OK;
-  }
-  for (const auto &t : c->tuned)
-    if (t.n == c->n && t.precision == precision) {
-      c->panel_cap = t.cap;
-      return MOM_OK;
-    }
-  if (!c->autotune) {
-    c->panel_cap = 0;
-    return MOM_OK;
-  }
-  const int64_t n = c->n, count = c->lda * n;
-  const bool mixed = precision == MOM_PREC_MIXED;
-  const size_t bytes = sizeof(double2) * (size_t)count;
-  double2 *backup = nullptr;
-  if (!mixed) {
-    if (bytes > (size_t)8 << 30 || cudaMalloc(&backup, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      c->tuned.push_back({n, precision, 0, 0.0});
-      c->panel_cap = 0;
-      return MOM_OK;
-    }
-    MOM_CUDA(c, cudaMemcpyAsync(backup, c->A, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  }
-  const bool prof = c->prof;
-  c->prof = false;
-  const int64_t l0 = c->launches, b0 = c->blas_calls;
-  const double f0 = c->tc_flops;
-  cudaEvent_t e0, e1;
-  MOM_CUDA(c, cudaEventCreate(&e0));
-  MOM_CUDA(c, cudaEventCreate(&e1));
-  int best = 0;
-  double best_ms = 1e30;
-  int rc = MOM_OK;
-  const int cands[] = {0, 96, 64, 48, 32, 24, 16};
+// Autotuner of the panel parallelism.  The panel is latency bound: one
+// device-wide pivot exchange per column, whose cost grows with the number of
+// CTAs, against per-CTA update work that shrinks with it.  For panel heights
+// m = n, n/2, n/4, ... (>= 128) the first 64 columns of the matrix, rows
+// 0 .. m, are copied to a scratch panel and factored once per candidate CTA
+// count (CUDA-event timed, best of two); the fastest count per height forms
+// the table panel_ctas() interpolates (nearest height on a log scale).
+template <typename T>
+int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
+  const int64_t n = c->n, lda = c->lda;
+  const int nb = c->nb;
   LuWork w;
-  rc = lu_workspace(c, precision, w);
-  for (int cand : cands) {
-    if (rc != MOM_OK) break;
-    if (cand >= c->nsm) continue;
-    if (mixed) widen_copy_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, count);
-    else cudaMemcpyAsync(c->A, backup, bytes, cudaMemcpyDeviceToDevice, c->stream);
-    c->panel_cap = cand;
-    cudaEventRecord(e0, c->stream);
-    rc = mixed ? lu_enqueue<float2>(c, c->A32, precision, w) : lu_enqueue<double2>(c, c->A, precision, w);
-    cudaEventRecord(e1, c->stream);
-    if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "autotune trial");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (rc == MOM_OK && ms < best_ms) {
-      best_ms = ms;
-      best = cand;
-    }
+  MOM_TRY(lu_workspace(c, t.precision, w));
+  T *S = nullptr;
+  int *ip = nullptr;
+  if (cudaMalloc(&S, sizeof(T) * (size_t)n * nb) != cudaSuccess || cudaMalloc(&ip, sizeof(int) * 2 * nb) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(S);
+    return fail(c, MOM_ERR_ALLOC, "autotune scratch allocation failed");
   }
-  // leave the matrix as it was
-  if (mixed) widen_copy_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, count);
-  else cudaMemcpyAsync(c->A, backup, bytes, cudaMemcpyDeviceToDevice, c->stream);
-  cudaStreamSynchronize(c->stream);
-  cudaFree(backup);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = MOM_OK;
+  const int cands[] = {148, 120, 96, 80, 64, 48, 40, 32, 24, 16, 12, 8};
+  for (int64_t m = n; m >= 128 && rc == MOM_OK; m /= 2) {
+    int best = c->nsm, last = -1;
+    double best_ms = 1e30;
+    for (int cand : cands) {
+      const int P0 = (int)std::min<int64_t>(c->nsm, std::max<int64_t>(std::min<int64_t>(cand, (m + 7) / 8), (m + 207) / 208));
+      const int rpc = (int)((m + P0 - 1) / P0);
+      const int P = (int)((m + rpc - 1) / rpc);
+      if (P == last) continue;
+      last = P;
+      double ms_min = 1e30;
+      for (int rep = 0; rep < 2 && rc == MOM_OK; rep++) {
+        MOM_CUDA(c, cudaMemcpy2DAsync(S, sizeof(T) * m, A, sizeof(T) * lda, sizeof(T) * m, nb,
+                                      cudaMemcpyDeviceToDevice, c->stream));
+        cudaEventRecord(e0, c->stream);
+        rc = launch_panel<T>(c, S, m, m, 0, P, ip, ip + nb, w);
+        cudaEventRecord(e1, c->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "panel autotune trial");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms_min = std::min(ms_min, (double)ms);
+      }
+      if (rc == MOM_OK && ms_min < best_ms) {
+        best_ms = ms_min;
+        best = P;
+      }
+    }
+    t.m.push_back(m);
+    t.P.push_back(best);
+    t.us.push_back(best_ms * 1e3 / nb);
+  }
+  int tmo = 0;
+  cudaMemcpy(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaFree(S);
+  cudaFree(ip);
+  if (rc == MOM_OK && tmo) rc = fail(c, MOM_ERR_TIMEOUT, "panel autotune trial timed out");
+  return rc;
+}
+
+int lu_autotune(Ctx *c, int precision) {
+  c->tune = nullptr;
+  if (c->panel_cap_env > 0 || !c->autotune) return MOM_OK;
+  for (const auto &t : c->tuned)
+    if (t.n == c->n && t.precision == precision) {
+      c->tune = &t;
+      return MOM_OK;
+    }
+  Ctx::Tuned t;
+  t.n = c->n;
+  t.precision = precision;
+  const bool prof = c->prof;
+  c->prof = false;
+  const int64_t l0 = c->launches;
+  const auto t0 = std::chrono::steady_clock::now();
+  MOM_CUDA(c, cudaMemsetAsync(c->dinfo, 0, sizeof(int) * 4, c->stream));
+  const int rc = precision == MOM_PREC_MIXED ? tune_panels<float2>(c, c->A32, t) : tune_panels<double2>(c, c->A, t);
   c->prof = prof;
   c->launches = l0;
-  c->blas_calls = b0;
-  c->tc_flops = f0;
   if (rc != MOM_OK) return rc;
-  c->tuned.push_back({n, precision, best, best_ms});
-  c->panel_cap = best;
+  t.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  c->tuned.push_back(t);
+  c->tune = &c->tuned.back();
   return MOM_OK;
 }
 
@@ -1284,6 +1325,116 @@ int lu_factor(Ctx *c, int precision) {
   if (precision == MOM_PREC_MIXED) return lu_factor_t<float2>(c, c->A32, precision);
   return lu_factor_t<double2>(c, c->A, precision);
 }
+
+namespace {
+
+constexpr int kMultiRhs = 16;  // from this many right-hand sides on, the solves are GEMM based
+
+// Y = P X (mode 0), Y = X (mode 1) or Y[perm[i]] = X[i] (mode 2), with a
+// type conversion, for nrhs columns.
+template <typename TI, typename TO>
+__global__ void permute_rows_kernel(const TI *X, int64_t ldx, TO *Y, int64_t ldy, int64_t n, const int *perm,
+                                    int mode) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= n) return;
+  const int64_t src = mode == 0 ? perm[i] : i, dst = mode == 2 ? perm[i] : i;
+  const TI v = X[(size_t)s * ldx + src];
+  TO o;
+  o.x = v.x;
+  o.y = v.y;
+  Y[(size_t)s * ldy + dst] = o;
+}
+
+__global__ void inv_to_fp32_kernel(const double2 *a, float2 *b, int64_t count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+
+template <typename T>
+int blas_gemm(Ctx *c, cublasOperation_t ta, int m, int nn, int k, double alpha, const T *A, int64_t lda, const T *B,
+              int64_t ldb, double beta, T *C, int64_t ldc);
+template <>
+int blas_gemm<double2>(Ctx *c, cublasOperation_t ta, int m, int nn, int k, double alpha, const double2 *A,
+                       int64_t lda, const double2 *B, int64_t ldb, double beta, double2 *C, int64_t ldc) {
+  const cuDoubleComplex al = make_cuDoubleComplex(alpha, 0), be = make_cuDoubleComplex(beta, 0);
+  MOM_BLAS(c, cublasZgemm(c->blas, ta, CUBLAS_OP_N, m, nn, k, &al, (const cuDoubleComplex *)A, (int)lda,
+                          (const cuDoubleComplex *)B, (int)ldb, &be, (cuDoubleComplex *)C, (int)ldc));
+  c->blas_calls++;
+  return MOM_OK;
+}
+template <>
+int blas_gemm<float2>(Ctx *c, cublasOperation_t ta, int m, int nn, int k, double alpha, const float2 *A, int64_t lda,
+                      const float2 *B, int64_t ldb, double beta, float2 *C, int64_t ldc) {
+  const cuComplex al = make_cuComplex((float)alpha, 0), be = make_cuComplex((float)beta, 0);
+  MOM_BLAS(c, cublasCgemm(c->blas, ta, CUBLAS_OP_N, m, nn, k, &al, (const cuComplex *)A, (int)lda,
+                          (const cuComplex *)B, (int)ldb, &be, (cuComplex *)C, (int)ldc));
+  c->blas_calls++;
+  return MOM_OK;
+}
+
+// Many right-hand sides: blocked substitution with the diagonal-block
+// inverses, every step a library GEMM (64-row blocks; the updates of the
+// rows below / above are tall GEMMs with K = 64).  X (n x nrhs, ld n) is
+// overwritten with A^{-1} X (trans: A^{-T} X).  T = float2 works on the FP32
+// factors in FP32 (no TF32), T = double2 on the FP64 factors.
+template <typename T>
+int getrs_multi(Ctx *c, const T *F, double2 *X, int nrhs, int trans) {
+  const int64_t n = c->n, lda = c->lda;
+  const int nb = c->nb, nblk = (int)(n / nb);
+  const bool f32 = sizeof(T) == sizeof(float2);
+  const size_t ybytes = sizeof(T) * (size_t)n * nrhs, tbytes = sizeof(T) * (size_t)nb * nrhs;
+  const size_t ibytes = f32 ? sizeof(float2) * (size_t)nblk * 2 * nb * nb : 0;
+  MOM_TRY(ensure_buffer(c, &c->ws2, &c->ws2_bytes, ybytes + tbytes + ibytes + 1024));
+  T *Y = (T *)c->ws2;
+  T *Tm = (T *)((char *)c->ws2 + ((ybytes + 255) / 256) * 256);
+  const T *inv = (const T *)c->invd;
+  if (f32) {
+    float2 *i32 = (float2 *)((char *)c->ws2 + ((ybytes + 255) / 256) * 256 + ((tbytes + 255) / 256) * 256);
+    inv_to_fp32_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(c->invd, i32, (int64_t)nblk * 2 * nb * nb);
+    c->launches++;
+    inv = (const T *)i32;
+  }
+  ProfScope ps(c, kProfTrsv);
+  const dim3 pg((unsigned)((n + 255) / 256), nrhs);
+  permute_rows_kernel<double2, T><<<pg, 256, 0, c->stream>>>(X, n, Y, n, n, c->perm, trans ? 1 : 0);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+  const cublasOperation_t op = trans ? CUBLAS_OP_T : CUBLAS_OP_N;
+  // block k of the pass: y_k <- inv_k y_k (through Tm), then the update
+  auto diag = [&](int kb, int which) -> int {
+    const int64_t k0 = (int64_t)kb * nb;
+    MOM_TRY(blas_gemm<T>(c, op, nb, nrhs, nb, 1.0, inv + ((size_t)kb * 2 + which) * nb * nb, nb, Y + k0, n, 0.0, Tm,
+                         nb));
+    MOM_CUDA(c, cudaMemcpy2DAsync(Y + k0, sizeof(T) * n, Tm, sizeof(T) * nb, sizeof(T) * nb, nrhs,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    return MOM_OK;
+  };
+  // forward: L (unit lower), or U^T; backward: U, or L^T (unit upper)
+  for (int kb = 0; kb < nblk; kb++) {
+    const int64_t k0 = (int64_t)kb * nb, m = n - k0 - nb;
+    MOM_TRY(diag(kb, trans ? 1 : 0));
+    if (m > 0) {
+      const T *Ab = trans ? F + k0 + (k0 + nb) * lda : F + (k0 + nb) + k0 * lda;
+      MOM_TRY(blas_gemm<T>(c, op, (int)m, nrhs, nb, -1.0, Ab, lda, Tm, nb, 1.0, Y + k0 + nb, n));
+    }
+  }
+  for (int kb = nblk - 1; kb >= 0; kb--) {
+    const int64_t k0 = (int64_t)kb * nb;
+    MOM_TRY(diag(kb, trans ? 0 : 1));
+    if (k0 > 0) {
+      const T *Ab = trans ? F + k0 : F + k0 * lda;
+      MOM_TRY(blas_gemm<T>(c, op, (int)k0, nrhs, nb, -1.0, Ab, lda, Tm, nb, 1.0, Y, n));
+    }
+  }
+  permute_rows_kernel<T, double2><<<pg, 256, 0, c->stream>>>(Y, n, X, n, n, c->perm, trans ? 2 : 1);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+}  // namespace
 
 // Solve A X = B (trans: A^T X = B) for nrhs columns (ld n) with the factors
 // of `precision` in place.  FP64: one triangular solve.  Mixed: x = 0,
@@ -1296,9 +1447,13 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
   const size_t vec = sizeof(double2) * (size_t)n * nrhs;
   if (precision == MOM_PREC_FP64) {
     if (X != B) MOM_CUDA(c, cudaMemcpyAsync(X, B, vec, cudaMemcpyDeviceToDevice, c->stream));
-    MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, vec));
-    if (trans) MOM_TRY((getrs_t<double2, true>(c, c->A, X, (double2 *)c->ws, nrhs)));
-    else MOM_TRY((getrs_t<double2, false>(c, c->A, X, (double2 *)c->ws, nrhs)));
+    if (nrhs >= kMultiRhs) {
+      MOM_TRY(getrs_multi<double2>(c, c->A, X, nrhs, trans));
+    } else {
+      MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, vec));
+      if (trans) MOM_TRY((getrs_t<double2, true>(c, c->A, X, (double2 *)c->ws, nrhs)));
+      else MOM_TRY((getrs_t<double2, false>(c, c->A, X, (double2 *)c->ws, nrhs)));
+    }
     if (iters) *iters = 0;
     int tmo = 0;
     MOM_CUDA(c, cudaMemcpyAsync(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1333,12 +1488,22 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
   double worst = 1.0;
   for (it = 1; it <= maxit; it++) {
     MOM_CUDA(c, cudaMemcpyAsync(Dv, R, vec, cudaMemcpyDeviceToDevice, c->stream));
-    if (trans) MOM_TRY((getrs_t<float2, true>(c, c->A32, Dv, Yv, nrhs)));
+    const bool multi = nrhs >= kMultiRhs;
+    if (multi) MOM_TRY(getrs_multi<float2>(c, c->A32, Dv, nrhs, trans));
+    else if (trans) MOM_TRY((getrs_t<float2, true>(c, c->A32, Dv, Yv, nrhs)));
     else MOM_TRY((getrs_t<float2, false>(c, c->A32, Dv, Yv, nrhs)));
     axpy_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(X, Dv, (int64_t)n * nrhs);
     c->launches++;
     ProfScope pr(c, kProfResidual);
-    for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
+    if (multi) {
+      // R = B - op(A) X as one FP64 library GEMM, then the column norms
+      MOM_CUDA(c, cudaMemcpyAsync(R, B, vec, cudaMemcpyDeviceToDevice, c->stream));
+      MOM_TRY(blas_gemm<double2>(c, trans ? CUBLAS_OP_T : CUBLAS_OP_N, (int)n, nrhs, (int)n, -1.0, c->A, c->lda, X,
+                                 n, 1.0, R, n));
+      residual_kernel<<<dim3(rblocks, nrhs), 256, 0, c->stream>>>(R, n, Pp, 0, n, nrhs, R, n, rn2);
+      c->launches++;
+    }
+    for (int s0 = 0, ns = 0; !multi && s0 < nrhs; s0 += ns) {
       ns = 8;
       while (ns > nrhs - s0) ns >>= 1;
       const double2 *xs0 = X + (size_t)s0 * n;

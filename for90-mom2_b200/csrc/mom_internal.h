@@ -97,6 +97,8 @@ struct Ctx {
   unsigned *flags = nullptr;  // [256] per-CTA barrier epochs of the cooperative solve kernel
   void *ws = nullptr;      // general device workspace
   size_t ws_bytes = 0;
+  void *ws2 = nullptr;     // workspace of the many-right-hand-side solve
+  size_t ws2_bytes = 0;
   int assembled = 0;       // 0 none, 1 FP64 matrix present
   int factored = -1;       // precision of the factors in place, -1 none
   int nb = 64;             // panel width
@@ -129,18 +131,21 @@ struct Ctx {
     void reset();
   } lu_graph[2];
   bool use_graph = true;   // MOM_LU_GRAPH=0 turns graph replay off (every launch issued eagerly)
-  // Panel parallelism: at most panel_cap CTAs per panel (0: one per SM).
-  // Autotuned per (matrix order, precision) at the first factorisation
-  // unless MOM_AUTOTUNE=0; MOM_PANEL_CTAS fixes it.
-  int panel_cap = 0;
+  // Panel parallelism: CTAs per panel as a function of the panel's rows m,
+  // autotuned per (matrix order, precision) at the first factorisation
+  // (unless MOM_AUTOTUNE=0: one CTA per SM); MOM_PANEL_CTAS fixes a cap.
   int panel_cap_env = 0;
   bool autotune = true;
   struct Tuned {
     int64_t n;
-    int precision, cap;
-    double ms;
+    int precision;
+    std::vector<int64_t> m;  // panel heights probed
+    std::vector<int> P;      // fastest CTA count at each height
+    std::vector<double> us;  // its time per panel column (microseconds)
+    double ms = 0;           // time spent tuning
   };
   std::vector<Tuned> tuned;
+  const Tuned *tune = nullptr;  // table in use by the factorisation being issued
   bool capturing = false;  // a stream capture is open on the context stream
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> cap_ev;
   int64_t blas_calls = 0;  // cuBLAS GEMM calls (library kernels, not counted in launches)

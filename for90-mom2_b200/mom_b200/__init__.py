@@ -109,7 +109,7 @@ def lib():
     L.mom_gpu_sweep_many.argtypes = [C.c_int32, C.POINTER(vp), ip, C.POINTER(dp), C.POINTER(dp), C.c_int32,
                                      C.POINTER(MomSrc), C.c_int32, C.c_double, C.c_int32, C.POINTER(dp),
                                      C.POINTER(dp), ip]
-    L.mom_gpu_autotune_result.argtypes = [vp, C.c_int32, ip, dp]
+    L.mom_gpu_autotune_result.argtypes = [vp, C.c_int32, C.c_int32, ip, C.POINTER(C.c_int64), ip, dp, dp]
     L.mom_problem_node_parent.argtypes = [vp, C.c_int32, ip]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
@@ -424,11 +424,19 @@ class Solver:
         return csca, cabs, it
 
     def autotune_result(self, precision):
-        """(panel CTAs, best trial ms) chosen by the LU autotuner for the current order."""
-        p = C.c_int32()
+        """The LU autotuner's table for the current order: dict(heights, ctas, us_per_column, tune_ms)."""
+        k = 32
+        nent = C.c_int32()
+        hs = np.zeros(k, dtype=np.int64)
+        ps = np.zeros(k, dtype=np.int32)
+        us = np.zeros(k)
         ms = C.c_double()
-        self._ck(lib().mom_gpu_autotune_result(self.h, precision, C.byref(p), C.byref(ms)), "autotune_result")
-        return p.value, ms.value
+        self._ck(lib().mom_gpu_autotune_result(self.h, precision, k, C.byref(nent), hs.ctypes.data_as(C.POINTER(C.c_int64)),
+                                               ps.ctypes.data_as(C.POINTER(C.c_int32)), _dp(us), C.byref(ms)),
+                 "autotune_result")
+        m = min(k, nent.value)
+        return dict(heights=hs[:m].tolist(), ctas=ps[:m].tolist(), us_per_column=us[:m].round(3).tolist(),
+                    tune_ms=ms.value)
 
     def adjoint_mean_eps(self, omega, ri, srcs, precision, eps_dom, tol=1e-12, maxit=30):
         """d(mean sigma_ext, mean sigma_abs) / d(Re eps, Im eps) of domain eps_dom: [2][2]."""

@@ -156,9 +156,13 @@ int mom_gpu_sweep(mom_ctx *ctx, int32_t nwl, const double *omega, const double *
 int mom_gpu_sweep_many(int32_t nctx, mom_ctx **ctx, const int32_t *nwl, const double *const *omega,
                        const double *const *ri, int32_t nsrc, const mom_src *src, int32_t precision, double tol,
                        int32_t maxit, double *const *csca, double *const *cabs, int32_t *status);
-/* Result of the LU autotuner (panel CTAs, best trial time in ms) for the
- * current matrix order; MOM_ERR_STATE before the first factorisation. */
-int mom_gpu_autotune_result(mom_ctx *ctx, int32_t precision, int32_t *panel_ctas, double *ms);
+/* Table of the LU autotuner for the current matrix order (no counterpart in
+ * the reference): for panel heights heights[i] the CTA count ctas[i] chosen
+ * and its time per panel column; up to max_entries entries, *nent = table
+ * size, *tune_ms = time spent tuning.  MOM_ERR_STATE before the first
+ * factorisation (or with MOM_AUTOTUNE=0 / MOM_PANEL_CTAS set). */
+int mom_gpu_autotune_result(mom_ctx *ctx, int32_t precision, int32_t max_entries, int32_t *nent, int64_t *heights,
+                            int32_t *ctas, double *us_per_column, double *tune_ms);
 
 /* ---- Adjoint gradients (no counterpart in the reference) ----
  * After mom_gpu_solve for the same sources (and the same omega and ri), the
