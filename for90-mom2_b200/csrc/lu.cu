@@ -37,7 +37,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 
-constexpr int kPanelThreads = 256;
+constexpr int kPanelThreads = 512;
 constexpr long long kSpinLimit = 1LL << 26;  // bounded barrier wait (a few seconds)
 
 struct PanelArgs {
@@ -219,6 +219,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         if (lane + 32 * q < a.P) pending |= 1u << q;
       long long it = 0;
       int ok = 1;
+      // the row of the best record seen so far is fetched while the others
+      // arrive (its data is visible once its record is: release / acquire)
+      unsigned long long pf_key = 0;
+      double2 pf0 = make_double2(0, 0), pf1 = make_double2(0, 0);
       while (true) {
 #pragma unroll
         for (int q = 0; q < 8; q++) {
@@ -233,7 +237,17 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
             }
           }
         }
-        if (__all_sync(0xffffffffu, pending == 0)) break;
+        const bool done = __all_sync(0xffffffffu, pending == 0);
+        const unsigned long long rk = warp_max_key(bw >= 0 ? (best & ~0xffull) : 0ull);
+        if (rk != 0ull && rk != pf_key) {
+          const int rw = __ffs(__ballot_sync(0xffffffffu, bw >= 0 && (best & ~0xffull) == rk)) - 1;
+          const int rcta = __shfl_sync(0xffffffffu, bw, rw);
+          const double2 *pd = a.cand_data + ((size_t)par * a.P + rcta) * nb;
+          pf0 = __ldcg(pd + lane);
+          pf1 = __ldcg(pd + lane + 32);
+          pf_key = rk;
+        }
+        if (done) break;
         if ((++it & 255) == 0) {
           int stop = 0;
           if (lane == 0) {
@@ -259,8 +273,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         const double2 *cdat = a.col_data + (size_t)par * nb;
         const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
         const bool own_c = col >= row0 && col < row0 + nrow;
+        const bool have = pf_key == gkey;  // the final best was prefetched
         for (int j = lane; j < nb; j += 32) {
-          const double2 pv = __ldcg(pdat + j), cvv = __ldcg(cdat + j);
+          const double2 pv = have ? (j < 32 ? pf0 : pf1) : __ldcg(pdat + j);
+          const double2 cvv = own_p ? __ldcg(cdat + j) : make_double2(0, 0);
           s_prow_data[j] = pv;
           if (own_p) slab[j * rpc + (gr - (int)row0)] = cvv;  // row prow <- old row col
           if (own_c) slab[j * rpc + (int)(col - row0)] = pv;  // row col  <- pivot row

@@ -23,7 +23,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmomgpu.so")
+# MOM_GPU_LIB selects another build of the same library (e.g. for A/B timing).
+LIB_PATH = os.environ.get("MOM_GPU_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libmomgpu.so")
 
 MOM_OK = 0
 MOM_ERR_ARG, MOM_ERR_ALLOC, MOM_ERR_CUDA, MOM_ERR_SINGULAR, MOM_ERR_TIMEOUT = 1, 2, 3, 4, 5
