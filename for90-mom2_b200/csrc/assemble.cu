@@ -270,7 +270,7 @@ struct PairArgs {
 
 // One thread per source face n; the CTA walks kTestPerCta test faces.
 template <typename T, int NQ>
-__global__ void __launch_bounds__(kPairThreads) pair_kernel(PairArgs a) {
+__global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
   __shared__ T s_src[NQ * 3][kPairThreads];
   __shared__ T s_tst[NQ * 3];
   __shared__ double s_tmu[9], s_tsl[3], s_tcp[3];
