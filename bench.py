@@ -361,6 +361,7 @@ def run_ours(args, rank, local_rank, world):
     if not args.no_extras and world == 1:
         line["sweep"] = bench_sweep(M, args.sweep_workers, local_rank)
         line["adjoint"] = bench_adjoint(M, local_rank)
+        line["core_shell"] = bench_core_shell(M, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
         info = cpu_sample(args.subdiv, cores)
@@ -408,6 +409,37 @@ def bench_sweep(M, workers, dev):
         out[name + "_sigma_ext_first"] = float(res[0][0][0, 0] + res[0][1][0, 0])
     for s in solvers:
         s.close()
+    return out
+
+
+def bench_core_shell(M, dev, nsrc=512):
+    """Core-shell (30,720 unknowns, 3 domains) with 512 incidences: one factorisation reused
+    for all right-hand sides (GEMM-based blocked solves, FP64 ZGEMM residuals), cross
+    sections, and d(mean sigma_ext, sigma_abs)/d(shell eps) by the adjoint; mixed and FP64."""
+    import numpy as np
+    from mom_b200 import workloads as W
+    nodes, faces, ids, doms = W.core_shell(4)
+    srcs = W.incidences(nsrc)
+    S = M.Solver(dev)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU), np.sqrt(W.EPS_SILICA)]
+    out = {"workload": "core-shell s=4 (r 40/60 nm, %d unknowns), %d pw_elliptic incidences" % (2 * S.N, nsrc)}
+    ext = {}
+    for prec, name in ((M.MIXED, "mixed"), (M.FP64, "fp64")):
+        S.solve_wavelength(om, ri, srcs[:1], prec, TOL, MAXIT, want_host=False)  # autotune + graph capture
+        S.synchronize()
+        t0 = time.perf_counter()
+        S.solve_wavelength(om, ri, srcs, prec, TOL, MAXIT, want_host=False)
+        a, b = S.cross_sections(om, ri[0], srcs)
+        t1 = time.perf_counter()
+        g = S.adjoint_mean_eps(om, ri, srcs, prec, eps_dom=1, tol=TOL, maxit=MAXIT)
+        t2 = time.perf_counter()
+        ext[name] = a + b
+        out[name] = {"solve_s": t1 - t0, "rhs_per_s": nsrc / (t1 - t0), "adjoint_mean_eps_s": t2 - t1,
+                     "refine_iters": S.iters, "dmean_ext_deps": [g[0, 0], g[0, 1]]}
+    out["sigma_ext_max_rel_mixed_vs_fp64"] = float(np.max(np.abs(ext["mixed"] - ext["fp64"]) / np.abs(ext["fp64"])))
+    S.close()
     return out
 
 
