@@ -354,7 +354,7 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
       cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess ||
-      cudaMalloc(&c->flags, sizeof(unsigned) * 256) != cudaSuccess) {
+      cudaMalloc(&c->flags, sizeof(unsigned) * kFlowFlags) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return MOM_ERR_CUDA;

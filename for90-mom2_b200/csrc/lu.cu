@@ -586,7 +586,7 @@ struct TrsvArgs {
   int nb, P, rpc, ns;
   const double2 *inv;  // [nblk][2][nb][nb]: inv(L_kk), inv(U_kk)
   const int *perm;
-  double2 *X, *Y;      // [ns][n]: right-hand sides in X, scratch Y; solution returned in X
+  double2 *X, *Y, *Z;  // [ns][n]: right-hand sides in X, scratch Y, Z; solution returned in X
   unsigned *bar;
   int *timeout;
   int direct;  // 1: factor tiles do not fit in shared memory; read them from global memory
@@ -647,16 +647,23 @@ __device__ __forceinline__ void upd_range(int pass, int64_t k0, int nb, int64_t 
 }
 
 // Forward (unit lower) and backward (upper) substitution of P A = L U for
-// NS right-hand sides in one cooperative launch: per diagonal block one
-// bounded grid barrier.  CTA c owns rows [c rpc, (c+1) rpc) for the updates;
-// the factor tile of the next block is fetched into shared memory with
-// cp.async while the CTA waits at the barrier.  TR solves A^T x = b instead:
-// forward with U^T, backward with L^T (unit), then x = P^T z; the factor
-// tile of block kb is then the block row kb of U (or L) to the right (left)
-// of the diagonal, stored row by row with a padded stride.
+// NS right-hand sides in one cooperative launch, scheduled by data flow
+// instead of grid barriers.  CTA c owns whole 64-row blocks, rows
+// [c rpc, (c+1) rpc) with rpc a multiple of 64, and is the only writer of
+// those rows.  For each block k of a pass every CTA waits for flag[pass][k]
+// (set by the owner of block k once all earlier blocks' updates reach its
+// rows), computes y_k = inv_k x_k itself, and updates its own rows; the
+// owner of the next block updates that block's rows first and releases its
+// flag before updating the rest.  The critical path per block is one flag
+// hand-off, one L2 read of x_k and a 64-row update.  The factor tile of the
+// next block is fetched with cp.async while the CTA waits.  TR solves
+// A^T x = b: forward with U^T, backward with L^T (unit), x = P^T z; its
+// tile is the block row of U (L) right (left) of the diagonal, row by row
+// with a padded stride.
 template <typename T, int NS, bool TR>
-__global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
+__global__ void __launch_bounds__(256, 1) trsv_flow_kernel(TrsvArgs a) {
   __shared__ double2 xs[8 * 64], ys[8 * 64], red[256];
+  __shared__ int s_ok;
   extern __shared__ __align__(16) unsigned char tile_raw[];  // tile of T, then [nb][nb] double2
   T *tile = reinterpret_cast<T *>(tile_raw);
   // tile element (row i, column j of the block): TR i * (nb + 1) + j, else j * rpc + i
@@ -668,7 +675,12 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
   constexpr int ns = NS;
   const int64_t r0 = (int64_t)blockIdx.x * rpc;
   const int64_t r1 = min(n, r0 + rpc);
-  unsigned step = 0;
+  unsigned *flag = a.bar;  // [2][nblk]
+  auto owns = [&](int kb) { return (int64_t)kb * nb >= r0 && (int64_t)kb * nb < r1; };
+  auto signal = [&](int pass, int kb) {  // after a __syncthreads
+    if (threadIdx.x == 0)
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag + pass * nblk + kb), "r"(1u) : "memory");
+  };
   auto prefetch = [&](int pass, int kk) {
     if (kk >= nblk) return;
     const int kb = pass == 0 ? kk : nblk - 1 - kk;
@@ -693,17 +705,75 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) cp_async(sinv + idx, ib + idx, 1);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  // Y = P X (TR: Y = X)
+  // src[i] -= sum_j M(i, block) ys[j] for own rows i in [lo, hi)
+  auto update = [&](int64_t k0, int64_t lo, int64_t hi, int64_t tlo, double2 *src) {
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      double2 acc[NS];
+#pragma unroll
+      for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
+      const T *mp = TR ? (a.direct ? M + k0 + i * lda : tile + (size_t)(i - tlo) * (nb + 1))
+                       : (a.direct ? M + i + k0 * lda : tile + (i - tlo));
+      const int64_t mstride = TR ? 1 : (a.direct ? lda : rpc);
+#pragma unroll 8
+      for (int j = 0; j < nb; j++) {
+        const double2 m = ld2(mp + (size_t)j * mstride);
+#pragma unroll
+        for (int sv = 0; sv < ns; sv++) {
+          const double2 y = ys[sv * nb + j];
+          acc[sv].x += m.x * y.x - m.y * y.y;
+          acc[sv].y += m.x * y.y + m.y * y.x;
+        }
+      }
+#pragma unroll
+      for (int sv = 0; sv < ns; sv++) {
+        double2 v = src[(size_t)sv * n + i];
+        v.x -= acc[sv].x;
+        v.y -= acc[sv].y;
+        src[(size_t)sv * n + i] = v;
+      }
+    }
+  };
+  // Y = P X (TR: Y = X) for the own rows; X is rewritten below, so all
+  // CTAs finish reading it first (one grid barrier); then block 0 is ready
   for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
     for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + (TR ? i : a.perm[i])];
   prefetch(0, 0);
-  if (!flag_barrier(a.bar, a.P, ++step, a.timeout)) return;
+  unsigned *bar = flag + 2 * nblk;  // [P] barrier epochs
+  if (!flag_barrier(bar, a.P, 1u, a.timeout)) return;
+  if (owns(0)) signal(0, 0);
+  // Pass 0 reduces Y and writes the solved blocks to X; pass 1 reduces X and
+  // writes to Z.  A CTA may still be reading Y in pass 0 while others are in
+  // pass 1, hence the third vector.
   for (int pass = 0; pass < 2; pass++) {
     double2 *src = pass == 0 ? a.Y : a.X;  // vector being reduced
-    double2 *dst = pass == 0 ? a.X : a.Y;  // solved blocks
+    double2 *dst = pass == 0 ? a.X : a.Z;  // solved blocks
     for (int kk = 0; kk < nblk; kk++) {
       const int kb = pass == 0 ? kk : nblk - 1 - kk;
       const int64_t k0 = (int64_t)kb * nb;
+      // wait until block kb's rows are final (bounded)
+      if (threadIdx.x == 0) {
+        long long it = 0;
+        int ok = 1;
+        while (true) {
+          unsigned f;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flag + pass * nblk + kb) : "memory");
+          if (f) break;
+          if ((++it & 1023) == 0) {
+            if (*(volatile int *)a.timeout) {
+              ok = 0;
+              break;
+            }
+            if (it > kSpinLimit) {
+              atomicExch(a.timeout, 1);
+              ok = 0;
+              break;
+            }
+          }
+        }
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) return;
       for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
         const int j = idx % nb, sv = idx / nb;
         xs[sv * nb + j] = __ldcg(src + (size_t)sv * n + k0 + j);
@@ -711,50 +781,44 @@ __global__ void __launch_bounds__(256, 1) trsv_coop_kernel(TrsvArgs a) {
       cp_async_wait_all();
       __syncthreads();
       block_apply(sinv, nb, ns, xs, ys, red, TR);
-      // owners of block kb's rows store the solved block
-      for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
-        const int j = idx % nb, sv = idx / nb;
-        const int64_t i = k0 + j;
-        if (i >= r0 && i < r1) dst[(size_t)sv * n + i] = ys[sv * nb + j];
-      }
       int64_t lo, hi;
       upd_range(pass, k0, nb, r0, r1, &lo, &hi);
-      for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        double2 acc[NS];
-#pragma unroll
-        for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
-        const T *mp = TR ? (a.direct ? M + k0 + i * lda : tile + (size_t)(i - lo) * (nb + 1))
-                         : (a.direct ? M + i + k0 * lda : tile + (i - lo));
-        const int64_t mstride = TR ? 1 : (a.direct ? lda : rpc);
-#pragma unroll 8
-        for (int j = 0; j < nb; j++) {
-          const double2 m = ld2(mp + (size_t)j * mstride);
-#pragma unroll
-          for (int sv = 0; sv < ns; sv++) {
-            const double2 y = ys[sv * nb + j];
-            acc[sv].x += m.x * y.x - m.y * y.y;
-            acc[sv].y += m.x * y.y + m.y * y.x;
-          }
+      // the next block of this pass: its rows first, then its flag
+      const int nk = pass == 0 ? kb + 1 : kb - 1;
+      const bool own_next = nk >= 0 && nk < nblk && owns(nk);
+      if (owns(kb)) {
+        for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
+          const int j = idx % nb, sv = idx / nb;
+          dst[(size_t)sv * n + k0 + j] = ys[sv * nb + j];
         }
-#pragma unroll
-        for (int sv = 0; sv < ns; sv++) {
-          double2 v = src[(size_t)sv * n + i];
-          v.x -= acc[sv].x;
-          v.y -= acc[sv].y;
-          src[(size_t)sv * n + i] = v;
-        }
+      }
+      int64_t alo = lo, ahi = lo;  // rows of the next block inside [lo, hi)
+      if (own_next) {
+        alo = (int64_t)nk * nb;
+        ahi = alo + nb;
+        update(k0, alo, ahi, lo, src);
+      }
+      __syncthreads();
+      if (own_next) signal(pass, nk);
+      if (pass == 0 && kb == nblk - 1 && owns(kb)) signal(1, nblk - 1);  // x of pass 1 starts here
+      if (own_next) {
+        update(k0, lo, alo, lo, src);
+        update(k0, ahi, hi, lo, src);
+      } else {
+        update(k0, lo, hi, lo, src);
       }
       __syncthreads();
       // next tile: the following block of this pass, or the first of the next pass
       if (kk + 1 < nblk) prefetch(pass, kk + 1);
       else if (pass == 0) prefetch(1, 0);
-      if (!flag_barrier(a.bar, a.P, ++step, a.timeout)) return;
     }
   }
   cp_async_wait_all();
-  // the solution is in Y; return it in X (TR: X = P^T Y)
+  // X is still read by CTAs in pass 1 until all are done
+  if (!flag_barrier(bar, a.P, 2u, a.timeout)) return;
+  // the solution is in Z (own rows); return it in X (TR: X = P^T Z)
   for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + (TR ? a.perm[i] : i)] = a.Y[(size_t)s * n + i];
+    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + (TR ? a.perm[i] : i)] = a.Z[(size_t)s * n + i];
 }
 
 constexpr int kGemvRows = 256;
@@ -1151,13 +1215,16 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
 // X (n x nrhs, ld n) <- A^{-1} X (TR: A^{-T} X) with the factors in place;
 // Y is scratch.
 template <typename T, bool TR = false>
-int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
+int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, double2 *Z, int nrhs) {
   const int64_t n = c->n;
   const int nb = c->nb;
   ProfScope ps(c, kProfTrsv);
-  int P = c->nsm;
-  int rpc = (int)((n + P - 1) / P);
-  P = (int)((n + rpc - 1) / rpc);
+  // whole 64-row blocks per CTA (each block has exactly one owner)
+  const int nblk = (int)(n / nb);
+  if (2 * nblk + 256 > kFlowFlags) return fail(c, MOM_ERR_ARG, "matrix order too large for the triangular solve");
+  const int bpc = (nblk + c->nsm - 1) / c->nsm;
+  const int rpc = bpc * nb;
+  const int P = (nblk + bpc - 1) / bpc;
   for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
     ns = 8;
     while (ns > nrhs - s0) ns >>= 1;  // chunks of 8, 4, 2, 1 vectors
@@ -1173,14 +1240,15 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, int nrhs) {
     ta.perm = c->perm;
     ta.X = X + (size_t)s0 * n;
     ta.Y = Y + (size_t)s0 * n;
+    ta.Z = Z + (size_t)s0 * n;
     ta.bar = c->flags;
     ta.timeout = c->dinfo + 1;
-    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned) * 256, c->stream));
+    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned) * (2 * nblk + P), c->stream));
     void *args[] = {&ta};
-    void *fn = ns == 1 ? (void *)trsv_coop_kernel<T, 1, TR>
-               : ns == 2 ? (void *)trsv_coop_kernel<T, 2, TR>
-               : ns == 4 ? (void *)trsv_coop_kernel<T, 4, TR>
-                         : (void *)trsv_coop_kernel<T, 8, TR>;
+    void *fn = ns == 1 ? (void *)trsv_flow_kernel<T, 1, TR>
+               : ns == 2 ? (void *)trsv_flow_kernel<T, 2, TR>
+               : ns == 4 ? (void *)trsv_flow_kernel<T, 4, TR>
+                         : (void *)trsv_flow_kernel<T, 8, TR>;
     const size_t elems = TR ? (size_t)rpc * (nb + 1) : (size_t)nb * rpc;
     size_t tile = ((sizeof(T) * elems + 15) / 16) * 16 + sizeof(double2) * nb * nb;
     ta.direct = 0;
@@ -1218,22 +1286,22 @@ int lu_init_kernels(Ctx *c) {
   MOM_CUDA(c, set_smem(diag_inv_kernel<double2>));
   MOM_CUDA(c, set_smem(diag_inv_kernel<float2>));
   MOM_CUDA(c, set_smem(compose_pivots_kernel));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8, false>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 1, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 2, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 4, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<double2, 8, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 1, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 2, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 4, true>));
-  MOM_CUDA(c, set_smem(trsv_coop_kernel<float2, 8, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 1, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 2, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 4, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 8, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 1, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 2, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 4, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 8, false>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 1, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 2, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 4, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 8, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 1, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 2, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 4, true>));
+  MOM_CUDA(c, set_smem(trsv_flow_kernel<float2, 8, true>));
   return MOM_OK;
 }
 
@@ -1466,9 +1534,10 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
     if (nrhs >= kMultiRhs) {
       MOM_TRY(getrs_multi<double2>(c, c->A, X, nrhs, trans));
     } else {
-      MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, vec));
-      if (trans) MOM_TRY((getrs_t<double2, true>(c, c->A, X, (double2 *)c->ws, nrhs)));
-      else MOM_TRY((getrs_t<double2, false>(c, c->A, X, (double2 *)c->ws, nrhs)));
+      MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, 2 * vec));
+      double2 *Yw = (double2 *)c->ws, *Zw = (double2 *)((char *)c->ws + vec);
+      if (trans) MOM_TRY((getrs_t<double2, true>(c, c->A, X, Yw, Zw, nrhs)));
+      else MOM_TRY((getrs_t<double2, false>(c, c->A, X, Yw, Zw, nrhs)));
     }
     if (iters) *iters = 0;
     int tmo = 0;
@@ -1482,10 +1551,11 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
   const size_t off_r = 0, off_d = vec, off_y = 2 * vec, off_p = 3 * vec;
   const size_t part = sizeof(double2) * (size_t)nchunk * 8 * n;
   const size_t off_n = off_p + part;
-  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off_n + sizeof(double) * rblocks * nrhs + 256));
+  const size_t off_z = off_n + ((sizeof(double) * rblocks * nrhs + 255) / 256) * 256;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off_z + vec + 256));
   char *ws = (char *)c->ws;
   double2 *R = (double2 *)(ws + off_r), *Dv = (double2 *)(ws + off_d), *Yv = (double2 *)(ws + off_y),
-          *Pp = (double2 *)(ws + off_p);
+          *Pp = (double2 *)(ws + off_p), *Zv = (double2 *)(ws + off_z);
   double *rn2 = (double *)(ws + off_n);
   // ||b|| per column
   std::vector<double> bn(nrhs), h(rblocks * (size_t)nrhs);
@@ -1506,8 +1576,8 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
     MOM_CUDA(c, cudaMemcpyAsync(Dv, R, vec, cudaMemcpyDeviceToDevice, c->stream));
     const bool multi = nrhs >= kMultiRhs;
     if (multi) MOM_TRY(getrs_multi<float2>(c, c->A32, Dv, nrhs, trans));
-    else if (trans) MOM_TRY((getrs_t<float2, true>(c, c->A32, Dv, Yv, nrhs)));
-    else MOM_TRY((getrs_t<float2, false>(c, c->A32, Dv, Yv, nrhs)));
+    else if (trans) MOM_TRY((getrs_t<float2, true>(c, c->A32, Dv, Yv, Zv, nrhs)));
+    else MOM_TRY((getrs_t<float2, false>(c, c->A32, Dv, Yv, Zv, nrhs)));
     axpy_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(X, Dv, (int64_t)n * nrhs);
     c->launches++;
     ProfScope pr(c, kProfResidual);

@@ -25,6 +25,7 @@ constexpr double kEta0 = 3.767303134622e2;
 
 constexpr int kMaxQ = 13;
 constexpr size_t kBlasWorkspace = 64u << 20;
+constexpr int kFlowFlags = 8192;  // 2 passes x 64-row blocks: orders up to 262,144
 
 // Per-domain device data (structure of arrays).  "Half-edge" h = 3*face +
 // local edge identifies one RWG half (one face of an edge).
@@ -94,7 +95,7 @@ struct Ctx {
   double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
   size_t invd_bytes = 0;
   int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout
-  unsigned *flags = nullptr;  // [256] per-CTA barrier epochs of the cooperative solve kernel
+  unsigned *flags = nullptr;  // [kFlowFlags] block-ready flags of the triangular solve kernel
   void *ws = nullptr;      // general device workspace
   size_t ws_bytes = 0;
   void *ws2 = nullptr;     // workspace of the many-right-hand-side solve
