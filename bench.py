@@ -305,8 +305,12 @@ def run_ours(args, rank, local_rank, world):
     if cnt:
         bytes_ = sum(2.0 * 8 * (n - k * nb) * nb for k in range(n // nb)) * args.steps  # FP32 panel read + write
         ach = bytes_ / (ms * 1e-3) / 1e9
-        roofs["panel"] = {"kernel": "panel_kernel<float2> (pivoted panel, grid barrier per column)", "bound": "hbm",
-                          "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs, "traffic": None,
+        # DRAM bytes of one panel launch at m = 3520 rows (ncu, profiles/panel_kernel_s3.md),
+        # scaled by rows to the average panel height of this order
+        traffic = 1.841e6 * (n / 2.0) / 3520.0
+        roofs["panel"] = {"kernel": "panel_kernel<float2> (pivoted panel, one device-wide exchange per column)",
+                          "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs,
+                          "traffic": traffic, "traffic_note": "bytes per launch, ncu at 3520 rows scaled by rows",
                           "peak_note": "%s; latency-bound: one device-wide pivot exchange per column" % peak_src}
     ms, cnt = prof["pair"]
     if cnt:
@@ -314,14 +318,18 @@ def run_ours(args, rank, local_rank, world):
         ach = flop / (ms * 1e-3) / 1e12
         peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         roofs["pair"] = {"kernel": "pair_kernel<float,13> (far-pair assembly, FP32 pipe)", "bound": "fp32",
-                         "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak, "traffic": None,
+                         "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak,
+                         "traffic": 430.4e6 * (F / 1280.0) ** 2,
+                         "traffic_note": "bytes per launch, ncu at 1280 faces scaled by face pairs",
                          "peak_note": "nominal FP32 SIMT at the sampled SM clock %.0f MHz" % sm_mhz}
     ms, cnt = prof["trsv"]
     if cnt:
         bytes_ = 8.0 * n * n * cnt  # FP32 L and U factors read once per solve
         ach = bytes_ / (ms * 1e-3) / 1e9
-        roofs["trsv"] = {"kernel": "trsv_flow_kernel<float2> (forward+backward substitution, data-flow schedule)", "bound": "hbm",
-                         "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs, "traffic": None,
+        roofs["trsv"] = {"kernel": "trsv_flow_kernel<float2> (forward+backward substitution, data-flow schedule)",
+                         "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": hbm_gbs, "frac": ach / hbm_gbs,
+                         "traffic": 127.8e6 * (n / 3840.0) ** 2,
+                         "traffic_note": "bytes per launch, ncu at 3840 unknowns scaled by n^2",
                          "peak_note": peak_src}
     ms, cnt = prof["residual"]
     if cnt:
