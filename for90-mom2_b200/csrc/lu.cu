@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <vector>
 
@@ -331,6 +332,177 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     const int c = idx / rpc, ii = idx % rpc;
     if (ii < nrow) st2(A + (row0 + ii) + (a.j0 + c) * a.lda, slab[idx]);
   }
+}
+
+// ---- short panels: one thread-block cluster, exchange in distributed shared memory ----
+
+constexpr int kMaxCluster = 16;
+constexpr int kClusterRows = 176;  // rows per CTA of a cluster panel (FP64 slab + pushed rows in shared memory)
+
+__device__ __forceinline__ unsigned map_shared(const void *p, unsigned rank) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster_u64(unsigned addr, unsigned long long v) {
+  asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
+}
+__device__ __forceinline__ double2 ld_cluster_d2(unsigned addr) {
+  double2 v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
+  return v;
+}
+// Every thread of every CTA of the cluster; orders shared-memory accesses
+// across the cluster (release / acquire).
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void st_cluster_d2(unsigned addr, double2 v) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y) : "memory");
+}
+
+// The same panel factorisation as panel_kernel for panels of at most
+// kClusterRows * kMaxCluster rows, on a grid that is exactly one cluster of
+// P CTAs (all co-scheduled by the hardware).  Per column each CTA pushes
+// its packed candidate key and the candidate row (and the owner of row col
+// that row) into every CTA's shared memory, then one cluster barrier; the
+// winner, the pivot row and the displaced row are then read locally.  The
+// pushed buffers alternate by column parity, so one barrier per column
+// suffices.  No global memory round trip and no spin-wait: every thread of
+// the cluster executes the same sequence of cluster barriers.
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelArgs a) {
+  extern __shared__ double2 slab[];  // [nb][rpc] column-major, then the pushed rows
+  __shared__ unsigned long long w_key[kPanelThreads / 32];
+  __shared__ unsigned long long c_key[2][kMaxCluster];
+  __shared__ double2 s_prow_data[64];
+  __shared__ double2 s_l[kPanelThreads];
+  __shared__ double2 s_rp;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;  // cta == cluster rank
+  const int nb = a.nb, rpc = a.rpc, P = a.P;
+  double2 *recv_row = slab + (size_t)nb * rpc;           // [2][P][nb] candidate rows by sender
+  double2 *recv_col = recv_row + (size_t)2 * P * nb;    // [2][nb] row col, from its owner
+  T *A = reinterpret_cast<T *>(a.A);
+  const int64_t row0 = a.j0 + (int64_t)cta * rpc;
+  const int64_t rem = a.n - row0;
+  const int nrow = rem <= 0 ? 0 : (rem < rpc ? (int)rem : rpc);
+  for (int base = tid; base < nb * rpc; base += 8 * kPanelThreads) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * kPanelThreads;
+      const int c = idx / rpc, i = idx % rpc;
+      v[u] = (idx < nb * rpc && i < nrow) ? ld2(A + (row0 + i) + (a.j0 + c) * a.lda) : make_double2(0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int idx = base + u * kPanelThreads;
+      if (idx < nb * rpc) slab[idx] = v[u];
+    }
+  }
+  __syncthreads();
+  const int S = kPanelThreads / rpc;  // threads per row (rpc <= kPanelThreads)
+  const int i = tid % rpc, sph = tid / rpc;
+  const bool mine = sph < S && i < nrow;
+  const int64_t g = row0 + i;  // global row of this thread
+  double cv = (mine && sph == 0) ? cabs1(slab[i]) : -1.0;  // candidate for column 0
+  for (int c = 0; c < nb; c++) {
+    const int64_t col = a.j0 + c;
+    const int par = c & 1;
+    // 1. CTA candidate; push key and row (and row col, if owned) to every CTA
+    const unsigned long long wk = warp_max_key(cv >= 0.0 ? pack_candidate(cv, g, a.j0, 0) : 0ull);
+    if (lane == 0) w_key[wid] = wk;
+    __syncthreads();
+    if (wid == 0) {
+      const unsigned long long bkey = warp_max_key(lane < kPanelThreads / 32 ? w_key[lane] : 0ull);
+      if (lane < P) st_cluster_u64(map_shared(&c_key[par][cta], (unsigned)lane), bkey);
+      if (bkey != 0ull) {
+        const int li = (int)(0xffffffu - (unsigned)((bkey >> 8) & 0xffffffu)) - (int)(row0 - a.j0);
+        const double2 v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
+        double2 *dst = recv_row + ((size_t)par * P + cta) * nb;
+        for (int t = 0; t < P; t++) {
+          const unsigned base = map_shared(dst, (unsigned)t);
+          st_cluster_d2(base + (unsigned)lane * 16u, v0);
+          st_cluster_d2(base + (unsigned)(lane + 32) * 16u, v1);
+        }
+      }
+      if (col >= row0 && col < row0 + nrow) {
+        const int li = (int)(col - row0);
+        const double2 v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
+        double2 *dst = recv_col + (size_t)par * nb;
+        for (int t = 0; t < P; t++) {
+          const unsigned base = map_shared(dst, (unsigned)t);
+          st_cluster_d2(base + (unsigned)lane * 16u, v0);
+          st_cluster_d2(base + (unsigned)(lane + 32) * 16u, v1);
+        }
+      }
+    }
+    cluster_sync();
+    // 2. the winner, read locally; swap
+    if (wid == 0) {
+      const unsigned long long k = lane < P ? c_key[par][lane] : 0ull;
+      const unsigned long long gkey = warp_max_key(k);
+      const int gw = __ffs(__ballot_sync(0xffffffffu, lane < P && k == gkey)) - 1;
+      const int gsrc = gw < 0 ? 0 : gw;
+      const int gr = (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
+      const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
+      const bool own_c = col >= row0 && col < row0 + nrow;
+      const double2 *prow = recv_row + ((size_t)par * P + gsrc) * nb, *crow = recv_col + (size_t)par * nb;
+      for (int j = lane; j < nb; j += 32) {
+        const double2 pv = prow[j];
+        s_prow_data[j] = pv;
+        if (own_p) slab[j * rpc + (gr - (int)row0)] = crow[j];  // row prow <- old row col
+        if (own_c) slab[j * rpc + (int)(col - row0)] = pv;      // row col  <- pivot row
+        if (j == c) {
+          const double pa = pv.x * pv.x + pv.y * pv.y;
+          s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
+          if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
+        }
+      }
+      if (lane == 0 && cta == 0) a.ipiv[col] = gr;
+    }
+    __syncthreads();
+    // 3. scale column c, rank-1 update of columns c+1 ..
+    const double2 rp = s_rp;
+    const bool live = mine && g > col && (rp.x != 0.0 || rp.y != 0.0);
+    if (live && sph == 0) {
+      const double2 l = cmul(slab[c * rpc + i], rp);
+      slab[c * rpc + i] = l;
+      s_l[i] = l;
+    }
+    __syncthreads();
+    cv = -1.0;
+    const int own = (c + 1) % S;
+    if (mine && g > col) {
+      const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
+      if (live) {
+        const double2 l = s_l[i];
+        for (int j = jst; j < nb; j += 4 * S) {
+          double2 x[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j + u * S < nb) x[u] = slab[(j + u * S) * rpc + i];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (j + u * S < nb) {
+              const double2 uu = s_prow_data[j + u * S];
+              x[u].x -= l.x * uu.x - l.y * uu.y;
+              x[u].y -= l.x * uu.y + l.y * uu.x;
+              slab[(j + u * S) * rpc + i] = x[u];
+            }
+        }
+      }
+      if (sph == own && c + 1 < nb) cv = cabs1(slab[(c + 1) * rpc + i]);
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
+    const int c = idx / rpc, ii = idx % rpc;
+    if (ii < nrow) st2(A + (row0 + ii) + (a.j0 + c) * a.lda, slab[idx]);
+  }
+  cluster_sync();  // no CTA leaves while another may still address its shared memory
 }
 
 // The nb row interchanges of a panel (ipiv[j0 .. j0+nb), applied in order)
@@ -999,6 +1171,41 @@ template <typename T>
 int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *ipiv, int *info, const LuWork &w) {
   const int nb = c->nb;
   const int64_t m = n - j0;
+  if (c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster) {
+    // short panel: one cluster, the smallest power of two with <= kClusterRows rows per CTA
+    int CL = 1;
+    while ((int64_t)kClusterRows * CL < m) CL *= 2;
+    const int rpc = (int)((m + CL - 1) / CL);
+    PanelArgs pa;
+    pa.A = A;
+    pa.lda = lda;
+    pa.n = n;
+    pa.j0 = j0;
+    pa.nb = nb;
+    pa.rpc = rpc;
+    pa.P = CL;
+    pa.ipiv = ipiv;
+    pa.info = info;
+    pa.timeout = w.timeout;
+    pa.rec = nullptr;
+    pa.cand_data = nullptr;
+    pa.col_data = nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL);
+    cfg.blockDim = dim3(kPanelThreads);
+    cfg.dynamicSmemBytes = sizeof(double2) * ((size_t)nb * rpc + (size_t)2 * CL * nb + 2 * nb);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    MOM_CUDA(c, cudaLaunchKernelEx(&cfg, panel_cluster_kernel<T>, pa));
+    c->launches++;
+    return MOM_OK;
+  }
   const int rpc = (int)((m + P - 1) / P);
   P = (int)((m + rpc - 1) / rpc);
   const size_t smem = sizeof(double2) * (size_t)nb * rpc;
@@ -1280,9 +1487,42 @@ cudaError_t set_smem(T *fn) {
 
 // Shared-memory opt-in of the LU kernels, once per context (outside any
 // stream capture and off the factorisation's critical path).
+// Largest cluster (power of two <= 16) with one panel CTA per SM that the
+// device can schedule; 0 when clusters are unavailable.
+template <typename T>
+int max_panel_cluster() {
+  if (cudaFuncSetAttribute(panel_cluster_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 8;
+  }
+  for (int cl = kMaxCluster; cl >= 2; cl /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(kPanelThreads);
+    cfg.dynamicSmemBytes = sizeof(double2) * (64 * kClusterRows + 2 * cl * 64 + 2 * 64);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, panel_cluster_kernel<T>, &cfg) == cudaSuccess && nclusters >= 1)
+      return cl;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
 int lu_init_kernels(Ctx *c) {
   MOM_CUDA(c, set_smem(panel_kernel<double2>));
   MOM_CUDA(c, set_smem(panel_kernel<float2>));
+  MOM_CUDA(c, set_smem(panel_cluster_kernel<double2>));
+  MOM_CUDA(c, set_smem(panel_cluster_kernel<float2>));
+  c->panel_cluster = std::min(max_panel_cluster<double2>(), max_panel_cluster<float2>());
+  const char *ec = std::getenv("MOM_PANEL_CLUSTER");
+  if (ec) c->panel_cluster = std::max(0, std::min(c->panel_cluster, std::atoi(ec)));
   MOM_CUDA(c, set_smem(diag_inv_kernel<double2>));
   MOM_CUDA(c, set_smem(diag_inv_kernel<float2>));
   MOM_CUDA(c, set_smem(compose_pivots_kernel));

@@ -136,6 +136,9 @@ struct Ctx {
   // autotuned per (matrix order, precision) at the first factorisation
   // (unless MOM_AUTOTUNE=0: one CTA per SM); MOM_PANEL_CTAS fixes a cap.
   int panel_cap_env = 0;
+  // Short panels run on one thread-block cluster of up to panel_cluster CTAs
+  // (the largest the device schedules; MOM_PANEL_CLUSTER caps it, 0 = off).
+  int panel_cluster = 0;
   bool autotune = true;
   struct Tuned {
     int64_t n;
