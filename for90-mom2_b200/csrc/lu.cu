@@ -1579,7 +1579,10 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
   for (int64_t m = n; m >= 128 && rc == MOM_OK; m /= 2) {
     int best = c->nsm, last = -1;
     double best_ms = 1e30;
+    // heights that run on one cluster have nothing to tune: one timed trial
+    const bool clustered = c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster;
     for (int cand : cands) {
+      if (clustered && cand != cands[0]) break;
       const int P0 = (int)std::min<int64_t>(c->nsm, std::max<int64_t>(std::min<int64_t>(cand, (m + 7) / 8), (m + 207) / 208));
       const int rpc = (int)((m + P0 - 1) / P0);
       const int P = (int)((m + rpc - 1) / rpc);
