@@ -1121,7 +1121,8 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
   const size_t o_w = take(esz * (size_t)nb * c->n);
   const size_t o_i32 = take(sizeof(float2) * (size_t)nb * c->n);
   const size_t o_pm = take(sizeof(int) * 260);
-  const size_t o_tc = take(precision == MOM_PREC_MIXED ? tc_cgemm_work_bytes((int)c->n, (int)c->n, 4 * nb) : 0);
+  const size_t o_tc =
+      take(precision == MOM_PREC_MIXED ? tc_cgemm_work_bytes((int)c->n, (int)c->n, c->outer_panels * nb) : 0);
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off));
   char *b = (char *)c->ws;
   w.bar = (unsigned *)(b + o_bar);
@@ -1271,7 +1272,7 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
                                   cudaMemcpyDeviceToDevice, c->stream));
     return MOM_OK;
   };
-  const int NB = 4 * nb;  // outer block: trailing updates run with K = NB
+  const int NB = c->outer_panels * nb;  // outer block: trailing updates run with K = NB
   for (int64_t J0 = 0; J0 < n; J0 += NB) {
     const int64_t NBc = std::min<int64_t>(NB, n - J0);
     for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
@@ -1389,7 +1390,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
-                                        (uintptr_t)tune_hash(c)};
+                                        (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels};
     g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
     if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));

@@ -139,6 +139,7 @@ struct Ctx {
   // Short panels run on one thread-block cluster of up to panel_cluster CTAs
   // (the largest the device schedules; MOM_PANEL_CLUSTER caps it, 0 = off).
   int panel_cluster = 0;
+  int outer_panels = 4;  // panels per outer block of the LU (MOM_LU_OUTER): trailing GEMMs have K = 64 * this
   bool autotune = true;
   struct Tuned {
     int64_t n;
