@@ -625,13 +625,14 @@ __device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
 // from o = 2 B p): C(o+cr.., o+cc..) = s * A(o+ar.., o+ac..) * B(o+br.., o+bc..),
 // B x B blocks of 64 x 64 column-major shared arrays, with k restricted to
 // the non-zero part of the triangular factor: MODE 0 k >= col, 1 k <= row,
-// 2 k <= col, 3 k >= row.  Thread u < 256 makes B / 8 outputs.
-template <int B, int MODE>
+// 2 k <= col, 3 k >= row.  NT threads (u < NT) share the 32 B outputs.
+template <int B, int MODE, int NT>
 __device__ __forceinline__ void join_product(int u, double s, const double2 *Am, int ar, int ac, const double2 *Bm,
                                              int br, int bc, double2 *Cm, int cr, int cc) {
 #pragma unroll
-  for (int i = 0; i < B / 8; i++) {
-    const int e = u + 256 * i;
+  for (int i = 0; i < (32 * B + NT - 1) / NT; i++) {
+    const int e = u + NT * i;
+    if (e >= 32 * B) break;
     const int p = e / (B * B), rem = e % (B * B);
     const int col = rem / B, row = rem % B;
     const int o = 2 * B * p;
@@ -647,21 +648,38 @@ __device__ __forceinline__ void join_product(int u, double s, const double2 *Am,
 
 // L: T = L21 X11 into the upper slot, then X21 = -X22 T;
 // U: T = U12 Y22 into the lower slot, then Y12 = -Y11 T.
-template <int B>
+// TRI 0: L only, 1: U only (all threads on one triangle), 2: both.
+template <int B, int TRI>
 __device__ __forceinline__ void join_level(int t, const double2 *D, double2 *XL, double2 *XU) {
-  if (t < 256) join_product<B, 0>(t, 1.0, D, B, 0, XL, 0, 0, XL, 0, B);
-  else join_product<B, 2>(t - 256, 1.0, D, 0, B, XU, B, B, XU, B, 0);
-  __syncthreads();
-  if (t < 256) join_product<B, 1>(t, -1.0, XL, B, B, XL, 0, B, XL, B, 0);
-  else join_product<B, 3>(t - 256, -1.0, XU, 0, 0, XU, B, 0, XU, 0, B);
+  if (TRI == 0) {
+    join_product<B, 0, kDiagThreads>(t, 1.0, D, B, 0, XL, 0, 0, XL, 0, B);
+    __syncthreads();
+    join_product<B, 1, kDiagThreads>(t, -1.0, XL, B, B, XL, 0, B, XL, B, 0);
+  } else if (TRI == 1) {
+    join_product<B, 2, kDiagThreads>(t, 1.0, D, 0, B, XU, B, B, XU, B, 0);
+    __syncthreads();
+    join_product<B, 3, kDiagThreads>(t, -1.0, XU, 0, 0, XU, B, 0, XU, 0, B);
+  } else {
+    if (t < 256) join_product<B, 0, 256>(t, 1.0, D, B, 0, XL, 0, 0, XL, 0, B);
+    else join_product<B, 2, 256>(t - 256, 1.0, D, 0, B, XU, B, B, XU, B, 0);
+    __syncthreads();
+    if (t < 256) join_product<B, 1, 256>(t, -1.0, XL, B, B, XL, 0, B, XL, B, 0);
+    else join_product<B, 3, 256>(t - 256, -1.0, XU, 0, 0, XU, B, 0, XU, 0, B);
+  }
   __syncthreads();
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int64_t lda, int64_t j0, double2 *invL,
-                                                                double2 *invU, float2 *invL32) {
+// CTA b inverts the diagonal block kb = kb0 + b (rows and columns 64 kb ..)
+// of the factors in A: inv(L11) into invd[kb][0] (and FP32 into
+// invL32[kb]), inv(U11) into invd[kb][1], for the triangles TRI selects.
+template <typename T, int TRI>
+__global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int64_t lda, int kb0, double2 *invd,
+                                                                float2 *invL32) {
   extern __shared__ double2 sm[];
   constexpr int nb = kDiagNb, nn = kDiagNb * kDiagNb;
+  const int kb = kb0 + blockIdx.x;
+  const int64_t j0 = (int64_t)kb * nb;
+  double2 *invL = invd + (size_t)kb * 2 * nn, *invU = invL + nn;
   double2 *D = sm, *XL = sm + nn, *XU = sm + 2 * nn, *rinv = sm + 3 * nn;
   const int t = threadIdx.x;
   // eight independent loads in flight per thread before the shared stores
@@ -676,14 +694,15 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int6
     for (int u = 0; u < nn / kDiagThreads; u++) D[t + u * kDiagThreads] = v[u];
   }
   __syncthreads();
-  if (t < nb) {  // 1 / U_ii (0 for a zero pivot; the panel reports it)
+  if (TRI != 0 && t < nb) {  // 1 / U_ii (0 for a zero pivot; the panel reports it)
     const double2 d = D[t + t * nb];
     const double dd = d.x * d.x + d.y * d.y;
     rinv[t] = dd != 0.0 ? make_double2(d.x / dd, -d.y / dd) : make_double2(0, 0);
   }
   __syncthreads();
   // the 8 x 8 diagonal blocks: thread (block q, column c) by substitution
-  if (t < 64) {
+  const int tl = TRI == 2 ? 256 : 0;  // first thread of the U triangle
+  if (TRI != 1 && t < 64) {
     const int q = t >> 3, c = t & 7, o = 8 * q;
     double2 x[8];
 #pragma unroll
@@ -700,8 +719,8 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int6
     }
 #pragma unroll
     for (int i = 0; i < 8; i++) XL[(o + i) + (o + c) * nb] = x[i];
-  } else if (t >= 256 && t < 256 + 64) {
-    const int q = (t - 256) >> 3, c = t & 7, o = 8 * q;
+  } else if (TRI != 0 && t >= tl && t < tl + 64) {
+    const int q = (t - tl) >> 3, c = t & 7, o = 8 * q;
     double2 y[8];
 #pragma unroll
     for (int i = 7; i >= 0; i--) {
@@ -719,16 +738,17 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(const T *A, int6
     for (int i = 0; i < 8; i++) XU[(o + i) + (o + c) * nb] = y[i];
   }
   __syncthreads();
-  join_level<8>(t, D, XL, XU);
-  join_level<16>(t, D, XL, XU);
-  join_level<32>(t, D, XL, XU);
+  join_level<8, TRI>(t, D, XL, XU);
+  join_level<16, TRI>(t, D, XL, XU);
+  join_level<32, TRI>(t, D, XL, XU);
   for (int idx = t; idx < nn; idx += kDiagThreads) {
     const int r = idx % nb, c = idx / nb;
-    const double2 l = r > c ? XL[idx] : make_double2(r == c ? 1.0 : 0.0, 0.0);
-    const double2 u = r <= c ? XU[idx] : make_double2(0, 0);
-    invL[idx] = l;
-    invU[idx] = u;
-    if (invL32) invL32[idx] = make_float2((float)l.x, (float)l.y);
+    if (TRI != 1) {
+      const double2 l = r > c ? XL[idx] : make_double2(r == c ? 1.0 : 0.0, 0.0);
+      invL[idx] = l;
+      if (invL32) invL32[(size_t)kb * nn + idx] = make_float2((float)l.x, (float)l.y);
+    }
+    if (TRI != 0) invU[idx] = r <= c ? XU[idx] : make_double2(0, 0);
   }
 }
 
@@ -1292,10 +1312,10 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
         }
       }
       {
+        // inv(L11) now (the block TRSM needs it); inv(U11) of all blocks after the loop
         ProfScope pd(c, kProfDiagInv);
-        double2 *invL = c->invd + (size_t)kb * 2 * nb * nb, *invU = invL + (size_t)nb * nb;
-        diag_inv_kernel<T><<<1, kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), c->stream>>>(
-            A, lda, j0, invL, invU, mixed ? w.invL32 + (size_t)kb * nb * nb : nullptr);
+        diag_inv_kernel<T, 0><<<1, kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), c->stream>>>(
+            A, lda, kb, c->invd, mixed ? w.invL32 : nullptr);
         c->launches++;
         MOM_CUDA(c, cudaGetLastError());
       }
@@ -1331,6 +1351,14 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
     }
   }
   MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+  {
+    // inv(U11) of every diagonal block (only the solves need them), one CTA per block
+    ProfScope pd(c, kProfDiagInv);
+    diag_inv_kernel<T, 1><<<(unsigned)(n / nb), kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), c->stream>>>(
+        A, lda, 0, c->invd, nullptr);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
   compose_pivots_kernel<<<1, 256, sizeof(int) * n, c->stream>>>(c->ipiv, (int)n, c->perm);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
@@ -1524,8 +1552,10 @@ int lu_init_kernels(Ctx *c) {
   c->panel_cluster = std::min(max_panel_cluster<double2>(), max_panel_cluster<float2>());
   const char *ec = std::getenv("MOM_PANEL_CLUSTER");
   if (ec) c->panel_cluster = std::max(0, std::min(c->panel_cluster, std::atoi(ec)));
-  MOM_CUDA(c, set_smem(diag_inv_kernel<double2>));
-  MOM_CUDA(c, set_smem(diag_inv_kernel<float2>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<double2, 0>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<float2, 0>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<double2, 1>));
+  MOM_CUDA(c, set_smem(diag_inv_kernel<float2, 1>));
   MOM_CUDA(c, set_smem(compose_pivots_kernel));
   MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 1, false>));
   MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 2, false>));
