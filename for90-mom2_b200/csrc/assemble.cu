@@ -80,7 +80,7 @@ __device__ __forceinline__ void zero(Cx<T> &a) {
 // Point-pair loop.  rho_t: test point offsets (stride 3), rho_s: source
 // offsets with stride sstride between coordinates; w from constant memory.
 // SMOOTH selects the singularity-subtracted kernels (green.f90:40-97).
-template <typename T, int NQ, bool SMOOTH>
+template <typename T, int NQ, bool SMOOTH, bool LOSSLESS = false>
 __device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int sstride, const T d[3], T kr, T ki,
                                              Moments<T> &M) {
   zero(M.TA);
@@ -114,7 +114,7 @@ __device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int
         const T R = R2 * iR;
         T sn, cs;
         fsincos(kr * R, &sn, &cs);
-        const T ea = fexp(-ki * R);
+        const T ea = LOSSLESS ? (T)1 : fexp(-ki * R);  // real k: no decay factor
         const T er = ea * cs, ei = ea * sn;  // e^{ikR}
         const T iR2 = iR * iR;
         const T iR3 = iR2 * iR;
@@ -265,11 +265,11 @@ struct PairArgs {
   double kr, ki;       // k * L0
   Cd fD, fH;
   double fK;
-  double2 *blk;        // [F][F][18]
+  double2 *blk;        // [F source][F test][18]
 };
 
 // One thread per source face n; the CTA walks kTestPerCta test faces.
-template <typename T, int NQ>
+template <typename T, int NQ, bool LOSSLESS>
 __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
   __shared__ T s_src[NQ * 3][kPairThreads];
   __shared__ T s_tst[NQ * 3];
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
       dT[i] = (T)dd[i];
     }
     Moments<T> Mt;
-    pair_moments<T, NQ, false>(s_tst, &s_src[0][tid], kPairThreads, dT, (T)a.kr, (T)a.ki, Mt);
+    pair_moments<T, NQ, false, LOSSLESS>(s_tst, &s_src[0][tid], kPairThreads, dT, (T)a.kr, (T)a.ki, Mt);
     double mu[3][3], slp[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
 #pragma unroll
       for (int j = 0; j < 3; j++) mu[i][j] = s_tmu[3 * i + j];
     }
-    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, m == n, a.blk + ((size_t)m * a.F + n) * 18);
+    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, m == n, a.blk + ((size_t)n * a.F + m) * 18);
   }
 }
 
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
   const double *st = a.stat + j * 54;
   const double f4 = 1.0 / (4.0 * kPi);
   const Cd f8 = {a.k2.re / (8.0 * kPi), a.k2.im / (8.0 * kPi)};
-  double2 *dst = a.blk + ((size_t)m * a.F + n) * 18;
+  double2 *dst = a.blk + ((size_t)n * a.F + m) * 18;
 #pragma unroll
   for (int i = 0; i < 9; i++) {
     Cd dterm = {f4 * st[i] - f8.re * st[9 + i], -f8.im * st[9 + i]};
@@ -602,7 +602,7 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherArgs a) {
     for (int j = 0; j < 2; j++) {
       if (h2[j] < 0) continue;
       const int m = h1[i] / 3, p = h1[i] % 3, n = h2[j] / 3, q = h2[j] % 3;
-      const double4 v = *reinterpret_cast<const double4 *>(a.blk + ((size_t)m * a.F + n) * 18 + 2 * (3 * p + q));
+      const double4 v = *reinterpret_cast<const double4 *>(a.blk + ((size_t)n * a.F + m) * 18 + 2 * (3 * p + q));
       sr += v.x;
       si += v.y;
       kr += v.z;
@@ -647,19 +647,25 @@ __global__ void convert_to_fp32(const double2 *__restrict__ A, float2 *__restric
   }
 }
 
-template <typename T>
-int launch_pair(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
+template <typename T, bool LOSSLESS>
+int launch_pair_k(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
   switch (nq) {
-    case 1: pair_kernel<T, 1><<<grid, kPairThreads, 0, c->stream>>>(a); break;
-    case 3: pair_kernel<T, 3><<<grid, kPairThreads, 0, c->stream>>>(a); break;
-    case 4: pair_kernel<T, 4><<<grid, kPairThreads, 0, c->stream>>>(a); break;
-    case 7: pair_kernel<T, 7><<<grid, kPairThreads, 0, c->stream>>>(a); break;
-    case 13: pair_kernel<T, 13><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 1: pair_kernel<T, 1, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 3: pair_kernel<T, 3, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 4: pair_kernel<T, 4, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 7: pair_kernel<T, 7, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 13: pair_kernel<T, 13, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
     default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
   }
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
   return MOM_OK;
+}
+
+// A lossless medium (real k) skips the decay factor e^{-Im(k) R}.
+template <typename T>
+int launch_pair(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
+  return a.ki == 0.0 ? launch_pair_k<T, true>(c, nq, grid, a) : launch_pair_k<T, false>(c, nq, grid, a);
 }
 
 }  // namespace

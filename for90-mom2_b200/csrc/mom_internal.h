@@ -88,7 +88,7 @@ struct Ctx {
   double2 *A = nullptr;    // FP64 matrix (LU in place in FP64 mode)
   float2 *A32 = nullptr;   // FP32 copy (LU in place in mixed mode)
   size_t A_bytes = 0, A32_bytes = 0;
-  double2 *blk = nullptr;  // face-pair blocks, [F][F][9][2] of the largest domain
+  double2 *blk = nullptr;  // face-pair blocks [source F][test F][9][2] of the largest domain
   size_t blk_bytes = 0;
   int *ipiv = nullptr;     // [n]
   int *perm = nullptr;     // [n] composed row permutation of the factorisation
