@@ -510,7 +510,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-extras", action="store_true", help="skip the sweep and adjoint side measurements")
-    ap.add_argument("--sweep-workers", type=int, default=3, help="concurrent contexts per sweep mesh")
+    ap.add_argument("--sweep-workers", type=int, default=6, help="concurrent contexts per sweep mesh")
     args = ap.parse_args()
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
