@@ -117,6 +117,7 @@ void free_problem(Ctx *c) {
   cudaFree(c->ipiv);
   cudaFree(c->perm);
   cudaFree(c->invd);
+  cudaFree(c->inv32);
   cudaFree(c->B);
   cudaFree(c->X);
   c->A = nullptr;
@@ -125,6 +126,7 @@ void free_problem(Ctx *c) {
   c->ipiv = nullptr;
   c->perm = nullptr;
   c->invd = nullptr;
+  c->inv32 = nullptr;
   c->B = c->X = nullptr;
   c->BX_cap = 0;
   c->have_problem = false;
@@ -309,8 +311,11 @@ int ensure_rhs(Ctx *c, int nsrc) {
 int ensure_a32(Ctx *c) {
   if (c->A32) return MOM_OK;
   const size_t bytes = sizeof(float2) * (size_t)c->lda * c->n;
-  if (cudaMalloc(&c->A32, bytes) != cudaSuccess) {
+  if (cudaMalloc(&c->A32, bytes) != cudaSuccess ||
+      cudaMalloc(&c->inv32, sizeof(float2) * 2 * (size_t)c->nb * c->n) != cudaSuccess) {
     cudaGetLastError();
+    cudaFree(c->A32);
+    c->A32 = nullptr;
     return fail(c, MOM_ERR_ALLOC, "FP32 matrix allocation failed");
   }
   c->A32_bytes = bytes;
@@ -353,8 +358,7 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   c->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess ||
-      cudaMalloc(&c->flags, sizeof(unsigned) * kFlowFlags) != cudaSuccess) {
+      cudaMalloc(&c->dinfo, sizeof(int) * 16) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return MOM_ERR_CUDA;
@@ -399,7 +403,6 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->adj_part);
   cudaFree(c->adjW);
   cudaFree(c->dinfo);
-  cudaFree(c->flags);
   if (c->pinned) cudaFreeHost(c->pinned);
   for (auto &g : c->lu_graph) g.reset();
   cublasDestroy(c->blas);
@@ -591,6 +594,21 @@ int mom_gpu_autotune_result(mom_ctx *c, int32_t precision, int32_t max_entries, 
       }
       *nent = (int32_t)t.m.size();
       if (tune_ms) *tune_ms = t.ms;
+      return MOM_OK;
+    }
+  return fail(c, MOM_ERR_STATE, "no autotuning result for this matrix order and precision");
+}
+
+int mom_gpu_autotune_placement(mom_ctx *c, int32_t precision, int32_t max_entries, int32_t *nent, int32_t *chosen,
+                               double *us_per_column) {
+  if (!c || !nent || !chosen) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  for (const auto &t : c->tuned)
+    if (t.n == c->n && t.precision == precision) {
+      const int k = std::min<int>(max_entries, (int)t.xslot_us.size());
+      for (int i = 0; us_per_column && i < k; i++) us_per_column[i] = t.xslot_us[i];
+      *nent = (int32_t)t.xslot_us.size();
+      *chosen = t.xslot;
       return MOM_OK;
     }
   return fail(c, MOM_ERR_STATE, "no autotuning result for this matrix order and precision");

@@ -82,60 +82,6 @@ __device__ __forceinline__ void argmax_warp(double &v, int &r, int &w) {
   }
 }
 
-// Grid barrier for warp 0 of each CTA: CTA c publishes its arrival epoch in
-// flags[c] with a release store (no same-address atomics), then the warp
-// polls all P flags with acquire loads until every CTA has reached epoch.
-// Bounded: after kSpinLimit polling rounds *timeout is set and the warp
-// returns false.  flags[] is zeroed before the launch.
-__device__ __forceinline__ bool flag_barrier_warp0(unsigned *flags, int P, unsigned epoch, int *timeout) {
-  const int lane = threadIdx.x & 31;
-  __threadfence();
-  __syncwarp();
-  if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flags + blockIdx.x), "r"(epoch) : "memory");
-  long long it = 0;
-  int ok = 1;
-  while (true) {
-    bool done = true;
-    for (int p = lane; p < P; p += 32) {
-      unsigned f;
-      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flags + p) : "memory");
-      done = done && (f >= epoch);
-    }
-    if (__all_sync(0xffffffffu, done)) {
-      __threadfence();  // acquire: order the later reads after the observed flags
-      break;
-    }
-    if ((++it & 255) == 0) {
-      int stop = 0;
-      if (lane == 0) {
-        if (*(volatile int *)timeout) stop = 1;
-        else if (it > kSpinLimit) {
-          atomicExch(timeout, 1);
-          stop = 1;
-        }
-      }
-      if (__shfl_sync(0xffffffffu, stop, 0)) {
-        ok = 0;
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
-  return ok != 0;
-}
-
-// Block-wide form: warp 0 crosses the barrier, the rest of the CTA waits.
-__device__ bool flag_barrier(unsigned *flags, int P, unsigned epoch, int *timeout) {
-  __syncthreads();
-  __shared__ int s_fok;
-  if (threadIdx.x < 32) {
-    const bool ok = flag_barrier_warp0(flags, P, epoch, timeout);
-    if (threadIdx.x == 0) s_fok = ok;
-  }
-  __syncthreads();
-  return s_fok != 0;
-}
-
 // Largest packed candidate over a warp: the magnitude word first, then the
 // row word among the lanes that hold that magnitude (two warp reductions).
 __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k) {
@@ -772,53 +718,85 @@ __global__ void compose_pivots_kernel(const int *ipiv, int n, int *perm) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = p[i];
 }
 
+__global__ void inv_to_fp32_kernel(const double2 *a, float2 *b, int64_t count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+
 struct TrsvArgs {
   const void *M;     // LU factors (T)
   int64_t lda, n;
   int nb, P, rpc, ns;
-  const double2 *inv;  // [nblk][2][nb][nb]: inv(L_kk), inv(U_kk)
+  const void *inv;   // [nblk][2][nb][nb] (T): inv(L_kk), inv(U_kk)
   const int *perm;
-  double2 *X, *Y, *Z;  // [ns][n]: right-hand sides in X, scratch Y, Z; solution returned in X
-  unsigned *bar;
+  double2 *X, *Y, *Z;  // [ns][n]: right-hand sides in X (solution returned there); the solved
+                       // blocks of the forward pass are published in Y, of the backward pass in Z
+                       // (both zeroed before the launch; published words carry a mark bit)
   int *timeout;
   int direct;  // 1: factor tiles do not fit in shared memory; read them from global memory
+  int stages;  // prefetch stages (1 or 2) of factor tile + diagonal-block inverse
 };
 
-// y = Inv * x for an nb x nb block and ns vectors held in shared memory;
-// several threads share one output and reduce through shared memory.
-// tr: apply the transpose of the block.
-__device__ void block_apply(const double2 *inv, int nb, int ns, const double2 *xs, double2 *ys, double2 *red,
-                            bool tr = false) {
-  const int O = nb * ns;
+// Complex multiply-add in the factor's precision (FP32 for the mixed
+// path's correction solves, as the single-precision solves of classical
+// mixed-precision refinement; FP64 otherwise).
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <typename T>
+__device__ __forceinline__ void cmac(T &acc, T m, T y) {
+  acc.x = fma_t(m.x, y.x, acc.x);
+  acc.x = fma_t(-m.y, y.y, acc.x);
+  acc.y = fma_t(m.x, y.y, acc.y);
+  acc.y = fma_t(m.y, y.x, acc.y);
+}
+template <typename T>
+__device__ __forceinline__ T cadd(T a, T b) {
+  a.x += b.x;
+  a.y += b.y;
+  return a;
+}
+// sum over groups of g adjacent lanes (g a power of two <= 32, all lanes present)
+template <typename T>
+__device__ __forceinline__ T group_sum(T v, int g) {
+  for (int o = g >> 1; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+// ys = Inv * xs for an nb x nb block (column-major, element type T) and NS
+// vectors xs[sv * nb + j] (type T); `parts` adjacent lanes share one output
+// and reduce with shuffles.  The result goes to ys (FP64) and ysc (T).
+// tr: apply the transpose.  Requires nb a multiple of 64.
+template <typename T, int NS>
+__device__ void block_apply(const T *inv, int nb, const T *xs, double2 *ys, T *ysc, bool tr) {
+  const int O = nb * NS;
   int parts = 1;
   while (parts * 2 * O <= (int)blockDim.x && parts < 16) parts *= 2;
-  const int tid = threadIdx.x;
   for (int base = 0; base < O * parts; base += blockDim.x) {
-    const int g = base + tid;
-    double2 acc = make_double2(0, 0);
-    if (g < O * parts) {
-      const int o = g / parts, part = g % parts;
-      const int r = o % nb, sv = o / nb;
-#pragma unroll 4
-      for (int j = part; j < nb; j += parts) {
-        const double2 iv = tr ? inv[j + (size_t)r * nb] : inv[r + (size_t)j * nb];
-        const double2 xv = xs[sv * nb + j];
-        acc.x += iv.x * xv.x - iv.y * xv.y;
-        acc.y += iv.x * xv.y + iv.y * xv.x;
+    const int g = base + threadIdx.x;
+    const bool valid = g < O * parts;
+    const int o = valid ? g / parts : 0, part = g % parts;
+    const int r = o % nb, sv = o / nb;
+    T a0 = {0, 0}, a1 = {0, 0}, a2 = {0, 0}, a3 = {0, 0};
+    if (valid) {
+      for (int j = part; j < nb; j += 4 * parts) {
+        const T *i0 = tr ? inv + j + (size_t)r * nb : inv + r + (size_t)j * nb;
+        const size_t st = tr ? (size_t)parts : (size_t)parts * nb;
+        cmac(a0, i0[0], xs[sv * nb + j]);
+        cmac(a1, i0[st], xs[sv * nb + j + parts]);
+        cmac(a2, i0[2 * st], xs[sv * nb + j + 2 * parts]);
+        cmac(a3, i0[3 * st], xs[sv * nb + j + 3 * parts]);
       }
     }
-    red[tid] = acc;
-    __syncthreads();
-    if (g < O * parts && (g % parts) == 0) {
-      double2 t = red[tid];
-      for (int q = 1; q < parts; q++) {
-        t.x += red[tid + q].x;
-        t.y += red[tid + q].y;
-      }
-      ys[g / parts] = t;
+    const T acc = group_sum(cadd(cadd(a0, a1), cadd(a2, a3)), parts);
+    if (valid && part == 0) {
+      ys[o] = make_double2(acc.x, acc.y);
+      ysc[o] = acc;
     }
-    __syncthreads();
   }
+  __syncthreads();
 }
 
 __device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes_is_16) {
@@ -838,179 +816,251 @@ __device__ __forceinline__ void upd_range(int pass, int64_t k0, int nb, int64_t 
   *hi = pass == 0 ? r1 : min(r1, k0);
 }
 
+// Published solution words: the lowest mantissa bit is forced to 1 (a
+// change of at most one unit in the last place), so that a word of a
+// buffer zeroed before the launch is known to be written once it reads
+// odd.  Each 64-bit word is single-copy atomic; no fence or flag is needed.
+__device__ __forceinline__ void publish_word2(double2 *p, double2 v) {
+  const unsigned long long x = (unsigned long long)__double_as_longlong(v.x) | 1ull;
+  const unsigned long long y = (unsigned long long)__double_as_longlong(v.y) | 1ull;
+  asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(x), "l"(y) : "memory");
+}
+__device__ __forceinline__ bool read_word2(const double2 *p, double2 *v) {
+  unsigned long long x, y;
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(x), "=l"(y) : "l"(p) : "memory");
+  *v = make_double2(__longlong_as_double((long long)x), __longlong_as_double((long long)y));
+  return (x & y & 1ull) != 0ull;
+}
+
 // Forward (unit lower) and backward (upper) substitution of P A = L U for
-// NS right-hand sides in one cooperative launch, scheduled by data flow
-// instead of grid barriers.  CTA c owns whole 64-row blocks, rows
-// [c rpc, (c+1) rpc) with rpc a multiple of 64, and is the only writer of
-// those rows.  For each block k of a pass every CTA waits for flag[pass][k]
-// (set by the owner of block k once all earlier blocks' updates reach its
-// rows), computes y_k = inv_k x_k itself, and updates its own rows; the
-// owner of the next block updates that block's rows first and releases its
-// flag before updating the rest.  The critical path per block is one flag
-// hand-off, one L2 read of x_k and a 64-row update.  The factor tile of the
-// next block is fetched with cp.async while the CTA waits.  TR solves
-// A^T x = b: forward with U^T, backward with L^T (unit), x = P^T z; its
-// tile is the block row of U (L) right (left) of the diagonal, row by row
-// with a padded stride.
+// NS right-hand sides in one cooperative launch, scheduled by data flow.
+// CTA c owns whole 64-row blocks, rows [c rpc, (c+1) rpc), and keeps its
+// rows of the vector in shared memory for both passes.  The owner of a
+// block solves it (y_k = inv_k x_k) and publishes y_k (pass 0 in Y, pass 1
+// in Z) as marked words; every other CTA with rows to update polls those
+// words until all are marked and updates its own rows with the factor tile
+// of block k (prefetched with cp.async while it waits, double-buffered when
+// shared memory allows).  A CTA that owns the next block updates that
+// block's rows first, solves and publishes it, and only then updates the
+// rest, so the critical path per block is one flag hand-off, one L2 read of
+// y_k, a 64-row update and one 64 x 64 apply; between consecutive blocks of
+// one CTA there is no hand-off at all.  The steps of both passes form one
+// sequence t = 0 .. 2 nblk - 1 (pass 0 block t, then pass 1 block
+// 2 nblk - 1 - t); the last block of pass 0 is the first of pass 1 and
+// stays with its owner.  TR solves A^T x = b: forward with U^T, backward
+// with L^T (unit), x = P^T z; its tile is the block row of U (L) right
+// (left) of the diagonal, row by row with a padded stride.
 template <typename T, int NS, bool TR>
 __global__ void __launch_bounds__(256, 1) trsv_flow_kernel(TrsvArgs a) {
-  __shared__ double2 xs[8 * 64], ys[8 * 64], red[256];
+  __shared__ double2 ysb[2][NS * 64];  // y of the current / next block (FP64)
+  __shared__ T ysc[2][NS * 64];        // the same in the factor's precision
+  __shared__ T xsc[NS * 64];           // the block being solved, in the factor's precision
   __shared__ int s_ok;
-  extern __shared__ __align__(16) unsigned char tile_raw[];  // tile of T, then [nb][nb] double2
-  T *tile = reinterpret_cast<T *>(tile_raw);
-  // tile element (row i, column j of the block): TR i * (nb + 1) + j, else j * rpc + i
-  const size_t tile_elems = TR ? (size_t)a.rpc * (a.nb + 1) : (size_t)a.nb * a.rpc;
-  double2 *sinv = reinterpret_cast<double2 *>(tile_raw + (a.direct ? 0 : ((sizeof(T) * tile_elems + 15) / 16) * 16));
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const T *M = reinterpret_cast<const T *>(a.M);
+  const T *inv = reinterpret_cast<const T *>(a.inv);
   const int64_t n = a.n, lda = a.lda;
-  const int nb = a.nb, nblk = (int)(n / nb), rpc = a.rpc;
-  constexpr int ns = NS;
+  const int nb = a.nb, nblk = (int)(n / nb), rpc = a.rpc, S = a.stages;
+  const int nsteps = 2 * nblk;
   const int64_t r0 = (int64_t)blockIdx.x * rpc;
   const int64_t r1 = min(n, r0 + rpc);
-  unsigned *flag = a.bar;  // [2][nblk]
+  // shared memory: own rows [NS][rpc] (double2) | inverses [S][nb][nb] | tiles [S]
+  double2 *xo = reinterpret_cast<double2 *>(smem_raw);
+  T *sinv = reinterpret_cast<T *>(smem_raw + sizeof(double2) * (size_t)NS * rpc);
+  // tile element (row i, column j of the block): TR i * (nb + 1) + j, else
+  // j * cs + i with the column stride cs padded by 64 bytes, so that the
+  // lanes of a warp reading 4 columns of 8 rows hit distinct banks
+  const int cs = rpc + 64 / (int)sizeof(T);
+  const size_t tile_elems = TR ? (size_t)rpc * (nb + 1) : (size_t)nb * cs;
+  const size_t tile_stride = ((sizeof(T) * tile_elems + 15) / 16) * 16 / sizeof(T);
+  T *tiles = sinv + (size_t)S * nb * nb;
+  auto blk_of = [&](int t) { return t < nblk ? t : nsteps - 1 - t; };
+  auto pass_of = [&](int t) { return t < nblk ? 0 : 1; };
   auto owns = [&](int kb) { return (int64_t)kb * nb >= r0 && (int64_t)kb * nb < r1; };
-  auto signal = [&](int pass, int kb) {  // after a __syncthreads
-    if (threadIdx.x == 0)
-      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag + pass * nblk + kb), "r"(1u) : "memory");
+  // prefetch group of step t: the factor tile of block t (stage t % S) and,
+  // when this CTA solves the block of step t + 1, its inverse (stage (t + 1) % S)
+  auto issue = [&](int t) {
+    if (t >= 0 && t < nsteps && !a.direct) {
+      const int pass = pass_of(t);
+      const int64_t k0 = (int64_t)blk_of(t) * nb;
+      int64_t lo, hi;
+      upd_range(pass, k0, nb, r0, r1, &lo, &hi);
+      const int cnt = hi <= lo ? 0 : (int)(hi - lo);
+      T *tile = tiles + (size_t)(t % S) * tile_stride;
+      if (TR) {
+        for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
+          const int j = idx % nb, i = idx / nb;
+          cp_async(tile + (size_t)i * (nb + 1) + j, M + (k0 + j) + (lo + i) * lda, sizeof(T) == 16);
+        }
+      } else {
+        for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
+          const int i = idx % cnt, j = idx / cnt;
+          cp_async(tile + (size_t)j * cs + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
+        }
+      }
+    }
+    const int u = t + 1;
+    if (u < nsteps && owns(blk_of(u))) {
+      // pass 0 applies inv(L) (or inv(U)^T), pass 1 inv(U) (or inv(L)^T)
+      const int pu = pass_of(u);
+      const T *ib = inv + ((size_t)blk_of(u) * 2 + (TR ? 1 - pu : pu)) * nb * nb;
+      T *dst = sinv + (size_t)(u % S) * nb * nb;
+      for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) cp_async(dst + idx, ib + idx, sizeof(T) == 16);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  auto prefetch = [&](int pass, int kk) {
-    if (kk >= nblk) return;
-    const int kb = pass == 0 ? kk : nblk - 1 - kk;
+  auto wait_stage = [&]() {
+    if (S == 2) asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;" ::: "memory");
+  };
+  // xo[i] -= sum_j M(i, block k0) y[j] for own rows i in [lo, hi); tl holds
+  // the tile rows from tlo.  G adjacent lanes share a row when there are few
+  // rows (shuffle reduction); products and the 64-term sums in the factor's
+  // precision, the running vector in FP64.  No barrier inside.
+  auto update = [&](int64_t k0, int64_t lo, int64_t hi, int64_t tlo, const T *tl, const T *y) {
+    const int rows = hi > lo ? (int)(hi - lo) : 0;
+    if (rows == 0) return;  // uniform over the CTA
+    const int G = NS > 2 ? 1 : (rows <= 64 ? 4 : (rows <= 128 ? 2 : 1));
+    const int part = threadIdx.x % G, rpr = (int)blockDim.x / G;
+    const int64_t mstride = TR ? 1 : (a.direct ? lda : cs);
+    for (int base = 0; base < rows; base += rpr) {
+      const int ri = base + (int)threadIdx.x / G;
+      const bool valid = ri < rows;
+      T a0[NS], a1[NS];
+#pragma unroll
+      for (int sv = 0; sv < NS; sv++) a0[sv] = a1[sv] = T{0, 0};
+      if (valid) {
+        const int64_t i = lo + ri;
+        const T *mp = TR ? (a.direct ? M + k0 + i * lda : tl + (size_t)(i - tlo) * (nb + 1))
+                         : (a.direct ? M + i + k0 * lda : tl + (i - tlo));
+#pragma unroll 2
+        for (int j = part; j < nb; j += 2 * G) {
+          const T m0 = mp[(size_t)j * mstride], m1 = mp[(size_t)(j + G) * mstride];
+#pragma unroll
+          for (int sv = 0; sv < NS; sv++) {
+            cmac(a0[sv], m0, y[sv * nb + j]);
+            cmac(a1[sv], m1, y[sv * nb + j + G]);
+          }
+        }
+      }
+#pragma unroll
+      for (int sv = 0; sv < NS; sv++) {
+        const T acc = group_sum(cadd(a0[sv], a1[sv]), G);
+        if (valid && part == 0) {
+          const int64_t li = lo + ri - r0;
+          double2 v = xo[(size_t)sv * rpc + li];
+          v.x -= (double)acc.x;
+          v.y -= (double)acc.y;
+          xo[(size_t)sv * rpc + li] = v;
+        }
+      }
+    }
+  };
+  // solve the own block of step u from xo and publish it
+  auto solve_publish = [&](int u) {
+    const int kb = blk_of(u), pu = pass_of(u);
+    const int64_t l0 = (int64_t)kb * nb - r0;
+    for (int idx = threadIdx.x; idx < nb * NS; idx += blockDim.x) {
+      const int j = idx % nb, sv = idx / nb;
+      st2(xsc + sv * nb + j, xo[(size_t)sv * rpc + l0 + j]);
+    }
+    __syncthreads();
+    double2 *y = ysb[u & 1];
+    block_apply<T, NS>(sinv + (size_t)(u % S) * nb * nb, nb, xsc, y, ysc[u & 1], TR);
+    double2 *E = pu == 0 ? a.Y : a.Z;
+    for (int idx = threadIdx.x; idx < nb * NS; idx += blockDim.x) {
+      const int j = idx % nb, sv = idx / nb;
+      const double2 v = y[sv * nb + j];
+      xo[(size_t)sv * rpc + l0 + j] = v;
+      publish_word2(E + (size_t)sv * n + (int64_t)kb * nb + j, v);
+    }
+    __syncthreads();
+  };
+  // own rows of P X (TR: X)
+  const int nrow = (int)(r1 - r0);
+  for (int idx = threadIdx.x; idx < NS * nrow; idx += blockDim.x) {
+    const int li = idx % nrow, sv = idx / nrow;
+    const int64_t i = r0 + li;
+    xo[(size_t)sv * rpc + li] = a.X[(size_t)sv * n + (TR ? i : a.perm[i])];
+  }
+  for (int t = -1; t <= S - 2; t++) issue(t);
+  wait_stage();
+  __syncthreads();
+  if (owns(blk_of(0))) solve_publish(0);
+  __syncthreads();
+  issue(S - 1);
+  for (int t = 0; t < nsteps; t++) {
+    const int kb = blk_of(t), pass = pass_of(t);
     const int64_t k0 = (int64_t)kb * nb;
     int64_t lo, hi;
     upd_range(pass, k0, nb, r0, r1, &lo, &hi);
-    const int cnt = (a.direct || hi <= lo) ? 0 : (int)(hi - lo);
-    if (TR) {
-      // block row: factor entries (k0 + j, lo + i), contiguous in j
-      for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
-        const int j = idx % nb, i = idx / nb;
-        cp_async(tile + (size_t)i * (nb + 1) + j, M + (k0 + j) + (lo + i) * lda, sizeof(T) == 16);
-      }
-    } else {
-      for (int idx = threadIdx.x; idx < cnt * nb; idx += blockDim.x) {
-        const int i = idx % cnt, j = idx / cnt;
-        cp_async(tile + (size_t)j * rpc + i, M + (lo + i) + (k0 + j) * lda, sizeof(T) == 16);
-      }
-    }
-    // pass 0 applies inv(L) (or inv(U)^T), pass 1 inv(U) (or inv(L)^T)
-    const double2 *ib = a.inv + ((size_t)kb * 2 + (TR ? 1 - pass : pass)) * nb * nb;
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) cp_async(sinv + idx, ib + idx, 1);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-  // src[i] -= sum_j M(i, block) ys[j] for own rows i in [lo, hi)
-  auto update = [&](int64_t k0, int64_t lo, int64_t hi, int64_t tlo, double2 *src) {
-    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      double2 acc[NS];
-#pragma unroll
-      for (int sv = 0; sv < ns; sv++) acc[sv] = make_double2(0, 0);
-      const T *mp = TR ? (a.direct ? M + k0 + i * lda : tile + (size_t)(i - tlo) * (nb + 1))
-                       : (a.direct ? M + i + k0 * lda : tile + (i - tlo));
-      const int64_t mstride = TR ? 1 : (a.direct ? lda : rpc);
-#pragma unroll 8
-      for (int j = 0; j < nb; j++) {
-        const double2 m = ld2(mp + (size_t)j * mstride);
-#pragma unroll
-        for (int sv = 0; sv < ns; sv++) {
-          const double2 y = ys[sv * nb + j];
-          acc[sv].x += m.x * y.x - m.y * y.y;
-          acc[sv].y += m.x * y.y + m.y * y.x;
-        }
-      }
-#pragma unroll
-      for (int sv = 0; sv < ns; sv++) {
-        double2 v = src[(size_t)sv * n + i];
-        v.x -= acc[sv].x;
-        v.y -= acc[sv].y;
-        src[(size_t)sv * n + i] = v;
-      }
-    }
-  };
-  // Y = P X (TR: Y = X) for the own rows; X is rewritten below, so all
-  // CTAs finish reading it first (one grid barrier); then block 0 is ready
-  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-    for (int s = 0; s < ns; s++) a.Y[(size_t)s * n + i] = a.X[(size_t)s * n + (TR ? i : a.perm[i])];
-  prefetch(0, 0);
-  unsigned *bar = flag + 2 * nblk;  // [P] barrier epochs
-  if (!flag_barrier(bar, a.P, 1u, a.timeout)) return;
-  if (owns(0)) signal(0, 0);
-  // Pass 0 reduces Y and writes the solved blocks to X; pass 1 reduces X and
-  // writes to Z.  A CTA may still be reading Y in pass 0 while others are in
-  // pass 1, hence the third vector.
-  for (int pass = 0; pass < 2; pass++) {
-    double2 *src = pass == 0 ? a.Y : a.X;  // vector being reduced
-    double2 *dst = pass == 0 ? a.X : a.Z;  // solved blocks
-    for (int kk = 0; kk < nblk; kk++) {
-      const int kb = pass == 0 ? kk : nblk - 1 - kk;
-      const int64_t k0 = (int64_t)kb * nb;
-      // wait until block kb's rows are final (bounded)
-      if (threadIdx.x == 0) {
-        long long it = 0;
+    const int u = t + 1;
+    const bool own_next = u < nsteps && owns(blk_of(u));
+    if ((hi > lo || own_next) && !owns(kb)) {
+      // poll the published words of block kb until all are marked (bounded)
+      const double2 *E = pass == 0 ? a.Y : a.Z;
+      long long it = 0;
+      while (true) {
         int ok = 1;
-        while (true) {
-          unsigned f;
-          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flag + pass * nblk + kb) : "memory");
-          if (f) break;
-          if ((++it & 1023) == 0) {
-            if (*(volatile int *)a.timeout) {
-              ok = 0;
-              break;
-            }
-            if (it > kSpinLimit) {
-              atomicExch(a.timeout, 1);
-              ok = 0;
-              break;
-            }
+        for (int idx = threadIdx.x; idx < nb * NS; idx += blockDim.x) {
+          const int j = idx % nb, sv = idx / nb;
+          double2 v;
+          if (read_word2(E + (size_t)sv * n + k0 + j, &v)) {
+            st2(&ysc[t & 1][sv * nb + j], v);
+          } else {
+            ok = 0;
           }
         }
-        s_ok = ok;
-      }
-      __syncthreads();
-      if (!s_ok) return;
-      for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
-        const int j = idx % nb, sv = idx / nb;
-        xs[sv * nb + j] = __ldcg(src + (size_t)sv * n + k0 + j);
-      }
-      cp_async_wait_all();
-      __syncthreads();
-      block_apply(sinv, nb, ns, xs, ys, red, TR);
-      int64_t lo, hi;
-      upd_range(pass, k0, nb, r0, r1, &lo, &hi);
-      // the next block of this pass: its rows first, then its flag
-      const int nk = pass == 0 ? kb + 1 : kb - 1;
-      const bool own_next = nk >= 0 && nk < nblk && owns(nk);
-      if (owns(kb)) {
-        for (int idx = threadIdx.x; idx < nb * ns; idx += blockDim.x) {
-          const int j = idx % nb, sv = idx / nb;
-          dst[(size_t)sv * n + k0 + j] = ys[sv * nb + j];
+        if (__syncthreads_and(ok)) break;
+        if ((++it & 255) == 0) {
+          if (threadIdx.x == 0) {
+            int go = 1;
+            if (*(volatile int *)a.timeout) go = 0;
+            else if (it > kSpinLimit) {
+              atomicExch(a.timeout, 1);
+              go = 0;
+            }
+            s_ok = go;
+          }
+          __syncthreads();
+          if (!s_ok) {
+            cp_async_wait_all();
+            return;
+          }
         }
       }
-      int64_t alo = lo, ahi = lo;  // rows of the next block inside [lo, hi)
-      if (own_next) {
-        alo = (int64_t)nk * nb;
-        ahi = alo + nb;
-        update(k0, alo, ahi, lo, src);
-      }
-      __syncthreads();
-      if (own_next) signal(pass, nk);
-      if (pass == 0 && kb == nblk - 1 && owns(kb)) signal(1, nblk - 1);  // x of pass 1 starts here
-      if (own_next) {
-        update(k0, lo, alo, lo, src);
-        update(k0, ahi, hi, lo, src);
-      } else {
-        update(k0, lo, hi, lo, src);
-      }
-      __syncthreads();
-      // next tile: the following block of this pass, or the first of the next pass
-      if (kk + 1 < nblk) prefetch(pass, kk + 1);
-      else if (pass == 0) prefetch(1, 0);
     }
+    wait_stage();
+    __syncthreads();
+    const T *tl = tiles + (size_t)(t % S) * tile_stride;
+    const T *yc = ysc[t & 1];
+    if (own_next) {
+      const int64_t a0 = (int64_t)blk_of(u) * nb;
+      const bool same = pass_of(u) == pass;
+      if (same) {
+        update(k0, a0, a0 + nb, lo, tl, yc);
+        __syncthreads();
+      }
+      solve_publish(u);
+      if (same) {
+        update(k0, lo, a0, lo, tl, yc);
+        update(k0, a0 + nb, hi, lo, tl, yc);
+      } else {
+        update(k0, lo, hi, lo, tl, yc);
+      }
+    } else {
+      update(k0, lo, hi, lo, tl, yc);
+    }
+    __syncthreads();
+    issue(t + S);
   }
   cp_async_wait_all();
-  // X is still read by CTAs in pass 1 until all are done
-  if (!flag_barrier(bar, a.P, 2u, a.timeout)) return;
-  // the solution is in Z (own rows); return it in X (TR: X = P^T Z)
-  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-    for (int s = 0; s < ns; s++) a.X[(size_t)s * n + (TR ? a.perm[i] : i)] = a.Z[(size_t)s * n + i];
+  // the solution of the own rows; TR: X = P^T Z
+  for (int idx = threadIdx.x; idx < NS * nrow; idx += blockDim.x) {
+    const int li = idx % nrow, sv = idx / nrow;
+    const int64_t i = r0 + li;
+    a.X[(size_t)sv * n + (TR ? a.perm[i] : i)] = xo[(size_t)sv * rpc + li];
+  }
 }
 
 constexpr int kGemvRows = 256;
@@ -1115,7 +1165,6 @@ __global__ void axpy_kernel(double2 *X, const double2 *D, int64_t count) {
 }
 
 struct LuWork {
-  unsigned *bar;
   int *info, *timeout;
   unsigned long long *rec;
   double2 *cand_data, *col_data;
@@ -1125,7 +1174,16 @@ struct LuWork {
   int *pmap;       // [257]: composed panel permutation (dst[128], src[128], count)
 };
 
-int lu_workspace(Ctx *c, int precision, LuWork &w) {
+// The panel kernel's exchange buffers (records polled by every CTA once per
+// column, candidate rows) can sit at kXSlots placements kXSlotBytes apart.
+// Their physical placement changes the exchange latency: at 15,360 rows on
+// 96 CTAs one B200 measured 5.2 to 6.5 us per column across eight 64 KB
+// steps, constant in 128 KB pairs; so the autotuner times each placement.
+constexpr int kXSlots = 16;
+constexpr size_t kXSlotBytes = 128 << 10;
+
+// slot < 0: the tuned placement (0 without a table)
+int lu_workspace(Ctx *c, int precision, LuWork &w, int slot = -1) {
   const int nb = c->nb, P = c->nsm;
   const size_t esz = precision == MOM_PREC_MIXED ? sizeof(float2) : sizeof(double2);
   size_t off = 0;
@@ -1134,10 +1192,10 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
     off += (bytes + 255) / 256 * 256;
     return o;
   };
-  const size_t o_bar = take(sizeof(unsigned) * 256);
-  const size_t o_ca = take(sizeof(unsigned long long) * 2 * P);
-  const size_t o_cd = take(sizeof(double2) * 2 * P * nb);
-  const size_t o_cl = take(sizeof(double2) * 2 * nb);
+  if (slot < 0) slot = c->tune ? c->tune->xslot : 0;
+  const size_t x_rec = 0, x_cd = x_rec + ((sizeof(unsigned long long) * 2 * P + 255) / 256) * 256;
+  const size_t x_cl = x_cd + sizeof(double2) * 2 * P * nb, x_end = x_cl + sizeof(double2) * 2 * nb;
+  const size_t o_x = take(kXSlots * kXSlotBytes + x_end);
   const size_t o_w = take(esz * (size_t)nb * c->n);
   const size_t o_i32 = take(sizeof(float2) * (size_t)nb * c->n);
   const size_t o_pm = take(sizeof(int) * 260);
@@ -1145,12 +1203,12 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
       take(precision == MOM_PREC_MIXED ? tc_cgemm_work_bytes((int)c->n, (int)c->n, c->outer_panels * nb) : 0);
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off));
   char *b = (char *)c->ws;
-  w.bar = (unsigned *)(b + o_bar);
+  char *x = b + o_x + (size_t)slot * kXSlotBytes;
   w.info = c->dinfo;
   w.timeout = c->dinfo + 1;
-  w.rec = (unsigned long long *)(b + o_ca);
-  w.cand_data = (double2 *)(b + o_cd);
-  w.col_data = (double2 *)(b + o_cl);
+  w.rec = (unsigned long long *)(x + x_rec);
+  w.cand_data = (double2 *)(x + x_cd);
+  w.col_data = (double2 *)(x + x_cl);
   w.W = (double2 *)(b + o_w);
   w.invL32 = (float2 *)(b + o_i32);
   w.tcw = (float *)(b + o_tc);
@@ -1161,6 +1219,7 @@ int lu_workspace(Ctx *c, int precision, LuWork &w) {
 // Identity of the panel table in use (part of the LU graph key).
 uint64_t tune_hash(const Ctx *c) {
   uint64_t h = 1469598103934665603ull ^ (uint64_t)c->panel_cap_env;
+  if (c->tune) h = (h ^ (uint64_t)(c->tune->xslot + 1)) * 1099511628211ull;
   if (c->tune)
     for (size_t i = 0; i < c->tune->m.size(); i++) h = (h ^ (uint64_t)(c->tune->m[i] * 1000 + c->tune->P[i])) * 1099511628211ull;
   return h;
@@ -1358,6 +1417,12 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
         A, lda, 0, c->invd, nullptr);
     c->launches++;
     MOM_CUDA(c, cudaGetLastError());
+    if (mixed) {
+      // FP32 copy of all inverses for the solves with the FP32 factors
+      inv_to_fp32_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(c->invd, c->inv32, 2 * (int64_t)nb * n);
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+    }
   }
   compose_pivots_kernel<<<1, 256, sizeof(int) * n, c->stream>>>(c->ipiv, (int)n, c->perm);
   c->launches++;
@@ -1418,7 +1483,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
-                                        (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels};
+                                        (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32};
     g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
     if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
@@ -1457,13 +1522,41 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, double2 *Z, int nrhs) {
   ProfScope ps(c, kProfTrsv);
   // whole 64-row blocks per CTA (each block has exactly one owner)
   const int nblk = (int)(n / nb);
-  if (2 * nblk + 256 > kFlowFlags) return fail(c, MOM_ERR_ARG, "matrix order too large for the triangular solve");
   const int bpc = (nblk + c->nsm - 1) / c->nsm;
   const int rpc = bpc * nb;
   const int P = (nblk + bpc - 1) / bpc;
+  auto kernel_of = [](int ns) -> void * {
+    return ns == 1 ? (void *)trsv_flow_kernel<T, 1, TR>
+           : ns == 2 ? (void *)trsv_flow_kernel<T, 2, TR>
+           : ns == 4 ? (void *)trsv_flow_kernel<T, 4, TR>
+                     : (void *)trsv_flow_kernel<T, 8, TR>;
+  };
+  const size_t tile_elems = TR ? (size_t)rpc * (nb + 1) : (size_t)nb * (rpc + 64 / sizeof(T));
+  const size_t tile_bytes = ((sizeof(T) * tile_elems + 15) / 16) * 16, inv_bytes = sizeof(T) * nb * nb;
+  const T *inv = sizeof(T) == sizeof(float2) ? (const T *)c->inv32 : (const T *)c->invd;
   for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
     ns = 8;
     while (ns > nrhs - s0) ns >>= 1;  // chunks of 8, 4, 2, 1 vectors
+    // shared memory: own rows, then per stage one inverse and (unless direct) one tile
+    int stages = 0, direct = 0;
+    size_t smem = 0;
+    for (;;) {
+      cudaFuncAttributes fa;
+      MOM_CUDA(c, cudaFuncGetAttributes(&fa, kernel_of(ns)));
+      const size_t cap = (size_t)fa.maxDynamicSharedSizeBytes, own = sizeof(double2) * (size_t)ns * rpc;
+      const size_t opt[3][2] = {{2, 0}, {1, 0}, {1, 1}};
+      for (int o = 0; o < 3 && !stages; o++) {
+        const size_t need = own + opt[o][0] * (inv_bytes + (opt[o][1] ? 0 : tile_bytes));
+        if (need <= cap) {
+          stages = (int)opt[o][0];
+          direct = (int)opt[o][1];
+          smem = need;
+        }
+      }
+      if (stages || ns == 1) break;
+      ns >>= 1;
+    }
+    if (!stages) return fail(c, MOM_ERR_ARG, "matrix order too large for the triangular solve");
     TrsvArgs ta;
     ta.M = A;
     ta.lda = c->lda;
@@ -1472,27 +1565,18 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, double2 *Z, int nrhs) {
     ta.P = P;
     ta.rpc = rpc;
     ta.ns = ns;
-    ta.inv = c->invd;
+    ta.inv = inv;
     ta.perm = c->perm;
     ta.X = X + (size_t)s0 * n;
     ta.Y = Y + (size_t)s0 * n;
     ta.Z = Z + (size_t)s0 * n;
-    ta.bar = c->flags;
     ta.timeout = c->dinfo + 1;
-    MOM_CUDA(c, cudaMemsetAsync(ta.bar, 0, sizeof(unsigned) * (2 * nblk + P), c->stream));
+    ta.direct = direct;
+    ta.stages = stages;
+    MOM_CUDA(c, cudaMemsetAsync(ta.Y, 0, sizeof(double2) * ns * n, c->stream));
+    MOM_CUDA(c, cudaMemsetAsync(ta.Z, 0, sizeof(double2) * ns * n, c->stream));
     void *args[] = {&ta};
-    void *fn = ns == 1 ? (void *)trsv_flow_kernel<T, 1, TR>
-               : ns == 2 ? (void *)trsv_flow_kernel<T, 2, TR>
-               : ns == 4 ? (void *)trsv_flow_kernel<T, 4, TR>
-                         : (void *)trsv_flow_kernel<T, 8, TR>;
-    const size_t elems = TR ? (size_t)rpc * (nb + 1) : (size_t)nb * rpc;
-    size_t tile = ((sizeof(T) * elems + 15) / 16) * 16 + sizeof(double2) * nb * nb;
-    ta.direct = 0;
-    if (tile > 200 * 1024) {
-      ta.direct = 1;
-      tile = sizeof(double2) * nb * nb;
-    }
-    MOM_CUDA(c, cudaLaunchCooperativeKernel(fn, dim3(P), dim3(256), args, tile, c->stream));
+    MOM_CUDA(c, cudaLaunchCooperativeKernel(kernel_of(ns), dim3(P), dim3(256), args, smem, c->stream));
     c->launches++;
   }
   return MOM_OK;
@@ -1594,7 +1678,7 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
   const int64_t n = c->n, lda = c->lda;
   const int nb = c->nb;
   LuWork w;
-  MOM_TRY(lu_workspace(c, t.precision, w));
+  MOM_TRY(lu_workspace(c, t.precision, w, 0));
   T *S = nullptr;
   int *ip = nullptr;
   if (cudaMalloc(&S, sizeof(T) * (size_t)n * nb) != cudaSuccess || cudaMalloc(&ip, sizeof(int) * 2 * nb) != cudaSuccess) {
@@ -1607,6 +1691,26 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
   cudaEventCreate(&e1);
   int rc = MOM_OK;
   const int cands[] = {148, 120, 96, 80, 64, 48, 40, 32, 24, 16, 12, 8};
+  // one panel of height m on P CTAs, best of two (milliseconds)
+  auto trial = [&](int64_t m, int P, const LuWork &wk) -> double {
+    double ms_min = 1e30;
+    for (int rep = 0; rep < 2 && rc == MOM_OK; rep++) {
+      const cudaError_t ce = cudaMemcpy2DAsync(S, sizeof(T) * m, A, sizeof(T) * lda, sizeof(T) * m, nb,
+                                               cudaMemcpyDeviceToDevice, c->stream);
+      if (ce != cudaSuccess) {
+        rc = cuda_fail(c, ce, "panel autotune copy");
+        break;
+      }
+      cudaEventRecord(e0, c->stream);
+      rc = launch_panel<T>(c, S, m, m, 0, P, ip, ip + nb, wk);
+      cudaEventRecord(e1, c->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "panel autotune trial");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms_min = std::min(ms_min, (double)ms);
+    }
+    return ms_min;
+  };
   for (int64_t m = n; m >= 128 && rc == MOM_OK; m /= 2) {
     int best = c->nsm, last = -1;
     double best_ms = 1e30;
@@ -1619,22 +1723,25 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
       const int P = (int)((m + rpc - 1) / rpc);
       if (P == last) continue;
       last = P;
-      double ms_min = 1e30;
-      for (int rep = 0; rep < 2 && rc == MOM_OK; rep++) {
-        MOM_CUDA(c, cudaMemcpy2DAsync(S, sizeof(T) * m, A, sizeof(T) * lda, sizeof(T) * m, nb,
-                                      cudaMemcpyDeviceToDevice, c->stream));
-        cudaEventRecord(e0, c->stream);
-        rc = launch_panel<T>(c, S, m, m, 0, P, ip, ip + nb, w);
-        cudaEventRecord(e1, c->stream);
-        if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "panel autotune trial");
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms_min = std::min(ms_min, (double)ms);
-      }
+      const double ms_min = trial(m, P, w);
       if (rc == MOM_OK && ms_min < best_ms) {
         best_ms = ms_min;
         best = P;
       }
+    }
+    if (m == n && !clustered && rc == MOM_OK) {
+      // placement of the exchange buffers, at the tallest height with its best P
+      for (int sl = 0; sl < kXSlots && rc == MOM_OK; sl++) {
+        LuWork ws;
+        rc = lu_workspace(c, t.precision, ws, sl);
+        const double ms = sl == 0 ? best_ms : trial(m, best, ws);
+        t.xslot_us.push_back(ms * 1e3 / nb);
+        if (rc == MOM_OK && ms < best_ms) {
+          best_ms = ms;
+          t.xslot = sl;
+        }
+      }
+      if (rc == MOM_OK) rc = lu_workspace(c, t.precision, w, t.xslot);
     }
     t.m.push_back(m);
     t.P.push_back(best);
@@ -1704,11 +1811,6 @@ __global__ void permute_rows_kernel(const TI *X, int64_t ldx, TO *Y, int64_t ldy
   Y[(size_t)s * ldy + dst] = o;
 }
 
-__global__ void inv_to_fp32_kernel(const double2 *a, float2 *b, int64_t count) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
-    b[i] = make_float2((float)a[i].x, (float)a[i].y);
-}
-
 template <typename T>
 int blas_gemm(Ctx *c, cublasOperation_t ta, int m, int nn, int k, double alpha, const T *A, int64_t lda, const T *B,
               int64_t ldb, double beta, T *C, int64_t ldc);
@@ -1742,17 +1844,10 @@ int getrs_multi(Ctx *c, const T *F, double2 *X, int nrhs, int trans) {
   const int nb = c->nb, nblk = (int)(n / nb);
   const bool f32 = sizeof(T) == sizeof(float2);
   const size_t ybytes = sizeof(T) * (size_t)n * nrhs, tbytes = sizeof(T) * (size_t)nb * nrhs;
-  const size_t ibytes = f32 ? sizeof(float2) * (size_t)nblk * 2 * nb * nb : 0;
-  MOM_TRY(ensure_buffer(c, &c->ws2, &c->ws2_bytes, ybytes + tbytes + ibytes + 1024));
+  MOM_TRY(ensure_buffer(c, &c->ws2, &c->ws2_bytes, ybytes + tbytes + 1024));
   T *Y = (T *)c->ws2;
   T *Tm = (T *)((char *)c->ws2 + ((ybytes + 255) / 256) * 256);
-  const T *inv = (const T *)c->invd;
-  if (f32) {
-    float2 *i32 = (float2 *)((char *)c->ws2 + ((ybytes + 255) / 256) * 256 + ((tbytes + 255) / 256) * 256);
-    inv_to_fp32_kernel<<<c->nsm * 4, 256, 0, c->stream>>>(c->invd, i32, (int64_t)nblk * 2 * nb * nb);
-    c->launches++;
-    inv = (const T *)i32;
-  }
+  const T *inv = f32 ? (const T *)c->inv32 : (const T *)c->invd;
   ProfScope ps(c, kProfTrsv);
   const dim3 pg((unsigned)((n + 255) / 256), nrhs);
   permute_rows_kernel<double2, T><<<pg, 256, 0, c->stream>>>(X, n, Y, n, n, c->perm, trans ? 1 : 0);

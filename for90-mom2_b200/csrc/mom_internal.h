@@ -25,7 +25,6 @@ constexpr double kEta0 = 3.767303134622e2;
 
 constexpr int kMaxQ = 13;
 constexpr size_t kBlasWorkspace = 64u << 20;
-constexpr int kFlowFlags = 8192;  // 2 passes x 64-row blocks: orders up to 262,144
 
 // Per-domain device data (structure of arrays).  "Half-edge" h = 3*face +
 // local edge identifies one RWG half (one face of an edge).
@@ -93,9 +92,9 @@ struct Ctx {
   int *ipiv = nullptr;     // [n]
   int *perm = nullptr;     // [n] composed row permutation of the factorisation
   double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
+  float2 *inv32 = nullptr; // FP32 copy of invd for the mixed-precision solves
   size_t invd_bytes = 0;
   int *dinfo = nullptr;    // device status words [0]=info, [1]=timeout
-  unsigned *flags = nullptr;  // [kFlowFlags] block-ready flags of the triangular solve kernel
   void *ws = nullptr;      // general device workspace
   size_t ws_bytes = 0;
   void *ws2 = nullptr;     // workspace of the many-right-hand-side solve
@@ -147,6 +146,8 @@ struct Ctx {
     std::vector<int64_t> m;  // panel heights probed
     std::vector<int> P;      // fastest CTA count at each height
     std::vector<double> us;  // its time per panel column (microseconds)
+    int xslot = 0;           // placement of the panel exchange buffers (kXSlotBytes apart)
+    std::vector<double> xslot_us;  // per-column time of each placement at the tallest height
     double ms = 0;           // time spent tuning
   };
   std::vector<Tuned> tuned;

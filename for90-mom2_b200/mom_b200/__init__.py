@@ -47,7 +47,7 @@ EXPORTS = [
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
     "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
-    "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result",
+    "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement",
 ]
 
 
@@ -111,6 +111,7 @@ def lib():
                                      C.POINTER(MomSrc), C.c_int32, C.c_double, C.c_int32, C.POINTER(dp),
                                      C.POINTER(dp), ip]
     L.mom_gpu_autotune_result.argtypes = [vp, C.c_int32, C.c_int32, ip, C.POINTER(C.c_int64), ip, dp, dp]
+    L.mom_gpu_autotune_placement.argtypes = [vp, C.c_int32, C.c_int32, ip, ip, dp]
     L.mom_problem_node_parent.argtypes = [vp, C.c_int32, ip]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
@@ -436,8 +437,13 @@ class Solver:
                                                ps.ctypes.data_as(C.POINTER(C.c_int32)), _dp(us), C.byref(ms)),
                  "autotune_result")
         m = min(k, nent.value)
+        nx = C.c_int32()
+        xs = C.c_int32()
+        xus = np.zeros(k)
+        self._ck(lib().mom_gpu_autotune_placement(self.h, precision, k, C.byref(nx), C.byref(xs), _dp(xus)),
+                 "autotune_placement")
         return dict(heights=hs[:m].tolist(), ctas=ps[:m].tolist(), us_per_column=us[:m].round(3).tolist(),
-                    tune_ms=ms.value)
+                    tune_ms=ms.value, placement=xs.value, placement_us_per_column=xus[:min(k, nx.value)].round(3).tolist())
 
     def adjoint_mean_eps(self, omega, ri, srcs, precision, eps_dom, tol=1e-12, maxit=30):
         """d(mean sigma_ext, mean sigma_abs) / d(Re eps, Im eps) of domain eps_dom: [2][2]."""

@@ -163,6 +163,13 @@ int mom_gpu_sweep_many(int32_t nctx, mom_ctx **ctx, const int32_t *nwl, const do
  * factorisation (or with MOM_AUTOTUNE=0 / MOM_PANEL_CTAS set). */
 int mom_gpu_autotune_result(mom_ctx *ctx, int32_t precision, int32_t max_entries, int32_t *nent, int64_t *heights,
                             int32_t *ctas, double *us_per_column, double *tune_ms);
+/* Placement of the panel exchange buffers chosen by the same autotuner (no
+ * counterpart in the reference): *chosen = index of the placement in use;
+ * us_per_column[i] = time per column of placement i at the tallest panel
+ * height (up to max_entries, *nent = number probed; 0 when the tallest
+ * panel runs on one thread-block cluster and has no global exchange). */
+int mom_gpu_autotune_placement(mom_ctx *ctx, int32_t precision, int32_t max_entries, int32_t *nent, int32_t *chosen,
+                               double *us_per_column);
 
 /* ---- Adjoint gradients (no counterpart in the reference) ----
  * After mom_gpu_solve for the same sources (and the same omega and ri), the
