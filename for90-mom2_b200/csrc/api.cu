@@ -383,6 +383,8 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   c->use_graph = !(eg && eg[0] == '0');
   const char *ea = std::getenv("MOM_AUTOTUNE");
   c->autotune = !(ea && ea[0] == '0');
+  const char *et = std::getenv("MOM_SMALL_TC");
+  if (et) c->small_tc = et[0] != '0';
   const char *eo = std::getenv("MOM_LU_OUTER");
   if (eo) c->outer_panels = std::max(1, std::min(16, std::atoi(eo)));
   const char *ep = std::getenv("MOM_PANEL_CTAS");

@@ -1341,6 +1341,15 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
     }
     return MOM_OK;
   };
+  // C(m x ncol) -= L(m x nb) U(nb x ncol): the rank-64 updates; on the
+  // tensor cores (3xTF32) in the mixed path, as the trailing update
+  auto update64 = [&](int64_t m, int64_t ncol, const T *Lm, const T *Um, T *Cm) -> int {
+    if (m <= 0 || ncol <= 0) return MOM_OK;
+    if (mixed && c->small_tc)
+      return tc_cgemm_update(c, reinterpret_cast<float2 *>(Cm), lda, reinterpret_cast<const float2 *>(Lm), lda,
+                             reinterpret_cast<const float2 *>(Um), lda, (int)m, (int)ncol, nb, w.tcw, c->dinfo + 2);
+    return gemm(m, ncol, nb, -1.0, Lm, lda, Um, lda, 1.0, Cm, lda);
+  };
   // B(nb x ncol, at A + j0 + col*lda) <- inv(L_jj) B, through the workspace
   auto trsm_l = [&](int64_t j0, int64_t col, int64_t ncol, int kb) -> int {
     if (ncol <= 0) return MOM_OK;
@@ -1383,8 +1392,8 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
       if (rest > 0) {
         ProfScope pg(c, kProfGemm);
         MOM_TRY(trsm_l(j0, j0 + nb, rest, kb));
-        MOM_TRY(gemm(n - j0 - nb, rest, nb, -1.0, A + (j0 + nb) + j0 * lda, lda, A + j0 + (j0 + nb) * lda, lda, 1.0,
-                     A + (j0 + nb) + (j0 + nb) * lda, lda));
+        MOM_TRY(update64(n - j0 - nb, rest, A + (j0 + nb) + j0 * lda, A + j0 + (j0 + nb) * lda,
+                         A + (j0 + nb) + (j0 + nb) * lda));
       }
     }
     // trailing columns: block-row TRSM with L_JJ, then A22 -= L21 U12 with K = NBc
@@ -1394,8 +1403,7 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
       for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
         MOM_TRY(trsm_l(j0, t0, nc, (int)(j0 / nb)));
         const int64_t below = J0 + NBc - (j0 + nb);
-        MOM_TRY(gemm(below, nc, nb, -1.0, A + (j0 + nb) + j0 * lda, lda, A + j0 + t0 * lda, lda, 1.0,
-                     A + (j0 + nb) + t0 * lda, lda));
+        MOM_TRY(update64(below, nc, A + (j0 + nb) + j0 * lda, A + j0 + t0 * lda, A + (j0 + nb) + t0 * lda));
       }
       if (mixed) {
         // the large update on the tensor cores (3xTF32, FP32-accurate)

@@ -14,7 +14,8 @@ def solver(built):
     s.close()
 
 
-@pytest.mark.parametrize("m,nc,k", [(64, 100, 256), (320, 600, 64), (128, 256, 256), (192, 513, 128)])
+@pytest.mark.parametrize("m,nc,k", [(64, 100, 256), (320, 600, 64), (128, 256, 256), (192, 513, 128), (64, 64, 64),
+                                    (1984, 192, 64)])
 def test_tensor_core_update_matches_fp64(solver, m, nc, k):
     """The LU trailing update C -= L U on tcgen05 (3xTF32) is FP32-accurate:
     relative Frobenius error <= 1e-5 against the FP64 product of the same FP32
