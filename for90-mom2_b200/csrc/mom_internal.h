@@ -139,7 +139,7 @@ struct Ctx {
   // (the largest the device schedules; MOM_PANEL_CLUSTER caps it, 0 = off).
   int panel_cluster = 0;
   int outer_panels = 4;  // panels per outer block of the LU (MOM_LU_OUTER): trailing GEMMs have K = 64 * this
-  int small_tc = 1;      // mixed path: K = 64 updates on the tensor cores too (MOM_SMALL_TC=0: library FP32 GEMM)
+  int small_tc = 0;      // mixed path: K = 64 updates on the tensor cores too (MOM_SMALL_TC=1), else library FP32 GEMM
   bool autotune = true;
   struct Tuned {
     int64_t n;
