@@ -84,3 +84,9 @@ def test_autotuner_records_a_choice(solvers):
     t = S.autotune_result(M.MIXED)
     assert len(t["heights"]) >= 1 and t["heights"][0] >= 2 * S.N
     assert all(1 <= p <= 148 for p in t["ctas"]) and t["tune_ms"] > 0
+    # exchange-buffer placement: probed at the tallest height unless that
+    # panel runs on one cluster; the placement kept is the fastest probed
+    us = t["placement_us_per_column"]
+    if us:
+        assert len(us) == 16 and 0 <= t["placement"] < 16
+        assert us[t["placement"]] <= min(us) + 1e-3
