@@ -1,0 +1,543 @@
+// mom_b200 -- the reference's `mom` command interpreter (msgloop,
+// interface.f90:1624-1734) over the C ABI, for the commands of the linear
+// PMCHWT scattering path:
+//
+//   name  mesh  wlrg  wlls  symm  nmed  smed  ndom  sdom  fdom  nsrc  ssrc
+//   quad  solv  crst  rcst  exit
+//
+// plus two settings this build adds (the reference always computes in FP64):
+//
+//   prec fp64 | mixed [tol [maxit]]   arithmetic of solv (default fp64;
+//                                     mixed: FP32 tensor-core LU + FP64
+//                                     refinement to ||r|| <= tol ||b||,
+//                                     default tol 1e-12, maxit 30)
+//   dev  <index>                      CUDA device (default 0, or $MOM_DEVICE)
+//
+// Commands read one line each from standard input with Fortran list-directed
+// syntax: blanks or commas separate items, strings may be quoted, complex
+// values are written (re, im) and exponents may use d (200d-9).  Results go
+// to the same files as the reference: `crst` writes <name>-s<source>.crs
+// (wavelength, sigma_sca, sigma_abs per row) and `rcst w s nt np` writes
+// <name>-wl<w>-s<s>.rcs (nt rows of np values), both as EN15.3 fields with a
+// blank line after each row (write_data, aux.f90:192-211).
+//
+// Commands of the reference outside this path (symmetry groups other than
+// id, periodic Green's functions, volume domains, second-harmonic media,
+// near fields, diffraction, polarizability, the VIE solver, source offsets
+// and scans) print an error and stop, as the reference does on invalid
+// input, instead of producing results this build does not compute.
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mom_gpu.h"
+
+namespace {
+
+// constants.f90:8-16: pi is a default-real literal, so it carries float
+// rounding into c0-derived frequencies and degree conversions.
+const double kPi = (double)3.141592653589f;
+const double kC0 = 2.997924580003e8;
+const double kDegToRad = kPi / 180.0;
+
+using cplx = std::complex<double>;
+
+[[noreturn]] void stop(const std::string &msg) {
+  std::printf(" %s\n", msg.c_str());
+  std::fflush(stdout);
+  std::exit(1);
+}
+
+// ---- list-directed input ----
+
+// Items of a list-directed record: quoted strings lose their quotes,
+// parenthesised complex values stay one item "(re,im)".
+std::vector<std::string> items(const std::string &line) {
+  std::vector<std::string> out;
+  size_t i = 0;
+  const size_t n = line.size();
+  while (i < n) {
+    const char ch = line[i];
+    if (ch == ' ' || ch == '\t' || ch == ',' || ch == '\r') {
+      i++;
+      continue;
+    }
+    if (ch == '/') break;  // list-directed input ends at a slash
+    if (ch == '\'' || ch == '"') {
+      const size_t j = line.find(ch, i + 1);
+      if (j == std::string::npos) stop("Error: unterminated string in '" + line + "'");
+      out.push_back(line.substr(i + 1, j - i - 1));
+      i = j + 1;
+      continue;
+    }
+    if (ch == '(') {
+      const size_t j = line.find(')', i + 1);
+      if (j == std::string::npos) stop("Error: unterminated complex value in '" + line + "'");
+      out.push_back(line.substr(i, j - i + 1));
+      i = j + 1;
+      continue;
+    }
+    size_t j = i;
+    while (j < n && line[j] != ' ' && line[j] != '\t' && line[j] != ',' && line[j] != '\r') j++;
+    out.push_back(line.substr(i, j - i));
+    i = j;
+  }
+  return out;
+}
+
+bool to_real(std::string s, double *v) {
+  for (char &c : s)
+    if (c == 'd' || c == 'D') c = 'e';
+  char *end = nullptr;
+  *v = std::strtod(s.c_str(), &end);
+  return end && *end == '\0' && !s.empty();
+}
+
+double real_item(const std::vector<std::string> &it, size_t k, const char *cmd) {
+  double v;
+  if (k >= it.size() || !to_real(it[k], &v)) stop(std::string("Error: bad or missing number in command ") + cmd);
+  return v;
+}
+
+int int_item(const std::vector<std::string> &it, size_t k, const char *cmd) {
+  const double v = real_item(it, k, cmd);
+  if (v != std::floor(v)) stop(std::string("Error: expected an integer in command ") + cmd);
+  return (int)v;
+}
+
+cplx complex_item(const std::vector<std::string> &it, size_t k, const char *cmd) {
+  if (k >= it.size()) stop(std::string("Error: missing complex value in command ") + cmd);
+  const std::string &s = it[k];
+  if (s.size() < 5 || s.front() != '(' || s.back() != ')')
+    stop(std::string("Error: complex values are written (re, im) in command ") + cmd);
+  const std::vector<std::string> p = items(s.substr(1, s.size() - 2));
+  double re, im;
+  if (p.size() != 2 || !to_real(p[0], &re) || !to_real(p[1], &im))
+    stop(std::string("Error: bad complex value in command ") + cmd);
+  return {re, im};
+}
+
+// ---- output ----
+
+// Fortran EN15.3: engineering notation (mantissa in [1, 1000), exponent a
+// multiple of three, three decimals), right-justified in 15 columns.
+std::string en15_3(double v) {
+  char buf[64];
+  if (v == 0.0 || !std::isfinite(v)) {
+    if (v == 0.0) std::snprintf(buf, sizeof buf, "0.000E+00");
+    else std::snprintf(buf, sizeof buf, "%s", std::isnan(v) ? "NaN" : (v > 0 ? "Infinity" : "-Infinity"));
+  } else {
+    const double a = std::fabs(v);
+    int e3 = (int)std::floor(std::log10(a) / 3.0) * 3;
+    double m = a / std::pow(10.0, e3);
+    if (m < 1.0) {  // log10 rounding just below a power of 1000
+      m *= 1000.0;
+      e3 -= 3;
+    }
+    char mb[32];
+    std::snprintf(mb, sizeof mb, "%.3f", m);
+    if (std::atof(mb) >= 1000.0) {
+      m /= 1000.0;
+      e3 += 3;
+      std::snprintf(mb, sizeof mb, "%.3f", m);
+    }
+    std::snprintf(buf, sizeof buf, "%s%sE%c%02d", v < 0 ? "-" : "", mb, e3 < 0 ? '-' : '+', std::abs(e3));
+  }
+  std::string s(buf);
+  if (s.size() < 15) s = std::string(15 - s.size(), ' ') + s;
+  return s;
+}
+
+// write_data (aux.f90:192-211): rows of EN15.3 fields, each row followed by
+// an empty record.
+void write_data(const std::string &path, const std::vector<std::vector<double>> &rows) {
+  std::FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) stop("Could not open output file" + path + "!");
+  for (const auto &r : rows) {
+    for (double v : r) std::fputs(en15_3(v).c_str(), f);
+    std::fputs("\n\n", f);
+  }
+  std::fclose(f);
+}
+
+// ---- state: the batch type (common.f90:71-108) reduced to this path ----
+
+struct Domain {
+  bool set = false;
+  int medium = 0;  // 1-based medium index
+};
+
+struct State {
+  std::string name = "unnamed";
+  std::string quad = "tri_gl13";  // batch_defaults (common.f90:111-122)
+  mom_problem *prob = nullptr;
+  bool finalized = false;
+  std::vector<double> wl;
+  std::vector<std::vector<cplx>> media;  // [medium][wavelength]
+  std::vector<Domain> doms;
+  std::vector<mom_src> src;
+  std::vector<bool> src_set;
+  int precision = MOM_PREC_FP64;
+  double tol = 1e-12;
+  int maxit = 30;
+  int device = 0;
+  mom_ctx *ctx = nullptr;
+  bool uploaded = false;
+  int64_t n2 = 0;                    // 2N unknowns
+  std::vector<std::vector<double>> x;  // per wavelength: [nsrc][2N] complex, interleaved
+};
+
+void check(State &s, int st, const char *what) {
+  if (st == MOM_OK) return;
+  std::string msg = std::string("Error in ") + what + ": " + mom_gpu_strerror(st);
+  if (s.ctx) {
+    const char *le = mom_gpu_last_error(s.ctx);
+    if (le && *le) msg += std::string(" (") + le + ")";
+  }
+  stop(msg);
+}
+
+double omega_of(double wl) { return 2.0 * kPi * kC0 / wl; }
+
+// get_refind (aux.f90:100-167): linear interpolation in a (wl, n, k) table;
+// the result passes through a default-kind (single precision) complex, and
+// wavelengths outside the table give unity.
+cplx refind_from_file(const std::string &path, double wl) {
+  std::ifstream f(path);
+  if (!f) stop("Could not open refractive index lookup file!");
+  std::string line;
+  auto next = [&](double *w, double *nr, double *ni) -> bool {
+    while (std::getline(f, line)) {
+      const std::vector<std::string> it = items(line);
+      if (it.size() < 3) continue;
+      if (to_real(it[0], w) && to_real(it[1], nr) && to_real(it[2], ni)) return true;
+    }
+    return false;
+  };
+  auto single = [](double re, double im) { return cplx((double)(float)re, (double)(float)im); };
+  double w1, n1, k1, w2, n2, k2;
+  if (!next(&w1, &n1, &k1)) stop("Could not read refractive index lookup file!");
+  if (wl < w1) {
+    std::printf(" Wavelength below refractive index sample range!\n Using unity refractive index.\n");
+    return 1.0;
+  }
+  while (next(&w2, &n2, &k2)) {
+    if (w1 <= wl && wl <= w2 && w1 != w2) {
+      const double t = (wl - w1) / (w2 - w1);
+      return single(n1 + t * (n2 - n1), k1 + t * (k2 - k1));
+    } else if (wl == w1) {
+      return single(n1, k1);
+    } else if (wl == w2) {
+      return single(n2, k2);
+    } else if (w1 > w2) {
+      stop("Refractive index data disordered!");
+    }
+    w1 = w2;
+    n1 = n2;
+    k1 = k2;
+  }
+  std::printf(" Wavelength above refractive index sample range!\n Using unity refractive index.\n");
+  return 1.0;
+}
+
+void ensure_ctx(State &s) {
+  if (s.ctx) return;
+  check(s, mom_gpu_create(s.device, &s.ctx), "mom_gpu_create");
+}
+
+std::vector<double> ri_table(const State &s, size_t n) {
+  std::vector<double> ri(2 * s.doms.size());
+  for (size_t d = 0; d < s.doms.size(); d++) {
+    const cplx v = s.media[s.doms[d].medium - 1][n];
+    ri[2 * d] = v.real();
+    ri[2 * d + 1] = v.imag();
+  }
+  return ri;
+}
+
+// solve_batch (solver.f90:17-142): every wavelength, all sources.
+void solve_batch(State &s) {
+  std::printf(" --- Begin wavelength batch ---\n");
+  if (s.wl.empty()) stop("Setup wavelengths prior to solving!");
+  if (!s.prob) stop("Load mesh prior to solving!");
+  if (s.doms.empty() || !s.finalized) stop("Set up domains prior to solving!");
+  if (s.media.empty()) stop("Set up media prior to solving!");
+  if (s.src.empty()) stop("Set up source prior to solving!");
+  for (size_t i = 0; i < s.src.size(); i++)
+    if (!s.src_set[i]) stop("Source " + std::to_string(i + 1) + " has not been set up!");
+  for (size_t d = 0; d < s.doms.size(); d++)
+    if (!s.doms[d].set || s.doms[d].medium < 1 || s.doms[d].medium > (int)s.media.size())
+      stop("Domain " + std::to_string(d + 1) + " has no valid medium!");
+  ensure_ctx(s);
+  if (!s.uploaded) {
+    check(s, mom_problem_upload(s.prob, s.ctx, s.quad.c_str()), "upload of the domains");
+    s.uploaded = true;
+  }
+  s.n2 = 2 * (int64_t)mom_problem_nedges(s.prob);
+  std::printf(" Name: %s\n Triangle quadrature: %s\n Arithmetic: %s\n", s.name.c_str(), s.quad.c_str(),
+              s.precision == MOM_PREC_FP64 ? "FP64" : "mixed (FP32 LU + FP64 refinement)");
+  const int nsrc = (int)s.src.size();
+  s.x.assign(s.wl.size(), std::vector<double>());
+  for (size_t n = 0; n < s.wl.size(); n++) {
+    std::printf(" Wavelength: %6.1f nm (%zu of %zu)\n", s.wl[n] * 1e9, n + 1, s.wl.size());
+    const std::vector<double> ri = ri_table(s, n);
+    for (size_t d = 0; d < s.doms.size(); d++)
+      std::printf(" Refractive index of domain %zu: (%6.3f,%6.3f)\n", d + 1, ri[2 * d], ri[2 * d + 1]);
+    s.x[n].assign((size_t)2 * s.n2 * nsrc, 0.0);
+    int32_t iters = 0;
+    check(s,
+          mom_gpu_solve_wavelength(s.ctx, omega_of(s.wl[n]), ri.data(), nsrc, s.src.data(), s.precision, s.tol,
+                                   s.maxit, s.x[n].data(), s.n2, &iters),
+          "solv");
+    if (s.precision == MOM_PREC_MIXED) std::printf(" Refinement steps: %d\n", iters);
+  }
+  std::fflush(stdout);
+}
+
+// read_crst (interface.f90:1384-1475).
+void crst(State &s, const std::vector<std::string> &it) {
+  int medium = 1, domain = 1;
+  double factor = 1.0;
+  if (it.size() > 1) {
+    medium = int_item(it, 1, "crst");
+    domain = int_item(it, 2, "crst");
+    factor = real_item(it, 3, "crst");
+  }
+  if (s.x.empty()) stop("Error: solve (solv) before computing cross sections!");
+  if (medium < 1 || medium > (int)s.media.size() || domain < 1 || domain > (int)s.doms.size())
+    stop("Error: medium or domain index out of range in crst!");
+  std::printf(" Computing extinction cross-section\n");
+  const int nsrc = (int)s.src.size();
+  std::vector<std::vector<std::vector<double>>> data(nsrc, std::vector<std::vector<double>>(s.wl.size()));
+  std::vector<double> csca(nsrc), cabs(nsrc);
+  for (size_t n = 0; n < s.wl.size(); n++) {
+    const cplx v = s.media[medium - 1][n];
+    const double ri[2] = {v.real(), v.imag()};
+    check(s,
+          mom_gpu_cross_sections(s.ctx, domain - 1, omega_of(s.wl[n]), ri, nsrc, s.src.data(), s.x[n].data(), s.n2,
+                                 csca.data(), cabs.data()),
+          "crst");
+    for (int k = 0; k < nsrc; k++) data[k][n] = {s.wl[n], csca[k] * factor, cabs[k] * factor};
+    std::printf(" Wavelength %zu of %zu\n", n + 1, s.wl.size());
+  }
+  for (int k = 0; k < nsrc; k++) write_data(s.name + "-s" + std::to_string(k + 1) + ".crs", data[k]);
+  std::fflush(stdout);
+}
+
+// read_rcst (interface.f90:1291-1334).
+void rcst(State &s, const std::vector<std::string> &it) {
+  const int w = int_item(it, 1, "rcst"), k = int_item(it, 2, "rcst");
+  const int nt = int_item(it, 3, "rcst"), np = int_item(it, 4, "rcst");
+  if (s.x.empty()) stop("Error: solve (solv) before computing radar cross-sections!");
+  if (w < 1 || w > (int)s.wl.size() || k < 1 || k > (int)s.src.size() || nt < 1 || np < 1)
+    stop("Error: index or grid size out of range in rcst!");
+  std::printf(" Computing radar cross-sections\n");
+  const cplx v = s.media[s.doms[0].medium - 1][w - 1];
+  const double ri[2] = {v.real(), v.imag()};
+  std::vector<double> out((size_t)nt * np);
+  check(s, mom_gpu_rcs(s.ctx, 0, omega_of(s.wl[w - 1]), ri, k - 1, s.x[w - 1].data(), s.n2, nt, np, out.data()),
+        "rcst");
+  std::vector<std::vector<double>> rows(nt, std::vector<double>(np));
+  for (int i = 0; i < nt; i++)
+    for (int j = 0; j < np; j++) rows[i][j] = out[(size_t)j * nt + i];  // rcsdata(1:nt, 1:np), column-major
+  write_data(s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + ".rcs", rows);
+  std::fflush(stdout);
+}
+
+void command(State &s, const std::string &cmd, const std::vector<std::string> &it) {
+  if (cmd == "name") {
+    if (it.size() < 2) stop("Error: name needs a value");
+    s.name = it[1];
+  } else if (cmd == "mesh") {
+    // read_mesh (interface.f90:357-366)
+    if (it.size() < 3) stop("Error: mesh needs a file and a scale");
+    const double scale = real_item(it, 2, "mesh");
+    if (s.prob) mom_problem_destroy(s.prob);
+    s.prob = nullptr;
+    check(s, mom_problem_create(&s.prob), "mesh");
+    check(s, mom_problem_load_gmsh(s.prob, it[1].c_str(), scale), ("mesh " + it[1]).c_str());
+    s.finalized = s.uploaded = false;
+    s.doms.clear();
+  } else if (cmd == "wlrg") {
+    // read_wlrange (interface.f90:368-389)
+    const int n = int_item(it, 1, "wlrg");
+    const double a = real_item(it, 2, "wlrg"), b = real_item(it, 3, "wlrg");
+    if (n < 1) stop("Error: wlrg needs at least one wavelength");
+    s.wl.assign(n, a);
+    for (int i = 0; n > 1 && i < n; i++) s.wl[i] = a + (b - a) * ((double)i / (double)(n - 1));
+    s.x.clear();
+  } else if (cmd == "wlls") {
+    // read_wllist (interface.f90:391-406)
+    const int n = int_item(it, 1, "wlls");
+    if (n < 1) stop("Error: wlls needs at least one wavelength");
+    s.wl.resize(n);
+    for (int i = 0; i < n; i++) s.wl[i] = real_item(it, 2 + i, "wlls");
+    s.x.clear();
+  } else if (cmd == "symm") {
+    // read_symm (interface.f90:160-210): only the identity group is on this path
+    const int n = int_item(it, 1, "symm");
+    for (int i = 0; i < n; i++) {
+      if (2 + i >= (int)it.size()) stop("Error: symm lists fewer groups than announced");
+      if (it[2 + i] != "id") stop("Error: symmetry group '" + it[2 + i] + "' is not supported by this build (only id)");
+    }
+    std::printf(" Created a symmetry group with 1 elements.\n");
+  } else if (cmd == "nmed") {
+    // read_nmed (interface.f90:213-232)
+    if (s.wl.empty()) {
+      std::printf(" Error: no wavelengths set up!\n");
+      return;
+    }
+    const int n = int_item(it, 1, "nmed");
+    s.media.assign(n, std::vector<cplx>(s.wl.size(), cplx(1.0, 0.0)));
+    std::printf(" Allocated %d media.\n", n);
+  } else if (cmd == "smed") {
+    // read_smed (interface.f90:234-355): linear media only
+    if (s.media.empty()) {
+      std::printf(" Error: no media allocated!\n");
+      return;
+    }
+    const int m = int_item(it, 1, "smed");
+    if (m < 1 || m > (int)s.media.size()) stop("Error: medium index out of range in smed");
+    if (it.size() < 4) stop("Error: smed needs a type, a method and a value");
+    if (it[2] != "linear") stop("Error: medium type '" + it[2] + "' is not supported by this build (only linear)");
+    if (it[3] == "value") {
+      const cplx v = complex_item(it, 4, "smed");
+      for (auto &r : s.media[m - 1]) r = v;
+      std::printf("Set medium %d refractive index to (%6.3f,%6.3f)\n", m, v.real(), v.imag());
+    } else if (it[3] == "file") {
+      if (it.size() < 5) stop("Error: smed file needs a file name");
+      for (size_t n = 0; n < s.wl.size(); n++) s.media[m - 1][n] = refind_from_file(it[4], s.wl[n]);
+      std::printf("Set medium %d refractive index to %s\n", m, it[4].c_str());
+    } else {
+      std::printf(" Unrecongnized method for retrieveing medium properties!\n");
+    }
+  } else if (cmd == "ndom") {
+    // read_ndom (interface.f90:32-42)
+    if (!s.prob) stop("Error: master mesh has not been loaded!");
+    const int n = int_item(it, 1, "ndom");
+    if (n < 1) stop("Error: ndom needs at least one domain");
+    check(s, mom_problem_set_ndom(s.prob, n), "ndom");
+    s.doms.assign(n, Domain());
+    s.finalized = s.uploaded = false;
+    std::printf(" Allocated %d domains.\n", n);
+  } else if (cmd == "sdom") {
+    // read_sdom (interface.f90:44-105): dom nsurf ids... nvol [vol ids] medium gf
+    if (s.doms.empty()) stop("Error: no domains allocated!");
+    if (!s.prob) stop("Error: master mesh has not been loaded!");
+    const int d = int_item(it, 1, "sdom"), ns = int_item(it, 2, "sdom");
+    if (d < 1 || d > (int)s.doms.size() || ns < 1) stop("Error: domain index or surface count out of range in sdom");
+    std::vector<int32_t> ids(ns);
+    for (int i = 0; i < ns; i++) {
+      ids[i] = int_item(it, 3 + i, "sdom");
+      if (ids[i] == 0) stop("Zero is not a valid surface id!");
+    }
+    const int nvol = int_item(it, 3 + ns, "sdom");
+    if (nvol != 0) stop("Error: volume domains (nvol > 0) are not supported by this build");
+    const int medium = int_item(it, 4 + ns, "sdom"), gf = int_item(it, 5 + ns, "sdom");
+    if (gf != -1) stop("Error: periodic Green's functions (gf != -1) are not supported by this build");
+    check(s, mom_problem_set_domain(s.prob, d - 1, ns, ids.data()), "sdom");
+    s.doms[d - 1].set = true;
+    s.doms[d - 1].medium = medium;
+    s.finalized = s.uploaded = false;
+  } else if (cmd == "fdom") {
+    // read_fdom (interface.f90:107-123)
+    if (!s.prob) stop("Error: master mesh has not been loaded!");
+    for (size_t d = 0; d < s.doms.size(); d++)
+      if (!s.doms[d].set) stop("Error: domain " + std::to_string(d + 1) + " has not been set up (sdom)");
+    check(s, mom_problem_finalize(s.prob), "fdom");
+    s.finalized = true;
+    s.uploaded = false;
+  } else if (cmd == "nsrc") {
+    // read_nsrc (interface.f90:460-470)
+    const int n = int_item(it, 1, "nsrc");
+    if (n < 1) stop("Error: nsrc needs at least one source");
+    s.src.assign(n, mom_src());
+    s.src_set.assign(n, false);
+    s.x.clear();
+    std::printf(" Allocated %d sources.\n", n);
+  } else if (cmd == "ssrc") {
+    // read_ssrc (interface.f90:486-550): plane waves only
+    if (s.src.empty()) stop("No sources allocated!");
+    const int k = int_item(it, 1, "ssrc");
+    if (k < 1 || k > (int)s.src.size()) stop("Error: source index out of range in ssrc");
+    if (it.size() < 3) stop("Error: ssrc needs a source type");
+    mom_src &src = s.src[k - 1];
+    src = mom_src();
+    if (it[2] == "pw") {
+      src.type = MOM_SRC_PW;
+      src.theta = real_item(it, 3, "ssrc") * kDegToRad;
+      src.phi = real_item(it, 4, "ssrc") * kDegToRad;
+      src.psi = real_item(it, 5, "ssrc") * kDegToRad;
+    } else if (it[2] == "pw_elliptic") {
+      src.type = MOM_SRC_PW_ELLIPTIC;
+      src.theta = real_item(it, 3, "ssrc") * kDegToRad;
+      src.phi = real_item(it, 4, "ssrc") * kDegToRad;
+      const cplx ph = complex_item(it, 5, "ssrc");
+      src.phase_re = ph.real();
+      src.phase_im = ph.imag();
+    } else {
+      stop("Error: source type '" + it[2] + "' is not supported by this build (pw, pw_elliptic)");
+    }
+    s.src_set[k - 1] = true;
+    s.x.clear();
+  } else if (cmd == "quad") {
+    // read_quad (interface.f90:18-30): the triangle rule; the tetrahedron rule
+    // belongs to the volume solver
+    if (it.size() < 2) stop("Error: quad needs a triangle rule name");
+    double w[13], q[39];
+    if (mom_tri_rule(it[1].c_str(), w, q) < 0) stop("Error: unknown triangle quadrature '" + it[1] + "'");
+    s.quad = it[1];
+    s.uploaded = false;
+  } else if (cmd == "prec") {
+    if (it.size() < 2) stop("Error: prec needs fp64 or mixed");
+    if (it[1] == "fp64") s.precision = MOM_PREC_FP64;
+    else if (it[1] == "mixed") s.precision = MOM_PREC_MIXED;
+    else stop("Error: prec takes fp64 or mixed");
+    if (it.size() > 2) s.tol = real_item(it, 2, "prec");
+    if (it.size() > 3) s.maxit = int_item(it, 3, "prec");
+  } else if (cmd == "dev") {
+    if (s.ctx) stop("Error: dev must come before the first solv");
+    s.device = int_item(it, 1, "dev");
+  } else if (cmd == "solv") {
+    solve_batch(s);
+  } else if (cmd == "crst") {
+    crst(s, it);
+  } else if (cmd == "rcst") {
+    rcst(s, it);
+  } else if (cmd == "osrc" || cmd == "npgf" || cmd == "ipgw" || cmd == "sbnd" || cmd == "nfms" || cmd == "nfdm" ||
+             cmd == "nfem" || cmd == "nfst" || cmd == "nfpl" || cmd == "rcs2" || cmd == "rcs3" || cmd == "diff" ||
+             cmd == "plrz" || cmd == "scan" || cmd == "trns" || cmd == "csca" || cmd == "test" || cmd == "vsol" ||
+             cmd == "vext" || cmd == "viem" || cmd == "msrc") {
+    stop("Error: command " + cmd + " is outside the linear PMCHWT path that this build implements");
+  } else {
+    std::printf(" Unrecognized command %s!\n", cmd.c_str());
+  }
+}
+
+}  // namespace
+
+int main() {
+  State s;
+  if (const char *ed = std::getenv("MOM_DEVICE")) s.device = std::atoi(ed);
+  std::string line;
+  while (true) {
+    std::printf("> ");
+    std::fflush(stdout);
+    if (!std::getline(std::cin, line)) break;
+    const std::vector<std::string> it = items(line);
+    if (it.empty()) continue;
+    if (it[0] == "exit") break;
+    command(s, it[0], it);
+  }
+  std::printf("\n");
+  if (s.ctx) mom_gpu_destroy(s.ctx);
+  if (s.prob) mom_problem_destroy(s.prob);
+  return 0;
+}
