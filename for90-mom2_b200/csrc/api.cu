@@ -105,6 +105,8 @@ void free_domain(DomDev &D) {
   cudaFree(D.near_bits);
   cudaFree(D.inc_node);
   cudaFree(D.inc_face);
+  cudaFree(D.nf_geo);
+  cudaFree(D.nf_bn);
   D = DomDev();
 }
 
@@ -401,6 +403,7 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->ws);
   cudaFree(c->ws2);
   cudaFree(c->Xh);
+  cudaFree(c->nf_buf);
   cudaFree(c->adj);
   cudaFree(c->adj_part);
   cudaFree(c->adjW);
@@ -752,6 +755,49 @@ int mom_gpu_rcs(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t
     xd = c->X + (size_t)isrc * c->n;
   }
   return far_field(c, dom, omega, ri, xd, ntheta, nphi, rcs);
+}
+
+int mom_gpu_scat_fields(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                        const double *x_host, int64_t ldx, int32_t npts, const double *pts, double *e, double *h) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (dom < 0 || dom >= c->ndom || nsrc < 1 || npts < 1 || !pts || !e || !h || !ri || !(omega > 0))
+    return fail(c, MOM_ERR_ARG, "invalid near-field arguments");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  const size_t pbytes = ((sizeof(double) * 3 * (size_t)npts + 255) / 256) * 256;
+  const size_t fbytes = ((sizeof(double2) * 3 * (size_t)npts * nsrc + 255) / 256) * 256;
+  const size_t xbytes = x_host ? sizeof(double2) * (size_t)c->n * nsrc : 0;
+  const size_t sbytes = (size_t)128 * nsrc;
+  MOM_TRY(ensure_buffer(c, &c->nf_buf, &c->nf_cap, pbytes + 2 * fbytes + sbytes + xbytes + 256));
+  char *b = (char *)c->nf_buf;
+  double *dp = (double *)b;
+  double2 *dE = (double2 *)(b + pbytes), *dH = (double2 *)(b + pbytes + fbytes);
+  void *dsrc = b + pbytes + 2 * fbytes;
+  const double2 *xd;
+  int64_t ldxd;
+  if (x_host) {
+    if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+    double2 *xh = (double2 *)(b + pbytes + 2 * fbytes + ((sbytes + 255) / 256) * 256);
+    MOM_CUDA(c, cudaMemcpy2DAsync(xh, sizeof(double2) * c->n, x_host, sizeof(double2) * ldx,
+                                  sizeof(double2) * 2 * c->N, nsrc, cudaMemcpyHostToDevice, c->stream));
+    xd = xh;
+    ldxd = c->n;
+  } else {
+    if (nsrc > c->nsrc) return fail(c, MOM_ERR_STATE, "no device solutions for that many sources");
+    xd = c->X;
+    ldxd = c->n;
+  }
+  MOM_CUDA(c, cudaMemcpyAsync(dp, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice, c->stream));
+  {
+    ProfScope ps(c, kProfPost);
+    MOM_TRY(scat_fields(c, dom, omega, ri, nsrc, xd, ldxd, npts, dp, dE, dH));
+    if (src) MOM_TRY(add_incident_fields(c, omega, ri, nsrc, src, npts, dp, dE, dH, dsrc));
+  }
+  MOM_CUDA(c, cudaMemcpyAsync(e, dE, sizeof(double2) * 3 * (size_t)npts * nsrc, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(h, dH, sizeof(double2) * 3 * (size_t)npts * nsrc, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
 }
 
 int mom_gpu_device_matrix(mom_ctx *c, void **A_dev, int64_t *lda) {

@@ -389,6 +389,53 @@ __device__ S d_intSm3h(const S *r, const FaceGeoT<S> &g) {
   return dot3(g.n, rp1) > 0.0 ? fabs(om) : -fabs(om);
 }
 
+// The closed-form static integrals of face g at one point r that the
+// singular parts need (int.f90:137-407 and the intK*singular routines of
+// srcint.f90): Sm1 and S1 (intSm1, intS1), rho = r - h n, the edge sums
+// mL1 = sum_e m_e L1_e and mL3, and the gradient integrals K3m1 (intK3m1)
+// and K31 (intK31).
+template <typename S>
+struct PointStatic {
+  S Sm1, S1, rho[3], mL1[3], mL3[3], K3m1[3], K31[3];
+};
+template <typename S>
+__device__ __forceinline__ void point_static(const S *r, const FaceGeoT<S> &g, PointStatic<S> &o) {
+  S Lm1[3], L1[3], L3[3];
+  // intSm1 (int.f90:181-226) decides per edge whether intLm1 is needed
+  // when h == 0; intL1 always calls intLm1 unless R02 == 0.
+  S r1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
+  S h = dot3(g.n, r1);
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    Lm1[e] = d_intLm1(r, g, e);
+    d_intL13(r, g, e, g.n, Lm1[e], &L1[e], &L3[e]);
+  }
+  S tt[3];
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    S re[3] = {r[0] - g.v[e][0], r[1] - g.v[e][1], r[2] - g.v[e][2]};
+    tt[e] = dot3(g.mm[e], re);
+  }
+  S Sm3h = d_intSm3h(r, g);
+  S Sm1;
+  if (h == 0) {
+    S e1 = tt[0] == 0 ? S(0.0) : Lm1[0], e2 = tt[1] == 0 ? S(0.0) : Lm1[1], e3 = tt[2] == 0 ? S(0.0) : Lm1[2];
+    Sm1 = -(tt[0] * e1 + tt[1] * e2 + tt[2] * e3);
+  } else {
+    Sm1 = -h * Sm3h - (tt[0] * Lm1[0] + tt[1] * Lm1[1] + tt[2] * Lm1[2]);
+  }
+  o.Sm1 = Sm1;
+  o.S1 = (h * h) / 3.0 * Sm1 - 1.0 / 3.0 * (tt[0] * L1[0] + tt[1] * L1[1] + tt[2] * L1[2]);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    o.rho[i] = r[i] - h * g.n[i];
+    o.mL1[i] = g.mm[0][i] * L1[0] + g.mm[1][i] * L1[1] + g.mm[2][i] * L1[2];
+    o.mL3[i] = g.mm[0][i] * L3[0] + g.mm[1][i] * L3[1] + g.mm[2][i] * L3[2];
+    o.K3m1[i] = g.mm[0][i] * Lm1[0] + g.mm[1][i] * Lm1[1] + g.mm[2][i] * Lm1[2] + g.n[i] * Sm3h;
+    o.K31[i] = (h == 0) ? o.mL1[i] : o.mL1[i] - h * g.n[i] * Sm1;
+  }
+}
+
 // The k-independent closed-form integrals of source face n (geometry g,
 // area An, RWG sl and free vertices bnn) at the NQ test points qm of face m
 // (area Am, sl slm, free vertices bnm), contracted with the test RWG
@@ -405,40 +452,10 @@ __device__ void static_terms(const S (*qm)[3], S Am, const S *slm, const S (*bnm
   for (int t = 0; t < NQ; t++) {
     const S *r = qm[t];
     const double wt = c_qw[t];
-    S Lm1[3], L1[3], L3[3];
-    // intSm1 (int.f90:181-226) decides per edge whether intLm1 is needed
-    // when h == 0; intL1 always calls intLm1 unless R02 == 0.
-    S r1[3] = {r[0] - g.v[0][0], r[1] - g.v[0][1], r[2] - g.v[0][2]};
-    S h = dot3(g.n, r1);
-#pragma unroll
-    for (int e = 0; e < 3; e++) {
-      Lm1[e] = d_intLm1(r, g, e);
-      d_intL13(r, g, e, g.n, Lm1[e], &L1[e], &L3[e]);
-    }
-    S tt[3];
-#pragma unroll
-    for (int e = 0; e < 3; e++) {
-      S re[3] = {r[0] - g.v[e][0], r[1] - g.v[e][1], r[2] - g.v[e][2]};
-      tt[e] = dot3(g.mm[e], re);
-    }
-    S Sm3h = d_intSm3h(r, g);
-    S Sm1;
-    if (h == 0) {
-      S e1 = tt[0] == 0 ? S(0.0) : Lm1[0], e2 = tt[1] == 0 ? S(0.0) : Lm1[1], e3 = tt[2] == 0 ? S(0.0) : Lm1[2];
-      Sm1 = -(tt[0] * e1 + tt[1] * e2 + tt[2] * e3);
-    } else {
-      Sm1 = -h * Sm3h - (tt[0] * Lm1[0] + tt[1] * Lm1[1] + tt[2] * Lm1[2]);
-    }
-    S S1 = (h * h) / 3.0 * Sm1 - 1.0 / 3.0 * (tt[0] * L1[0] + tt[1] * L1[1] + tt[2] * L1[2]);
-    S rho[3], K3m1[3], K31[3], mL1[3], mL3[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-      rho[i] = r[i] - h * g.n[i];
-      mL1[i] = g.mm[0][i] * L1[0] + g.mm[1][i] * L1[1] + g.mm[2][i] * L1[2];
-      mL3[i] = g.mm[0][i] * L3[0] + g.mm[1][i] * L3[1] + g.mm[2][i] * L3[2];
-      K3m1[i] = g.mm[0][i] * Lm1[0] + g.mm[1][i] * Lm1[1] + g.mm[2][i] * Lm1[2] + g.n[i] * Sm3h;
-      K31[i] = (h == 0) ? mL1[i] : mL1[i] - h * g.n[i] * Sm1;
-    }
+    PointStatic<S> ps;
+    point_static(r, g, ps);
+    const S Sm1 = ps.Sm1, S1 = ps.S1;
+    const S *rho = ps.rho, *K3m1 = ps.K3m1, *K31 = ps.K31, *mL1 = ps.mL1, *mL3 = ps.mL3;
     // test functions at r: f_p = sl_p/(2 Am) (r - u_p), div f_p = sl_p / Am
     S fp[3][3], dvp[3];
 #pragma unroll
@@ -851,6 +868,7 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
 }
 
 #include "adjoint_impl.cuh"
+#include "nfields_impl.cuh"
 
 namespace {
 

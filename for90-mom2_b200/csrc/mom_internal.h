@@ -61,6 +61,9 @@ struct DomDev {
   unsigned *near_bits = nullptr;                 // [F*F] bits
   int ninc = 0;                                  // (vertex, face) incidences, by vertex
   int *inc_node = nullptr, *inc_face = nullptr;
+  // Face geometry of the near-field kernel (uploaded on first use).
+  void *nf_geo = nullptr;
+  double *nf_bn = nullptr;
 };
 
 struct Ctx {
@@ -110,6 +113,8 @@ struct Ctx {
   size_t BX_cap = 0;
   double2 *Xh = nullptr;   // solutions uploaded from the host for post-processing
   size_t Xh_cap = 0;
+  void *nf_buf = nullptr;   // near-field points, fields and source records
+  size_t nf_cap = 0;
   std::vector<mom_src> srcs;
   double omega_rhs = 0;
   double ri1[2] = {1, 0};
@@ -234,6 +239,15 @@ int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, co
                    const double2 *xdev, int64_t ldx, double *csca, double *cabs);
 int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
               double *rcs);
+// Near fields (nfields.f90 scat_fields; csrc/nfields_impl.cuh): E, H
+// [nsrc][npts][3] of the currents X ([nsrc][ldx], device) at device points.
+int scat_fields(Ctx *c, int d, double omega, const double *ri, int nsrc, const double2 *X, int64_t ldx, int npts,
+                const double *pts, double2 *E, double2 *H);
+// Adds the incident plane-wave fields of the sources at the device points
+// (field_plane's addsrc, nfpost.f90:342-348); srcbuf: device scratch of at
+// least 128 bytes per source.
+int add_incident_fields(Ctx *c, double omega, const double *ri, int nsrc, const mom_src *src, int npts,
+                        const double *pts, double2 *E, double2 *H, void *srcbuf);
 int cs_gradient(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src, const double2 *xdev,
                 int64_t ldx, double2 *G);
 void src_geometry(const mom_src &s, double dir[3], double pol[3]);

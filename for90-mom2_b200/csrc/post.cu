@@ -640,4 +640,43 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   return MOM_OK;
 }
 
+namespace {
+
+// Thread per (point, source): E, H += the source's plane-wave fields at the point.
+__global__ void incident_kernel(const SrcDev *src, Z k, double omega, const double *pts, int npts, double2 *E,
+                                double2 *H) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= npts) return;
+  Z ef[3], hf[3];
+  src_fields(src[s], k, omega, pts + 3 * i, ef, hf);
+  double2 *e = E + ((size_t)s * npts + i) * 3, *h = H + ((size_t)s * npts + i) * 3;
+  for (int c = 0; c < 3; c++) {
+    e[c].x += ef[c].re;
+    e[c].y += ef[c].im;
+    h[c].x += hf[c].re;
+    h[c].y += hf[c].im;
+  }
+}
+
+}  // namespace
+
+int add_incident_fields(Ctx *c, double omega, const double *ri, int nsrc, const mom_src *src, int npts,
+                        const double *pts, double2 *E, double2 *H, void *srcbuf) {
+  static_assert(sizeof(SrcDev) <= 128, "source record larger than the caller's scratch");
+  std::vector<SrcDev> h(nsrc);
+  for (int i = 0; i < nsrc; i++) {
+    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC)
+      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+    make_src(src[i], h[i]);
+  }
+  SrcDev *d = reinterpret_cast<SrcDev *>(srcbuf);
+  MOM_CUDA(c, cudaMemcpyAsync(d, h.data(), sizeof(SrcDev) * nsrc, cudaMemcpyHostToDevice, c->stream));
+  const Z k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
+  incident_kernel<<<dim3((npts + 127) / 128, nsrc), 128, 0, c->stream>>>(d, k, omega, pts, npts, E, H);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
 }  // namespace mom

@@ -3,7 +3,7 @@
 // PMCHWT scattering path:
 //
 //   name  mesh  wlrg  wlls  symm  nmed  smed  ndom  sdom  fdom  nsrc  ssrc
-//   quad  solv  crst  rcst  exit
+//   quad  solv  crst  rcst  nfpl  exit
 //
 // plus two settings this build adds (the reference always computes in FP64):
 //
@@ -19,7 +19,8 @@
 // to the same files as the reference: `crst` writes <name>-s<source>.crs
 // (wavelength, sigma_sca, sigma_abs per row) and `rcst w s nt np` writes
 // <name>-wl<w>-s<s>.rcs (nt rows of np values), both as EN15.3 fields with a
-// blank line after each row (write_data, aux.f90:192-211).
+// blank line after each row (write_data, aux.f90:192-211); `nfpl` writes the
+// field-component files of read_nfpl.
 //
 // Commands of the reference outside this path (symmetry groups other than
 // id, periodic Green's functions, volume domains, second-harmonic media,
@@ -351,6 +352,75 @@ void rcst(State &s, const std::vector<std::string> &it) {
   std::fflush(stdout);
 }
 
+// read_nfpl (interface.f90:805-894) with field_plane (nfpost.f90:316-374):
+// fields of domain d on the n1 x n2 grid origin + i/(n1-1) v1 + j/(n2-1) v2,
+// plus the incident field in domain 1, expressed in the basis (v1/|v1|,
+// v2/|v2|, their cross product); 12 files per source, each n2 rows of n1.
+void nfpl(State &s, const std::vector<std::string> &it) {
+  const int w = int_item(it, 1, "nfpl"), d = int_item(it, 2, "nfpl");
+  double o[3], v1[3], v2[3];
+  for (int i = 0; i < 3; i++) {
+    o[i] = real_item(it, 3 + i, "nfpl");
+    v1[i] = real_item(it, 6 + i, "nfpl");
+    v2[i] = real_item(it, 9 + i, "nfpl");
+  }
+  const int n1 = int_item(it, 12, "nfpl"), n2 = int_item(it, 13, "nfpl");
+  if (it.size() < 15) stop("Error: nfpl needs a tag");
+  const std::string tag = it[14];
+  if (s.x.empty()) stop("Error: solve (solv) before computing near fields!");
+  if (w < 1 || w > (int)s.wl.size() || d < 1 || d > (int)s.doms.size() || n1 < 2 || n2 < 2)
+    stop("Error: index or grid size out of range in nfpl (grids need at least 2 x 2 points)");
+  const int nsrc = (int)s.src.size(), npts = n1 * n2;
+  std::vector<double> pts(3 * (size_t)npts);
+  for (int a = 0; a < n1; a++)
+    for (int b = 0; b < n2; b++)
+      for (int i = 0; i < 3; i++)
+        pts[3 * ((size_t)a * n2 + b) + i] = o[i] + (double)a / (n1 - 1) * v1[i] + (double)b / (n2 - 1) * v2[i];
+  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  const double ri[2] = {v.real(), v.imag()};
+  std::vector<double> e(6 * (size_t)npts * nsrc), h(6 * (size_t)npts * nsrc);
+  std::printf(" Computing near fields on a plane\n");
+  check(s,
+        mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, d == 1 ? s.src.data() : nullptr,
+                            s.x[w - 1].data(), s.n2, npts, pts.data(), e.data(), h.data()),
+        "nfpl");
+  double b1[3], b2[3], b3[3];
+  const double l1 = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
+  const double l2 = std::sqrt(v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2]);
+  for (int i = 0; i < 3; i++) {
+    b1[i] = v1[i] / l1;
+    b2[i] = v2[i] / l2;
+  }
+  b3[0] = b1[1] * b2[2] - b1[2] * b2[1];
+  b3[1] = b1[2] * b2[0] - b1[0] * b2[2];
+  b3[2] = b1[0] * b2[1] - b1[1] * b2[0];
+  const double *basis[3] = {b1, b2, b3};
+  const char *comp[3] = {"x", "y", "z"};
+  for (int k = 0; k < nsrc; k++) {
+    const std::string stem = s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k + 1) + "-d" +
+                             std::to_string(d) + "-" + tag + "-";
+    for (int f = 0; f < 2; f++) {
+      const std::vector<double> &src = f == 0 ? e : h;
+      std::vector<std::vector<std::vector<double>>> R(3, std::vector<std::vector<double>>(n2, std::vector<double>(n1)));
+      std::vector<std::vector<std::vector<double>>> I(3, std::vector<std::vector<double>>(n2, std::vector<double>(n1)));
+      for (int a = 0; a < n1; a++)
+        for (int b = 0; b < n2; b++) {
+          const double *fv = &src[6 * (((size_t)k * npts) + (size_t)a * n2 + b)];  // 3 complex
+          for (int c = 0; c < 3; c++) {
+            // dotc (linalg.f90:15-21): no conjugation
+            const double *bc = basis[c];
+            R[c][b][a] = bc[0] * fv[0] + bc[1] * fv[2] + bc[2] * fv[4];
+            I[c][b][a] = bc[0] * fv[1] + bc[1] * fv[3] + bc[2] * fv[5];
+          }
+        }
+      const char fl = f == 0 ? 'e' : 'h';
+      for (int c = 0; c < 3; c++) write_data(stem + fl + comp[c] + "-re.dat", R[c]);
+      for (int c = 0; c < 3; c++) write_data(stem + fl + comp[c] + "-im.dat", I[c]);
+    }
+  }
+  std::fflush(stdout);
+}
+
 void command(State &s, const std::string &cmd, const std::vector<std::string> &it) {
   if (cmd == "name") {
     if (it.size() < 2) stop("Error: name needs a value");
@@ -511,8 +581,10 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     crst(s, it);
   } else if (cmd == "rcst") {
     rcst(s, it);
+  } else if (cmd == "nfpl") {
+    nfpl(s, it);
   } else if (cmd == "osrc" || cmd == "npgf" || cmd == "ipgw" || cmd == "sbnd" || cmd == "nfms" || cmd == "nfdm" ||
-             cmd == "nfem" || cmd == "nfst" || cmd == "nfpl" || cmd == "rcs2" || cmd == "rcs3" || cmd == "diff" ||
+             cmd == "nfem" || cmd == "nfst" || cmd == "rcs2" || cmd == "rcs3" || cmd == "diff" ||
              cmd == "plrz" || cmd == "scan" || cmd == "trns" || cmd == "csca" || cmd == "test" || cmd == "vsol" ||
              cmd == "vext" || cmd == "viem" || cmd == "msrc") {
     stop("Error: command " + cmd + " is outside the linear PMCHWT path that this build implements");

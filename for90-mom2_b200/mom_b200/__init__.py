@@ -47,7 +47,7 @@ EXPORTS = [
     "mom_problem_set_mesh", "mom_problem_set_ndom", "mom_problem_set_domain", "mom_problem_finalize",
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
     "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
-    "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement",
+    "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement", "mom_gpu_scat_fields",
 ]
 
 
@@ -98,6 +98,8 @@ def lib():
     L.mom_gpu_cross_sections.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp, C.c_int64,
                                          dp, dp]
     L.mom_gpu_rcs.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, C.c_int32, C.c_int32, dp]
+    L.mom_gpu_scat_fields.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp, C.c_int64,
+                                      C.c_int32, dp, dp, dp]
     L.mom_gpu_cross_sections_noalloc.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), vp,
                                                  C.c_int64, dp, dp]
     L.mom_gpu_adjoint.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, C.POINTER(MomSrc), C.c_int32, C.c_double,
@@ -485,6 +487,33 @@ class Solver:
         ns = C.c_int32()
         self._ck(lib().mom_gpu_device_solution(self.h, C.byref(p), C.byref(ld), C.byref(ns)), "device_solution")
         return p.value, ld.value, ns.value
+
+    def scat_fields(self, omega, ri, pts, x=None, nsrc=None, srcs=None, dom=0):
+        """scat_fields (nfields.f90:29-197) at pts[npts][3] (metres) from the currents of
+        domain dom with that domain's refractive index ri: (e, h), each [nsrc][npts][3]
+        complex.  x: 2N x nsrc host solutions, or None for the first nsrc device
+        solutions.  srcs: add each source's incident field (the exterior-domain
+        total field of field_plane)."""
+        r = _ri(ri)
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        xp = None
+        if x is not None:
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            xp = x.ctypes.data
+            ns = x.shape[1]
+        else:
+            ns = nsrc if nsrc is not None else (len(srcs) if srcs else 1)
+        arr = None
+        if srcs:
+            arr, nss = _srcs(srcs)
+            if nss != ns:
+                raise ValueError("one source per solution column")
+        e = np.zeros((ns, len(pts), 3), dtype=np.complex128)
+        h = np.zeros_like(e)
+        self._ck(lib().mom_gpu_scat_fields(self.h, dom, omega, _dp(r), ns, arr, xp, 2 * self.N, len(pts), _dp(pts),
+                                           e.ctypes.data_as(C.POINTER(C.c_double)),
+                                           h.ctypes.data_as(C.POINTER(C.c_double))), "scat_fields")
+        return e, h
 
     def rcs(self, omega, ri, ntheta, nphi, isrc=0, x=None, dom=0):
         r = _ri(ri)

@@ -126,6 +126,18 @@ int mom_gpu_cross_sections(mom_ctx *ctx, int32_t dom, double omega, const double
 int mom_gpu_rcs(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
                 int64_t ldx, int32_t ntheta, int32_t nphi, double *rcs);
 
+/* Replaces scat_fields (nfields.f90:29-197, identity group) at npts points
+ * pts[npts][3] (metres): the fields radiated by the surface currents of
+ * domain dom (0-based) with that domain's refractive index ri (re/im), for
+ * the nsrc solution columns of x_host (2N x nsrc, ldx) or, if NULL, the
+ * device solutions.  e, h: [nsrc][npts][3] complex (2 doubles each).  If src
+ * is not NULL the incident field of src[s] is added to column s (what
+ * field_plane and field_domain do in the exterior domain, nfpost.f90:85-165,
+ * 316-374).  Faces within three average edge lengths of a point use the
+ * singularity-subtracted integrals (srcint.f90 intK2/3/4). */
+int mom_gpu_scat_fields(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t nsrc, const mom_src *src,
+                        const double *x_host, int64_t ldx, int32_t npts, const double *pts, double *e, double *h);
+
 /* Allocation-free cross sections.  No counterpart in the reference.  For
  * callers that cannot allocate device memory at call time (their device
  * memory is reserved up front by another allocator, or they cannot accept

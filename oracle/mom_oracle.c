@@ -1189,6 +1189,88 @@ void oracle_rcs(void *p, int d, double omega, const double *ri_ri, const cplx *x
     }
 }
 
+/* srcint.f90:264-325 intK3 with 227-260 intK3singular (identity group,
+ * non-periodic): int_T grad'G div'f_e dS' for the three RWG functions of
+ * face f; res[3 edges][3]. */
+static void intK3(const double *r, int f, const omesh *m, cplx k, int near, const oquad *qd, cplx *res) {
+  double qpn[13 * 3];
+  double An = m->face_area[f];
+  quad_tri_points(qd, m, f, qpn);
+  cplx tmp[3] = {0, 0, 0};
+  for (int t = 0; t < qd->nq; t++) {
+    cplx g[3];
+    gradG_or_s(r, qpn + 3 * t, k, near, g);
+    for (int i = 0; i < 3; i++) tmp[i] += g[i] * qd->w[t];
+  }
+  for (int i = 0; i < 3; i++) tmp[i] *= An;
+  cplx sing[3] = {0, 0, 0};
+  if (near) {
+    double km1[3], k1[3];
+    intK3m1(r, f, m, km1);
+    intK31(r, f, m, k1);
+    for (int i = 0; i < 3; i++) sing[i] = 1.0 / (4.0 * O_PI) * km1[i] - (k * k) / (8.0 * O_PI) * k1[i];
+  }
+  for (int e = 0; e < 3; e++) {
+    double divfn = rwgDiv(m, f, e);
+    for (int i = 0; i < 3; i++) res[3 * e + i] = tmp[i] * divfn + sing[i] * divfn;
+  }
+}
+
+/* Scattered fields of the surface currents of domain d at points
+ * (nfields.f90:29-49 scat_fields with 109-197 scat_fields_frags, identity
+ * group: one fragment, group factors 1): per face the integrals intK2,
+ * intK3, intK4 (no test face), singular parts when the point is within three
+ * average edge lengths of the face centroid.  With addsrc the incident field
+ * of each source is added (field_plane, nfpost.f90:316-374, does so in the
+ * exterior domain).  x: [nsrc][ldx] (J in 0..N-1, M in N..2N-1); pts[npts][3];
+ * e, h: [nsrc][npts][3]. */
+void oracle_scat_fields(void *p, int d, double omega, const double *ri_ri, int nsrc, const cplx *x, int64_t ldx,
+                        const osrc *src, int addsrc, int npts, const double *pts, cplx *e, cplx *h) {
+  oproblem *P = p;
+  const omesh *m = P->dom + d;
+  const oquad *qd = &P->qd;
+  const int N = P->master.nedges;
+  const cplx ri = ri_ri[0] + I * ri_ri[1];
+  const cplx k = ri * omega / O_C0;
+  const double thr2 = (m->avelen * 3) * (m->avelen * 3);
+  const cplx c1 = I * omega * O_MU0;
+  const cplx c2 = 1.0 / (I * omega * O_EPS0 * (ri * ri));
+  for (int ip = 0; ip < npts; ip++) {
+    const double *r = pts + 3 * ip;
+    for (int s = 0; s < nsrc; s++)
+      for (int i = 0; i < 3; i++) e[((size_t)s * npts + ip) * 3 + i] = h[((size_t)s * npts + ip) * 3 + i] = 0;
+    for (int f = 0; f < m->nfaces; f++) {
+      const double *cp = m->face_cp + 3 * f;
+      double df[3] = {r[0] - cp[0], r[1] - cp[1], r[2] - cp[2]};
+      int near = dotr(df, df) < thr2;
+      cplx k2[9], k3[9], k4[9];
+      intK2(r, f, m, k, near, qd, k2);
+      intK3(r, f, m, k, near, qd, k3);
+      intK4(r, f, m, k, -1, near, qd, k4);
+      for (int q = 0; q < 3; q++) {
+        int idx = m->edge_parent[m->face_edge[3 * f + q]];
+        for (int s = 0; s < nsrc; s++) {
+          cplx xj = x[(size_t)s * ldx + idx], xm = x[(size_t)s * ldx + idx + N];
+          cplx *es = e + ((size_t)s * npts + ip) * 3, *hs = h + ((size_t)s * npts + ip) * 3;
+          for (int i = 0; i < 3; i++) {
+            es[i] += xj * (c1 * k2[3 * q + i] + c2 * k3[3 * q + i]) + xm * k4[3 * q + i];
+            hs[i] += xm * (k2[3 * q + i] / c2 + k3[3 * q + i] / c1) - xj * k4[3 * q + i];
+          }
+        }
+      }
+    }
+    if (addsrc)
+      for (int s = 0; s < nsrc; s++) {
+        cplx einc[3], hinc[3];
+        src_fields(src + s, omega, ri, r, einc, hinc);
+        for (int i = 0; i < 3; i++) {
+          e[((size_t)s * npts + ip) * 3 + i] += einc[i];
+          h[((size_t)s * npts + ip) * 3 + i] += hinc[i];
+        }
+      }
+  }
+}
+
 /* Single-point access to the kernels for unit tests.  which: 1 = intK1,
  * 2 = intK2, 4 = intK4; res holds 3 (intK1) or 9 complex values. */
 void oracle_srcint(void *p, int d, int which, const double *r, int f, int tface, const double *k_ri, int near,

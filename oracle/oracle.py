@@ -66,6 +66,8 @@ def lib():
         L.oracle_static_integrals.argtypes = [C.c_void_p, C.c_int, dp, C.c_int, C.c_int, dp]
         L.oracle_face_geometry.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, dp, ip, dp, dp]
         L.oracle_tri_rule.argtypes = [C.c_char_p, ip, dp, dp]
+        L.oracle_scat_fields.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_int, C.c_void_p, C.c_int64,
+                                         C.c_void_p, C.c_int, C.c_int, dp, C.c_void_p, C.c_void_p]
         L.oracle_pi.restype = C.c_double
     return _LIB
 
@@ -192,6 +194,25 @@ class OracleProblem:
         out = np.zeros((ntheta, nphi), order="F")
         lib().oracle_rcs(self.h, d, omega, _dp(rr), x.ctypes.data, ntheta, nphi, _dp(out), nthreads)
         return out
+
+    def scat_fields(self, omega, ri, x, pts, srcs=None, d=0):
+        """scat_fields (nfields.f90:29-197) of domain d at pts[npts][3]; x[2N, nsrc]
+        (columns = sources).  With srcs the incident fields are added, as
+        field_plane (nfpost.f90:316-374) does in the exterior domain.
+        Returns (e, h), each [nsrc][npts][3] complex."""
+        x = np.asarray(x, dtype=np.complex128)
+        if x.ndim == 1:
+            x = x[:, None]
+        xs = np.ascontiguousarray(x.T)
+        nsrc = xs.shape[0]
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        e = np.zeros((nsrc, len(pts), 3), dtype=np.complex128)
+        h = np.zeros_like(e)
+        arr = (OSrc * max(1, nsrc))(*([make_src(s) for s in srcs] if srcs else [OSrc()]))
+        lib().oracle_scat_fields(self.h, d, omega, _dp(rr), nsrc, xs.ctypes.data, xs.shape[1], arr,
+                                 1 if srcs else 0, len(pts), _dp(pts), e.ctypes.data, h.ctypes.data)
+        return e, h
 
     def srcint(self, d, which, r, f, tface, k, near):
         r = np.ascontiguousarray(r, dtype=np.float64)

@@ -64,7 +64,7 @@ def test_unknown_command_is_reported_and_skipped(workdir):
 
 @pytest.mark.parametrize("line,msg", [
     ("symm 1 mxp", "symmetry group 'mxp'"),
-    ("nfpl 1 2 3", "outside the linear PMCHWT path"),
+    ("nfms 1 2 3", "outside the linear PMCHWT path"),
 ])
 def test_input_outside_the_path_stops(workdir, line, msg):
     r = run(line + "\nexit\n", workdir)
@@ -95,7 +95,8 @@ def half_ulp(token):
 @pytest.mark.gpu
 def test_fp64_command_script_matches_oracle(workdir):
     ref = np.load(GOLD)
-    script = setup_script(np.sqrt(W.EPS_AU)) + "solv\ncrst\nrcst 1 1 91 180\nexit\n"
+    script = setup_script(np.sqrt(W.EPS_AU)) + ("solv\ncrst\nrcst 1 1 91 180\n"
+                                                "nfpl 1 1 -100d-9 0 -100d-9 200d-9 0 0 0 0 200d-9 5 4 'xz'\nexit\n")
     r = run(script, workdir)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     crs, tok = read_en(workdir / "sphere-s1.crs")
@@ -108,3 +109,28 @@ def test_fp64_command_script_matches_oracle(workdir):
     sub = rcs[::5, ::9]
     tol = np.array([[half_ulp(t) for t in row[::9]] for row in tok[::5]])
     assert np.all(np.abs(sub - ref["rcs_sub"]) <= tol * 1.001 + 1e-9 * np.abs(ref["rcs_sub"]))
+    # nfpl: total field (scattered + incident) of domain 1 on a 5 x 4 grid in the
+    # xz plane, in the basis (x, z, x cross z = -y), against the library's
+    # scat_fields on the same FP64 solution
+    import mom_b200 as M
+    nodes, faces, ids, doms = W.sphere(3)
+    S = M.Solver(0)
+    try:
+        S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+        om, src = M.omega_of(600e-9), M.src_pw(0, 90, 0)
+        x = S.solve_wavelength(om, [1.0, np.sqrt(W.EPS_AU)], [src], M.FP64, 1e-12, 30)
+        a, b = np.meshgrid(np.arange(5), np.arange(4), indexing="ij")
+        pts = np.stack([-100e-9 + a.ravel() / 4 * 200e-9, 0 * a.ravel(), -100e-9 + b.ravel() / 3 * 200e-9], axis=1)
+        e, h = S.scat_fields(om, 1.0, pts, x=x, srcs=[src], dom=0)
+    finally:
+        S.close()
+    basis = np.array([[1, 0, 0], [0, 0, 1], [0, -1, 0]], dtype=float)
+    for name, f in (("e", e[0]), ("h", h[0])):
+        loc = f @ basis.T  # [npts][3] in the plane basis
+        for c, comp in enumerate("xyz"):
+            for part, fn in (("re", np.real), ("im", np.imag)):
+                vals, tok = read_en(workdir / ("sphere-wl1-s1-d1-xz-%s%s-%s.dat" % (name, comp, part)))
+                assert vals.shape == (4, 5)
+                want = fn(loc[:, c]).reshape(5, 4).T
+                tol = np.array([[half_ulp(t) for t in row] for row in tok])
+                assert np.all(np.abs(vals - want) <= tol * 1.001 + 1e-9 * np.abs(want).max())

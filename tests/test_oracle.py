@@ -179,3 +179,64 @@ def test_adjoint_fd_fixture_is_the_oracles():
     h = g["deps_step"]
     fd = (sig(eps + h) - sig(eps - h)) / (2 * h)
     assert np.allclose(fd, g["deps"][0], rtol=1e-8)
+
+
+# ---- near fields (nfields.f90 scat_fields), pinned by physics ----
+
+@pytest.fixture(scope="module")
+def s2_solution():
+    """The s=2 gold sphere (960 unknowns) solved by the oracle at 600 nm."""
+    from mom_b200 import workloads as W
+    nodes, faces, ids, doms = W.sphere(2)
+    P = O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+    om = O.omega_of(600e-9)
+    n_in = np.sqrt(W.EPS_AU)
+    src = dict(type="pw", theta=0.0, phi=90 * O.PI_F / 180, psi=0.0)
+    A = P.sysmat(om, np.array([1.0, n_in]))
+    x = O.solve(A, P.srcvec(om, 1.0, src)[:, None])[:, 0]
+    return P, om, n_in, src, x, np.asarray(nodes) * 1e-9, np.asarray(faces)
+
+
+def test_near_field_matches_far_field_at_one_metre(s2_solution):
+    """At r = 1 m the scattered |E|^2 equals the rcs routine's value (ffields.f90)
+    in the same direction, to O(size / r)."""
+    P, om, n_in, src, x, _, _ = s2_solution
+    rcs = P.rcs(om, 1.0, x, 19, 37)
+    for th, it in ((0.0, 0), (float(O.PI_F), 18)):
+        e, _ = P.scat_fields(om, 1.0, x, [[np.sin(th), 0.0, np.cos(th)]], d=0)
+        assert abs(np.sum(np.abs(e[0, 0]) ** 2) / rcs[it, 0] - 1) < 1e-6
+
+
+def test_extinction_theorem_and_null_field(s2_solution):
+    """Inside the particle the exterior representation cancels the incident field,
+    and outside it the interior representation vanishes (to the s=2 discretisation)."""
+    P, om, n_in, src, x, _, _ = s2_solution
+    inside = [[0, 0, 0], [10e-9, 5e-9, -8e-9]]
+    e, _ = P.scat_fields(om, 1.0, x, inside, srcs=[src], d=0)
+    einc, _ = P.scat_fields(om, 1.0, np.zeros_like(x), inside, srcs=[src], d=0)
+    assert np.abs(e).max() < 2e-2 * np.abs(einc).max()
+    outside = [[0, 0, 120e-9], [80e-9, 0, 0]]
+    e2, _ = P.scat_fields(om, n_in, x, outside, d=1)
+    es, _ = P.scat_fields(om, 1.0, x, outside, d=0)
+    assert np.abs(e2).max() < 5e-3 * np.abs(es).max()
+
+
+def test_normal_field_jump_at_the_surface(s2_solution):
+    """Just outside / inside a face centroid (0.01 edge lengths along the face
+    normal, the singular integrals in use) eps_out E_n^out = eps_in E_n^in and the
+    tangential H is continuous, to a few per cent."""
+    P, om, n_in, src, x, nodes, faces = s2_solution
+    eps_in = n_in ** 2
+    for fi in (0, 17, 100):
+        tri = nodes[faces[fi]]
+        cp = tri.mean(axis=0)
+        nn = np.cross(tri[1] - tri[0], tri[2] - tri[0])
+        nn /= np.linalg.norm(nn)
+        nn = nn if np.dot(nn, cp) > 0 else -nn
+        d = 0.01 * np.linalg.norm(tri[1] - tri[0])
+        eo, ho = P.scat_fields(om, 1.0, x, [cp + d * nn], srcs=[src], d=0)
+        ei, hi = P.scat_fields(om, n_in, x, [cp - d * nn], d=1)
+        ratio = np.dot(eo[0, 0], nn) / (eps_in * np.dot(ei[0, 0], nn))
+        assert abs(ratio - 1) < 0.05
+        tan = lambda v: v - np.dot(v, nn) * nn
+        assert np.linalg.norm(tan(ho[0, 0]) - tan(hi[0, 0])) < 0.06 * np.linalg.norm(tan(ho[0, 0]))
