@@ -370,6 +370,10 @@ def run_ours(args, rank, local_rank, world):
         line["sweep"] = bench_sweep(M, args.sweep_workers, local_rank)
         line["adjoint"] = bench_adjoint(M, local_rank)
         line["core_shell"] = bench_core_shell(M, local_rank)
+        try:
+            line["near_field"] = bench_nearfield(M, local_rank, with_cpu=not args.no_cpu)
+        except Exception as exc:  # a side measurement must not cost the bench line
+            line["near_field"] = {"error": repr(exc)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
         info = cpu_sample(args.subdiv, cores)
@@ -381,6 +385,53 @@ def run_ours(args, rank, local_rank, world):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def bench_nearfield(M, dev, n=101, with_cpu=True):
+    """Near fields (scat_fields + incident, the nfpl plane) of the cfg1 sphere
+    (s=3, FP64 solution at 600 nm): an n x n grid 200 nm wide in the xz plane
+    through the particle, exterior domain.  GPU time per plane through the C ABI
+    (host points in, host fields out); with with_cpu, the CPU baseline of this
+    row: the oracle on a sample of points on one host core, and the largest
+    relative difference on that sample."""
+    import numpy as np
+    from mom_b200 import workloads as W
+    nodes, faces, ids, doms = W.sphere(3)
+    S = M.Solver(dev)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    om = M.omega_of(WL)
+    src = [M.src_pw(0, 90, 0)]
+    x = S.solve_wavelength(om, [1.0, np.sqrt(EPS_IN)], src, M.FP64, 1e-12, 30)
+    a, b = np.meshgrid(np.linspace(-100e-9, 100e-9, n), np.linspace(-100e-9, 100e-9, n), indexing="ij")
+    pts = np.stack([a.ravel(), np.zeros(n * n), b.ravel()], axis=1)
+    S.scat_fields(om, 1.0, pts, x=x, srcs=src, dom=0)  # warm-up
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        e, h = S.scat_fields(om, 1.0, pts, x=x, srcs=src, dom=0)
+    gpu_s = (time.perf_counter() - t0) / reps
+    S.close()
+    F = len(faces)
+    flop = 1300.0 * n * n * F  # ~13 x 70 FLOP of quadrature + ~400 of contraction per point-face pair
+    out = {"workload": "nfpl plane %d x %d points (200 nm, xz) on the s=3 sphere, exterior domain, + incident" % (n, n),
+           "gpu_ms_per_plane": gpu_s * 1e3, "points_per_s": n * n / gpu_s,
+           "point_face_pairs_per_s": n * n * F / gpu_s,
+           "fp64_tflops_est": flop / gpu_s / 1e12,
+           "fp64_peak_note": "nominal FP64 SIMT 148 SM x 64 FMA x 2 x 1.965 GHz = 37 TFLOP/s; FLOP per pair estimated"}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        P = O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+        idx = np.linspace(0, n * n - 1, 16).astype(int)
+        t0 = time.perf_counter()
+        eo, ho = P.scat_fields(om, 1.0, x, pts[idx], srcs=src, d=0)
+        cpu_s = time.perf_counter() - t0
+        err = max(float(np.abs(e[0, idx] - eo[0]).max() / np.abs(eo[0]).max()),
+                  float(np.abs(h[0, idx] - ho[0]).max() / np.abs(ho[0]).max()))
+        out["cpu_baseline"] = {"value": len(idx) / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
+                               "sample": "16 of the plane's points"}
+        out["max_rel_diff_vs_oracle"] = err
+    return out
 
 
 def bench_sweep(M, workers, dev):
