@@ -134,3 +134,24 @@ def test_fp64_command_script_matches_oracle(workdir):
                 want = fn(loc[:, c]).reshape(5, 4).T
                 tol = np.array([[half_ulp(t) for t in row] for row in tok])
                 assert np.all(np.abs(vals - want) <= tol * 1.001 + 1e-9 * np.abs(want).max())
+
+
+def test_en15_3_output_format(tmp_path):
+    """write_data's EN15.3 fields (aux.f90:192-211): engineering notation, three
+    decimals, 15 columns; checked by compiling the interpreter's formatter alone."""
+    import shutil
+    if not shutil.which("g++"):
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "en.cpp"
+    src.write_text(
+        '#define main mom_main_unused\n#include "%s"\n#undef main\n'
+        'int main() { const double v[] = {6e-7, 0.0, -3.5e-16, 999.9996, 12345.6789, 1.0, 9.9999996e-10};\n'
+        '  for (double x : v) std::printf("[%%s]\\n", en15_3(x).c_str()); }\n'
+        % os.path.join(ROOT, "for90-mom2_b200", "host", "mom_main.cpp"))
+    exe = tmp_path / "en"
+    subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-o", str(exe), str(src),
+                    "-L" + os.path.join(ROOT, "for90-mom2_b200", "lib"), "-lmomgpu",
+                    "-Wl,-rpath," + os.path.join(ROOT, "for90-mom2_b200", "lib")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert out == ["[    600.000E-09]", "[      0.000E+00]", "[   -350.000E-18]", "[      1.000E+03]",
+                   "[     12.346E+03]", "[      1.000E+00]", "[      1.000E-09]"]
