@@ -33,7 +33,8 @@ def _nvcc() -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return (glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) +
+            glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def _stale(out: str, deps) -> bool:
