@@ -61,6 +61,69 @@ def icosphere(subdiv: int, radius: float = 1.0):
     return nodes, faces
 
 
+def octasphere(subdiv: int, radius: float = 1.0):
+    """(nodes, faces) of an outward-oriented sphere from the subdivided octahedron:
+    no face crosses a coordinate plane, so the mesh has the three mirror symmetries
+    x -> -x, y -> -y, z -> -z exactly (nodes on a plane stay on it)."""
+    v = [np.array(p, dtype=np.float64) for p in
+         ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))]
+    faces = [(0, 2, 4), (2, 1, 4), (1, 3, 4), (3, 0, 4), (2, 0, 5), (1, 2, 5), (3, 1, 5), (0, 3, 5)]
+    for _ in range(subdiv):
+        cache = {}
+        nf = []
+
+        def mid(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[key] = len(v) - 1
+            return cache[key]
+
+        for (a, b, c) in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    nodes = np.array(v) * radius
+    faces = np.array(faces, dtype=np.int64)
+    p1, p2, p3 = nodes[faces[:, 0]], nodes[faces[:, 1]], nodes[faces[:, 2]]
+    nrm = np.cross(p2 - p1, p3 - p1)
+    inward = np.einsum("ij,ij->i", nrm, (p1 + p2 + p3)) < 0
+    faces[inward] = faces[inward][:, ::-1]
+    return nodes, faces
+
+
+def symmetry_fragment(nodes, faces, planes):
+    """The part of a mirror-symmetric mesh on the positive side of each plane in
+    `planes` (0 = x, 1 = y, 2 = z): (nodes, faces, lines), where lines[plane] lists
+    the fragment's edges (node pairs) that lie on that plane, the boundary edges a
+    reference script marks with `sbnd <id> xplane` (yplane, zplane)."""
+    nodes = np.asarray(nodes, dtype=np.float64)
+    faces = np.asarray(faces)
+    keep = np.ones(len(faces), bool)
+    cen = nodes[faces].mean(axis=1)
+    for ax in planes:
+        keep &= cen[:, ax] > 0
+    sub = faces[keep]
+    used = np.unique(sub)
+    remap = -np.ones(len(nodes), np.int64)
+    remap[used] = np.arange(len(used))
+    fn = nodes[used]
+    ff = remap[sub]
+    lines = {}
+    scale = np.abs(fn).max()
+    for ax in planes:
+        on = np.abs(fn[:, ax]) <= 1e-12 * scale
+        pairs = set()
+        for f in ff:
+            for k in range(3):
+                a, b = int(f[k]), int(f[(k + 1) % 3])
+                if on[a] and on[b]:
+                    pairs.add((min(a, b), max(a, b)))
+        lines[ax] = sorted(pairs)
+    return fn, ff, lines
+
+
 def ellipsoid(subdiv: int, axes):
     nodes, faces = icosphere(subdiv, 1.0)
     return nodes * np.asarray(axes, dtype=np.float64)[None, :], faces

@@ -161,11 +161,30 @@ typedef struct {
   double avelen;
 } omesh;
 
+/* symmetry.f90:24-40 group_action: point action j (row-major here,
+ * j[3 i + k] = J(i, k)), its determinant, a special-action identifier,
+ * generator bits and the field actions ef(1:nga) (conjugated representation
+ * values). */
+#define O_MAXGA 32
+enum { O_GID_IDENTITY = 1, O_GID_MXP = 2, O_GID_MYP = 3, O_GID_MZP = 4, O_GID_RZ = 5 };
+/* mesh.f90:16-25 boundary types of edges */
+enum { O_BND_NONE = 1, O_BND_XPLANE = 2, O_BND_YPLANE = 3, O_BND_ZPLANE = 4, O_BND_RZ1 = 9, O_BND_RZ2 = 10 };
+typedef struct {
+  double j[9];
+  double detj;
+  int id, genbits;
+  double complex ef[O_MAXGA];
+} ogact;
+
 typedef struct {
   omesh master;
   int ndom;
   omesh *dom;
   oquad qd;
+  int nga;       /* group of the batch (read_symm); identity unless set */
+  ogact *ga;
+  int *mbnd;     /* [master nedges] edge boundary type (classify_edges) */
+  int **dbnd;    /* per domain [nedges], inherited from the master edge */
 } oproblem;
 
 static void *xcalloc(size_t n, size_t s) {
@@ -463,6 +482,22 @@ int oracle_problem_create(int nnodes, const double *nodes, int nfaces, const int
   if (submesh_edge_connectivity(ms, ndom, P->dom)) return -3;
   orient_basis(ms, P->dom);
   if (oracle_tri_rule(quad_name, &P->qd.nq, P->qd.w, &P->qd.nd[0][0])) return -4;
+  /* batch_defaults / read_symm with no groups: the identity group; no
+   * classified boundary edges */
+  P->ga = xcalloc(O_MAXGA, sizeof(ogact));
+  P->nga = 1;
+  P->ga[0].j[0] = P->ga[0].j[4] = P->ga[0].j[8] = 1.0;
+  P->ga[0].detj = 1.0;
+  P->ga[0].id = O_GID_IDENTITY;
+  P->ga[0].genbits = 1 << O_GID_IDENTITY;
+  P->ga[0].ef[0] = 1.0;
+  P->mbnd = xcalloc(ms->nedges, sizeof(int));
+  for (int e = 0; e < ms->nedges; e++) P->mbnd[e] = O_BND_NONE;
+  P->dbnd = xcalloc(ndom, sizeof(int *));
+  for (int d = 0; d < ndom; d++) {
+    P->dbnd[d] = xcalloc(P->dom[d].nedges, sizeof(int));
+    for (int e = 0; e < P->dom[d].nedges; e++) P->dbnd[d][e] = O_BND_NONE;
+  }
   *out = P;
   return 0;
 }
@@ -472,6 +507,11 @@ void oracle_problem_free(void *p) {
   if (!P) return;
   mesh_free(&P->master);
   for (int d = 0; d < P->ndom; d++) mesh_free(P->dom + d);
+  if (P->dbnd)
+    for (int d = 0; d < P->ndom; d++) free(P->dbnd[d]);
+  free(P->dbnd);
+  free(P->mbnd);
+  free(P->ga);
   free(P->dom);
   free(P);
 }
@@ -1269,6 +1309,429 @@ void oracle_scat_fields(void *p, int d, double omega, const double *ri_ri, int n
         }
       }
   }
+}
+
+/* ==== Symmetry groups (symmetry.f90, bc.f90; the nga > 1 parts of
+ * sysmat.f90, source.f90 and cs.f90), mirror planes only ==== */
+
+/* symmetry.f90:45-58 group_id, 60-103 group_mp */
+static void ga_identity(ogact *g) {
+  memset(g, 0, sizeof *g);
+  g->j[0] = g->j[4] = g->j[8] = 1.0;
+  g->detj = 1.0;
+  g->id = O_GID_IDENTITY;
+  g->genbits = 1 << O_GID_IDENTITY;
+  g->ef[0] = 1.0;
+}
+static void ga_mirror(int np, ogact *g /* [2] */) {
+  ga_identity(g);
+  g[0].ef[1] = 1.0;
+  memset(g + 1, 0, sizeof *g);
+  g[1].j[0] = g[1].j[4] = g[1].j[8] = 1.0;
+  g[1].j[4 * (np - 1)] = -1.0;
+  g[1].detj = -1.0;
+  g[1].ef[0] = 1.0;
+  g[1].ef[1] = -1.0;
+  g[1].id = np == 1 ? O_GID_MXP : np == 2 ? O_GID_MYP : O_GID_MZP;
+  g[1].genbits = 1 << g[1].id;
+}
+
+/* symmetry.f90:178-241 product_group: element k = n nb + m is a_n b_m;
+ * field actions multiply likewise. */
+static int ga_product(ogact *a, int na, const ogact *b, int nb) {
+  if (na * nb > O_MAXGA) return -1;
+  ogact *t = xcalloc((size_t)na * nb, sizeof(ogact));
+  for (int n = 0; n < na; n++)
+    for (int m = 0; m < nb; m++) {
+      ogact *g = t + n * nb + m;
+      for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) {
+          double v = 0;
+          for (int l = 0; l < 3; l++) v += a[n].j[3 * i + l] * b[m].j[3 * l + k];
+          g->j[3 * i + k] = v;
+        }
+      g->detj = a[n].detj * b[m].detj;
+      g->genbits = a[n].genbits | b[m].genbits;
+      g->id = 0;
+      if (a[n].id == O_GID_IDENTITY && b[m].id == O_GID_IDENTITY) g->id = O_GID_IDENTITY;
+      else if (a[n].id != 0 && a[n].id != O_GID_IDENTITY && b[m].id == O_GID_IDENTITY) g->id = a[n].id;
+      else if (b[m].id != 0 && b[m].id != O_GID_IDENTITY && a[n].id == O_GID_IDENTITY) g->id = b[m].id;
+      for (int n2 = 0; n2 < na; n2++)
+        for (int m2 = 0; m2 < nb; m2++) g->ef[n2 * nb + m2] = a[n].ef[n2] * b[m].ef[m2];
+    }
+  memcpy(a, t, sizeof(ogact) * (size_t)na * nb);
+  free(t);
+  return na * nb;
+}
+
+/* interface.f90:160-210 read_symm: the product of the named groups, starting
+ * from the identity.  Names: "id", "mxp", "myp", "mzp" (the rotation groups
+ * rN of the reference are not restated).  Returns the group order or < 0. */
+int oracle_problem_set_symmetry(void *p, int nnames, const char *const *names) {
+  oproblem *P = p;
+  ogact *g = P->ga;
+  ga_identity(g);
+  int n = 1;
+  for (int i = 0; i < nnames; i++) {
+    ogact two[2];
+    if (!strcmp(names[i], "id")) {
+      ga_identity(two);
+      n = ga_product(g, n, two, 1);
+    } else if (!strcmp(names[i], "mxp") || !strcmp(names[i], "myp") || !strcmp(names[i], "mzp")) {
+      ga_mirror(names[i][1] - 'w', two);
+      n = ga_product(g, n, two, 2);
+    } else {
+      return -1;
+    }
+    if (n < 0) return -2;
+  }
+  P->nga = n;
+  return n;
+}
+
+/* Group of the problem for tests: j [nga][9] (row-major), detj, ef [nga][nga]
+ * (ef[a * nga + r] = field action of element a in representation r). */
+void oracle_group_info(void *p, double *j, double *detj, cplx *ef) {
+  oproblem *P = p;
+  for (int a = 0; a < P->nga; a++) {
+    memcpy(j + 9 * a, P->ga[a].j, 9 * sizeof(double));
+    detj[a] = P->ga[a].detj;
+    for (int r = 0; r < P->nga; r++) ef[a * P->nga + r] = P->ga[a].ef[r];
+  }
+}
+
+/* mesh.f90:155-175 classify_edges: master edges whose end nodes match a
+ * line (0-based master node pair) get boundary type bnd; domain edges take
+ * the type of their master edge (mesh.f90:434). */
+int oracle_problem_classify_edges(void *p, int nlines, const int *line_nodes, int bnd) {
+  oproblem *P = p;
+  omesh *ms = &P->master;
+  int cnt = 0;
+  for (int e = 0; e < ms->nedges; e++)
+    for (int l = 0; l < nlines; l++)
+      if (cmp_pairs(ms->edge_node + 2 * e, line_nodes + 2 * l)) {
+        P->mbnd[e] = bnd;
+        cnt++;
+      }
+  for (int d = 0; d < P->ndom; d++)
+    for (int e = 0; e < P->dom[d].nedges; e++) P->dbnd[d][e] = P->mbnd[P->dom[d].edge_parent[e]];
+  return cnt;
+}
+
+static int has_bnd(const oproblem *P, int d, int bnd) {
+  for (int e = 0; e < P->dom[d].nedges; e++)
+    if (P->dbnd[d][e] == bnd) return 1;
+  return 0;
+}
+
+/* bc.f90:237-257 admissible_ga */
+static int admissible_ga(const oproblem *P, int d, const ogact *g) {
+  if (d == 0) return 1;
+  if ((g->genbits >> O_GID_MXP & 1) && !has_bnd(P, d, O_BND_XPLANE)) return 0;
+  if ((g->genbits >> O_GID_MYP & 1) && !has_bnd(P, d, O_BND_YPLANE)) return 0;
+  if ((g->genbits >> O_GID_MZP & 1) && !has_bnd(P, d, O_BND_ZPLANE)) return 0;
+  return 1;
+}
+
+/* bc.f90:28-117 edge_bc (mirror planes): for representation nr, id[k] = -1
+ * removes coefficient k (J: k < N, M: k >= N) when the field action of a
+ * mirror element on a boundary edge of its plane is not -1 (for M the action
+ * times det J).  Returns the number of removed coefficients. */
+int oracle_edge_bc(void *p, int nr, int *id, cplx *phase) {
+  oproblem *P = p;
+  int N = P->master.nedges, cnt = 0;
+  for (int k = 0; k < 2 * N; k++) {
+    id[k] = 0;
+    phase[k] = 1.0;
+  }
+  for (int k = 0; k < N; k++) {
+    int bnd = P->mbnd[k];
+    for (int n = 0; n < P->nga; n++) {
+      const ogact *g = P->ga + n;
+      cplx gae = g->ef[nr], gah = g->ef[nr] * g->detj;
+      if ((g->id == O_GID_MXP && bnd == O_BND_XPLANE) || (g->id == O_GID_MYP && bnd == O_BND_YPLANE) ||
+          (g->id == O_GID_MZP && bnd == O_BND_ZPLANE)) {
+        if (creal(-gae) < 0.99) id[k] = -1;
+        if (creal(-gah) < 0.99) id[k + N] = -1;
+      }
+    }
+  }
+  for (int k = 0; k < 2 * N; k++) cnt += id[k] == -1;
+  return cnt;
+}
+
+/* J^T r, J v (real) and J v (complex) */
+static void jt_vec(const double *j, const double *r, double *o) {
+  for (int i = 0; i < 3; i++) o[i] = j[i] * r[0] + j[3 + i] * r[1] + j[6 + i] * r[2];
+}
+static void j_cvec(const double *j, const cplx *v, cplx *o) {
+  for (int i = 0; i < 3; i++) o[i] = j[3 * i] * v[0] + j[3 * i + 1] * v[1] + j[3 * i + 2] * v[2];
+}
+
+/* srcint.f90 with a group action g (orthogonal J): the source face mapped by
+ * J seen from r equals the face itself seen from J^T r, so
+ *   intK1_g(r) = intK1(J^T r),  intK2_g(r) = J intK2(J^T r),
+ *   intK4_g(r) = det J  J intK4(J^T r)      ((J a) x (J b) = det J  J (a x b)),
+ * the singular parts included (srcint.f90:97-117, 208-223, 418-447). */
+static void intK1_g(const double *r, int f, const omesh *m, cplx k, const ogact *g, int near, const oquad *qd,
+                    cplx *res) {
+  if (g->id == O_GID_IDENTITY) {
+    intK1(r, f, m, k, near, qd, res);
+    return;
+  }
+  double rt[3];
+  jt_vec(g->j, r, rt);
+  intK1(rt, f, m, k, near, qd, res);
+}
+static void intK2_g(const double *r, int f, const omesh *m, cplx k, const ogact *g, int near, const oquad *qd,
+                    cplx *res) {
+  if (g->id == O_GID_IDENTITY) {
+    intK2(r, f, m, k, near, qd, res);
+    return;
+  }
+  double rt[3];
+  cplx t[9];
+  jt_vec(g->j, r, rt);
+  intK2(rt, f, m, k, near, qd, t);
+  for (int e = 0; e < 3; e++) j_cvec(g->j, t + 3 * e, res + 3 * e);
+}
+static void intK4_g(const double *r, int f, const omesh *m, cplx k, const ogact *g, int tface, int near,
+                    const oquad *qd, cplx *res) {
+  if (g->id == O_GID_IDENTITY) { /* the self-face shortcut holds for the identity only */
+    intK4(r, f, m, k, tface, near, qd, res);
+    return;
+  }
+  double rt[3];
+  cplx t[9];
+  jt_vec(g->j, r, rt);
+  intK4(rt, f, m, k, -1, near, qd, t);
+  for (int e = 0; e < 3; e++) {
+    j_cvec(g->j, t + 3 * e, res + 3 * e);
+    for (int i = 0; i < 3; i++) res[3 * e + i] *= g->detj;
+  }
+}
+
+/* sysmat.f90:233-260 near_faces: |cp_m - J cp_n| < 3 avelen */
+static int near_faces_g(const omesh *m, int n, int mm, const ogact *g) {
+  double threshold = m->avelen * 3, jc[3], d[3];
+  const double *c = m->face_cp + 3 * n;
+  for (int i = 0; i < 3; i++) jc[i] = g->j[3 * i] * c[0] + g->j[3 * i + 1] * c[1] + g->j[3 * i + 2] * c[2];
+  for (int i = 0; i < 3; i++) d[i] = m->face_cp[3 * mm + i] - jc[i];
+  return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < threshold * threshold;
+}
+
+/* compute_op for one group action (sysmat.f90:272-519 with ga) */
+static void compute_op_g(int op, double omega, cplx ri, const omesh *m, const oquad *qd, const ogact *g, cplx *M) {
+  int Nd = m->nedges, F = m->nfaces, nq = qd->nq;
+  memset(M, 0, sizeof(cplx) * (size_t)Nd * Nd);
+  cplx k = ri * omega / O_C0;
+  cplx c1 = -I * omega * O_MU0;
+  cplx c2 = -1.0 / (I * omega * O_EPS0 * (ri * ri));
+  size_t per = (op == 1) ? 3 : 9;
+  cplx *intaux = malloc(sizeof(cplx) * per * nq * (size_t)F);
+  if (!intaux) abort();
+  for (int mm = 0; mm < F; mm++) {
+    double qpm[13 * 3], fmv[3][13][3], fmDiv[3];
+    quad_tri_points(qd, m, mm, qpm);
+    double Am = m->face_area[mm];
+    for (int pq = 0; pq < 3; pq++) {
+      for (int r = 0; r < nq; r++) rwg(m, qpm + 3 * r, mm, pq, fmv[pq][r]);
+      fmDiv[pq] = rwgDiv(m, mm, pq);
+    }
+#pragma omp parallel for schedule(static)
+    for (int n = 0; n < F; n++) {
+      int near = near_faces_g(m, n, mm, g);
+      for (int r = 0; r < nq; r++) {
+        cplx *dst = intaux + ((size_t)n * nq + r) * per;
+        if (op == 0) intK2_g(qpm + 3 * r, n, m, k, g, near, qd, dst);
+        else if (op == 1) intK1_g(qpm + 3 * r, n, m, k, g, near, qd, dst);
+        else intK4_g(qpm + 3 * r, n, m, k, g, mm, near, qd, dst);
+      }
+    }
+    for (int n = 0; n < F; n++)
+      for (int pp = 0; pp < 3; pp++)
+        for (int q = 0; q < 3; q++) {
+          cplx int1 = 0;
+          for (int r = 0; r < nq; r++) {
+            const cplx *a = intaux + ((size_t)n * nq + r) * per;
+            if (op == 1) int1 += qd->w[r] * a[q];
+            else int1 += qd->w[r] * (fmv[pp][r][0] * a[3 * q] + fmv[pp][r][1] * a[3 * q + 1] + fmv[pp][r][2] * a[3 * q + 2]);
+          }
+          int1 = (op == 1) ? int1 * Am * fmDiv[pp] : int1 * Am;
+          int i1 = m->face_edge[3 * mm + pp], i2 = m->face_edge[3 * n + q];
+          M[i1 + (size_t)i2 * Nd] += (op == 0) ? c1 * int1 : (op == 1) ? c2 * int1 : int1;
+        }
+  }
+  free(intaux);
+}
+
+/* sysmat.f90:18-105 sysmat_pmchwt with the problem's group: one 2N x 2N
+ * matrix per representation, A[nf] at A + nf (2N)^2 (column-major). */
+void oracle_sysmat_sym(void *p, double omega, const double *ri_ri, cplx *A, int nthreads) {
+  oproblem *P = p;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int N = P->master.nedges, nga = P->nga;
+  const size_t n2 = 2 * (size_t)N;
+  memset(A, 0, sizeof(cplx) * n2 * n2 * nga);
+  for (int d = 0; d < P->ndom; d++) {
+    omesh *m = P->dom + d;
+    cplx ri = ri_ri[2 * d] + I * ri_ri[2 * d + 1];
+    cplx Zsi = (ri * ri) / (O_ETA0 * O_ETA0);
+    const int Nd = m->nedges, *ind = m->edge_parent;
+    cplx *M = malloc(sizeof(cplx) * (size_t)Nd * Nd);
+    if (!M) abort();
+    for (int ns = 0; ns < nga; ns++) {
+      const ogact *g = P->ga + ns;
+      if (!admissible_ga(P, d, g)) continue;
+      for (int op = 0; op < 3; op++) {
+        compute_op_g(op, omega, ri, m, &P->qd, g, M);
+        for (int nf = 0; nf < nga; nf++) {
+          cplx gae = g->ef[nf], *Af = A + (size_t)nf * n2 * n2;
+          for (int jj = 0; jj < Nd; jj++)
+            for (int i = 0; i < Nd; i++) {
+              cplx v = gae * M[i + (size_t)jj * Nd];
+              size_t r = ind[i], c = ind[jj];
+              if (op < 2) {
+                Af[r + c * n2] += v;
+                Af[(r + N) + (c + N) * n2] += g->detj * Zsi * v;
+              } else {
+                Af[(r + N) + c * n2] += v;
+                Af[r + (c + N) * n2] -= g->detj * v;
+              }
+            }
+        }
+      }
+    }
+    free(M);
+  }
+}
+
+/* source.f90:250-315 src_field_frags: the source at J^T pt for each element,
+ * projected on the representations; ef, hf [nga][3]. */
+static void src_field_frags(const oproblem *P, const osrc *s, double omega, cplx ri, const double *pt, cplx *ef,
+                            cplx *hf) {
+  const int nga = P->nga;
+  for (int i = 0; i < 3 * nga; i++) ef[i] = hf[i] = 0;
+  for (int na = 0; na < nga; na++) {
+    const ogact *g = P->ga + na;
+    double pp[3];
+    cplx e[3], h[3], je[3], jh[3];
+    jt_vec(g->j, pt, pp);
+    src_fields(s, omega, ri, pp, e, h);
+    j_cvec(g->j, e, je);
+    j_cvec(g->j, h, jh);
+    for (int nr = 0; nr < nga; nr++)
+      for (int i = 0; i < 3; i++) {
+        ef[3 * nr + i] += je[i] * g->ef[nr];
+        hf[3 * nr + i] += jh[i] * g->ef[nr] * g->detj;
+      }
+  }
+  for (int i = 0; i < 3 * nga; i++) {
+    ef[i] /= nga;
+    hf[i] /= nga;
+  }
+}
+
+/* source.f90:136-247 srcvec with the group: q[nr] (2N each) on domain 0. */
+void oracle_srcvec_sym(void *p, double omega, const double *ri_ri, const osrc *src, cplx *q) {
+  oproblem *P = p;
+  const omesh *m = P->dom;
+  const oquad *qd = &P->qd;
+  const int N = P->master.nedges, nq = qd->nq, nga = P->nga;
+  cplx ri = ri_ri[0] + I * ri_ri[1];
+  for (size_t i = 0; i < 2 * (size_t)N * nga; i++) q[i] = 0;
+  cplx *ef = xcalloc((size_t)3 * nga * nq, sizeof(cplx)), *hf = xcalloc((size_t)3 * nga * nq, sizeof(cplx));
+  for (int f = 0; f < m->nfaces; f++) {
+    double qpm[13 * 3];
+    quad_tri_points(qd, m, f, qpm);
+    double Am = m->face_area[f];
+    for (int r = 0; r < nq; r++)
+      src_field_frags(P, src, omega, ri, qpm + 3 * r, ef + (size_t)3 * nga * r, hf + (size_t)3 * nga * r);
+    for (int pp = 0; pp < 3; pp++) {
+      int idx = m->edge_parent[m->face_edge[3 * f + pp]];
+      for (int nr = 0; nr < nga; nr++) {
+        cplx Ie = 0, Ih = 0;
+        for (int r = 0; r < nq; r++) {
+          double fm[3];
+          rwg(m, qpm + 3 * r, f, pp, fm);
+          const cplx *e = ef + (size_t)3 * nga * r + 3 * nr, *h = hf + (size_t)3 * nga * r + 3 * nr;
+          Ie += qd->w[r] * (fm[0] * e[0] + fm[1] * e[1] + fm[2] * e[2]);
+          Ih += qd->w[r] * (fm[0] * h[0] + fm[1] * h[1] + fm[2] * h[2]);
+        }
+        q[(size_t)nr * 2 * N + idx] += Ie * Am;
+        q[(size_t)nr * 2 * N + idx + N] += Ih * Am;
+      }
+    }
+  }
+  free(ef);
+  free(hf);
+}
+
+/* cs.f90:14-104 cs_prtsrf with the group, over domain d's mesh: x holds the
+ * solution of every representation for one source, x[nf] at x + nf 2N. */
+void oracle_cs_sym(void *p, int d, double omega, const double *ri_ri, const cplx *x, const osrc *src,
+                   double *csca, double *cabs) {
+  oproblem *P = p;
+  const omesh *m = P->dom + d;
+  const oquad *qd = &P->qd;
+  const int N = P->master.nedges, nq = qd->nq, nga = P->nga;
+  cplx ri = ri_ri[0] + I * ri_ri[1];
+  double c = 2.0 / (O_EPS0 * O_C0 * creal(ri));
+  double sca = 0, abs_ = 0;
+  for (int f = 0; f < m->nfaces; f++) {
+    double qpn[13 * 3];
+    quad_tri_points(qd, m, f, qpn);
+    double An = m->face_area[f];
+    const double *n0 = m->face_n + 3 * f;
+    double int1 = 0, int2 = 0;
+    for (int t = 0; t < nq; t++) {
+      for (int ns = 0; ns < nga; ns++) {
+        const ogact *g = P->ga + ns;
+        cplx Et[3] = {0, 0, 0}, Ht[3] = {0, 0, 0};
+        double nor[3];
+        for (int i = 0; i < 3; i++) nor[i] = g->j[3 * i] * n0[0] + g->j[3 * i + 1] * n0[1] + g->j[3 * i + 2] * n0[2];
+        for (int nf = 0; nf < nga; nf++) {
+          cplx gae = g->ef[nf];
+          for (int pp = 0; pp < 3; pp++) {
+            double fr[3], fn0[3], fn[3];
+            rwg(m, qpn + 3 * t, f, pp, fr);
+            crossr(n0, fr, fn0);
+            for (int i = 0; i < 3; i++) fn[i] = g->j[3 * i] * fn0[0] + g->j[3 * i + 1] * fn0[1] + g->j[3 * i + 2] * fn0[2];
+            int idx = m->edge_parent[m->face_edge[3 * f + pp]];
+            cplx xj = x[(size_t)nf * 2 * N + idx], xm = x[(size_t)nf * 2 * N + idx + N];
+            for (int i = 0; i < 3; i++) {
+              Ht[i] -= xj * fn[i] * gae * g->detj;
+              Et[i] += xm * fn[i] * gae;
+            }
+          }
+        }
+        double pt[3];
+        for (int i = 0; i < 3; i++)
+          pt[i] = g->j[3 * i] * qpn[3 * t] + g->j[3 * i + 1] * qpn[3 * t + 1] + g->j[3 * i + 2] * qpn[3 * t + 2];
+        cplx einc[3], hinc[3], norc[3] = {nor[0], nor[1], nor[2]}, t1[3], Eti[3], Hti[3], Ets[3], Hts[3];
+        src_fields(src, omega, ri, pt, einc, hinc);
+        crossc(norc, hinc, t1);
+        crossc(t1, norc, Hti);
+        crossc(norc, einc, t1);
+        crossc(t1, norc, Eti);
+        for (int i = 0; i < 3; i++) {
+          Hts[i] = Ht[i] - Hti[i];
+          Ets[i] = Et[i] - Eti[i];
+        }
+        cplx ch[3], cx[3];
+        cplx Hc[3] = {conj(Ht[0]), conj(Ht[1]), conj(Ht[2])};
+        crossc(Et, Hc, ch);
+        int1 += qd->w[t] * 0.5 * creal(ch[0] * nor[0] + ch[1] * nor[1] + ch[2] * nor[2]);
+        cplx Hsc[3] = {conj(Hts[0]), conj(Hts[1]), conj(Hts[2])};
+        crossc(Ets, Hsc, cx);
+        int2 += qd->w[t] * 0.5 * creal(cx[0] * nor[0] + cx[1] * nor[1] + cx[2] * nor[2]);
+      }
+    }
+    abs_ += int1 * An;
+    sca += int2 * An;
+  }
+  *cabs = -c * abs_;
+  *csca = c * sca;
 }
 
 /* Single-point access to the kernels for unit tests.  which: 1 = intK1,

@@ -66,6 +66,13 @@ def lib():
         L.oracle_static_integrals.argtypes = [C.c_void_p, C.c_int, dp, C.c_int, C.c_int, dp]
         L.oracle_face_geometry.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, dp, ip, dp, dp]
         L.oracle_tri_rule.argtypes = [C.c_char_p, ip, dp, dp]
+        L.oracle_problem_set_symmetry.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_char_p)]
+        L.oracle_group_info.argtypes = [C.c_void_p, dp, dp, C.c_void_p]
+        L.oracle_problem_classify_edges.argtypes = [C.c_void_p, C.c_int, ip, C.c_int]
+        L.oracle_edge_bc.argtypes = [C.c_void_p, C.c_int, ip, C.c_void_p]
+        L.oracle_sysmat_sym.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_int]
+        L.oracle_srcvec_sym.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_void_p]
+        L.oracle_cs_sym.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p, dp, dp]
         L.oracle_scat_fields.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_int, C.c_void_p, C.c_int64,
                                          C.c_void_p, C.c_int, C.c_int, dp, C.c_void_p, C.c_void_p]
         L.oracle_pi.restype = C.c_double
@@ -194,6 +201,84 @@ class OracleProblem:
         out = np.zeros((ntheta, nphi), order="F")
         lib().oracle_rcs(self.h, d, omega, _dp(rr), x.ctypes.data, ntheta, nphi, _dp(out), nthreads)
         return out
+
+    # ---- symmetry groups (read_symm, sbnd; mirror planes) ----
+    BND = {"xplane": 2, "yplane": 3, "zplane": 4}
+
+    def set_symmetry(self, names):
+        """read_symm (interface.f90:160-210): product of the named groups ("id", "mxp",
+        "myp", "mzp"); returns the group order."""
+        arr = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+        n = lib().oracle_problem_set_symmetry(self.h, len(names), arr)
+        if n < 0:
+            raise ValueError("unsupported symmetry group %r" % (names,))
+        self.nga = n
+        return n
+
+    def group_info(self):
+        n = getattr(self, "nga", 1)
+        j = np.zeros((n, 9))
+        detj = np.zeros(n)
+        ef = np.zeros((n, n), dtype=np.complex128)
+        lib().oracle_group_info(self.h, _dp(j), _dp(detj), ef.ctypes.data)
+        return j.reshape(n, 3, 3), detj, ef
+
+    def classify_edges(self, lines, bnd):
+        """sbnd / classify_edges (mesh.f90:155-175): lines = master node pairs (0-based)."""
+        ln = np.ascontiguousarray(np.asarray(lines, dtype=np.int32).reshape(-1, 2))
+        return lib().oracle_problem_classify_edges(self.h, len(ln), _ip(ln), self.BND.get(bnd, bnd))
+
+    def edge_bc(self, nr):
+        idv = np.zeros(2 * self.N, dtype=np.int32)
+        ph = np.zeros(2 * self.N, dtype=np.complex128)
+        lib().oracle_edge_bc(self.h, nr, _ip(idv), ph.ctypes.data)
+        return idv, ph
+
+    def sysmat_sym(self, omega, ri, nthreads=0):
+        """sysmat_pmchwt with the group: A[nga][2N][2N]."""
+        rr = np.array([[complex(v).real, complex(v).imag] for v in ri]).ravel()
+        n = getattr(self, "nga", 1)
+        A = np.zeros((n, 2 * self.N, 2 * self.N), dtype=np.complex128)  # [nf] column-major blocks
+        lib().oracle_sysmat_sym(self.h, omega, _dp(rr), A.ctypes.data, nthreads)
+        return np.ascontiguousarray(A.transpose(0, 2, 1))
+
+    def srcvec_sym(self, omega, ri, src):
+        n = getattr(self, "nga", 1)
+        q = np.zeros((n, 2 * self.N), dtype=np.complex128)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        s = make_src(src)
+        lib().oracle_srcvec_sym(self.h, omega, _dp(rr), C.byref(s), q.ctypes.data)
+        return q
+
+    def solve_sym(self, A, q):
+        """solve_systems (solver.f90:325-357): per representation the boundary
+        conditions of edge_bc (bc.f90:28-117), reduce_system, solve, expand_solution."""
+        x = np.zeros_like(q)
+        for r in range(A.shape[0]):
+            idv, ph = self.edge_bc(r)
+            Ar, br = A[r].copy(), q[r][:, None].copy()
+            for n in np.nonzero(idv > 0)[0]:  # resolve_system_dependencies (coupled edges)
+                Ar[:, n] += Ar[:, idv[n] - 1] * ph[n]
+            for n in np.nonzero(idv > 0)[0]:
+                Ar[n, :] += Ar[idv[n] - 1, :] * np.conj(ph[n])
+                br[n, :] += br[idv[n] - 1, :] * np.conj(ph[n])
+            keep = np.nonzero(idv != -1)[0]
+            xr = solve(Ar[np.ix_(keep, keep)], br[keep])[:, 0]
+            full = np.zeros(2 * self.N, dtype=np.complex128)
+            full[keep] = xr
+            for n in np.nonzero(idv > 0)[0]:
+                full[idv[n] - 1] = full[n] * ph[n]
+            x[r] = full
+        return x
+
+    def cs_sym(self, omega, ri, x, src, d=0):
+        """cs_prtsrf with the group: x[nga][2N] for one source; (csca, cabs)."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        rr = np.array([complex(ri).real, complex(ri).imag])
+        s = make_src(src)
+        a, b = C.c_double(), C.c_double()
+        lib().oracle_cs_sym(self.h, d, omega, _dp(rr), x.ctypes.data, C.byref(s), C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def scat_fields(self, omega, ri, x, pts, srcs=None, d=0):
         """scat_fields (nfields.f90:29-197) of domain d at pts[npts][3]; x[2N, nsrc]

@@ -240,3 +240,63 @@ def test_normal_field_jump_at_the_surface(s2_solution):
         assert abs(ratio - 1) < 0.05
         tan = lambda v: v - np.dot(v, nn) * nn
         assert np.linalg.norm(tan(ho[0, 0]) - tan(hi[0, 0])) < 0.06 * np.linalg.norm(tan(ho[0, 0]))
+
+
+# ---- symmetry groups (read_symm, sbnd, bc.f90), mirror planes ----
+
+def _octa(s):
+    nodes, faces = meshgen.octasphere(s, 50.0)
+    return nodes, faces
+
+
+@pytest.mark.parametrize("s,tol", [(1, 1e-12), (2, 1e-8)])
+def test_symmetry_fragments_reproduce_the_full_sphere(s, tol):
+    """The half, quarter and eighth of a mirror-symmetric sphere, solved per
+    representation with the mirror groups and the symmetry-plane boundary
+    conditions, give the cross sections of the full sphere (the same
+    discretisation; at s=2 the near-pair threshold, 3 average edge lengths of the
+    fragment's own mesh, differs slightly from the full mesh's)."""
+    nodes, faces = _octa(s)
+    om = O.omega_of(600e-9)
+    n_in = np.sqrt(complex(-9, 1.3))
+    srcs = [dict(type="pw", theta=0.3, phi=0.7, psi=0.4), dict(type="pw_elliptic", theta=1.1, phi=-0.4, phase=1j)]
+    P = O.OracleProblem(nodes, faces, np.ones(len(faces), int), 1e-9, [[1], [-1]])
+    A = P.sysmat(om, np.array([1.0, n_in]))
+    ref = []
+    for src in srcs:
+        x = O.solve(A, P.srcvec(om, 1.0, src)[:, None])[:, 0]
+        ref.append(P.cs(om, 1.0, x, src))
+    for planes, names in (([0], ["mxp"]), ([0, 1], ["mxp", "myp"]), ([0, 1, 2], ["mxp", "myp", "mzp"])):
+        fn, ff, lines = meshgen.symmetry_fragment(nodes, faces, planes)
+        Q = O.OracleProblem(fn, ff, np.ones(len(ff), int), 1e-9, [[1], [-1]])
+        assert Q.set_symmetry(names) == 2 ** len(planes)
+        for ax in planes:
+            assert Q.classify_edges(lines[ax], ["xplane", "yplane", "zplane"][ax]) == len(lines[ax])
+        As = Q.sysmat_sym(om, [1.0, n_in])
+        for src, (csca, cabs) in zip(srcs, ref):
+            xs = Q.solve_sym(As, Q.srcvec_sym(om, 1.0, src))
+            a, b = Q.cs_sym(om, 1.0, xs, src)
+            assert abs(a / csca - 1) < tol and abs(b / cabs - 1) < tol
+
+
+def test_mirror_group_structure_and_boundary_conditions():
+    """symmetry.f90 product_group: orthogonal characters, det J = +-1; bc.f90
+    edge_bc removes, per representation, J on the plane edges where the mirror's
+    field action is +1 and M where its action times det J is +1."""
+    nodes, faces = _octa(1)
+    fn, ff, lines = meshgen.symmetry_fragment(nodes, faces, [0, 1])
+    Q = O.OracleProblem(fn, ff, np.ones(len(ff), int), 1e-9, [[1], [-1]])
+    n = Q.set_symmetry(["mxp", "myp"])
+    j, detj, ef = Q.group_info()
+    assert n == 4 and np.allclose(np.abs(detj), 1)
+    assert np.allclose(ef.conj().T @ ef, n * np.eye(n))
+    for a in range(n):
+        assert np.allclose(j[a] @ j[a].T, np.eye(3)) and np.isclose(np.linalg.det(j[a]), detj[a])
+    Q.classify_edges(lines[0], "xplane")
+    Q.classify_edges(lines[1], "yplane")
+    N = Q.N
+    for r in range(n):
+        idv, _ = Q.edge_bc(r)
+        # a plane edge loses exactly one of J, M in each representation
+        assert np.count_nonzero(idv == -1) == len(lines[0]) + len(lines[1])
+        assert np.all(idv[:N][idv[N:] == -1] == 0)
