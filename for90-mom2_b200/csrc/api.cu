@@ -800,6 +800,27 @@ int mom_gpu_scat_fields(mom_ctx *c, int32_t dom, double omega, const double *ri,
   return MOM_OK;
 }
 
+int mom_gpu_set_wait_limits(mom_ctx *c, int64_t panel_polls, int64_t gemm_polls, int64_t solve_polls) {
+  if (!c || panel_polls < 0 || gemm_polls < 0 || solve_polls < 0) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  c->wait_limit[0] = panel_polls;
+  c->wait_limit[1] = gemm_polls;
+  c->wait_limit[2] = solve_polls;
+  return MOM_OK;
+}
+
+int mom_gpu_set_matrix(mom_ctx *c, int32_t precision, const double *A_host, int64_t lda) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before the matrix");
+  MOM_TRY(check_prec(c, precision));
+  if (!A_host || lda < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "invalid matrix or lda < 2N");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  if (precision == MOM_PREC_MIXED) MOM_TRY(ensure_a32(c));
+  MOM_TRY(load_matrix(c, A_host, lda, precision));
+  return MOM_OK;
+}
+
 int mom_gpu_device_matrix(mom_ctx *c, void **A_dev, int64_t *lda) {
   if (!c || !A_dev || !lda) return MOM_ERR_ARG;
   *A_dev = c->A;

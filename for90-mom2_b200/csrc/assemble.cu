@@ -867,6 +867,28 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
   return MOM_OK;
 }
 
+// A caller's 2N x 2N matrix (host, column-major, lda) in place of an
+// assembled one: the same padding and FP32 copy as assemble().
+int load_matrix(Ctx *c, const double *A_host, int64_t ldh, int precision) {
+  const int64_t n = c->n, lda = c->lda, n2 = 2 * (int64_t)c->N;
+  MOM_CUDA(c, cudaMemsetAsync(c->A, 0, sizeof(double2) * (size_t)lda * n, c->stream));
+  MOM_CUDA(c, cudaMemcpy2DAsync(c->A, sizeof(double2) * lda, A_host, sizeof(double2) * ldh, sizeof(double2) * n2, n2,
+                                cudaMemcpyHostToDevice, c->stream));
+  if (n > n2) {
+    pad_identity<<<(unsigned)((n - n2 + 127) / 128), 128, 0, c->stream>>>(c->A, lda, n2, n);
+    c->launches++;
+  }
+  if (precision == MOM_PREC_MIXED) {
+    convert_to_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, (int64_t)lda * n);
+    c->launches++;
+  }
+  MOM_CUDA(c, cudaGetLastError());
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->assembled = 1;
+  c->factored = -1;
+  return MOM_OK;
+}
+
 #include "adjoint_impl.cuh"
 #include "nfields_impl.cuh"
 

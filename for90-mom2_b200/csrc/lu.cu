@@ -39,7 +39,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 
 constexpr int kPanelThreads = 512;
-constexpr long long kSpinLimit = 1LL << 26;  // bounded barrier wait (a few seconds)
+constexpr long long kSpinLimit = 1LL << 26;  // default bound of a barrier wait (a few seconds)
 
 struct PanelArgs {
   void *A;
@@ -48,6 +48,7 @@ struct PanelArgs {
   int *ipiv;
   int *info;      // first zero pivot (1-based), 0 if none
   int *timeout;   // set when a barrier wait ran out
+  long long spin; // polls before a wait is declared timed out
   unsigned long long *rec;  // [2][P] candidate records, zeroed before launch
   double2 *cand_data;       // [2][P][nb]
   double2 *col_data;        // [2][nb]
@@ -195,11 +196,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
           pf_key = rk;
         }
         if (done) break;
-        if ((++it & 255) == 0) {
+        if ((++it & 255) == 0 || it > a.spin) {
           int stop = 0;
           if (lane == 0) {
             if (*(volatile int *)a.timeout) stop = 1;
-            else if (it > kSpinLimit) {
+            else if (it > a.spin) {
               atomicExch(a.timeout, 1);
               stop = 1;
             }
@@ -215,20 +216,23 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         const unsigned long long gkey = warp_max_key(bw >= 0 ? (best & ~0xffull) : 0ull);
         const int gw = __ffs(__ballot_sync(0xffffffffu, bw >= 0 && (best & ~0xffull) == gkey)) - 1;
         const int gcta = gw < 0 ? 0 : __shfl_sync(0xffffffffu, bw, gw);
-        const int gr = (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
+        // no candidate at all (every entry of the column NaN): no interchange,
+        // reported as a failed pivot, so ipiv stays within the panel's rows
+        const bool none = gkey == 0ull;
+        const int gr = none ? (int)col : (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
         const double2 *pdat = a.cand_data + ((size_t)par * a.P + gcta) * nb;
         const double2 *cdat = a.col_data + (size_t)par * nb;
         const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
         const bool own_c = col >= row0 && col < row0 + nrow;
         const bool have = pf_key == gkey;  // the final best was prefetched
         for (int j = lane; j < nb; j += 32) {
-          const double2 pv = have ? (j < 32 ? pf0 : pf1) : __ldcg(pdat + j);
+          const double2 pv = none ? __ldcg(cdat + j) : have ? (j < 32 ? pf0 : pf1) : __ldcg(pdat + j);
           const double2 cvv = own_p ? __ldcg(cdat + j) : make_double2(0, 0);
           s_prow_data[j] = pv;
           if (own_p) slab[j * rpc + (gr - (int)row0)] = cvv;  // row prow <- old row col
           if (own_c) slab[j * rpc + (int)(col - row0)] = pv;  // row col  <- pivot row
           if (j == c) {
-            const double pa = pv.x * pv.x + pv.y * pv.y;
+            const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
             s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
             if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
           }
@@ -392,17 +396,19 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
       const unsigned long long gkey = warp_max_key(k);
       const int gw = __ffs(__ballot_sync(0xffffffffu, lane < P && k == gkey)) - 1;
       const int gsrc = gw < 0 ? 0 : gw;
-      const int gr = (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
+      // no candidate (every entry of the column NaN): no interchange, failed pivot
+      const bool none = gkey == 0ull;
+      const int gr = none ? (int)col : (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
       const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
       const bool own_c = col >= row0 && col < row0 + nrow;
       const double2 *prow = recv_row + ((size_t)par * P + gsrc) * nb, *crow = recv_col + (size_t)par * nb;
       for (int j = lane; j < nb; j += 32) {
-        const double2 pv = prow[j];
+        const double2 pv = none ? crow[j] : prow[j];
         s_prow_data[j] = pv;
         if (own_p) slab[j * rpc + (gr - (int)row0)] = crow[j];  // row prow <- old row col
         if (own_c) slab[j * rpc + (int)(col - row0)] = pv;      // row col  <- pivot row
         if (j == c) {
-          const double pa = pv.x * pv.x + pv.y * pv.y;
+          const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
           s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
           if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
         }
@@ -733,6 +739,7 @@ struct TrsvArgs {
                        // blocks of the forward pass are published in Y, of the backward pass in Z
                        // (both zeroed before the launch; published words carry a mark bit)
   int *timeout;
+  long long spin;  // polls before a wait is declared timed out
   int direct;  // 1: factor tiles do not fit in shared memory; read them from global memory
   int stages;  // prefetch stages (1 or 2) of factor tile + diagonal-block inverse
 };
@@ -1012,11 +1019,11 @@ __global__ void __launch_bounds__(256, 1) trsv_flow_kernel(TrsvArgs a) {
           }
         }
         if (__syncthreads_and(ok)) break;
-        if ((++it & 255) == 0) {
+        if ((++it & 255) == 0 || it > a.spin) {
           if (threadIdx.x == 0) {
             int go = 1;
             if (*(volatile int *)a.timeout) go = 0;
-            else if (it > kSpinLimit) {
+            else if (it > a.spin) {
               atomicExch(a.timeout, 1);
               go = 0;
             }
@@ -1267,6 +1274,7 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
     pa.ipiv = ipiv;
     pa.info = info;
     pa.timeout = w.timeout;
+    pa.spin = wait_polls(c, 0);
     pa.rec = nullptr;
     pa.cand_data = nullptr;
     pa.col_data = nullptr;
@@ -1302,6 +1310,7 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
   pa.ipiv = ipiv;
   pa.info = info;
   pa.timeout = w.timeout;
+  pa.spin = wait_polls(c, 0);
   pa.rec = w.rec;
   pa.cand_data = w.cand_data;
   pa.col_data = w.col_data;
@@ -1491,7 +1500,8 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)A,         (uintptr_t)c->ws,    (uintptr_t)c->ws_bytes,
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
-                                        (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32};
+                                        (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32,
+                                        (uintptr_t)wait_polls(c, 0), (uintptr_t)wait_polls(c, 1)};
     g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
     if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
@@ -1579,6 +1589,7 @@ int getrs_t(Ctx *c, const T *A, double2 *X, double2 *Y, double2 *Z, int nrhs) {
     ta.Y = Y + (size_t)s0 * n;
     ta.Z = Z + (size_t)s0 * n;
     ta.timeout = c->dinfo + 1;
+    ta.spin = wait_polls(c, 2);
     ta.direct = direct;
     ta.stages = stages;
     MOM_CUDA(c, cudaMemsetAsync(ta.Y, 0, sizeof(double2) * ns * n, c->stream));

@@ -175,7 +175,18 @@ struct Ctx {
   // Host-side staging (pinned)
   double *pinned = nullptr;
   size_t pinned_bytes = 0;
+
+  // Polls before a bounded device wait gives up (MOM_ERR_TIMEOUT), per kind:
+  // 0 LU panel exchange, 1 tensor-core GEMM mbarriers, 2 triangular-solve
+  // hand-offs; 0 selects the default (mom_gpu_set_wait_limits).
+  int64_t wait_limit[3] = {0, 0, 0};
 };
+
+// Default bounds of the device waits (a few seconds each).
+constexpr int64_t kDefaultWaitPolls[3] = {int64_t(1) << 26, int64_t(1) << 22, int64_t(1) << 26};
+inline long long wait_polls(const Ctx *c, int kind) {
+  return (long long)(c->wait_limit[kind] > 0 ? c->wait_limit[kind] : kDefaultWaitPolls[kind]);
+}
 
 // Kernel categories for the optional timers.
 enum ProfCat {
@@ -219,6 +230,7 @@ int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes);
 int upload_quadrature(Ctx *c);
 int near_precompute(Ctx *c, int d);
 int assemble(Ctx *c, double omega, const double *ri, int precision);
+int load_matrix(Ctx *c, const double *A_host, int64_t ldh, int precision);
 
 // lu.cu
 int lu_init_kernels(Ctx *c);

@@ -16,9 +16,14 @@
 // kNaMaxBlocks * kNaThreads faces in the domain (scratch ~263 KB, held by
 // every device that loads the library until the process exits).
 //
-// Set-up: the first call on a device looks up the array's device address
-// with cudaGetSymbolAddress (host code must not use the symbol itself as a
-// device address); make that first call before any stream capture.
+// Set-up: every call looks up the array's device address in the current
+// context with cudaGetSymbolAddress (host code must not use the symbol
+// itself as a device address).  With lazy module loading (the CUDA
+// default) the first call on a device may load this module, which
+// allocates the array and can synchronise the device; callers that must
+// not allocate at all make one warm-up call at set-up.  Every call copies
+// its sources to the device and synchronises the context's stream before
+// returning, so it must not be called while a stream capture is open.
 // Sharing: every call on a device uses the same array and it keeps the last
 // call's contents.  Calls on one context are serialised by its mutex; calls
 // from different contexts (or processes sharing a context) that overlap on
@@ -27,7 +32,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "mom_internal.h"
 
@@ -190,22 +194,14 @@ __global__ void na_reduce_kernel(NaScratch *scr, int nblocks, int nsrc) {
   scr->result[s][1] = sc;
 }
 
-constexpr int kNaMaxDevices = 64;
-std::mutex g_na_mu;
-NaScratch *g_na_addr[kNaMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (looked up
-// once per device).
+// Device address of the scratch array in the current CUDA context, looked
+// up on every call: the address belongs to the context, and a context
+// recreated after a device reset places the array elsewhere.
 int na_scratch_address(Ctx *c, NaScratch **out) {
-  if (c->device < 0 || c->device >= kNaMaxDevices) return fail(c, MOM_ERR_ARG, "device index too large");
-  std::lock_guard<std::mutex> g(g_na_mu);
-  if (!g_na_addr[c->device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetSymbolAddress(g_na_scratch)");
-    g_na_addr[c->device] = reinterpret_cast<NaScratch *>(p);
-  }
-  *out = g_na_addr[c->device];
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetSymbolAddress(g_na_scratch)");
+  *out = reinterpret_cast<NaScratch *>(p);
   return MOM_OK;
 }
 

@@ -20,7 +20,8 @@
 //   warp 2   TMEM allocator (512 columns = two 128 x 256 accumulators)
 //   warps 4-7 epilogue: tcgen05.ld the accumulator, C -= acc (coalesced)
 // Every mbarrier wait is bounded; on timeout the kernel records the error,
-// stops issuing work, waits (bounded) for its own copies, frees TMEM and exits.
+// stops issuing work, waits (bounded) for its own copies and for the MMAs
+// already issued, frees TMEM and exits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -37,7 +38,7 @@ constexpr int kTileA = kBM * kBK * 4;  // bytes of one A tile (hi or lo)
 constexpr int kTileB = kBN * kBK * 4;  // bytes of one B tile
 constexpr int kStageBytes = 2 * kTileA + 2 * kTileB;
 constexpr int kTcThreads = 256;
-constexpr long long kWaitLimit = 1LL << 22;  // polls before a wait is declared timed out
+constexpr long long kDrainPolls = 1LL << 22;  // bound of the waits for work already issued
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -50,8 +51,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded parity wait; returns false (and raises *abort) after kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort) {
+// Bounded parity wait; returns false (and raises *abort) after `limit` polls,
+// or when another warp of the CTA has raised *abort.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort, long long limit) {
   const uint32_t a = smem_u32(bar);
   for (long long it = 0;; it++) {
     uint32_t done;
@@ -63,9 +65,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volati
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 1023) == 1023) {
+    if ((it & 1023) == 1023 || it >= limit) {
       if (*abort) return false;
-      if (it > kWaitLimit) {
+      if (it >= limit) {
         *abort = 1;
         return false;
       }
@@ -115,6 +117,7 @@ struct TcArgs {
   int64_t ldc;     // in floats
   int Mr, Nc, Kr;  // real rows of C, columns, real K
   int *err;        // device error word (timeout)
+  long long spin;  // polls before an mbarrier wait is declared timed out
 };
 
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (SWIZZLE_128B atoms need it)
   unsigned char *smem = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2];
+  __shared__ uint64_t full[kStages], empty[kStages], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -138,6 +141,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
     }
+    mbar_init(&drain, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       for (int t = blockIdx.x; t < ntiles && !*abort; t += gridDim.x) {
         const int tm = t % numM, tn = t / numM;
         for (int kb = 0; kb < nk; kb++) {
-          if (!mbar_wait(&empty[s], ph ^ 1, abort)) break;
+          if (!mbar_wait(&empty[s], ph ^ 1, abort, a.spin)) break;
           unsigned char *st = smem + (size_t)s * kStageBytes;
           mbar_expect_tx(&full[s], kStageBytes);
           tma_load_2d(st, &mAhi, &full[s], kb * kBK, tm * kBM);
@@ -179,12 +183,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
         }
       }
-      // on abort, wait (bounded) for the copies already in flight
-      if (*abort) {
-        volatile int dummy = 0;
-        for (int i = 0; i < kStages; i++)
-          if (pending[i]) mbar_wait(&full[i], last_ph[i], &dummy);
-      }
+      // wait (bounded) until the last copy into every stage has landed: the
+      // MMA warp may give up on a stage whose copy is still in flight, and
+      // the CTA must not exit before its shared memory is written
+      volatile int dummy = 0;
+      for (int i = 0; i < kStages; i++)
+        if (pending[i]) mbar_wait(&full[i], last_ph[i], &dummy, kDrainPolls);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -195,12 +199,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       for (int t = blockIdx.x; t < ntiles && !*abort; t += gridDim.x, it++) {
         const int acc = it & 1;
         const unsigned acc_ph = (it >> 1) & 1;
-        if (!mbar_wait(&acc_empty[acc], acc_ph ^ 1, abort)) break;
+        if (!mbar_wait(&acc_empty[acc], acc_ph ^ 1, abort, a.spin)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + (uint32_t)(acc * kBN);
         bool ok = true;
         for (int kb = 0; kb < nk; kb++) {
-          if (!mbar_wait(&full[s], ph, abort)) {
+          if (!mbar_wait(&full[s], ph, abort, a.spin)) {
             ok = false;
             break;
           }
@@ -223,6 +227,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (!ok) break;
         mma_commit(&acc_full[acc]);
       }
+      // on abort, wait (bounded) until every MMA issued so far has completed
+      // (they read the stage buffers and write TMEM, both released below)
+      if (*abort) {
+        volatile int dummy = 0;
+        mma_commit(&drain);
+        mbar_wait(&drain, 0, &dummy, kDrainPolls);
+      }
     }
   } else if (warp >= 4) {
     // ---------------- epilogue ----------------
@@ -232,7 +243,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const int acc = it & 1;
       const unsigned acc_ph = (it >> 1) & 1;
       int ok = 1;
-      if (lane == 0) ok = mbar_wait(&acc_full[acc], acc_ph, abort) ? 1 : 0;
+      if (lane == 0) ok = mbar_wait(&acc_full[acc], acc_ph, abort, a.spin) ? 1 : 0;
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -368,6 +379,7 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   ta.Nc = nc;
   ta.Kr = Kr;
   ta.err = err;
+  ta.spin = wait_polls(c, 1);
   const int ntiles = (Mr / kBM) * ((nc + kBN - 1) / kBN);
   const int grid = ntiles < c->nsm ? ntiles : c->nsm;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;

@@ -48,6 +48,7 @@ EXPORTS = [
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
     "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
     "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement", "mom_gpu_scat_fields",
+    "mom_gpu_set_matrix", "mom_gpu_set_wait_limits",
 ]
 
 
@@ -116,6 +117,8 @@ def lib():
     L.mom_gpu_autotune_placement.argtypes = [vp, C.c_int32, C.c_int32, ip, ip, dp]
     L.mom_problem_node_parent.argtypes = [vp, C.c_int32, ip]
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
+    L.mom_gpu_set_matrix.argtypes = [vp, C.c_int32, vp, C.c_int64]
+    L.mom_gpu_set_wait_limits.argtypes = [vp, C.c_int64, C.c_int64, C.c_int64]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
     L.mom_gpu_launch_count.argtypes = [vp]
@@ -345,6 +348,17 @@ class Solver:
         self._ck(lib().mom_gpu_sysmat(self.h, omega, _dp(r), precision, A.ctypes.data if A is not None else None,
                                       2 * self.N), "sysmat")
         return A
+
+    def set_matrix(self, A, precision=FP64):
+        """A caller's 2N x 2N system matrix in place of sysmat (mom_gpu_set_matrix)."""
+        A = np.asfortranarray(np.asarray(A, dtype=np.complex128))
+        if A.shape != (2 * self.N, 2 * self.N):
+            raise ValueError("the matrix must be 2N x 2N")
+        self._ck(lib().mom_gpu_set_matrix(self.h, precision, A.ctypes.data, 2 * self.N), "set_matrix")
+
+    def set_wait_limits(self, panel=0, gemm=0, solve=0):
+        """Polls before the bounded device waits give up (0: the defaults)."""
+        self._ck(lib().mom_gpu_set_wait_limits(self.h, panel, gemm, solve), "set_wait_limits")
 
     def srcvec(self, omega, ri1, srcs, want_host=False):
         arr, ns = _srcs(srcs)

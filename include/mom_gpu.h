@@ -147,10 +147,13 @@ int mom_gpu_scat_fields(mom_ctx *ctx, int32_t dom, double omega, const double *r
  * device pointer to the 2N x nsrc solutions (leading dimension ldx >= 2N,
  * e.g. from mom_gpu_device_solution); csca / cabs are host arrays.
  * Limits: 1 <= nsrc <= 64 and at most 65536 faces in domain dom; larger
- * requests return MOM_ERR_ARG.  The first call on a device looks up the
- * scratch array's device address, so make it before any stream capture.
- * All calls on a device share the scratch array: calls that overlap on the
- * GPU (from different contexts) race. */
+ * requests return MOM_ERR_ARG.  With lazy module loading (the CUDA default)
+ * the first call on a device may load the library's module, which allocates
+ * the scratch array: callers that must not allocate at all make one warm-up
+ * call at set-up.  Every call synchronises the context's stream, so none may
+ * be made while a stream capture is open.  All calls on a device share the
+ * scratch array: calls that overlap on the GPU (from different contexts)
+ * race. */
 int mom_gpu_cross_sections_noalloc(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t nsrc,
                                    const mom_src *src, const void *x_dev, int64_t ldx, double *csca,
                                    double *cabs);
@@ -214,6 +217,23 @@ int32_t mom_gpu_domain_nodes(mom_ctx *ctx, int32_t dom);
  * U k x nc, C m x nc; m a multiple of 64, k of 16) through the tensor-core
  * kernel that performs the trailing updates of the mixed-precision LU. */
 int mom_gpu_selftest_cgemm(mom_ctx *ctx, int32_t m, int32_t nc, int32_t k, const float *L, const float *U, float *C);
+
+/* Replaces the device system matrix by a caller's 2N x 2N matrix (host,
+ * column-major, lda >= 2N), as if mom_gpu_sysmat had built it; the next
+ * mom_gpu_solve factors and solves it.  The matrix argument of
+ * solve_multi_linsys (linalg.f90:159-180) for callers that assemble A
+ * themselves; a zero pivot returns MOM_ERR_SINGULAR as ZGETRF's INFO > 0
+ * makes the reference STOP (linalg.f90:170-173). */
+int mom_gpu_set_matrix(mom_ctx *ctx, int32_t precision, const double *A_host, int64_t lda);
+
+/* Bounds of the device waits (no counterpart in the reference): polls
+ * before the LU panel exchange, the tensor-core GEMM's mbarrier waits and
+ * the triangular solve's hand-offs give up with MOM_ERR_TIMEOUT; 0 restores
+ * each default (a few seconds).  A kernel that gives up records the error,
+ * waits (bounded) for its own copies and tensor-core work, frees its tensor
+ * memory and returns, so the context stays usable: the next call that
+ * rebuilds the matrix (mom_gpu_sysmat or mom_gpu_set_matrix) starts clean. */
+int mom_gpu_set_wait_limits(mom_ctx *ctx, int64_t panel_polls, int64_t gemm_polls, int64_t solve_polls);
 
 /* Device views for callers that keep data resident (bench, tests). */
 int mom_gpu_device_matrix(mom_ctx *ctx, void **A_dev, int64_t *lda);

@@ -30,6 +30,78 @@ ETA0 = 3.767303134622e2
 DEGTORAD = PI_F / 180.0
 
 
+def load_mesh_gmsh(path: str):
+    """load_mesh_gmsh (mesh.f90:610-705): Gmsh 2.1 / 2.2 ASCII.  Returns
+    (nodes [V][3], faces [F][3] 0-based, physical ids [F]) of the triangle
+    elements (type 2); the physical id is the first tag and the node indices
+    follow the ntags tags, as element_data(4) and element_data(4+ntags:6+ntags)."""
+    with open(path) as fh:
+        tok = [ln.split() for ln in fh]
+    nodes = faces = ids = None
+    i = 0
+    while i < len(tok):
+        head = tok[i][0] if tok[i] else ""
+        if head == "$MeshFormat":
+            if tok[i + 1][0][:3] not in ("2.1", "2.2"):
+                raise ValueError("Mesh version is unsupported!")
+            if tok[i + 2][0] != "$EndMeshFormat":
+                raise ValueError("Could not find $MeshFormatNodes specifier!")
+            i += 3
+        elif head == "$Nodes":
+            nn = int(tok[i + 1][0])
+            nodes = np.zeros((nn, 3))
+            for r in tok[i + 2:i + 2 + nn]:
+                nodes[int(r[0]) - 1] = [float(v) for v in r[1:4]]
+            if tok[i + 2 + nn][0] != "$EndNodes":
+                raise ValueError("Could not find $EndNodes specifier!")
+            i += nn + 3
+        elif head == "$Elements":
+            ne = int(tok[i + 1][0])
+            fl, il = [], []
+            for r in tok[i + 2:i + 2 + ne]:
+                d = [int(v) for v in r]
+                if d[1] == 2:
+                    nt = d[2]
+                    il.append(d[3])
+                    fl.append([d[3 + nt] - 1, d[4 + nt] - 1, d[5 + nt] - 1])
+            if tok[i + 2 + ne][0] != "$EndElements":
+                raise ValueError("Could not find $EndElements specifier!")
+            faces = np.array(fl, dtype=np.int32)
+            ids = np.array(il, dtype=np.int32)
+            i += ne + 3
+        else:
+            i += 1
+    return nodes, faces, ids
+
+
+def get_refind(path: str, wl: float) -> complex:
+    """get_refind (aux.f90:100-167): linear interpolation in a (wl, n, k) table
+    with linterp (aux.f90:58-63); CMPLX without a kind rounds to single
+    precision; wavelengths outside the table give 1."""
+    rows = []
+    with open(path) as fh:
+        for ln in fh:
+            p = ln.split()
+            if len(p) >= 3:
+                rows.append([float(v.replace("d", "e").replace("D", "e")) for v in p[:3]])
+    f32 = np.float32
+    wl1, nr1, ni1 = rows[0]
+    if wl < wl1:
+        return 1.0 + 0j
+    for wl2, nr2, ni2 in rows[1:]:
+        if wl1 <= wl <= wl2 and wl1 != wl2:
+            t = (wl - wl1) / (wl2 - wl1)
+            return complex(float(f32(nr1 + t * (nr2 - nr1))), float(f32(ni1 + t * (ni2 - ni1))))
+        if wl == wl1:
+            return complex(float(f32(nr1)), float(f32(ni1)))
+        if wl == wl2:
+            return complex(float(f32(nr2)), float(f32(ni2)))
+        if wl1 > wl2:
+            raise ValueError("Refractive index data disordered!")
+        wl1, nr1, ni1 = wl2, nr2, ni2
+    return 1.0 + 0j
+
+
 def omega_of(wl: float) -> float:
     """Angular frequency as solve_batch computes it (solver.f90:77)."""
     return 2.0 * PI_F * C0 / wl
@@ -135,10 +207,7 @@ class OracleProblem:
 
     @classmethod
     def from_msh(cls, path, scale, domains, quad="tri_gl13"):
-        import sys
-        sys.path.insert(0, os.path.join(os.path.dirname(_HERE), "for90-mom2_b200"))
-        from mom_b200.meshgen import read_gmsh
-        nodes, faces, ids = read_gmsh(path)
+        nodes, faces, ids = load_mesh_gmsh(path)
         return cls(nodes, faces, ids, scale, domains, quad)
 
     def __del__(self):

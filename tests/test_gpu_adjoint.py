@@ -152,3 +152,25 @@ def test_matches_oracle_finite_differences(solver, prec):
     for v, k, fd in ref["dverts"]:
         for o in range(2):
             assert abs(gm[o, v, k] - fd[o]) <= 1e-5 * scale[o], (v, k, o, gm[o, v, k], fd[o])
+
+
+def test_autograd_wrapper_gradcheck(solver):
+    """torch.autograd.gradcheck of the autograd wrapper (mom_b200.autograd): its
+    backward (one adjoint call) against torch's own central differences of the
+    forward (FP64 solves) in eps and in every node coordinate of the s=1
+    perturbed sphere; cross sections normalised by their value at the start."""
+    import torch
+    from mom_b200 import autograd as AG
+    nodes, faces, ids, doms = sphere(1, perturbed=True)
+    om = M.omega_of(WL)
+    ri = ri_of([EPS])
+    s0 = sigmas(solver, (nodes, faces, ids, doms), ri)[0]
+    scale = torch.tensor(1.0 / s0, dtype=torch.float64)
+
+    def f(er, ei, nd):
+        return AG.cross_sections(solver, er, ei, nd, faces, ids, doms, 1, om, ri, SRC[0], M.FP64) * scale
+
+    er = torch.tensor(EPS.real, dtype=torch.float64, requires_grad=True)
+    ei = torch.tensor(EPS.imag, dtype=torch.float64, requires_grad=True)
+    nd = torch.tensor(nodes, dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(f, (er, ei, nd), eps=1e-6, atol=1e-8, rtol=1e-5)

@@ -34,9 +34,23 @@ def test_noalloc_cross_sections_match_allocating_entry_point(built):
             sca, ab = S.cross_sections_noalloc(om, ri[0], srcs, x_dev, ldx)
             np.testing.assert_allclose(sca, ref_sca, rtol=1e-12, atol=0)
             np.testing.assert_allclose(ab, ref_abs, rtol=1e-12, atol=0)
+        # after the warm-up calls above, further calls leave the device's free
+        # memory unchanged (nothing is allocated per call)
+        import torch
+        torch.cuda.synchronize(0)
+        free0 = torch.cuda.mem_get_info(0)[0]
+        for _ in range(3):
+            sca, ab = S.cross_sections_noalloc(om, ri[0], srcs, x_dev, ldx)
+        torch.cuda.synchronize(0)
+        assert torch.cuda.mem_get_info(0)[0] == free0
+        np.testing.assert_allclose(sca, ref_sca, rtol=1e-12, atol=0)
         # a request beyond the fixed scratch size is rejected, not truncated
         with pytest.raises(M.MomError) as err:
             S.cross_sections_noalloc(om, ri[0], [srcs[0]] * 65, x_dev, ldx)
+        assert err.value.status == M.MOM_ERR_ARG
+        # so is a leading dimension shorter than the 2N unknowns
+        with pytest.raises(M.MomError) as err:
+            S.cross_sections_noalloc(om, ri[0], srcs, x_dev, 2 * S.N - 1)
         assert err.value.status == M.MOM_ERR_ARG
     finally:
         S.close()
