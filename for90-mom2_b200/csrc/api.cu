@@ -111,24 +111,32 @@ void free_domain(DomDev &D) {
 }
 
 void free_problem(Ctx *c) {
-  for (auto &D : c->dom) free_domain(D);
+  for (auto &D : c->dom) {
+    free_actions(D);
+    free_domain(D);
+  }
   c->dom.clear();
-  cudaFree(c->A);
-  cudaFree(c->A32);
+  cudaFree(c->A_all);
+  cudaFree(c->A32_all);
   cudaFree(c->blk);
-  cudaFree(c->ipiv);
-  cudaFree(c->perm);
-  cudaFree(c->invd);
-  cudaFree(c->inv32);
+  cudaFree(c->ipiv_all);
+  cudaFree(c->perm_all);
+  cudaFree(c->invd_all);
+  cudaFree(c->inv32_all);
   cudaFree(c->B);
   cudaFree(c->X);
-  c->A = nullptr;
-  c->A32 = nullptr;
+  cudaFree(c->removed_dev);
+  c->A_all = c->A = nullptr;
+  c->A32_all = c->A32 = nullptr;
   c->blk = nullptr;
-  c->ipiv = nullptr;
-  c->perm = nullptr;
-  c->invd = nullptr;
-  c->inv32 = nullptr;
+  c->ipiv_all = c->ipiv = nullptr;
+  c->perm_all = c->perm = nullptr;
+  c->invd_all = c->invd = nullptr;
+  c->inv32_all = c->inv32 = nullptr;
+  c->removed_dev = nullptr;
+  c->removed.clear();
+  c->removed_off.assign(2, 0);
+  c->nga = 1;
   c->B = c->X = nullptr;
   c->BX_cap = 0;
   c->have_problem = false;
@@ -311,25 +319,45 @@ int ensure_rhs(Ctx *c, int nsrc) {
 }
 
 int ensure_a32(Ctx *c) {
-  if (c->A32) return MOM_OK;
-  const size_t bytes = sizeof(float2) * (size_t)c->lda * c->n;
-  if (cudaMalloc(&c->A32, bytes) != cudaSuccess ||
-      cudaMalloc(&c->inv32, sizeof(float2) * 2 * (size_t)c->nb * c->n) != cudaSuccess) {
+  if (c->A32_all) return MOM_OK;
+  const size_t bytes = sizeof(float2) * (size_t)c->lda * c->n * c->nga;
+  if (cudaMalloc(&c->A32_all, bytes) != cudaSuccess ||
+      cudaMalloc(&c->inv32_all, sizeof(float2) * 2 * (size_t)c->nb * c->n * c->nga) != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(c->A32);
-    c->A32 = nullptr;
+    cudaFree(c->A32_all);
+    c->A32_all = nullptr;
     return fail(c, MOM_ERR_ALLOC, "FP32 matrix allocation failed");
   }
   c->A32_bytes = bytes;
+  select_rep(c, 0);
   return MOM_OK;
 }
 
-// Copy a 2N x ncol column block of device data (ld = c->n) to host (ld).
+// Copy the 2N x ncol column blocks of every representation (device: rep r,
+// column s at dev + (r ncol + s) n) to the host layout (2N, nga, ncol) with
+// leading dimension ld (column (r, s) at host + 2 (s nga + r) ld doubles).
 int copy_block_to_host(Ctx *c, const double2 *dev, int64_t ncol, double *host, int64_t ld) {
   const int64_t rows = 2 * (int64_t)c->N;
-  MOM_CUDA(c, cudaMemcpy2DAsync(host, sizeof(double2) * ld, dev, sizeof(double2) * c->n, sizeof(double2) * rows, ncol,
-                                cudaMemcpyDeviceToHost, c->stream));
+  for (int r = 0; r < c->nga; r++)
+    MOM_CUDA(c, cudaMemcpy2DAsync(host + 2 * (size_t)r * ld, sizeof(double2) * ld * c->nga,
+                                  dev + (size_t)r * ncol * c->n, sizeof(double2) * c->n, sizeof(double2) * rows, ncol,
+                                  cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+// The host layout (2N, nga, ncol), ld, to the device layout of copy_block_to_host.
+int copy_block_to_device(Ctx *c, const double *host, int64_t ld, int64_t ncol, double2 *dev) {
+  const int64_t rows = 2 * (int64_t)c->N;
+  for (int r = 0; r < c->nga; r++)
+    MOM_CUDA(c, cudaMemcpy2DAsync(dev + (size_t)r * ncol * c->n, sizeof(double2) * c->n, host + 2 * (size_t)r * ld,
+                                  sizeof(double2) * ld * c->nga, sizeof(double2) * rows, ncol, cudaMemcpyHostToDevice,
+                                  c->stream));
+  return MOM_OK;
+}
+
+int no_group(Ctx *c, const char *what) {
+  if (c->nga > 1) return fail(c, MOM_ERR_ARG, std::string(what) + " is not available with a symmetry group");
   return MOM_OK;
 }
 
@@ -409,7 +437,11 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->adjW);
   cudaFree(c->dinfo);
   if (c->pinned) cudaFreeHost(c->pinned);
-  for (auto &g : c->lu_graph) g.reset();
+  for (auto *g : c->lu_graphs) {
+    g->reset();
+    delete g;
+  }
+  c->lu_graphs.clear();
   cublasDestroy(c->blas);
   cudaFree(c->blas_ws);
   cudaStreamDestroy(c->stream);
@@ -464,11 +496,19 @@ int mom_gpu_set_problem(mom_ctx *c, int32_t nedges_total, int32_t ndom, const mo
   c->nb = 64;
   c->n = (n2 + c->nb - 1) / c->nb * c->nb;
   c->lda = c->n;
-  c->A_bytes = sizeof(double2) * (size_t)c->lda * c->n;
   c->blk_bytes = sizeof(double2) * 18 * maxF * maxF;
-  if (cudaMalloc(&c->A, c->A_bytes) != cudaSuccess || cudaMalloc(&c->blk, c->blk_bytes) != cudaSuccess ||
-      cudaMalloc(&c->ipiv, sizeof(int) * c->n) != cudaSuccess || cudaMalloc(&c->perm, sizeof(int) * c->n) != cudaSuccess ||
-      cudaMalloc(&c->invd, sizeof(double2) * 2 * (size_t)c->nb * c->n) != cudaSuccess) {
+  // the identity group: one element, one representation, nothing removed
+  std::memset(c->ga, 0, sizeof c->ga);
+  c->ga[0].j[0] = c->ga[0].j[4] = c->ga[0].j[8] = 1.0;
+  c->ga[0].detj = 1.0;
+  c->ga[0].id = 1;
+  c->ga[0].genbits = 2u;
+  c->ga[0].ef[0] = 1.0;
+  c->nga = 1;
+  c->removed.assign(1, {});
+  c->removed_off.assign(2, 0);
+  c->edge_bnd.assign(c->N, MOM_BND_NONE);
+  if (cudaMalloc(&c->blk, c->blk_bytes) != cudaSuccess || alloc_representations(c, 1) != MOM_OK) {
     cudaGetLastError();
     free_problem(c);
     return fail(c, MOM_ERR_ALLOC, "device allocation for the system matrix failed");
@@ -488,7 +528,13 @@ int mom_gpu_sysmat(mom_ctx *c, double omega, const double *ri, int32_t precision
   MOM_CUDA(c, cudaSetDevice(c->device));
   if (precision == MOM_PREC_MIXED) MOM_TRY(ensure_a32(c));
   MOM_TRY(assemble(c, omega, ri, precision));
-  if (A_host) MOM_TRY(copy_block_to_host(c, c->A, 2 * (int64_t)c->N, A_host, lda));
+  for (int r = 0; A_host && r < c->nga; r++) {
+    const int64_t rows = 2 * (int64_t)c->N;
+    MOM_CUDA(c, cudaMemcpy2DAsync(A_host + 2 * (size_t)r * lda * rows, sizeof(double2) * lda,
+                                  c->A_all + (size_t)r * c->lda * c->n, sizeof(double2) * c->lda,
+                                  sizeof(double2) * rows, rows, cudaMemcpyDeviceToHost, c->stream));
+  }
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
   return MOM_OK;
 }
 
@@ -500,7 +546,7 @@ int mom_gpu_srcvec(mom_ctx *c, double omega, const double *ri1, int32_t nsrc, co
   if (!ri1 || nsrc <= 0 || !src || !(omega > 0)) return fail(c, MOM_ERR_ARG, "invalid sources");
   if (q_host && ldq < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldq < 2N");
   MOM_CUDA(c, cudaSetDevice(c->device));
-  MOM_TRY(ensure_rhs(c, nsrc));
+  MOM_TRY(ensure_rhs(c, nsrc * c->nga));
   MOM_TRY(rhs_build(c, omega, ri1, nsrc, src));
   c->nsrc = nsrc;
   c->srcs.assign(src, src + nsrc);
@@ -523,10 +569,32 @@ int mom_gpu_solve(mom_ctx *c, int32_t precision, double tol, int32_t maxit, doub
   if (precision == MOM_PREC_MIXED && (!c->A32 || maxit <= 0 || !(tol > 0)))
     return fail(c, MOM_ERR_ARG, "mixed solve needs a mixed sysmat and tol > 0, maxit > 0");
   MOM_CUDA(c, cudaSetDevice(c->device));
-  if (c->factored != precision) MOM_TRY(lu_factor(c, precision));
+  // one factorisation and solve per representation (solve_systems, solver.f90:325-357)
   int it = 0;
-  MOM_TRY(lu_solve(c, precision, tol, maxit, &it));
-  if (precision == MOM_PREC_FP64) c->assembled = 0;  // the matrix now holds its LU factors
+  if (c->factored != precision) {
+    for (int r = 0; r < c->nga; r++) {
+      select_rep(c, r);
+      const int rc = lu_factor(c, precision);
+      if (rc != MOM_OK) {
+        select_rep(c, 0);
+        c->factored = -1;
+        return rc;
+      }
+    }
+  }
+  for (int r = 0; r < c->nga; r++) {
+    select_rep(c, r);
+    int itr = 0;
+    const size_t off = (size_t)r * c->nsrc * c->n;
+    const int rc = lu_solve_ex(c, precision, 0, c->B + off, c->X + off, c->nsrc, tol, maxit, &itr);
+    if (rc != MOM_OK) {
+      select_rep(c, 0);
+      return rc;
+    }
+    it = std::max(it, itr);
+  }
+  select_rep(c, 0);
+  if (precision == MOM_PREC_FP64) c->assembled = 0;  // the matrices now hold their LU factors
   if (iters_out) *iters_out = it;
   if (x_host) MOM_TRY(copy_block_to_host(c, c->X, c->nsrc, x_host, ldx));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -658,6 +726,7 @@ int mom_gpu_adjoint(mom_ctx *c, int32_t precision, double omega, const double *r
   if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
   if (nsrc < 1 || nsrc > 4) return fail(c, MOM_ERR_ARG, "per-source adjoint gradients take 1 to 4 sources");
   if (deps && (eps_dom < 1 || eps_dom >= c->ndom)) return fail(c, MOM_ERR_ARG, "eps_dom must be an interior domain");
+  MOM_TRY(no_group(c, "adjoint gradients"));
   MOM_CUDA(c, cudaSetDevice(c->device));
   double2 *G = nullptr, *lam = nullptr, *xo = nullptr;
   MOM_TRY(adjoint_currents(c, precision, omega, ri, nsrc, src, tol, maxit, &G, &lam, &xo, iters_out));
@@ -690,6 +759,7 @@ int mom_gpu_adjoint_mean_eps(mom_ctx *c, int32_t precision, double omega, const 
   std::lock_guard<std::mutex> g(c->mu);
   if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
   if (!dmean || eps_dom < 1 || eps_dom >= c->ndom) return fail(c, MOM_ERR_ARG, "eps_dom must be an interior domain");
+  MOM_TRY(no_group(c, "adjoint gradients"));
   MOM_CUDA(c, cudaSetDevice(c->device));
   double2 *G = nullptr, *lam = nullptr, *xo = nullptr;
   MOM_TRY(adjoint_currents(c, precision, omega, ri, nsrc, src, tol, maxit, &G, &lam, &xo, iters_out));
@@ -722,17 +792,17 @@ int mom_gpu_cross_sections(mom_ctx *c, int32_t dom, double omega, const double *
     return fail(c, MOM_ERR_ARG, "invalid cross-section arguments");
   MOM_CUDA(c, cudaSetDevice(c->device));
   const double2 *xd = c->X;
-  int64_t ld = c->n;
+  int64_t ld = c->n, xrep = (int64_t)c->nsrc * c->n;
   if (x_host) {
     if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
-    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n * nsrc));
-    MOM_CUDA(c, cudaMemcpy2DAsync(c->Xh, sizeof(double2) * c->n, x_host, sizeof(double2) * ldx,
-                                  sizeof(double2) * 2 * c->N, nsrc, cudaMemcpyHostToDevice, c->stream));
+    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n * nsrc * c->nga));
+    MOM_TRY(copy_block_to_device(c, x_host, ldx, nsrc, c->Xh));
     xd = c->Xh;
+    xrep = (int64_t)nsrc * c->n;
   } else if (nsrc > c->nsrc) {
     return fail(c, MOM_ERR_STATE, "no device solution for that many sources");
   }
-  return cross_sections(c, dom, omega, ri, nsrc, src, xd, ld, csca, cabs);
+  return cross_sections(c, dom, omega, ri, nsrc, src, xd, ld, csca, cabs, xrep);
 }
 
 int mom_gpu_rcs(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
@@ -744,17 +814,19 @@ int mom_gpu_rcs(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t
     return fail(c, MOM_ERR_ARG, "invalid far-field arguments");
   MOM_CUDA(c, cudaSetDevice(c->device));
   const double2 *xd;
+  int64_t xrep;
   if (x_host) {
     if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
-    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n));
-    MOM_CUDA(c, cudaMemcpyAsync(c->Xh, x_host + 2 * (size_t)isrc * ldx, sizeof(double2) * 2 * c->N,
-                                cudaMemcpyHostToDevice, c->stream));
+    MOM_TRY(ensure_buffer(c, (void **)&c->Xh, &c->Xh_cap, sizeof(double2) * c->n * c->nga));
+    MOM_TRY(copy_block_to_device(c, x_host + 2 * (size_t)isrc * c->nga * ldx, ldx, 1, c->Xh));
     xd = c->Xh;
+    xrep = c->n;
   } else {
     if (isrc >= c->nsrc) return fail(c, MOM_ERR_STATE, "no device solution for that source");
     xd = c->X + (size_t)isrc * c->n;
+    xrep = (int64_t)c->nsrc * c->n;
   }
-  return far_field(c, dom, omega, ri, xd, ntheta, nphi, rcs);
+  return far_field(c, dom, omega, ri, xd, ntheta, nphi, rcs, xrep);
 }
 
 int mom_gpu_scat_fields(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t nsrc, const mom_src *src,
@@ -764,6 +836,7 @@ int mom_gpu_scat_fields(mom_ctx *c, int32_t dom, double omega, const double *ri,
   if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
   if (dom < 0 || dom >= c->ndom || nsrc < 1 || npts < 1 || !pts || !e || !h || !ri || !(omega > 0))
     return fail(c, MOM_ERR_ARG, "invalid near-field arguments");
+  MOM_TRY(no_group(c, "near fields"));
   MOM_CUDA(c, cudaSetDevice(c->device));
   const size_t pbytes = ((sizeof(double) * 3 * (size_t)npts + 255) / 256) * 256;
   const size_t fbytes = ((sizeof(double2) * 3 * (size_t)npts * nsrc + 255) / 256) * 256;
@@ -815,6 +888,7 @@ int mom_gpu_set_matrix(mom_ctx *c, int32_t precision, const double *A_host, int6
   if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before the matrix");
   MOM_TRY(check_prec(c, precision));
   if (!A_host || lda < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "invalid matrix or lda < 2N");
+  MOM_TRY(no_group(c, "a caller's matrix"));
   MOM_CUDA(c, cudaSetDevice(c->device));
   if (precision == MOM_PREC_MIXED) MOM_TRY(ensure_a32(c));
   MOM_TRY(load_matrix(c, A_host, lda, precision));

@@ -257,10 +257,12 @@ __device__ __forceinline__ void blocks_from_moments(const Moments<T> &Mt, const 
 
 struct PairArgs {
   int F;
-  const double *qrel;  // [F][NQ][3]
+  const double *qrel;  // [F][NQ][3]  source faces
   const double *cp;    // [F][3]
   const double *mu;    // [F][3][3]
   const double *sl;    // [F][3]
+  const double *tqrel, *tcp, *tmu;  // test faces (mapped by J^T for a group action g != identity)
+  int ident;           // identity action: the self pair m == n has no K term
   double inv_unit;     // 1/L0
   double kr, ki;       // k * L0
   Cd fD, fH;
@@ -294,11 +296,11 @@ __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
     const int m = m0 + mi;
     if (m >= a.F) break;
     __syncthreads();
-    if (tid < NQ * 3) s_tst[tid] = (T)(a.qrel[(size_t)m * NQ * 3 + tid] * a.inv_unit);
-    if (tid < 9) s_tmu[tid] = a.mu[9 * m + tid] * a.inv_unit;
+    if (tid < NQ * 3) s_tst[tid] = (T)(a.tqrel[(size_t)m * NQ * 3 + tid] * a.inv_unit);
+    if (tid < 9) s_tmu[tid] = a.tmu[9 * m + tid] * a.inv_unit;
     if (tid < 3) {
       s_tsl[tid] = a.sl[3 * m + tid] * a.inv_unit;
-      s_tcp[tid] = a.cp[3 * m + tid];
+      s_tcp[tid] = a.tcp[3 * m + tid];
     }
     __syncthreads();
     if (!active) continue;
@@ -318,7 +320,8 @@ __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
 #pragma unroll
       for (int j = 0; j < 3; j++) mu[i][j] = s_tmu[3 * i + j];
     }
-    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, m == n, a.blk + ((size_t)n * a.F + m) * 18);
+    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
+                           a.blk + ((size_t)n * a.F + m) * 18);
   }
 }
 
@@ -507,10 +510,12 @@ struct StaticArgs {
   int64_t nnear;
   const int *near_m, *near_n;
   const FaceGeo *geo;  // [F]
-  const double *qabs;  // [F][NQ][3]
+  const double *qabs;  // [F][NQ][3]  test points (mapped by J^T for a group action)
   const double *area;  // [F]
   const double *sl;    // [F][3]
-  const double *bn;    // [F][3][3] free vertex (absolute) of local edge e
+  const double *bn;    // [F][3][3] free vertex (absolute) of local edge e, source faces
+  const double *tbn;   // the same of the test faces (mapped by J^T for a group action)
+  int ident;           // identity action: the self pair has no K term
   double *out;         // [nnear][6][9]
 };
 
@@ -524,10 +529,11 @@ __global__ void __launch_bounds__(128) near_static_kernel(StaticArgs a) {
   const int m = a.near_m[j], n = a.near_n[j];
   const FaceGeo g = a.geo[n];
   const double(*qm)[3] = reinterpret_cast<const double(*)[3]>(a.qabs + (size_t)m * NQ * 3);
-  const double(*bnm)[3] = reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)m);
+  const double(*bnm)[3] = reinterpret_cast<const double(*)[3]>(a.tbn + 9 * (size_t)m);
   const double(*bnn)[3] = reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)n);
   double out[6][9];
-  static_terms<double, NQ>(qm, a.area[m], a.sl + 3 * m, bnm, g, a.area[n], a.sl + 3 * n, bnn, m == n, out);
+  static_terms<double, NQ>(qm, a.area[m], a.sl + 3 * m, bnm, g, a.area[n], a.sl + 3 * n, bnn, a.ident && m == n,
+                           out);
   double *o = a.out + j * 54;
 #pragma unroll
   for (int k = 0; k < 6; k++)
@@ -540,6 +546,8 @@ struct NearArgs {
   int F;
   const int *near_m, *near_n;
   const double *qrel, *cp, *mu, *sl;
+  const double *tqrel, *tcp, *tmu;  // test faces (mapped by J^T for a group action)
+  int ident;
   const double *stat;  // [nnear][54]
   double kr, ki;
   Cd c1, c2;           // -i w mu0, -1/(i w eps0 n^2)
@@ -557,21 +565,21 @@ __global__ void __launch_bounds__(128) near_kernel(NearArgs a) {
   double d[3], mu[3][3], nu[3][3], slp[3], slq[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    d[i] = a.cp[3 * m + i] - a.cp[3 * n + i];
+    d[i] = a.tcp[3 * m + i] - a.cp[3 * n + i];
     slp[i] = a.sl[3 * m + i];
     slq[i] = a.sl[3 * n + i];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      mu[i][k] = a.mu[9 * m + 3 * i + k];
+      mu[i][k] = a.tmu[9 * m + 3 * i + k];
       nu[i][k] = a.mu[9 * n + 3 * i + k];
     }
   }
   Moments<double> Mt;
-  pair_moments<double, NQ, true>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)n * NQ * 3, 1, d, a.kr, a.ki, Mt);
+  pair_moments<double, NQ, true>(a.tqrel + (size_t)m * NQ * 3, a.qrel + (size_t)n * NQ * 3, 1, d, a.kr, a.ki, Mt);
   double2 out[18];
   const Cd fD = {a.c1.re * kOofpi / 4.0, a.c1.im * kOofpi / 4.0};
   const Cd fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
-  blocks_from_moments<double>(Mt, mu, nu, slp, slq, d, fD, fH, kOofpi / 4.0, m == n, out);
+  blocks_from_moments<double>(Mt, mu, nu, slp, slq, d, fD, fH, kOofpi / 4.0, a.ident && m == n, out);
   // closed-form parts: (1/(4 pi)) X_m1 - (k^2/(8 pi)) X_1
   const double *st = a.stat + j * 54;
   const double f4 = 1.0 / (4.0 * kPi);
@@ -598,7 +606,12 @@ struct GatherArgs {
   const int *eh;    // [Nd][2]
   const int *epar;  // [Nd]
   const double2 *blk;
-  Cd Zsi;
+  // coefficients of the four PMCHWT blocks (sysmat.f90:70-99): [J,J] += cJJ S,
+  // [M,M] += cMM S, [M,J] += cMJ K, [J,M] += cJM K; for the identity action
+  // 1, Zsi, 1, -1; for group action g in representation r, with its field
+  // action e = ef_g(r): e, e det J Zsi, e det J, -e (K here being the mapped
+  // pair's K, det J times the reference's).
+  Cd cJJ, cMM, cMJ, cJM;
   double2 *A;
   int64_t lda;
 };
@@ -631,20 +644,20 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherArgs a) {
   double2 *A = a.A;
   double2 t;
   t = A[r + c * a.lda];
-  t.x += sr;
-  t.y += si;
+  t.x += a.cJJ.re * sr - a.cJJ.im * si;
+  t.y += a.cJJ.re * si + a.cJJ.im * sr;
   A[r + c * a.lda] = t;
   t = A[(r + N) + (c + N) * a.lda];
-  t.x += a.Zsi.re * sr - a.Zsi.im * si;
-  t.y += a.Zsi.re * si + a.Zsi.im * sr;
+  t.x += a.cMM.re * sr - a.cMM.im * si;
+  t.y += a.cMM.re * si + a.cMM.im * sr;
   A[(r + N) + (c + N) * a.lda] = t;
   t = A[(r + N) + c * a.lda];
-  t.x += kr;
-  t.y += ki;
+  t.x += a.cMJ.re * kr - a.cMJ.im * ki;
+  t.y += a.cMJ.re * ki + a.cMJ.im * kr;
   A[(r + N) + c * a.lda] = t;
   t = A[r + (c + N) * a.lda];
-  t.x -= kr;
-  t.y -= ki;
+  t.x += a.cJM.re * kr - a.cJM.im * ki;
+  t.y += a.cJM.re * ki + a.cJM.im * kr;
   A[r + (c + N) * a.lda] = t;
 }
 
@@ -694,16 +707,19 @@ int upload_quadrature(Ctx *c) {
   return MOM_OK;
 }
 
-// Near pairs of domain d (sysmat.f90:233-260: |cp_m - cp_n|^2 < (3 avelen)^2
-// with the domain's own average edge length) and their closed-form terms.
-// The list is wavelength independent and built once per geometry.
-int near_precompute(Ctx *c, int d) {
-  DomDev &D = c->dom[d];
+// Near pairs of one domain (sysmat.f90:233-260: |cp_m - J cp_n|^2 <
+// (3 avelen)^2 with the domain's own average edge length, here as
+// |J^T cp_m - cp_n| with the test centroids tcp already mapped) and their
+// closed-form terms, from the test points tqabs and free vertices tbn (device,
+// mapped likewise).  The list is wavelength independent, built once per
+// geometry.
+int near_setup(Ctx *c, DomDev &D, const double *tcp, const double *tqabs, const double *tbn, bool ident,
+               int64_t *nnear, int **near_m, int **near_n, double **near_static) {
   const int F = D.F;
   const double thr = D.avelen * 3;
   std::vector<int> nm, nn;
   for (int m = 0; m < F; m++) {
-    const double *cm = &D.h_cp[3 * (size_t)m];
+    const double *cm = tcp + 3 * (size_t)m;
     for (int n = 0; n < F; n++) {
       const double *cn = &D.h_cp[3 * (size_t)n];
       const double d0 = cm[0] - cn[0], d1 = cm[1] - cn[1], d2 = cm[2] - cn[2];
@@ -714,14 +730,14 @@ int near_precompute(Ctx *c, int d) {
       }
     }
   }
-  D.nnear = (int64_t)nm.size();
-  const size_t cap = (size_t)std::max<int64_t>(1, D.nnear);
-  MOM_CUDA(c, cudaMalloc(&D.near_m, sizeof(int) * cap));
-  MOM_CUDA(c, cudaMalloc(&D.near_n, sizeof(int) * cap));
-  MOM_CUDA(c, cudaMalloc(&D.near_static, sizeof(double) * 54 * cap));
-  if (D.nnear == 0) return MOM_OK;
-  MOM_CUDA(c, cudaMemcpyAsync(D.near_m, nm.data(), sizeof(int) * D.nnear, cudaMemcpyHostToDevice, c->stream));
-  MOM_CUDA(c, cudaMemcpyAsync(D.near_n, nn.data(), sizeof(int) * D.nnear, cudaMemcpyHostToDevice, c->stream));
+  *nnear = (int64_t)nm.size();
+  const size_t cap = (size_t)std::max<int64_t>(1, *nnear);
+  MOM_CUDA(c, cudaMalloc(near_m, sizeof(int) * cap));
+  MOM_CUDA(c, cudaMalloc(near_n, sizeof(int) * cap));
+  MOM_CUDA(c, cudaMalloc(near_static, sizeof(double) * 54 * cap));
+  if (*nnear == 0) return MOM_OK;
+  MOM_CUDA(c, cudaMemcpyAsync(*near_m, nm.data(), sizeof(int) * *nnear, cudaMemcpyHostToDevice, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(*near_n, nn.data(), sizeof(int) * *nnear, cudaMemcpyHostToDevice, c->stream));
   std::vector<FaceGeo> geo(F);
   for (int f = 0; f < F; f++) {
     FaceGeo &g = geo[f];
@@ -740,16 +756,18 @@ int near_precompute(Ctx *c, int d) {
   MOM_CUDA(c, cudaMemcpyAsync(dgeo, geo.data(), sizeof(FaceGeo) * F, cudaMemcpyHostToDevice, c->stream));
   MOM_CUDA(c, cudaMemcpyAsync(dbn, D.h_bn.data(), sizeof(double) * 9 * F, cudaMemcpyHostToDevice, c->stream));
   StaticArgs a;
-  a.nnear = D.nnear;
-  a.near_m = D.near_m;
-  a.near_n = D.near_n;
+  a.nnear = *nnear;
+  a.near_m = *near_m;
+  a.near_n = *near_n;
   a.geo = dgeo;
-  a.qabs = D.qabs;
+  a.qabs = tqabs;
   a.area = D.area;
   a.sl = D.sl;
   a.bn = dbn;
-  a.out = D.near_static;
-  const unsigned blocks = (unsigned)((D.nnear + 127) / 128);
+  a.tbn = tbn ? tbn : dbn;
+  a.ident = ident ? 1 : 0;
+  a.out = *near_static;
+  const unsigned blocks = (unsigned)((*nnear + 127) / 128);
   switch (c->nq) {
     case 1: near_static_kernel<1><<<blocks, 128, 0, c->stream>>>(a); break;
     case 3: near_static_kernel<3><<<blocks, 128, 0, c->stream>>>(a); break;
@@ -766,17 +784,82 @@ int near_precompute(Ctx *c, int d) {
   return MOM_OK;
 }
 
-// sysmat_pmchwt (sysmat.f90:18-105), identity group: A = 0, then for every
-// domain the face-pair blocks (far pairs in the requested precision, near
-// pairs in FP64) are gathered into the four PMCHWT blocks.
+int near_precompute(Ctx *c, int d) {
+  DomDev &D = c->dom[d];
+  return near_setup(c, D, D.h_cp.data(), D.qabs, nullptr, true, &D.nnear, &D.near_m, &D.near_n, &D.near_static);
+}
+
+void free_actions(DomDev &D) {
+  for (ActDev &A : D.act) {
+    cudaFree(A.qrel);
+    cudaFree(A.cp);
+    cudaFree(A.mu);
+    cudaFree(A.near_m);
+    cudaFree(A.near_n);
+    cudaFree(A.near_static);
+    A = ActDev();
+  }
+  D.act.clear();
+}
+
+// Test faces of domain d mapped by J^T of group action g: points relative
+// to the mapped centroid, mapped centroids and free vertices, their near
+// pairs and closed-form terms.
+int action_precompute(Ctx *c, int d, int g) {
+  DomDev &D = c->dom[d];
+  ActDev &A = D.act[g];
+  const double *J = c->ga[g].j;
+  auto jt = [&](const double *v, double *o) {
+    for (int i = 0; i < 3; i++) o[i] = J[i] * v[0] + J[3 + i] * v[1] + J[6 + i] * v[2];
+  };
+  const int F = D.F, nq = c->nq;
+  std::vector<double> qrel((size_t)F * nq * 3), qabs((size_t)F * nq * 3), cp(3 * (size_t)F), mu(9 * (size_t)F),
+      bn(9 * (size_t)F);
+  for (size_t i = 0; i < (size_t)F * nq; i++) {
+    jt(&D.h_qrel[3 * i], &qrel[3 * i]);
+    jt(&D.h_qabs[3 * i], &qabs[3 * i]);
+  }
+  for (size_t f = 0; f < (size_t)F; f++) {
+    jt(&D.h_cp[3 * f], &cp[3 * f]);
+    for (int e = 0; e < 3; e++) {
+      jt(&D.h_mu[9 * f + 3 * e], &mu[9 * f + 3 * e]);
+      jt(&D.h_bn[9 * f + 3 * e], &bn[9 * f + 3 * e]);
+    }
+  }
+  double *dqabs = nullptr, *dbn = nullptr;
+  auto up = [&](double **dst, const std::vector<double> &h) -> int {
+    MOM_CUDA(c, cudaMalloc(dst, sizeof(double) * h.size()));
+    MOM_CUDA(c, cudaMemcpyAsync(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    return MOM_OK;
+  };
+  MOM_TRY(up(&A.qrel, qrel));
+  MOM_TRY(up(&A.cp, cp));
+  MOM_TRY(up(&A.mu, mu));
+  MOM_TRY(up(&dqabs, qabs));
+  MOM_TRY(up(&dbn, bn));
+  const int rc = near_setup(c, D, cp.data(), dqabs, dbn, false, &A.nnear, &A.near_m, &A.near_n, &A.near_static);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(dqabs);
+  cudaFree(dbn);
+  return rc;
+}
+
+// sysmat_pmchwt (sysmat.f90:18-105): A = 0, then for every domain and every
+// admissible group action the face-pair blocks (far pairs in the requested
+// precision, near pairs in FP64) are gathered into the four PMCHWT blocks of
+// every representation (sysmat.f90:56-100; the identity group has one
+// action and one representation).
 int assemble(Ctx *c, double omega, const double *ri, int precision) {
   const int64_t n = c->n, lda = c->lda;
-  MOM_CUDA(c, cudaMemsetAsync(c->A, 0, sizeof(double2) * (size_t)lda * n, c->stream));
+  const size_t mat = (size_t)lda * n;
+  const int nga = c->nga;
+  MOM_CUDA(c, cudaMemsetAsync(c->A_all, 0, sizeof(double2) * mat * nga, c->stream));
   const int64_t n2 = 2 * (int64_t)c->N;
-  if (n > n2) {
-    pad_identity<<<(unsigned)((n - n2 + 127) / 128), 128, 0, c->stream>>>(c->A, lda, n2, n);
-    c->launches++;
-  }
+  if (n > n2)
+    for (int r = 0; r < nga; r++) {
+      pad_identity<<<(unsigned)((n - n2 + 127) / 128), 128, 0, c->stream>>>(c->A_all + r * mat, lda, n2, n);
+      c->launches++;
+    }
   for (int d = 0; d < c->ndom; d++) {
     DomDev &D = c->dom[d];
     const Cd rid = {ri[2 * d], ri[2 * d + 1]};
@@ -789,76 +872,99 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
     const Cd c2 = {-den.re / dn2, den.im / dn2};
     const Cd Zsi = {ri2.re / (kEta0 * kEta0), ri2.im / (kEta0 * kEta0)};
     const double L0 = (precision == MOM_PREC_MIXED) ? D.avelen : 1.0;
-    PairArgs pa;
-    pa.F = D.F;
-    pa.qrel = D.qrel;
-    pa.cp = D.cp;
-    pa.mu = D.mu;
-    pa.sl = D.sl;
-    pa.inv_unit = 1.0 / L0;
-    pa.kr = kr * L0;
-    pa.ki = ki * L0;
-    pa.fD = {c1.re * L0 * L0 * L0 * kOofpi / 4.0, c1.im * L0 * L0 * L0 * kOofpi / 4.0};
-    pa.fH = {c2.re * L0 * kOofpi, c2.im * L0 * kOofpi};
-    pa.fK = L0 * L0 * kOofpi / 4.0;
-    pa.blk = c->blk;
-    dim3 grid((D.F + kPairThreads - 1) / kPairThreads, (D.F + kTestPerCta - 1) / kTestPerCta);
-    {
-      ProfScope ps(c, kProfPair);
-      if (precision == MOM_PREC_MIXED) {
-        MOM_TRY(launch_pair<float>(c, c->nq, grid, pa));
-      } else {
-        MOM_TRY(launch_pair<double>(c, c->nq, grid, pa));
+    for (int g = 0; g < nga; g++) {
+      const bool ident = g == 0;
+      if (!ident && !D.act[g].admissible) continue;
+      const double *tqrel = ident ? D.qrel : D.act[g].qrel, *tcp = ident ? D.cp : D.act[g].cp,
+                   *tmu = ident ? D.mu : D.act[g].mu;
+      const int64_t nnear = ident ? D.nnear : D.act[g].nnear;
+      PairArgs pa;
+      pa.F = D.F;
+      pa.qrel = D.qrel;
+      pa.cp = D.cp;
+      pa.mu = D.mu;
+      pa.sl = D.sl;
+      pa.tqrel = tqrel;
+      pa.tcp = tcp;
+      pa.tmu = tmu;
+      pa.ident = ident ? 1 : 0;
+      pa.inv_unit = 1.0 / L0;
+      pa.kr = kr * L0;
+      pa.ki = ki * L0;
+      pa.fD = {c1.re * L0 * L0 * L0 * kOofpi / 4.0, c1.im * L0 * L0 * L0 * kOofpi / 4.0};
+      pa.fH = {c2.re * L0 * kOofpi, c2.im * L0 * kOofpi};
+      pa.fK = L0 * L0 * kOofpi / 4.0;
+      pa.blk = c->blk;
+      dim3 grid((D.F + kPairThreads - 1) / kPairThreads, (D.F + kTestPerCta - 1) / kTestPerCta);
+      {
+        ProfScope ps(c, kProfPair);
+        if (precision == MOM_PREC_MIXED) {
+          MOM_TRY(launch_pair<float>(c, c->nq, grid, pa));
+        } else {
+          MOM_TRY(launch_pair<double>(c, c->nq, grid, pa));
+        }
+      }
+      if (nnear > 0) {
+        NearArgs na;
+        na.nnear = nnear;
+        na.F = D.F;
+        na.near_m = ident ? D.near_m : D.act[g].near_m;
+        na.near_n = ident ? D.near_n : D.act[g].near_n;
+        na.qrel = D.qrel;
+        na.cp = D.cp;
+        na.mu = D.mu;
+        na.sl = D.sl;
+        na.tqrel = tqrel;
+        na.tcp = tcp;
+        na.tmu = tmu;
+        na.ident = ident ? 1 : 0;
+        na.stat = ident ? D.near_static : D.act[g].near_static;
+        na.kr = kr;
+        na.ki = ki;
+        na.c1 = c1;
+        na.c2 = c2;
+        na.k2 = {kr * kr - ki * ki, 2 * kr * ki};
+        na.blk = c->blk;
+        const unsigned blocks = (unsigned)((nnear + 127) / 128);
+        ProfScope ps(c, kProfNear);
+        switch (c->nq) {
+          case 1: near_kernel<1><<<blocks, 128, 0, c->stream>>>(na); break;
+          case 3: near_kernel<3><<<blocks, 128, 0, c->stream>>>(na); break;
+          case 4: near_kernel<4><<<blocks, 128, 0, c->stream>>>(na); break;
+          case 7: near_kernel<7><<<blocks, 128, 0, c->stream>>>(na); break;
+          case 13: near_kernel<13><<<blocks, 128, 0, c->stream>>>(na); break;
+          default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+        }
+        c->launches++;
+        MOM_CUDA(c, cudaGetLastError());
+      }
+      const double detj = c->ga[g].detj;
+      for (int r = 0; r < nga; r++) {
+        const double e = c->ga[g].ef[r];
+        GatherArgs ga;
+        ga.F = D.F;
+        ga.Nd = D.Nd;
+        ga.N = c->N;
+        ga.eh = D.eh;
+        ga.epar = D.epar;
+        ga.blk = c->blk;
+        ga.cJJ = {e, 0.0};
+        ga.cMM = {e * detj * Zsi.re, e * detj * Zsi.im};
+        ga.cMJ = {e * detj, 0.0};
+        ga.cJM = {-e, 0.0};
+        ga.A = c->A_all + r * mat;
+        ga.lda = lda;
+        dim3 gg((D.Nd + 255) / 256, D.Nd);
+        ProfScope ps(c, kProfGather);
+        gather_kernel<<<gg, 256, 0, c->stream>>>(ga);
+        c->launches++;
+        MOM_CUDA(c, cudaGetLastError());
       }
     }
-    if (D.nnear > 0) {
-      NearArgs na;
-      na.nnear = D.nnear;
-      na.F = D.F;
-      na.near_m = D.near_m;
-      na.near_n = D.near_n;
-      na.qrel = D.qrel;
-      na.cp = D.cp;
-      na.mu = D.mu;
-      na.sl = D.sl;
-      na.stat = D.near_static;
-      na.kr = kr;
-      na.ki = ki;
-      na.c1 = c1;
-      na.c2 = c2;
-      na.k2 = {kr * kr - ki * ki, 2 * kr * ki};
-      na.blk = c->blk;
-      const unsigned blocks = (unsigned)((D.nnear + 127) / 128);
-      ProfScope ps(c, kProfNear);
-      switch (c->nq) {
-        case 1: near_kernel<1><<<blocks, 128, 0, c->stream>>>(na); break;
-        case 3: near_kernel<3><<<blocks, 128, 0, c->stream>>>(na); break;
-        case 4: near_kernel<4><<<blocks, 128, 0, c->stream>>>(na); break;
-        case 7: near_kernel<7><<<blocks, 128, 0, c->stream>>>(na); break;
-        case 13: near_kernel<13><<<blocks, 128, 0, c->stream>>>(na); break;
-        default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
-      }
-      c->launches++;
-      MOM_CUDA(c, cudaGetLastError());
-    }
-    GatherArgs ga;
-    ga.F = D.F;
-    ga.Nd = D.Nd;
-    ga.N = c->N;
-    ga.eh = D.eh;
-    ga.epar = D.epar;
-    ga.blk = c->blk;
-    ga.Zsi = Zsi;
-    ga.A = c->A;
-    ga.lda = lda;
-    dim3 gg((D.Nd + 255) / 256, D.Nd);
-    ProfScope ps(c, kProfGather);
-    gather_kernel<<<gg, 256, 0, c->stream>>>(ga);
-    c->launches++;
-    MOM_CUDA(c, cudaGetLastError());
   }
+  for (int r = 0; r < nga && nga > 1; r++) MOM_TRY(apply_bc_matrix(c, r));
   if (precision == MOM_PREC_MIXED) {
-    convert_to_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A, c->A32, (int64_t)lda * n);
+    convert_to_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A_all, c->A32_all, (int64_t)mat * nga);
     c->launches++;
     MOM_CUDA(c, cudaGetLastError());
   }

@@ -1502,8 +1502,24 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
                                         (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32,
                                         (uintptr_t)wait_polls(c, 0), (uintptr_t)wait_polls(c, 1)};
-    g = &c->lu_graph[precision == MOM_PREC_MIXED ? 1 : 0];
-    if (!g->exec || g->key != key) MOM_TRY(lu_capture<T>(c, A, precision, w, *g, key));
+    for (Ctx::LuGraph *h : c->lu_graphs)
+      if (h->exec && h->key == key) g = h;
+    if (!g) {
+      // one graph per (precision, representation); the oldest goes first
+      if (c->lu_graphs.size() >= 2 * (size_t)kMaxGroup) {
+        c->lu_graphs.front()->reset();
+        delete c->lu_graphs.front();
+        c->lu_graphs.erase(c->lu_graphs.begin());
+      }
+      g = new Ctx::LuGraph();
+      c->lu_graphs.push_back(g);
+      const int rc = lu_capture<T>(c, A, precision, w, *g, key);
+      if (rc != MOM_OK) {
+        delete g;
+        c->lu_graphs.pop_back();
+        return rc;
+      }
+    }
     MOM_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
     c->launches += g->launches;
     c->blas_calls += g->blas_calls;

@@ -26,6 +26,38 @@ constexpr double kEta0 = 3.767303134622e2;
 constexpr int kMaxQ = 13;
 constexpr size_t kBlasWorkspace = 64u << 20;
 
+constexpr int kMaxGroup = MOM_MAX_GROUP;
+
+// One element of a symmetry group (group_action, symmetry.f90:24-40): point
+// action J (row-major, j[3 i + k] = J(i, k)), det J, the special-action id
+// (0 none, 1 identity, 2/3/4 the mirrors x/y/z, symmetry.f90:20-23), the
+// generator bits and the field action per representation (+1 / -1 for the
+// mirror groups, whose characters are real).
+struct GroupAction {
+  double j[9];
+  double detj;
+  int id;
+  unsigned genbits;
+  double ef[kMaxGroup];
+};
+
+// A non-identity group action g on one domain: the domain's test faces
+// mapped by J^T.  The reference maps the source face by J; for an orthogonal
+// J the pair (test r, source J r') equals (test J^T r, source r'), so the
+// identity kernels run on the mapped test side: D_g, H_g from the mapped
+// pair as they are, K_g = det J times the mapped pair's K.  Near pairs
+// (|cp_m - J cp_n| < 3 avelen) and their closed-form integrals follow the
+// mapped test faces.
+struct ActDev {
+  bool admissible = false;  // admissible_ga (bc.f90:237-257)
+  double *qrel = nullptr;   // [F][nq][3] mapped test points minus the mapped centroid
+  double *cp = nullptr;     // [F][3] mapped centroids
+  double *mu = nullptr;     // [F][3][3] mapped free vertices minus the mapped centroid
+  int64_t nnear = 0;
+  int *near_m = nullptr, *near_n = nullptr;
+  double *near_static = nullptr;  // [nnear][6][9]
+};
+
 // Per-domain device data (structure of arrays).  "Half-edge" h = 3*face +
 // local edge identifies one RWG half (one face of an edge).
 struct DomDev {
@@ -64,6 +96,9 @@ struct DomDev {
   // Face geometry of the near-field kernel (uploaded on first use).
   void *nf_geo = nullptr;
   double *nf_bn = nullptr;
+  // Symmetry group actions on this domain, [nga] (element 0 is the identity,
+  // which uses the arrays above).
+  std::vector<ActDev> act;
 };
 
 struct Ctx {
@@ -85,7 +120,23 @@ struct Ctx {
   std::vector<DomDev> dom;
   bool have_problem = false;
 
-  // System matrix and factors
+  // Symmetry group (identity unless mom_gpu_set_symmetry) and, per
+  // representation, the unknowns its symmetry-plane boundary conditions
+  // remove (edge_bc, bc.f90:28-117; rows and columns replaced by identity).
+  int nga = 1;
+  GroupAction ga[kMaxGroup];
+  std::vector<int> edge_bnd;                 // [N] master-edge boundary types
+  std::vector<std::vector<int>> removed;     // [nga]
+  int *removed_dev = nullptr;                // concatenated lists
+  std::vector<int> removed_off;              // [nga + 1]
+
+  // System matrix and factors.  With a symmetry group there is one matrix
+  // (and one set of factors) per representation: the *_all buffers hold
+  // them all and A, A32, ipiv, perm, invd, inv32 point at the
+  // representation being worked on (select_rep).
+  double2 *A_all = nullptr, *invd_all = nullptr;
+  float2 *A32_all = nullptr, *inv32_all = nullptr;
+  int *ipiv_all = nullptr, *perm_all = nullptr;
   int64_t n = 0, lda = 0;  // n = 2N
   double2 *A = nullptr;    // FP64 matrix (LU in place in FP64 mode)
   float2 *A32 = nullptr;   // FP32 copy (LU in place in mixed mode)
@@ -134,7 +185,8 @@ struct Ctx {
     int64_t launches = 0, blas_calls = 0;  // per replay
     double tc_flops = 0;
     void reset();
-  } lu_graph[2];
+  };
+  std::vector<LuGraph *> lu_graphs;  // by key (one per precision and representation)
   bool use_graph = true;   // MOM_LU_GRAPH=0 turns graph replay off (every launch issued eagerly)
   // Panel parallelism: CTAs per panel as a function of the panel's rows m,
   // autotuned per (matrix order, precision) at the first factorisation
@@ -226,10 +278,29 @@ int cuda_fail(Ctx *c, cudaError_t e, const char *where);
 
 int ensure_buffer(Ctx *c, void **p, size_t *cap, size_t bytes);
 
+// Points A, A32, ipiv, perm, invd, inv32 at representation r's buffers.
+inline void select_rep(Ctx *c, int r) {
+  const size_t mat = (size_t)c->lda * c->n, vec = (size_t)c->n, inv = 2 * (size_t)c->nb * c->n;
+  c->A = c->A_all ? c->A_all + r * mat : nullptr;
+  c->A32 = c->A32_all ? c->A32_all + r * mat : nullptr;
+  c->ipiv = c->ipiv_all ? c->ipiv_all + r * vec : nullptr;
+  c->perm = c->perm_all ? c->perm_all + r * vec : nullptr;
+  c->invd = c->invd_all ? c->invd_all + r * inv : nullptr;
+  c->inv32 = c->inv32_all ? c->inv32_all + r * inv : nullptr;
+}
+
 // assemble.cu
 int upload_quadrature(Ctx *c);
 int near_precompute(Ctx *c, int d);
 int assemble(Ctx *c, double omega, const double *ri, int precision);
+// The test faces of domain d mapped by group action g (J^T), their near
+// pairs and closed-form integrals (set-up of a symmetry group).
+int action_precompute(Ctx *c, int d, int g);
+void free_actions(DomDev &D);
+// group.cu: the symmetry-plane boundary conditions of representation r
+int apply_bc_matrix(Ctx *c, int r);
+int apply_bc_rhs(Ctx *c, int r, double2 *B, int ncol);
+int alloc_representations(Ctx *c, int nga);
 int load_matrix(Ctx *c, const double *A_host, int64_t ldh, int precision);
 
 // lu.cu
@@ -247,10 +318,12 @@ int tc_init_kernels(Ctx *c);
 
 // post.cu
 int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src);
+// With a symmetry group, the solution of representation r, source s is at
+// xdev + r xrep + s ldx (xrep unused for the identity group).
 int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src,
-                   const double2 *xdev, int64_t ldx, double *csca, double *cabs);
+                   const double2 *xdev, int64_t ldx, double *csca, double *cabs, int64_t xrep = 0);
 int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
-              double *rcs);
+              double *rcs, int64_t xrep = 0);
 // Near fields (nfields.f90 scat_fields; csrc/nfields_impl.cuh): E, H
 // [nsrc][npts][3] of the currents X ([nsrc][ldx], device) at device points.
 int scat_fields(Ctx *c, int d, double omega, const double *ri, int nsrc, const double2 *X, int64_t ldx, int npts,

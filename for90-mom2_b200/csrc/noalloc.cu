@@ -223,6 +223,7 @@ extern "C" int mom_gpu_cross_sections_noalloc(mom_ctx *c, int32_t dom, double om
     return fail(c, MOM_ERR_ARG, "invalid cross-section arguments");
   if (nsrc < 1 || nsrc > kNaMaxSrc)
     return fail(c, MOM_ERR_ARG, "allocation-free cross sections take 1 to 64 sources per call");
+  if (c->nga > 1) return fail(c, MOM_ERR_ARG, "allocation-free cross sections take the identity group only");
   const DomDev &D = c->dom[dom];
   const int blocks = (D.F + kNaThreads - 1) / kNaThreads;
   if (blocks > kNaMaxBlocks)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "mom_internal.h"
@@ -454,6 +455,214 @@ __global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const doub
   rcs[(size_t)it + (size_t)ip * ntheta] = a * a + b * b;
 }
 
+// ---- symmetry groups (nga > 1) ----
+
+// The group as kernel argument: point actions J (row-major), det J and the
+// field actions ef[g][r] (real for mirror groups).
+struct GroupArg {
+  int nga;
+  double j[kMaxGroup][9];
+  double detj[kMaxGroup];
+  double ef[kMaxGroup][kMaxGroup];
+};
+
+__device__ __forceinline__ void jvec(const double *J, const double *v, double *o) {
+  for (int i = 0; i < 3; i++) o[i] = J[3 * i] * v[0] + J[3 * i + 1] * v[1] + J[3 * i + 2] * v[2];
+}
+__device__ __forceinline__ void jtvec(const double *J, const double *v, double *o) {
+  for (int i = 0; i < 3; i++) o[i] = J[i] * v[0] + J[3 + i] * v[1] + J[6 + i] * v[2];
+}
+__device__ __forceinline__ void jzvec(const double *J, const Z *v, Z *o) {
+  for (int i = 0; i < 3; i++)
+    o[i] = zadd(zadd(zscale(v[0], J[3 * i]), zscale(v[1], J[3 * i + 1])), zscale(v[2], J[3 * i + 2]));
+}
+
+// srcvec with a group (source.f90:136-247 with src_field_frags 250-315):
+// thread per (face, source, representation r); the incident fields at the
+// test point seen by every element g (at J^T r, mapped back by J, H with
+// det J), projected on representation r with ef[g][r] / nga.
+__global__ void rhs_half_sym_kernel(RhsArgs a, GroupArg G) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y, r = blockIdx.z;
+  if (f >= a.F) return;
+  const SrcDev S = a.src[s];
+  Z Ie[3] = {{0, 0}, {0, 0}, {0, 0}}, Ih[3] = {{0, 0}, {0, 0}, {0, 0}};
+  const double Am = a.area[f];
+  for (int t = 0; t < a.nq; t++) {
+    const double *pt = a.qabs + ((size_t)f * a.nq + t) * 3;
+    Z ef[3] = {{0, 0}, {0, 0}, {0, 0}}, hf[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int g = 0; g < G.nga; g++) {
+      double pp[3];
+      jtvec(G.j[g], pt, pp);
+      Z e[3], h[3], je[3], jh[3];
+      src_fields(S, a.k, a.omega, pp, e, h);
+      jzvec(G.j[g], e, je);
+      jzvec(G.j[g], h, jh);
+      const double ce = G.ef[g][r], ch = G.ef[g][r] * G.detj[g];
+      for (int i = 0; i < 3; i++) {
+        ef[i] = zadd(ef[i], zscale(je[i], ce));
+        hf[i] = zadd(hf[i], zscale(jh[i], ch));
+      }
+    }
+    for (int i = 0; i < 3; i++) {
+      ef[i] = zscale(ef[i], 1.0 / G.nga);
+      hf[i] = zscale(hf[i], 1.0 / G.nga);
+    }
+    const double w = a.w[t];
+    for (int p = 0; p < 3; p++) {
+      const double cc = a.sl[3 * f + p] / (2.0 * Am);
+      double fm[3];
+      for (int i = 0; i < 3; i++) fm[i] = cc * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * p + i]));
+      Z de = {0, 0}, dh = {0, 0};
+      for (int i = 0; i < 3; i++) {
+        de = zadd(de, zscale(ef[i], fm[i]));
+        dh = zadd(dh, zscale(hf[i], fm[i]));
+      }
+      Ie[p] = zadd(Ie[p], zscale(de, w));
+      Ih[p] = zadd(Ih[p], zscale(dh, w));
+    }
+  }
+  double2 *o = a.half + ((((size_t)r * a.nsrc + s) * a.F + f) * 3) * 2;
+  for (int p = 0; p < 3; p++) {
+    o[2 * p] = make_double2(Ie[p].re * Am, Ie[p].im * Am);
+    o[2 * p + 1] = make_double2(Ih[p].re * Am, Ih[p].im * Am);
+  }
+}
+
+// cs_prtsrf with a group (cs.f90:14-104): per face and source, the Poynting
+// fluxes on every image J(face) of the fragment, with the image's fields
+// built from all representations' currents; x of representation r, source
+// s at x + r xrep + s ldx.
+__global__ void __launch_bounds__(256) cs_sym_kernel(CsArgs a, GroupArg G, int64_t xrep) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  double i1 = 0, i2 = 0;
+  if (f < a.F) {
+    const SrcDev S = a.src[s];
+    const double An = a.area[f];
+    const double *n0 = a.nrm + 3 * f;
+    double int1 = 0, int2 = 0;
+    for (int t = 0; t < a.nq; t++) {
+      const double *qp = a.qabs + ((size_t)f * a.nq + t) * 3;
+      double fn0[3][3];
+      for (int p = 0; p < 3; p++) {
+        const double cc = a.sl[3 * f + p] / (2.0 * An);
+        double fr[3];
+        for (int i = 0; i < 3; i++) fr[i] = cc * (qp[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * p + i]));
+        fn0[p][0] = n0[1] * fr[2] - n0[2] * fr[1];
+        fn0[p][1] = n0[2] * fr[0] - n0[0] * fr[2];
+        fn0[p][2] = n0[0] * fr[1] - n0[1] * fr[0];
+      }
+      for (int g = 0; g < G.nga; g++) {
+        const double *J = G.j[g];
+        double nor[3], pt[3], fn[3][3];
+        jvec(J, n0, nor);
+        jvec(J, qp, pt);
+        for (int p = 0; p < 3; p++) jvec(J, fn0[p], fn[p]);
+        Z Et[3] = {{0, 0}, {0, 0}, {0, 0}}, Ht[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int r = 0; r < G.nga; r++) {
+          const double gae = G.ef[g][r];
+          const double2 *x = a.x + (size_t)r * xrep + (size_t)s * a.ldx;
+          for (int p = 0; p < 3; p++) {
+            const int idx = a.hpar[3 * f + p];
+            const Z xj = {x[idx].x, x[idx].y}, xm = {x[idx + a.N].x, x[idx + a.N].y};
+            for (int i = 0; i < 3; i++) {
+              Ht[i] = zsub(Ht[i], zscale(xj, fn[p][i] * gae * G.detj[g]));
+              Et[i] = zadd(Et[i], zscale(xm, fn[p][i] * gae));
+            }
+          }
+        }
+        const Z nc[3] = {{nor[0], 0}, {nor[1], 0}, {nor[2], 0}};
+        Z einc[3], hinc[3], t1[3], Eti[3], Hti[3], Ets[3], Hts[3], cr[3], cj[3];
+        src_fields(S, a.k, a.omega, pt, einc, hinc);
+        zcross(nc, hinc, t1);
+        zcross(t1, nc, Hti);
+        zcross(nc, einc, t1);
+        zcross(t1, nc, Eti);
+        for (int i = 0; i < 3; i++) {
+          Hts[i] = zsub(Ht[i], Hti[i]);
+          Ets[i] = zsub(Et[i], Eti[i]);
+          cj[i] = zconj(Ht[i]);
+        }
+        zcross(Et, cj, cr);
+        const double w = a.w[t];
+        int1 += w * 0.5 * (cr[0].re * nor[0] + cr[1].re * nor[1] + cr[2].re * nor[2]);
+        for (int i = 0; i < 3; i++) cj[i] = zconj(Hts[i]);
+        zcross(Ets, cj, cr);
+        int2 += w * 0.5 * (cr[0].re * nor[0] + cr[1].re * nor[1] + cr[2].re * nor[2]);
+      }
+    }
+    i1 = int1 * An;
+    i2 = int2 * An;
+  }
+  __shared__ double r1[256], r2[256];
+  r1[threadIdx.x] = i1;
+  r2[threadIdx.x] = i2;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      r1[threadIdx.x] += r1[threadIdx.x + w];
+      r2[threadIdx.x] += r2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.part[((size_t)s * gridDim.x + blockIdx.x) * 2] = r1[0];
+    a.part[((size_t)s * gridDim.x + blockIdx.x) * 2 + 1] = r2[0];
+  }
+}
+
+// far_fields with a group (ffields.f90:52-91): the weighted currents at the
+// images J r of every quadrature point, J f times the representations'
+// coefficients with ef[g][r] (M also with det J); point index
+// (g F + f) nq + t.  x of representation r at x + r xrep.
+__global__ void ff_current_sym_kernel(FfArgs a, GroupArg G, int64_t xrep) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int per = a.F * a.nq;
+  if (j >= per * G.nga) return;
+  const int g = j / per, ft = j % per, f = ft / a.nq, t = ft % a.nq;
+  const double *pt = a.qabs + (size_t)ft * 3;
+  const double An = a.area[f];
+  const double w = a.w[t] * An;
+  const double *J = G.j[g];
+  double Jr[3][2] = {{0, 0}, {0, 0}, {0, 0}}, Mr[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  for (int q = 0; q < 3; q++) {
+    const int idx = a.hpar[3 * f + q];
+    const double cc = a.sl[3 * f + q] / (2.0 * An);
+    double fq[3], jf[3];
+    for (int i = 0; i < 3; i++) fq[i] = cc * (pt[i] - (a.cp[3 * f + i] + a.mu[9 * f + 3 * q + i]));
+    jvec(J, fq, jf);
+    for (int r = 0; r < G.nga; r++) {
+      const double gae = G.ef[g][r];
+      const double2 al = a.x[(size_t)r * xrep + idx], be = a.x[(size_t)r * xrep + idx + a.N];
+      for (int i = 0; i < 3; i++) {
+        Jr[i][0] += jf[i] * gae * al.x;
+        Jr[i][1] += jf[i] * gae * al.y;
+        Mr[i][0] += jf[i] * gae * G.detj[g] * be.x;
+        Mr[i][1] += jf[i] * gae * G.detj[g] * be.y;
+      }
+    }
+  }
+  double pos[3];
+  jvec(J, pt, pos);
+  for (int i = 0; i < 3; i++) {
+    a.cur[(size_t)j * 3 + i] = make_double4(w * Jr[i][0], w * Jr[i][1], w * Mr[i][0], w * Mr[i][1]);
+    a.pos[(size_t)j * 3 + i] = pos[i];
+  }
+}
+
+GroupArg group_arg(const Ctx *c) {
+  GroupArg G;
+  std::memset(&G, 0, sizeof G);
+  G.nga = c->nga;
+  for (int g = 0; g < c->nga; g++) {
+    for (int i = 0; i < 9; i++) G.j[g][i] = c->ga[g].j[i];
+    G.detj[g] = c->ga[g].detj;
+    for (int r = 0; r < c->nga; r++) G.ef[g][r] = c->ga[g].ef[r];
+  }
+  return G;
+}
+
 void make_src(const mom_src &s, SrcDev &d) {
   src_geometry(s, d.dir, d.pol);
   d.ph_re = s.phase_re;
@@ -481,7 +690,7 @@ int upload_sources(Ctx *c, int nsrc, const mom_src *src, SrcDev **out) {
 int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *src) {
   const DomDev &D = c->dom[0];
   const size_t src_bytes = ((sizeof(SrcDev) * nsrc + 255) / 256) * 256;
-  const size_t half_bytes = sizeof(double2) * 6 * (size_t)D.F * nsrc;
+  const size_t half_bytes = sizeof(double2) * 6 * (size_t)D.F * nsrc * c->nga;
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, src_bytes + half_bytes));
   SrcDev *dsrc = nullptr;
   MOM_TRY(upload_sources(c, nsrc, src, &dsrc));
@@ -499,8 +708,23 @@ int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *
   a.k = {ri1[0] * omega / kC0, ri1[1] * omega / kC0};
   a.omega = omega;
   a.half = reinterpret_cast<double2 *>((char *)c->ws + src_bytes);
-  MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * c->n * nsrc, c->stream));
+  MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * c->n * nsrc * c->nga, c->stream));
   ProfScope ps(c, kProfPost);
+  if (c->nga > 1) {
+    // one block of right-hand sides per representation: B + r nsrc n
+    rhs_half_sym_kernel<<<dim3((D.F + 127) / 128, nsrc, c->nga), 128, 0, c->stream>>>(a, group_arg(c));
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+    for (int r = 0; r < c->nga; r++) {
+      double2 *Br = c->B + (size_t)r * nsrc * c->n;
+      rhs_edge_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(
+          D.Nd, D.F, c->N, c->n, D.eh, D.epar, a.half + (size_t)r * nsrc * D.F * 6, Br);
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+      MOM_TRY(apply_bc_rhs(c, r, Br, nsrc));
+    }
+    return MOM_OK;
+  }
   rhs_half_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
@@ -512,7 +736,7 @@ int rhs_build(Ctx *c, double omega, const double *ri1, int nsrc, const mom_src *
 }
 
 int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src,
-                   const double2 *xdev, int64_t ldx, double *csca, double *cabs) {
+                   const double2 *xdev, int64_t ldx, double *csca, double *cabs, int64_t xrep) {
   const DomDev &D = c->dom[dom];
   const int blocks = (D.F + 255) / 256;
   const size_t src_bytes = ((sizeof(SrcDev) * nsrc + 255) / 256) * 256;
@@ -540,7 +764,8 @@ int cross_sections(Ctx *c, int dom, double omega, const double *ri, int nsrc, co
   a.part = reinterpret_cast<double *>((char *)c->ws + src_bytes);
   {
   ProfScope ps(c, kProfPost);
-  cs_kernel<<<dim3(blocks, nsrc), 256, 0, c->stream>>>(a);
+  if (c->nga > 1) cs_sym_kernel<<<dim3(blocks, nsrc), 256, 0, c->stream>>>(a, group_arg(c), xrep);
+  else cs_kernel<<<dim3(blocks, nsrc), 256, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
   }
@@ -600,9 +825,9 @@ int cs_gradient(Ctx *c, int dom, double omega, const double *ri, int nsrc, const
 }
 
 int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int ntheta, int nphi,
-              double *rcs) {
+              double *rcs, int64_t xrep) {
   const DomDev &D = c->dom[dom];
-  const int npts = D.F * c->nq;
+  const int npts = D.F * c->nq * c->nga;
   const int nd = ntheta * nphi;
   const size_t cur_bytes = sizeof(double4) * 3 * (size_t)npts;
   const size_t pos_bytes = sizeof(double) * 3 * (size_t)npts;
@@ -625,7 +850,8 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   double *dout = reinterpret_cast<double *>((char *)c->ws + cur_bytes + pos_bytes);
   {
   ProfScope ps(c, kProfPost);
-  ff_current_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a);
+  if (c->nga > 1) ff_current_sym_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a, group_arg(c), xrep);
+  else ff_current_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a);
   c->launches++;
   MOM_CUDA(c, cudaGetLastError());
   const Z k = {ri[0] * omega / kC0, ri[1] * omega / kC0};

@@ -2,8 +2,8 @@
 // interface.f90:1624-1734) over the C ABI, for the commands of the linear
 // PMCHWT scattering path:
 //
-//   name  mesh  wlrg  wlls  symm  nmed  smed  ndom  sdom  fdom  nsrc  ssrc
-//   quad  solv  crst  rcst  nfpl  exit
+//   name  mesh  wlrg  wlls  symm  sbnd  nmed  smed  ndom  sdom  fdom  nsrc
+//   ssrc  quad  solv  crst  rcst  nfpl  exit
 //
 // plus two settings this build adds (the reference always computes in FP64):
 //
@@ -22,8 +22,10 @@
 // blank line after each row (write_data, aux.f90:192-211); `nfpl` writes the
 // field-component files of read_nfpl.
 //
-// Commands of the reference outside this path (symmetry groups other than
-// id, periodic Green's functions, volume domains, second-harmonic media,
+// Symmetry groups are products of id and the mirror groups mxp, myp, mzp
+// with the xplane / yplane / zplane boundaries of sbnd.  Commands of the
+// reference outside this path (rotation groups, periodic boundaries and
+// Green's functions, volume domains, second-harmonic media,
 // near fields, diffraction, polarizability, the VIE solver, source offsets
 // and scans) print an error and stop, as the reference does on invalid
 // input, instead of producing results this build does not compute.
@@ -192,7 +194,9 @@ struct State {
   mom_ctx *ctx = nullptr;
   bool uploaded = false;
   int64_t n2 = 0;                    // 2N unknowns
-  std::vector<std::vector<double>> x;  // per wavelength: [nsrc][2N] complex, interleaved
+  std::vector<std::string> symm;     // named groups of the symmetry group (read_symm)
+  int nga = 1;                       // its order
+  std::vector<std::vector<double>> x;  // per wavelength: [nsrc][nga][2N] complex, interleaved
 };
 
 void check(State &s, int st, const char *what) {
@@ -279,6 +283,14 @@ void solve_batch(State &s) {
   ensure_ctx(s);
   if (!s.uploaded) {
     check(s, mom_problem_upload(s.prob, s.ctx, s.quad.c_str()), "upload of the domains");
+    if (!s.symm.empty()) {
+      std::vector<int32_t> bnd(mom_problem_nedges(s.prob));
+      check(s, mom_problem_edge_bnd(s.prob, bnd.data()), "symm");
+      std::vector<const char *> names;
+      for (const auto &nm : s.symm) names.push_back(nm.c_str());
+      check(s, mom_gpu_set_symmetry(s.ctx, (int32_t)names.size(), names.data(), bnd.data()), "symm");
+    }
+    s.nga = mom_gpu_group_order(s.ctx);
     s.uploaded = true;
   }
   s.n2 = 2 * (int64_t)mom_problem_nedges(s.prob);
@@ -291,7 +303,7 @@ void solve_batch(State &s) {
     const std::vector<double> ri = ri_table(s, n);
     for (size_t d = 0; d < s.doms.size(); d++)
       std::printf(" Refractive index of domain %zu: (%6.3f,%6.3f)\n", d + 1, ri[2 * d], ri[2 * d + 1]);
-    s.x[n].assign((size_t)2 * s.n2 * nsrc, 0.0);
+    s.x[n].assign((size_t)2 * s.n2 * s.nga * nsrc, 0.0);
     int32_t iters = 0;
     check(s,
           mom_gpu_solve_wavelength(s.ctx, omega_of(s.wl[n]), ri.data(), nsrc, s.src.data(), s.precision, s.tol,
@@ -451,13 +463,47 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     for (int i = 0; i < n; i++) s.wl[i] = real_item(it, 2 + i, "wlls");
     s.x.clear();
   } else if (cmd == "symm") {
-    // read_symm (interface.f90:160-210): only the identity group is on this path
+    // read_symm (interface.f90:160-210): products of id and the mirror
+    // groups mxp, myp, mzp (the rotation groups rN are not supported)
     const int n = int_item(it, 1, "symm");
+    std::vector<std::string> names;
+    int order = 1;
     for (int i = 0; i < n; i++) {
       if (2 + i >= (int)it.size()) stop("Error: symm lists fewer groups than announced");
-      if (it[2 + i] != "id") stop("Error: symmetry group '" + it[2 + i] + "' is not supported by this build (only id)");
+      const std::string &g = it[2 + i];
+      if (g == "mxp" || g == "myp" || g == "mzp") {
+        order *= 2;
+      } else if (!g.empty() && g[0] == 'r') {
+        stop("Error: rotation symmetry group '" + g + "' is not supported by this build (id, mxp, myp, mzp)");
+      } else if (g != "id") {
+        std::printf(" Error: unrecognized group!\n");
+        return;
+      }
+      names.push_back(g);
     }
-    std::printf(" Created a symmetry group with 1 elements.\n");
+    if (order > MOM_MAX_GROUP) stop("Error: symmetry group too large");
+    s.symm = order > 1 ? names : std::vector<std::string>();
+    s.uploaded = false;
+    s.x.clear();
+    std::printf(" Created a symmetry group with %d elements.\n", order);
+  } else if (cmd == "sbnd") {
+    // read_sbnd (interface.f90:125-157) -> classify_edges (mesh.f90:155-175)
+    if (!s.prob) stop("Error: master mesh has not been loaded!");
+    const int id = int_item(it, 1, "sbnd");
+    if (it.size() < 3) stop("Error: sbnd needs an id and a boundary type");
+    const std::string &bn = it[2];
+    int bnd = 0;
+    if (bn == "xplane") bnd = MOM_BND_XPLANE;
+    else if (bn == "yplane") bnd = MOM_BND_YPLANE;
+    else if (bn == "zplane") bnd = MOM_BND_ZPLANE;
+    else if (bn == "prdx1" || bn == "prdx2" || bn == "prdy1" || bn == "prdy2" || bn == "rz1" || bn == "rz2")
+      stop("Error: boundary type '" + bn + "' is not supported by this build (xplane, yplane, zplane)");
+    else
+      stop("Unrecognized boundary type!");
+    int32_t cnt = 0;
+    check(s, mom_problem_classify_edges(s.prob, id, bnd, &cnt), "sbnd");
+    s.uploaded = false;
+    std::printf(" Classified %d boundary edges\n", cnt);
   } else if (cmd == "nmed") {
     // read_nmed (interface.f90:213-232)
     if (s.wl.empty()) {

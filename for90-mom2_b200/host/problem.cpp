@@ -117,6 +117,9 @@ void invert_faces(Mesh &m, int id) {
 struct mom_problem {
   Mesh master;
   bool have_mesh = false;
+  std::vector<int> line_node;  // [nlines][2] line elements of the mesh file (master node indices)
+  std::vector<int> line_id;    // [nlines] their physical ids
+  std::vector<int> edge_bnd;   // [master nedges] boundary type (classify_edges), MOM_BND_NONE by default
   std::vector<Mesh> dom;
   std::vector<char> dom_set;
   bool finalized = false;
@@ -150,6 +153,9 @@ int mom_problem_set_mesh(mom_problem *p, int32_t nnodes, const double *nodes, in
   build_edges(m, scale);
   p->master = std::move(m);
   p->have_mesh = true;
+  p->line_node.clear();
+  p->line_id.clear();
+  p->edge_bnd.assign(p->master.nedges, MOM_BND_NONE);
   p->dom.clear();
   p->dom_set.clear();
   p->finalized = false;
@@ -164,7 +170,7 @@ int mom_problem_load_gmsh(mom_problem *p, const char *path, double scale) {
   if (!in) return MOM_ERR_IO;
   std::string tok;
   std::vector<double> nodes;
-  std::vector<int> faces, ids;
+  std::vector<int> faces, ids, lines, line_ids;
   int nn = 0;
   bool have_nodes = false, have_elems = false;
   while (in >> tok) {
@@ -215,6 +221,14 @@ int mom_problem_load_gmsh(mom_problem *p, const char *path, double scale) {
           faces.push_back((int)b - 1);
           faces.push_back((int)c - 1);
           ids.push_back((int)tags[0]);
+        } else if (type == 1) {
+          // line elements: boundary curves that sbnd classifies (mesh.f90:680-684)
+          long a, b;
+          ls >> a >> b;
+          if (!ls || ntags < 1) return MOM_ERR_IO;
+          lines.push_back((int)a - 1);
+          lines.push_back((int)b - 1);
+          line_ids.push_back((int)tags[0]);
         }
       }
       in >> tok;
@@ -223,7 +237,50 @@ int mom_problem_load_gmsh(mom_problem *p, const char *path, double scale) {
     }
   }
   if (!have_nodes || !have_elems || ids.empty()) return MOM_ERR_IO;
-  return mom_problem_set_mesh(p, nn, nodes.data(), (int32_t)ids.size(), faces.data(), ids.data(), scale);
+  for (int v : lines)
+    if (v < 0 || v >= nn) return MOM_ERR_IO;
+  const int rc = mom_problem_set_mesh(p, nn, nodes.data(), (int32_t)ids.size(), faces.data(), ids.data(), scale);
+  if (rc != MOM_OK) return rc;
+  p->line_node = lines;
+  p->line_id = line_ids;
+  return MOM_OK;
+}
+
+int mom_problem_set_lines(mom_problem *p, int32_t nlines, const int32_t *line_nodes, const int32_t *line_ids) {
+  if (!p || !p->have_mesh) return MOM_ERR_STATE;
+  if (nlines < 0 || (nlines > 0 && (!line_nodes || !line_ids))) return MOM_ERR_ARG;
+  for (int i = 0; i < 2 * nlines; i++)
+    if (line_nodes[i] < 0 || line_nodes[i] >= p->master.nnodes) return MOM_ERR_MESH;
+  p->line_node.assign(line_nodes, line_nodes + 2 * (size_t)nlines);
+  p->line_id.assign(line_ids, line_ids + nlines);
+  return MOM_OK;
+}
+
+// classify_edges (mesh.f90:155-175): every master edge whose end nodes are
+// those of a line element with physical id `id` gets boundary type bnd.
+int mom_problem_classify_edges(mom_problem *p, int32_t id, int32_t bnd, int32_t *nclassified) {
+  if (!p || !p->have_mesh) return MOM_ERR_STATE;
+  if (bnd < MOM_BND_NONE || bnd > MOM_BND_ZPLANE) return MOM_ERR_ARG;
+  const Mesh &ms = p->master;
+  std::unordered_map<uint64_t, std::vector<int>> byedge;
+  for (size_t l = 0; l < p->line_id.size(); l++)
+    if (p->line_id[l] == id) byedge[pair_key(p->line_node[2 * l], p->line_node[2 * l + 1])].push_back((int)l);
+  int cnt = 0;
+  for (int e = 0; e < ms.nedges; e++) {
+    auto it = byedge.find(pair_key(ms.edge_node[2 * e], ms.edge_node[2 * e + 1]));
+    if (it == byedge.end()) continue;
+    p->edge_bnd[e] = bnd;
+    cnt += (int)it->second.size();  // the reference counts every matching line
+  }
+  if (nclassified) *nclassified = cnt;
+  return MOM_OK;
+}
+
+int mom_problem_edge_bnd(const mom_problem *p, int32_t *bnd) {
+  if (!p || !bnd) return MOM_ERR_ARG;
+  if (!p->have_mesh) return MOM_ERR_STATE;
+  std::copy(p->edge_bnd.begin(), p->edge_bnd.end(), bnd);
+  return MOM_OK;
 }
 
 int mom_problem_set_ndom(mom_problem *p, int32_t ndom) {

@@ -48,8 +48,13 @@ EXPORTS = [
     "mom_problem_nedges", "mom_problem_ndom", "mom_problem_domain", "mom_tri_rule", "mom_problem_upload",
     "mom_gpu_adjoint", "mom_gpu_adjoint_mean_eps", "mom_gpu_domain_nodes", "mom_problem_node_parent",
     "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement", "mom_gpu_scat_fields",
-    "mom_gpu_set_matrix", "mom_gpu_set_wait_limits",
+    "mom_gpu_set_matrix", "mom_gpu_set_wait_limits", "mom_gpu_set_symmetry", "mom_gpu_group_order",
+    "mom_problem_set_lines", "mom_problem_classify_edges", "mom_problem_edge_bnd",
 ]
+
+# Boundary types of mesh edges (sbnd; mesh.f90:16-25).
+BND_NONE, BND_XPLANE, BND_YPLANE, BND_ZPLANE = 1, 2, 3, 4
+BND_NAMES = {"xplane": BND_XPLANE, "yplane": BND_YPLANE, "zplane": BND_ZPLANE}
 
 
 class MomError(RuntimeError):
@@ -119,6 +124,11 @@ def lib():
     L.mom_gpu_device_matrix.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64)]
     L.mom_gpu_set_matrix.argtypes = [vp, C.c_int32, vp, C.c_int64]
     L.mom_gpu_set_wait_limits.argtypes = [vp, C.c_int64, C.c_int64, C.c_int64]
+    L.mom_gpu_set_symmetry.argtypes = [vp, C.c_int32, C.POINTER(C.c_char_p), ip]
+    L.mom_gpu_group_order.argtypes = [vp]
+    L.mom_problem_set_lines.argtypes = [vp, C.c_int32, ip, ip]
+    L.mom_problem_classify_edges.argtypes = [vp, C.c_int32, C.c_int32, ip]
+    L.mom_problem_edge_bnd.argtypes = [vp, ip]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
     L.mom_gpu_launch_count.argtypes = [vp]
@@ -241,6 +251,25 @@ class Problem:
         p.set_domains(domains)
         return p
 
+    def set_lines(self, line_nodes, line_ids):
+        """Line elements of the master mesh (0-based node pairs and physical ids)."""
+        ln = np.ascontiguousarray(np.asarray(line_nodes, dtype=np.int32).reshape(-1, 2))
+        li = np.ascontiguousarray(np.broadcast_to(np.asarray(line_ids, dtype=np.int32), (len(ln),)))
+        _check(lib().mom_problem_set_lines(self.h, len(ln), _ip(ln), _ip(li)), what="lines")
+
+    def classify_edges(self, line_id, bnd):
+        """sbnd: master edges on the lines of physical id line_id get boundary type
+        bnd ("xplane", "yplane", "zplane" or a BND_* value); returns the match count."""
+        b = BND_NAMES.get(bnd, bnd)
+        cnt = C.c_int32()
+        _check(lib().mom_problem_classify_edges(self.h, line_id, b, C.byref(cnt)), what="sbnd")
+        return cnt.value
+
+    def edge_bnd(self):
+        out = np.zeros(self.nedges, dtype=np.int32)
+        _check(lib().mom_problem_edge_bnd(self.h, _ip(out)), what="edge_bnd")
+        return out
+
     def set_domains(self, domains):
         L = lib()
         _check(L.mom_problem_set_ndom(self.h, len(domains)), what="ndom")
@@ -322,6 +351,7 @@ class Solver:
         self.h = h
         self.N = None
         self.ndom = None
+        self.nga = 1
 
     def close(self):
         if getattr(self, "h", None):
@@ -338,16 +368,34 @@ class Solver:
         self._ck(lib().mom_problem_upload(problem.h, self.h, quad.encode()), "set_problem")
         self.N = problem.nedges
         self.ndom = problem.ndom
+        self.nga = 1
+
+    def set_symmetry(self, names, problem: Problem):
+        """read_symm: the product of the named groups ("id", "mxp", "myp", "mzp") with the
+        boundary types of the problem's master edges (sbnd); returns the group order."""
+        arr = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+        bnd = problem.edge_bnd()
+        self._ck(lib().mom_gpu_set_symmetry(self.h, len(names), arr, _ip(bnd)), "set_symmetry")
+        self.nga = lib().mom_gpu_group_order(self.h)
+        return self.nga
+
+    def _cols(self, ns):
+        """Host array of solutions or right-hand sides: (2N, ns), or (2N, nga, ns) with a group."""
+        shape = (2 * self.N, ns) if self.nga == 1 else (2 * self.N, self.nga, ns)
+        return np.zeros(shape, dtype=np.complex128, order="F")
 
     def sysmat(self, omega, ri, precision=FP64, want_host=False):
-        """sysmat_pmchwt: build the 2N x 2N matrix on the device (optionally copy it back)."""
+        """sysmat_pmchwt: build the 2N x 2N matrix (one per representation) on the
+        device, optionally copied back: (2N, 2N), or (nga, 2N, 2N) with a group."""
         r = _ri(ri)
         if len(r) != 2 * self.ndom:
             raise ValueError("one refractive index per domain")
-        A = np.zeros((2 * self.N, 2 * self.N), dtype=np.complex128, order="F") if want_host else None
+        A = np.zeros((2 * self.N, 2 * self.N, self.nga), dtype=np.complex128, order="F") if want_host else None
         self._ck(lib().mom_gpu_sysmat(self.h, omega, _dp(r), precision, A.ctypes.data if A is not None else None,
                                       2 * self.N), "sysmat")
-        return A
+        if A is None:
+            return None
+        return A[:, :, 0] if self.nga == 1 else np.moveaxis(A, 2, 0)
 
     def set_matrix(self, A, precision=FP64):
         """A caller's 2N x 2N system matrix in place of sysmat (mom_gpu_set_matrix)."""
@@ -363,14 +411,14 @@ class Solver:
     def srcvec(self, omega, ri1, srcs, want_host=False):
         arr, ns = _srcs(srcs)
         r = _ri(ri1)
-        q = np.zeros((2 * self.N, ns), dtype=np.complex128, order="F") if want_host else None
+        q = self._cols(ns) if want_host else None
         self._ck(lib().mom_gpu_srcvec(self.h, omega, _dp(r), ns, arr, q.ctypes.data if q is not None else None,
                                       2 * self.N), "srcvec")
         self.nsrc = ns
         return q
 
     def solve(self, precision=FP64, tol=1e-12, maxit=30, want_host=True):
-        x = np.zeros((2 * self.N, self.nsrc), dtype=np.complex128, order="F") if want_host else None
+        x = self._cols(self.nsrc) if want_host else None
         it = C.c_int32()
         self._ck(lib().mom_gpu_solve(self.h, precision, tol, maxit, x.ctypes.data if x is not None else None,
                                      2 * self.N, C.byref(it)), "solve")
@@ -380,7 +428,7 @@ class Solver:
     def solve_wavelength(self, omega, ri, srcs, precision=FP64, tol=1e-12, maxit=30, want_host=True):
         arr, ns = _srcs(srcs)
         r = _ri(ri)
-        x = np.zeros((2 * self.N, ns), dtype=np.complex128, order="F") if want_host else None
+        x = self._cols(ns) if want_host else None
         it = C.c_int32()
         self._ck(lib().mom_gpu_solve_wavelength(self.h, omega, _dp(r), ns, arr, precision, tol, maxit,
                                                 x.ctypes.data if x is not None else None, 2 * self.N, C.byref(it)),
@@ -397,7 +445,7 @@ class Solver:
         cabs = np.zeros(ns)
         xp = None
         if x is not None:
-            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1, order="F"))
             xp = x.ctypes.data
         self._ck(lib().mom_gpu_cross_sections(self.h, dom, omega, _dp(r), ns, arr, xp, 2 * self.N, _dp(csca),
                                               _dp(cabs)), "cross_sections")
@@ -512,7 +560,7 @@ class Solver:
         pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
         xp = None
         if x is not None:
-            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1, order="F"))
             xp = x.ctypes.data
             ns = x.shape[1]
         else:
@@ -534,7 +582,7 @@ class Solver:
         out = np.zeros((ntheta, nphi), order="F")
         xp = None
         if x is not None:
-            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1))
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1, order="F"))
             xp = x.ctypes.data
         self._ck(lib().mom_gpu_rcs(self.h, dom, omega, _dp(r), isrc, xp, 2 * self.N, ntheta, nphi, _dp(out)), "rcs")
         return out

@@ -39,6 +39,15 @@ extern "C" {
 #define MOM_PREC_MIXED 1 /* FP32 far pairs + FP64 near pairs; FP32 LU with TF32
                             tensor-core trailing updates; FP64 refinement */
 
+/* Boundary types of mesh edges (mesh.f90:16-25): the symmetry planes. */
+#define MOM_BND_NONE 1
+#define MOM_BND_XPLANE 2
+#define MOM_BND_YPLANE 3
+#define MOM_BND_ZPLANE 4
+
+/* Largest symmetry group (three mirror planes). */
+#define MOM_MAX_GROUP 8
+
 /* Source types (source.f90:20-30). */
 #define MOM_SRC_PW 1
 #define MOM_SRC_PW_ELLIPTIC 10
@@ -84,10 +93,31 @@ const char *mom_gpu_last_error(mom_ctx *ctx);
 int mom_gpu_set_problem(mom_ctx *ctx, int32_t nedges_total, int32_t ndom, const mom_mesh *doms, int32_t nq,
                         const double *qw, const double *qnodes);
 
-/* Replaces sysmat_pmchwt (sysmat.f90:18-105) for the identity group: builds
- * the 2N x 2N PMCHWT matrix for angular frequency omega and one refractive
- * index per domain (ri[2*ndom], re/im).  The matrix stays on the device; if
- * A_host is not NULL it is also copied there (leading dimension lda >= 2N). */
+/* Symmetry group of the problem (read_symm, interface.f90:160-210, and the
+ * sbnd boundary classification, mesh.f90:155-175): the product of the named
+ * groups "id", "mxp", "myp", "mzp" (mirror planes x = 0, y = 0, z = 0;
+ * symmetry.f90:45-103, 178-241), nga = 2^(number of mirrors) elements and
+ * as many representations.  edge_bnd[N] holds the boundary type of every
+ * master edge (MOM_BND_*, from mom_problem_edge_bnd), which decides the
+ * symmetry-plane boundary conditions of each representation (edge_bc,
+ * bc.f90:28-117) and which group actions act on interior domains
+ * (admissible_ga, bc.f90:237-257).  Call after mom_gpu_set_problem (which
+ * resets the group to the identity).  With nga > 1, every matrix, right-hand
+ * side and solution exists once per representation: host arrays of
+ * solutions and right-hand sides are 2N x nga x nsrc (x(2N, nga, nsrc) of
+ * the reference, solver.f90:116), and sysmat's A_host receives nga
+ * consecutive 2N x 2N blocks.  Rotation groups (rN) are not supported. */
+int mom_gpu_set_symmetry(mom_ctx *ctx, int32_t nnames, const char *const *names, const int32_t *edge_bnd);
+/* Number of group elements (and representations) of the context, 1 for the
+ * identity, -1 without a problem. */
+int32_t mom_gpu_group_order(mom_ctx *ctx);
+
+/* Replaces sysmat_pmchwt (sysmat.f90:18-105): builds the 2N x 2N PMCHWT
+ * matrix of every representation (one for the identity group) for angular
+ * frequency omega and one refractive index per domain (ri[2*ndom], re/im).
+ * The matrices stay on the device; if A_host is not NULL they are also
+ * copied there (leading dimension lda >= 2N, representation r at
+ * A_host + 2 r lda 2N doubles). */
 int mom_gpu_sysmat(mom_ctx *ctx, double omega, const double *ri, int32_t precision, double *A_host, int64_t lda);
 
 /* Replaces srcvec (source.f90:136-247) for nsrc sources on domain 1's
@@ -272,6 +302,16 @@ int mom_problem_set_mesh(mom_problem *p, int32_t nnodes, const double *nodes, in
  * negative id inverts those faces (invert_faces, mesh.f90:278-288). */
 int mom_problem_set_ndom(mom_problem *p, int32_t ndom);
 int mom_problem_set_domain(mom_problem *p, int32_t dom, int32_t nsurf, const int32_t *surf_ids);
+/* Line elements of the master mesh (node pairs, 0-based, and physical ids),
+ * as load_mesh_gmsh keeps them for sbnd; set by mom_problem_load_gmsh from
+ * the file's type-1 elements. */
+int mom_problem_set_lines(mom_problem *p, int32_t nlines, const int32_t *line_nodes, const int32_t *line_ids);
+/* read_sbnd / classify_edges (interface.f90:125-157, mesh.f90:155-175):
+ * master edges that coincide with a line of physical id `id` get boundary
+ * type bnd (MOM_BND_*); *nclassified (may be NULL) = number of matches. */
+int mom_problem_classify_edges(mom_problem *p, int32_t id, int32_t bnd, int32_t *nclassified);
+/* Boundary type of every master edge: bnd[N]. */
+int mom_problem_edge_bnd(const mom_problem *p, int32_t *bnd);
 /* read_fdom (interface.f90:107-123): submesh_edge_connectivity +
  * orient_basis. */
 int mom_problem_finalize(mom_problem *p);

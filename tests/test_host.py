@@ -119,3 +119,40 @@ def test_bench_reference_arm_json():
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "solves/s"
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_sbnd_classifies_plane_edges(built, tmp_path):
+    """sbnd / classify_edges on the host: line elements read from a Gmsh file
+    (type 1, physical id as the first tag) mark the master edges they cover;
+    edges elsewhere stay MOM_BND_NONE."""
+    nodes, faces = meshgen.octasphere(2, 50.0)
+    fn, ff, lines = meshgen.symmetry_fragment(nodes, faces, [0, 1])
+    path = tmp_path / "quarter.msh"
+    with open(path, "w") as fh:
+        fh.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(fn))
+        for i, p in enumerate(fn):
+            fh.write("%d %.17g %.17g %.17g\n" % (i + 1, p[0], p[1], p[2]))
+        ne = len(lines[0]) + len(lines[1]) + len(ff)
+        fh.write("$EndNodes\n$Elements\n%d\n" % ne)
+        k = 1
+        for ax, pid in ((0, 21), (1, 22)):
+            for a, b in lines[ax]:
+                fh.write("%d 1 2 %d %d %d %d\n" % (k, pid, pid, a + 1, b + 1))
+                k += 1
+        for f in ff:
+            fh.write("%d 2 2 1 1 %d %d %d\n" % (k, f[0] + 1, f[1] + 1, f[2] + 1))
+            k += 1
+        fh.write("$EndElements\n")
+    P = M.Problem.from_gmsh(str(path), 1e-9, [[1], [-1]])
+    assert P.classify_edges(21, "xplane") == len(lines[0])
+    assert P.classify_edges(22, "yplane") == len(lines[1])
+    assert P.classify_edges(99, "zplane") == 0
+    bnd = P.edge_bnd()
+    assert np.count_nonzero(bnd == M.BND_XPLANE) == len(lines[0])
+    assert np.count_nonzero(bnd == M.BND_YPLANE) == len(lines[1])
+    assert np.count_nonzero(bnd == M.BND_NONE) == len(bnd) - len(lines[0]) - len(lines[1])
+    # the same through line arrays
+    Q = M.Problem.from_arrays(fn, ff, np.ones(len(ff), int), 1e-9, [[1], [-1]])
+    Q.set_lines(np.asarray(lines[0]), 21)
+    assert Q.classify_edges(21, M.BND_XPLANE) == len(lines[0])
+    assert np.array_equal(Q.edge_bnd() == M.BND_XPLANE, bnd == M.BND_XPLANE)

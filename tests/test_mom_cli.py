@@ -63,12 +63,22 @@ def test_unknown_command_is_reported_and_skipped(workdir):
 
 
 @pytest.mark.parametrize("line,msg", [
-    ("symm 1 mxp", "symmetry group 'mxp'"),
+    ("symm 1 r4", "rotation symmetry group 'r4'"),
     ("nfms 1 2 3", "outside the linear PMCHWT path"),
 ])
 def test_input_outside_the_path_stops(workdir, line, msg):
     r = run(line + "\nexit\n", workdir)
     assert r.returncode == 1 and msg in r.stdout
+
+
+def test_mirror_groups_and_sbnd_are_accepted(workdir):
+    """symm with mirror groups and sbnd run on the host (the reference's console lines)."""
+    r = run("symm 3 mxp myp id\nmesh 'ico3.msh' 1d-9\nsbnd 7 xplane\nexit\n", workdir)
+    assert r.returncode == 0, r.stdout
+    assert "Created a symmetry group with 4 elements." in r.stdout
+    assert "Classified 0 boundary edges" in r.stdout
+    r = run("mesh 'ico3.msh' 1d-9\nsbnd 7 prdx1\nexit\n", workdir)
+    assert r.returncode == 1 and "boundary type 'prdx1'" in r.stdout
 
 
 def test_periodic_green_function_stops(workdir):
