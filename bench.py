@@ -705,6 +705,36 @@ def bench_adjoint(M, dev):
     return out
 
 
+def run_kernel_cases(subdiv):
+    """One pass over the kernels outside the LU on the icosphere of `subdiv`
+    (default 3: 1280 faces, 3840 unknowns; the matrix and the face-pair
+    buffer exceed L2), for per-kernel profiling captures: FP64 assembly
+    (pair_kernel<double>, near_kernel, gather_kernel), srcvec, cs_prtsrf,
+    the 91 x 180 far field, a 41 x 41 near-field plane, the FP64 eps adjoint
+    (adj_pair_kernel), then the mixed solve (pair_kernel<float>, the FP64
+    refinement residual gemv_partial_kernel)."""
+    import numpy as np
+    import mom_b200 as M
+    nodes, faces, ids, doms = make_problem(M, subdiv)
+    S = M.Solver(0)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(EPS_IN)]
+    src = [M.src_pw(0, 90, 0)]
+    S.solve_wavelength(om, ri, src, M.FP64, want_host=False)
+    a, b = S.cross_sections(om, ri[0], src)
+    S.rcs(om, ri[0], 91, 180)
+    g = np.linspace(-100e-9, 100e-9, 41)
+    pts = np.stack(np.meshgrid(g, [0.0], g, indexing="ij"), axis=-1).reshape(-1, 3)
+    S.scat_fields(om, 1.0, pts, srcs=src, dom=0)
+    S.adjoint(om, ri, src, M.FP64, eps_dom=1)
+    S.solve_wavelength(om, ri, src, M.MIXED, TOL, MAXIT, want_host=False)
+    S.synchronize()
+    S.close()
+    print(json.dumps({"kernel_cases": workload_name(subdiv), "sigma_ext_fp64": float(a[0] + b[0])}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -717,8 +747,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-extras", action="store_true", help="skip the sweep and adjoint side measurements")
     ap.add_argument("--sweep-workers", type=int, default=6, help="concurrent contexts per sweep mesh")
+    ap.add_argument("--kernels", action="store_true",
+                    help="run the non-LU kernels once on the --subdiv sphere (for profiling captures), no timing")
     args = ap.parse_args()
     rank, local_rank, world = dist_env()
+    if args.kernels:
+        return run_kernel_cases(args.subdiv)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, local_rank, world)

@@ -25,7 +25,7 @@ int cuda_fail(Ctx *c, cudaError_t e, const char *where) {
   return fail(c, MOM_ERR_CUDA, std::string(cudaGetErrorString(e)) + " in " + where);
 }
 
-ProfScope::ProfScope(Ctx *c_, int cat_) : c(c_), cat(cat_) {
+ProfScope::ProfScope(Ctx *c_, int cat_, cudaStream_t s_) : c(c_), cat(cat_), s(s_ ? s_ : c_->stream) {
   if (!c->prof) return;
   if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
     cudaGetLastError();
@@ -33,18 +33,18 @@ ProfScope::ProfScope(Ctx *c_, int cat_) : c(c_), cat(cat_) {
     return;
   }
   // Inside a capture the records become event nodes of the graph.
-  if (c->capturing) cudaEventRecordWithFlags(a, c->stream, cudaEventRecordExternal);
-  else cudaEventRecord(a, c->stream);
+  if (c->capturing) cudaEventRecordWithFlags(a, s, cudaEventRecordExternal);
+  else cudaEventRecord(a, s);
 }
 
 ProfScope::~ProfScope() {
   if (!a) return;
   if (c->capturing) {
-    cudaEventRecordWithFlags(b, c->stream, cudaEventRecordExternal);
+    cudaEventRecordWithFlags(b, s, cudaEventRecordExternal);
     c->cap_ev.emplace_back(cat, a, b);
     return;
   }
-  cudaEventRecord(b, c->stream);
+  cudaEventRecord(b, s);
   c->prof_ev[cat].push_back({a, b});
   c->prof_launch[cat]++;
 }
@@ -398,13 +398,25 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
     delete c;
     return MOM_ERR_CUDA;
   }
-  // A fixed cuBLAS workspace (no allocation inside the captured LU graph).
-  if (cudaMalloc(&c->blas_ws, kBlasWorkspace) != cudaSuccess ||
-      cublasSetWorkspace(c->blas, c->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS || lu_init_kernels(c) != MOM_OK ||
-      tc_init_kernels(c) != MOM_OK) {
+  // A fixed cuBLAS workspace (no allocation inside the captured LU graph);
+  // the look-ahead stream has its own handle and workspace.
+  bool ok = cudaMalloc(&c->blas_ws, kBlasWorkspace) == cudaSuccess &&
+            cublasSetWorkspace(c->blas, c->blas_ws, kBlasWorkspace) == CUBLAS_STATUS_SUCCESS &&
+            cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) == cudaSuccess &&
+            cublasCreate(&c->blas2) == CUBLAS_STATUS_SUCCESS &&
+            cublasSetStream(c->blas2, c->stream2) == CUBLAS_STATUS_SUCCESS &&
+            cudaMalloc(&c->blas_ws2, kBlasWorkspace) == cudaSuccess &&
+            cublasSetWorkspace(c->blas2, c->blas_ws2, kBlasWorkspace) == CUBLAS_STATUS_SUCCESS;
+  for (int i = 0; ok && i < 3; i++) ok = cudaEventCreateWithFlags(&c->la_ev[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok || lu_init_kernels(c) != MOM_OK || tc_init_kernels(c) != MOM_OK) {
     cudaGetLastError();
     cublasDestroy(c->blas);
+    if (c->blas2) cublasDestroy(c->blas2);
     cudaFree(c->blas_ws);
+    cudaFree(c->blas_ws2);
+    for (auto &e : c->la_ev)
+      if (e) cudaEventDestroy(e);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     cudaStreamDestroy(c->stream);
     delete c;
     return MOM_ERR_CUDA;
@@ -419,6 +431,12 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (eo) c->outer_panels = std::max(1, std::min(16, std::atoi(eo)));
   const char *ep = std::getenv("MOM_PANEL_CTAS");
   if (ep) c->panel_cap_env = std::max(0, std::atoi(ep));
+  const char *el = std::getenv("MOM_LOOKAHEAD");
+  if (el) c->lookahead = el[0] != '0';
+  const char *ec = std::getenv("MOM_LA_CTAS");
+  if (ec) c->la_ctas = std::max(0, std::atoi(ec));
+  const char *ef = std::getenv("MOM_LA_FROM");
+  if (ef) c->la_from = std::atof(ef);
   *out = c;
   return MOM_OK;
 }
@@ -443,7 +461,11 @@ void mom_gpu_destroy(mom_ctx *c) {
   }
   c->lu_graphs.clear();
   cublasDestroy(c->blas);
+  cublasDestroy(c->blas2);
   cudaFree(c->blas_ws);
+  cudaFree(c->blas_ws2);
+  for (auto &e : c->la_ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->stream2);
   cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -550,6 +550,61 @@ __global__ void laswp_kernel(T *A, int64_t lda, int64_t n, int64_t j0, int nb, c
   }
 }
 
+// The same interchanges on the columns [c0, c0 + ncols) outside the panel
+// [j0, j0 + nb): one warp per column.
+template <typename T>
+__global__ void laswp_range_kernel(T *A, int64_t lda, int64_t c0, int64_t ncols, int64_t j0, int nb, const int *dst,
+                                   const int *src, const int *count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t idx = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (idx >= ncols) return;
+  const int64_t col = c0 + idx;
+  if (col >= j0 && col < j0 + nb) return;
+  const int k = *count;
+  T *a = A + col * lda;
+  T v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = lane + 32 * q;
+    if (i < k) v[q] = a[src[i]];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = lane + 32 * q;
+    if (i < k) a[dst[i]] = v[q];
+  }
+}
+
+// The interchanges of the np panels of an outer block [J0, J0 + NBc), in
+// panel order, on every column outside that block: one warp per column,
+// maps at pm + 260 p (dst[128], src[128], count).
+template <typename T>
+__global__ void laswp_block_kernel(T *A, int64_t lda, int64_t n, int64_t J0, int64_t NBc, const int *pm, int np) {
+  const int lane = threadIdx.x & 31;
+  int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (col >= n - NBc) return;
+  if (col >= J0) col += NBc;
+  T *a = A + col * lda;
+  for (int p = 0; p < np; p++) {
+    const int *dst = pm + 260 * p, *src = dst + 128;
+    const int k = dst[256];
+    T v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = lane + 32 * q;
+      if (i < k) v[q] = a[src[i]];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = lane + 32 * q;
+      if (i < k) a[dst[i]] = v[q];
+    }
+    __syncwarp();
+  }
+}
+
 // Inverses of the unit-lower L11 and upper U11 diagonal blocks of a panel
 // (FP64), stored as inv[0] = inv(L11), inv[1] = inv(U11), column-major
 // 64 x 64.  One CTA of 512 threads (256 per triangle), all in shared memory,
@@ -1179,6 +1234,8 @@ struct LuWork {
   float2 *invL32;  // nb x nb
   float *tcw;      // tensor-core GEMM operands (mixed path)
   int *pmap;       // [257]: composed panel permutation (dst[128], src[128], count)
+  int *pmb;        // [2][16][260]: the composed permutations of every panel of an outer block, double-buffered
+  void *W2;        // nb x 16 nb workspace of the look-ahead stream's block TRSM
 };
 
 // The panel kernel's exchange buffers (records polled by every CTA once per
@@ -1206,6 +1263,8 @@ int lu_workspace(Ctx *c, int precision, LuWork &w, int slot = -1) {
   const size_t o_w = take(esz * (size_t)nb * c->n);
   const size_t o_i32 = take(sizeof(float2) * (size_t)nb * c->n);
   const size_t o_pm = take(sizeof(int) * 260);
+  const size_t o_pmb = take(sizeof(int) * 260 * 2 * 16);
+  const size_t o_w2 = take(esz * (size_t)nb * 16 * nb);
   const size_t o_tc =
       take(precision == MOM_PREC_MIXED ? tc_cgemm_work_bytes((int)c->n, (int)c->n, c->outer_panels * nb) : 0);
   MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, off));
@@ -1220,6 +1279,8 @@ int lu_workspace(Ctx *c, int precision, LuWork &w, int slot = -1) {
   w.invL32 = (float2 *)(b + o_i32);
   w.tcw = (float *)(b + o_tc);
   w.pmap = (int *)(b + o_pm);
+  w.pmb = (int *)(b + o_pmb);
+  w.W2 = (void *)(b + o_w2);
   return MOM_OK;
 }
 
@@ -1255,7 +1316,9 @@ int panel_ctas(const Ctx *c, int64_t m) {
 
 // One panel (rows j0 .. n of columns j0 .. j0+nb) on P CTAs.
 template <typename T>
-int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *ipiv, int *info, const LuWork &w) {
+int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *ipiv, int *info, const LuWork &w,
+                 cudaStream_t st = nullptr) {
+  if (!st) st = c->stream;
   const int nb = c->nb;
   const int64_t m = n - j0;
   if (c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster) {
@@ -1282,7 +1345,7 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
     cfg.gridDim = dim3(CL);
     cfg.blockDim = dim3(kPanelThreads);
     cfg.dynamicSmemBytes = sizeof(double2) * ((size_t)nb * rpc + (size_t)2 * CL * nb + 2 * nb);
-    cfg.stream = c->stream;
+    cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = CL;
@@ -1314,10 +1377,9 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
   pa.rec = w.rec;
   pa.cand_data = w.cand_data;
   pa.col_data = w.col_data;
-  MOM_CUDA(c, cudaMemsetAsync(w.rec, 0, sizeof(unsigned long long) * 2 * P, c->stream));
+  MOM_CUDA(c, cudaMemsetAsync(w.rec, 0, sizeof(unsigned long long) * 2 * P, st));
   void *args[] = {&pa};
-  MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem,
-                                          c->stream));
+  MOM_CUDA(c, cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(P), dim3(kPanelThreads), args, smem, st));
   c->launches++;
   return MOM_OK;
 }
@@ -1447,6 +1509,170 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
   return MOM_OK;
 }
 
+// The mixed-precision factorisation with look-ahead.  Right-looking over
+// outer blocks of NB = outer_panels * 64 columns as lu_enqueue, reordered so
+// that the next outer block is factored on the second stream while the
+// trailing update of the current one runs:
+//   stream 1: J's interchanges on every column outside J; the block-row
+//             TRSM and update of J on the next block's columns (L), then
+//             record eL; the same on the rest (R), its tensor-core GEMM on
+//             fewer SMs; then wait for eF;
+//   stream 2: wait eL; factor block J+1 (panels, interchanges inside the
+//             block only, diagonal inverses, in-block TRSM and updates on its
+//             own cuBLAS handle); record eF.
+// Interchanges commute with the row-wise trailing update, so applying a
+// block's interchanges to the columns outside it after its factorisation
+// (instead of panel by panel) gives the same factors; the columns left of
+// the block are swapped at the same time (they hold L of earlier blocks,
+// which nothing reads any more).  Blocks taller than la_from * n run without
+// the overlap (the panel would take too many SMs from the larger GEMM).
+template <typename T>
+int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
+  const int64_t n = c->n, lda = c->lda;
+  const int nb = c->nb;
+  const int NB = c->outer_panels * nb;
+  cudaStream_t sa = c->stream, sb = c->stream2;
+  if (sizeof(T) != sizeof(float2)) return fail(c, MOM_ERR_ARG, "the look-ahead schedule serves the mixed path");
+  MOM_CUDA(c, cudaMemsetAsync(c->dinfo, 0, sizeof(int) * 4, sa));
+  MOM_BLAS(c, cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+  MOM_BLAS(c, cublasSetMathMode(c->blas2, CUBLAS_DEFAULT_MATH));
+  auto gemm = [&](cublasHandle_t h, int64_t m, int64_t ncol, int64_t k, float alpha, const T *Am, int64_t la,
+                  const T *Bm, int64_t lb, float beta, T *Cm, int64_t lc) -> int {
+    if (m <= 0 || ncol <= 0 || k <= 0) return MOM_OK;
+    c->blas_calls++;
+    const cuComplex al = make_cuComplex(alpha, 0), be = make_cuComplex(beta, 0);
+    MOM_BLAS(c, cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)ncol, (int)k, &al, (const cuComplex *)Am, (int)la,
+                            (const cuComplex *)Bm, (int)lb, &be, (cuComplex *)Cm, (int)lc));
+    return MOM_OK;
+  };
+  // B(nb x ncol at rows j0, columns col) <- inv(L_jj) B through the workspace Wk
+  auto trsm_l = [&](cublasHandle_t h, cudaStream_t st, T *Wk, int64_t j0, int64_t col, int64_t ncol) -> int {
+    if (ncol <= 0) return MOM_OK;
+    const T *inv = (const T *)(w.invL32 + (size_t)(j0 / nb) * nb * nb);
+    T *B = A + j0 + col * lda;
+    MOM_TRY(gemm(h, nb, ncol, nb, 1.0f, inv, nb, B, lda, 0.0f, Wk, nb));
+    MOM_CUDA(c, cudaMemcpy2DAsync(B, sizeof(T) * lda, Wk, sizeof(T) * nb, sizeof(T) * nb, ncol, cudaMemcpyDeviceToDevice,
+                                  st));
+    return MOM_OK;
+  };
+  // factor the outer block at J0 on stream st (panel CTAs capped at pcap > 0)
+  auto factor_block = [&](int64_t J0, cudaStream_t st, cublasHandle_t h, int *pm, int pcap) -> int {
+    const int64_t NBc = std::min<int64_t>(NB, n - J0);
+    for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
+      const int p = (int)((j0 - J0) / nb), kb = (int)(j0 / nb);
+      const int64_t m = n - j0;
+      int P = panel_ctas(c, m);
+      if (pcap > 0) P = (int)std::max<int64_t>(std::min(P, pcap), (m + 207) / 208);
+      {
+        ProfScope ps(c, kProfPanel, st);
+        MOM_TRY(launch_panel<T>(c, A, lda, n, j0, P, c->ipiv, w.info, w, st));
+      }
+      {
+        ProfScope pz(c, kProfPivotAux, st);
+        int *mp = pm + 260 * p;
+        pivot_map_kernel<<<1, 32, 0, st>>>(c->ipiv, j0, nb, mp, mp + 128, mp + 256);
+        if (NBc > nb)
+          laswp_range_kernel<T><<<(unsigned)((NBc * 32 + 255) / 256), 256, 0, st>>>(A, lda, J0, NBc, j0, nb, mp,
+                                                                                      mp + 128, mp + 256);
+        c->launches += NBc > nb ? 2 : 1;
+      }
+      {
+        ProfScope pd(c, kProfDiagInv, st);
+        diag_inv_kernel<T, 0><<<1, kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), st>>>(A, lda, kb, c->invd,
+                                                                                              w.invL32);
+        c->launches++;
+        MOM_CUDA(c, cudaGetLastError());
+      }
+      const int64_t rest = J0 + NBc - (j0 + nb);
+      if (rest > 0) {
+        ProfScope pg(c, kProfGemm, st);
+        MOM_TRY(trsm_l(h, st, (T *)w.W2, j0, j0 + nb, rest));
+        MOM_TRY(gemm(h, n - j0 - nb, rest, nb, -1.0f, A + (j0 + nb) + j0 * lda, lda, A + j0 + (j0 + nb) * lda, lda,
+                     1.0f, A + (j0 + nb) + (j0 + nb) * lda, lda));
+      }
+    }
+    return MOM_OK;
+  };
+  // trailing update of block J0 on columns [c0, c0 + ncol), stream 1
+  auto trailing = [&](int64_t J0, int64_t c0, int64_t ncol, int gemm_ctas) -> int {
+    if (ncol <= 0) return MOM_OK;
+    const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc;
+    ProfScope pg(c, kProfGemm);
+    for (int64_t j0 = J0; j0 < t0; j0 += nb) {
+      MOM_TRY(trsm_l(c->blas, sa, (T *)w.W, j0, c0, ncol));
+      const int64_t below = t0 - (j0 + nb);
+      MOM_TRY(gemm(c->blas, below, ncol, nb, -1.0f, A + (j0 + nb) + j0 * lda, lda, A + j0 + c0 * lda, lda, 1.0f,
+                   A + (j0 + nb) + c0 * lda, lda));
+    }
+    MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(A + t0 + c0 * lda), lda,
+                            reinterpret_cast<const float2 *>(A + t0 + J0 * lda), lda,
+                            reinterpret_cast<const float2 *>(A + J0 + c0 * lda), lda, (int)(n - t0), (int)ncol,
+                            (int)NBc, w.tcw, c->dinfo + 2, gemm_ctas));
+    return MOM_OK;
+  };
+  // stream 2 joins the stream (and any capture open on it)
+  MOM_CUDA(c, cudaEventRecord(c->la_ev[0], sa));
+  MOM_CUDA(c, cudaStreamWaitEvent(sb, c->la_ev[0], 0));
+  MOM_TRY(factor_block(0, sa, c->blas, w.pmb, 0));
+  for (int64_t J0 = 0; J0 < n; J0 += NB) {
+    const int J = (int)(J0 / NB);
+    const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc, nc = n - t0;
+    int *pmJ = w.pmb + 260 * 16 * (J & 1), *pmN = w.pmb + 260 * 16 * ((J + 1) & 1);
+    {
+      ProfScope pz(c, kProfPivotAux);
+      if (n > NBc) {
+        laswp_block_kernel<T><<<(unsigned)(((n - NBc) * 32 + 255) / 256), 256, 0, sa>>>(A, lda, n, J0, NBc, pmJ,
+                                                                                         (int)(NBc / nb));
+        c->launches++;
+      }
+    }
+    if (nc <= 0) break;
+    const int64_t L = std::min<int64_t>(NB, nc);
+    MOM_TRY(trailing(J0, t0, L, 0));
+    const bool overlap = (double)nc < c->la_from * (double)n && nc > L;
+    if (overlap) {
+      // panel CTAs of the next block (the tallest of its panels), the GEMM gets the rest
+      int P = panel_ctas(c, nc);
+      const int pcap = c->la_ctas > 0 ? c->la_ctas : 1;
+      P = (int)std::max<int64_t>(std::min(P, pcap), (nc + 207) / 208);
+      if (c->panel_cluster > 0 && nc <= (int64_t)kClusterRows * c->panel_cluster) P = c->panel_cluster;
+      MOM_CUDA(c, cudaEventRecord(c->la_ev[1], sa));
+      MOM_CUDA(c, cudaStreamWaitEvent(sb, c->la_ev[1], 0));
+      MOM_TRY(factor_block(t0, sb, c->blas2, pmN, pcap));
+      MOM_CUDA(c, cudaEventRecord(c->la_ev[2], sb));
+      MOM_TRY(trailing(J0, t0 + L, nc - L, std::max(8, c->nsm - P)));
+      MOM_CUDA(c, cudaStreamWaitEvent(sa, c->la_ev[2], 0));
+    } else {
+      MOM_TRY(trailing(J0, t0 + L, nc - L, 0));
+      MOM_TRY(factor_block(t0, sa, c->blas, pmN, 0));
+    }
+  }
+  // stream 2 rejoins stream 1 (closes any capture branch it holds)
+  MOM_CUDA(c, cudaEventRecord(c->la_ev[2], sb));
+  MOM_CUDA(c, cudaStreamWaitEvent(sa, c->la_ev[2], 0));
+  {
+    ProfScope pd(c, kProfDiagInv);
+    diag_inv_kernel<T, 1><<<(unsigned)(n / nb), kDiagThreads, sizeof(double2) * (3 * nb * nb + nb), sa>>>(
+        A, lda, 0, c->invd, nullptr);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+    inv_to_fp32_kernel<<<c->nsm * 4, 256, 0, sa>>>(c->invd, c->inv32, 2 * (int64_t)nb * n);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  compose_pivots_kernel<<<1, 256, sizeof(int) * n, sa>>>(c->ipiv, (int)n, c->perm);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
+  return MOM_OK;
+}
+
+// The look-ahead schedule serves the mixed path (tensor-core trailing
+// updates) with at least two outer blocks.
+bool use_lookahead(const Ctx *c, int precision) {
+  return c->lookahead && precision == MOM_PREC_MIXED && !c->small_tc && c->outer_panels <= 16 &&
+         c->n > 2 * (int64_t)c->outer_panels * c->nb;
+}
+
 // Captures the factorisation of this precision into g (replacing what g held).
 template <typename T>
 int lu_capture(Ctx *c, T *A, int precision, const LuWork &w, Ctx::LuGraph &g, const std::vector<uintptr_t> &key) {
@@ -1455,7 +1681,7 @@ int lu_capture(Ctx *c, T *A, int precision, const LuWork &w, Ctx::LuGraph &g, co
   const double f0 = c->tc_flops;
   MOM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   c->capturing = true;
-  const int st = lu_enqueue<T>(c, A, precision, w);
+  const int st = use_lookahead(c, precision) ? lu_enqueue_la<T>(c, A, w) : lu_enqueue<T>(c, A, precision, w);
   c->capturing = false;
   cudaGraph_t graph = nullptr;
   const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
@@ -1501,7 +1727,9 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)c->ipiv,   (uintptr_t)c->invd,  (uintptr_t)c->perm,
                                         (uintptr_t)c->dinfo,  (uintptr_t)c->nsm,   (uintptr_t)c->prof,
                                         (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32,
-                                        (uintptr_t)wait_polls(c, 0), (uintptr_t)wait_polls(c, 1)};
+                                        (uintptr_t)wait_polls(c, 0), (uintptr_t)wait_polls(c, 1),
+                                        (uintptr_t)use_lookahead(c, precision), (uintptr_t)c->la_ctas,
+                                        (uintptr_t)(c->la_from * 1e6)};
     for (Ctx::LuGraph *h : c->lu_graphs)
       if (h->exec && h->key == key) g = h;
     if (!g) {
@@ -1525,7 +1753,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
     c->blas_calls += g->blas_calls;
     c->tc_flops += g->tc_flops;
   } else {
-    MOM_TRY(lu_enqueue<T>(c, A, precision, w));
+    MOM_TRY(use_lookahead(c, precision) ? lu_enqueue_la<T>(c, A, w) : lu_enqueue<T>(c, A, precision, w));
   }
   int hinfo[3] = {0, 0, 0};
   MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));

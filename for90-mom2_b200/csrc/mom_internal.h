@@ -107,6 +107,16 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   cublasHandle_t blas = nullptr;
   void *blas_ws = nullptr;  // fixed cuBLAS workspace
+  // Look-ahead of the LU: the next outer block is factored on a second stream
+  // (with its own cuBLAS handle and workspace) while the trailing update of
+  // the current one runs on `stream`.
+  cudaStream_t stream2 = nullptr;
+  cublasHandle_t blas2 = nullptr;
+  void *blas_ws2 = nullptr;
+  cudaEvent_t la_ev[3] = {nullptr, nullptr, nullptr};
+  int lookahead = 1;       // MOM_LOOKAHEAD=0 turns it off
+  int la_ctas = 0;         // MOM_LA_CTAS: CTA cap of the look-ahead panels (0: the smallest that fits)
+  double la_from = 0.9;    // MOM_LA_FROM: overlap blocks whose height is below this fraction of n
   std::mutex mu;
   std::string last_error;
   int64_t launches = 0;
@@ -247,12 +257,14 @@ enum ProfCat {
   kProfCount
 };
 
-// Records start/end events around a launch when profiling is on.
+// Records start/end events around a launch when profiling is on (on the
+// context stream, or on the stream given).
 struct ProfScope {
   struct Ctx *c;
   int cat;
+  cudaStream_t s;
   cudaEvent_t a = nullptr, b = nullptr;
-  ProfScope(struct Ctx *c_, int cat_);
+  ProfScope(struct Ctx *c_, int cat_, cudaStream_t s_ = nullptr);
   ~ProfScope();
 };
 
@@ -312,7 +324,7 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
 
 // tc_gemm.cu: C -= L U (complex FP32) on the tensor cores, 3xTF32
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
-                    int nc, int k, float *work, int *err);
+                    int nc, int k, float *work, int *err, int max_ctas = 0);
 size_t tc_cgemm_work_bytes(int m, int nc, int k);
 int tc_init_kernels(Ctx *c);
 

@@ -357,9 +357,10 @@ int make_map(Ctx *c, CUtensorMap *m, const float *base, int64_t rows, int64_t co
 
 // C (m x nc complex FP32, ldc) -= L (m x k, ldl) * U (k x nc, ldu) with the
 // 3xTF32 tensor-core kernel.  m must be a multiple of 64, k of 16.
-// work: >= (4 m k + 4 k nc) * 4 bytes of device scratch.
+// work: >= (4 m k + 4 k nc) * 4 bytes of device scratch.  max_ctas > 0
+// caps the persistent grid.
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
-                    int nc, int k, float *work, int *err) {
+                    int nc, int k, float *work, int *err, int max_ctas) {
   if (m <= 0 || nc <= 0 || k <= 0) return MOM_OK;
   if ((2 * m) % kBM != 0 || (2 * k) % kBK != 0) return fail(c, MOM_ERR_ARG, "tc_cgemm_update: unsupported shape");
   const int Mr = 2 * m, Kr = 2 * k;
@@ -381,7 +382,10 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   ta.err = err;
   ta.spin = wait_polls(c, 1);
   const int ntiles = (Mr / kBM) * ((nc + kBN - 1) / kBN);
-  const int grid = ntiles < c->nsm ? ntiles : c->nsm;
+  // persistent: one CTA per SM, or fewer when another kernel (the look-ahead
+  // panel) is to run beside it
+  const int cap = (max_ctas > 0 && max_ctas < c->nsm) ? max_ctas : c->nsm;
+  const int grid = ntiles < cap ? ntiles : cap;
   const size_t smem = (size_t)kStages * kStageBytes + 1024;
   {
     ProfScope ps(c, kProfTc);
