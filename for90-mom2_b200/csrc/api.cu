@@ -917,6 +917,50 @@ int mom_gpu_set_matrix(mom_ctx *c, int32_t precision, const double *A_host, int6
   return MOM_OK;
 }
 
+int mom_gpu_surface_fields(mom_ctx *c, int32_t dom, double omega, const double *ri, int32_t isrc, const double *x_host,
+                           int64_t ldx, double *e, double *h) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (dom < 0 || dom >= c->ndom || !ri || !e || !h || isrc < 0 || !(omega > 0))
+    return fail(c, MOM_ERR_ARG, "invalid surface-field arguments");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  const size_t fbytes = ((sizeof(double2) * 3 * (size_t)c->dom[dom].F * c->nga + 255) / 256) * 256;
+  const size_t xbytes = x_host ? sizeof(double2) * (size_t)c->n * c->nga : 0;
+  MOM_TRY(ensure_buffer(c, &c->nf_buf, &c->nf_cap, 2 * fbytes + xbytes + 256));
+  char *b = (char *)c->nf_buf;
+  double2 *dE = (double2 *)b, *dH = (double2 *)(b + fbytes);
+  const double2 *xd;
+  int64_t xrep;
+  if (x_host) {
+    if (ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+    double2 *xh = (double2 *)(b + 2 * fbytes);
+    MOM_TRY(copy_block_to_device(c, x_host + 2 * (size_t)isrc * c->nga * ldx, ldx, 1, xh));
+    xd = xh;
+    xrep = c->n;
+  } else {
+    if (isrc >= c->nsrc) return fail(c, MOM_ERR_STATE, "no device solution for that source");
+    xd = c->X + (size_t)isrc * c->n;
+    xrep = (int64_t)c->nsrc * c->n;
+  }
+  MOM_TRY(surface_fields(c, dom, omega, ri, xd, xrep, dE, dH));
+  const size_t out = sizeof(double2) * 3 * (size_t)c->dom[dom].F * c->nga;
+  MOM_CUDA(c, cudaMemcpyAsync(e, dE, out, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(h, dH, out, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int mom_gpu_group_action(mom_ctx *c, int32_t g, double *j, double *detj) {
+  if (!c || !j || !detj) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem first");
+  if (g < 0 || g >= c->nga) return fail(c, MOM_ERR_ARG, "group element out of range");
+  for (int i = 0; i < 9; i++) j[i] = c->ga[g].j[i];
+  *detj = c->ga[g].detj;
+  return MOM_OK;
+}
+
 int mom_gpu_device_matrix(mom_ctx *c, void **A_dev, int64_t *lda) {
   if (!c || !A_dev || !lda) return MOM_ERR_ARG;
   *A_dev = c->A;

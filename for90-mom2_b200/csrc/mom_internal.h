@@ -345,6 +345,8 @@ int scat_fields(Ctx *c, int d, double omega, const double *ri, int nsrc, const d
 // least 128 bytes per source.
 int add_incident_fields(Ctx *c, double omega, const double *ri, int nsrc, const mom_src *src, int npts,
                         const double *pts, double2 *E, double2 *H, void *srcbuf);
+int surface_fields(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int64_t xrep, double2 *E,
+                   double2 *H);
 int cs_gradient(Ctx *c, int dom, double omega, const double *ri, int nsrc, const mom_src *src, const double2 *xdev,
                 int64_t ldx, double2 *G);
 void src_geometry(const mom_src &s, double dir[3], double pol[3]);

@@ -651,6 +651,60 @@ __global__ void ff_current_sym_kernel(FfArgs a, GroupArg G, int64_t xrep) {
   }
 }
 
+// field_mesh (nfpost.f90:167-262): the fields on the boundary of a domain
+// at the centroid of every face of every image J_g(face), from the surface
+// currents alone (the jump conditions): with the image normal n = J n0 and
+// f' = J (n0 x f_q(cp)),
+//   E = sum_r ef[g][r] sum_q (beta_q f' + n div f_q alpha_q / (i w eps)),
+//   H = sum_r ef[g][r] det J sum_q (-alpha_q f' + n div f_q beta_q / (i w mu0)).
+// Thread per (element g, face f), output index g F + f.
+__global__ void surface_field_kernel(int F, int N, const double *cp, const double *nrm, const double *area,
+                                     const double *sl, const double *mu, const int *hpar, const double2 *x,
+                                     int64_t xrep, GroupArg G, Z iwe, Z iwm, double2 *E, double2 *H) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= F * G.nga) return;
+  const int g = j / F, f = j % F;
+  const double *J = G.j[g], *n0 = nrm + 3 * f;
+  const double An = area[f];
+  double nor[3];
+  jvec(J, n0, nor);
+  Z et[3] = {{0, 0}, {0, 0}, {0, 0}}, ht[3] = {{0, 0}, {0, 0}, {0, 0}}, en = {0, 0}, hn = {0, 0};
+  for (int r = 0; r < G.nga; r++) {
+    const double gae = G.ef[g][r];
+    for (int q = 0; q < 3; q++) {
+      const int idx = hpar[3 * f + q];
+      const double2 al = x[(size_t)r * xrep + idx], be = x[(size_t)r * xrep + idx + N];
+      // rwg at the centroid: sl/(2A) (cp - v_q) = -sl/(2A) mu_q
+      const double cc = -sl[3 * f + q] / (2.0 * An);
+      double fr[3], fn0[3], fn[3];
+      for (int i = 0; i < 3; i++) fr[i] = cc * mu[9 * f + 3 * q + i];
+      fn0[0] = n0[1] * fr[2] - n0[2] * fr[1];
+      fn0[1] = n0[2] * fr[0] - n0[0] * fr[2];
+      fn0[2] = n0[0] * fr[1] - n0[1] * fr[0];
+      jvec(J, fn0, fn);
+      const double dv = sl[3 * f + q] / An;
+      for (int i = 0; i < 3; i++) {
+        ht[i] = zsub(ht[i], zscale(Z{al.x, al.y}, fn[i] * gae * G.detj[g]));
+        et[i] = zadd(et[i], zscale(Z{be.x, be.y}, fn[i] * gae));
+      }
+      hn = zadd(hn, zscale(Z{be.x, be.y}, dv * gae * G.detj[g]));
+      en = zadd(en, zscale(Z{al.x, al.y}, dv * gae));
+    }
+  }
+  // en / (i w eps), hn / (i w mu0)
+  auto zdiv = [](Z a, Z b) -> Z {
+    const double d = b.re * b.re + b.im * b.im;
+    return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+  };
+  en = zdiv(en, iwe);
+  hn = zdiv(hn, iwm);
+  for (int i = 0; i < 3; i++) {
+    const Z e = zadd(et[i], zscale(en, nor[i])), h = zadd(ht[i], zscale(hn, nor[i]));
+    E[(size_t)j * 3 + i] = make_double2(e.re, e.im);
+    H[(size_t)j * 3 + i] = make_double2(h.re, h.im);
+  }
+}
+
 GroupArg group_arg(const Ctx *c) {
   GroupArg G;
   std::memset(&G, 0, sizeof G);
@@ -863,6 +917,24 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   }
   MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+// Surface fields (field_mesh) of domain dom for one solution column: x at
+// xdev (representation r at xdev + r xrep), E, H device [nga F][3].
+int surface_fields(Ctx *c, int dom, double omega, const double *ri, const double2 *xdev, int64_t xrep, double2 *E,
+                   double2 *H) {
+  const DomDev &D = c->dom[dom];
+  const Z n = {ri[0], ri[1]};
+  const Z eps = {kEps0 * (n.re * n.re - n.im * n.im), kEps0 * 2.0 * n.re * n.im};
+  const Z iwe = {-omega * eps.im, omega * eps.re};  // i omega eps
+  const Z iwm = {0.0, omega * kMu0};                // i omega mu0
+  const int total = D.F * c->nga;
+  ProfScope ps(c, kProfPost);
+  surface_field_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(D.F, c->N, D.cp, D.nrm, D.area, D.sl, D.mu,
+                                                                   D.hpar, xdev, xrep, group_arg(c), iwe, iwm, E, H);
+  c->launches++;
+  MOM_CUDA(c, cudaGetLastError());
   return MOM_OK;
 }
 

@@ -29,6 +29,7 @@
 // near fields, diffraction, polarizability, the VIE solver, source offsets
 // and scans) print an error and stop, as the reference does on invalid
 // input, instead of producing results this build does not compute.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -194,6 +195,7 @@ struct State {
   mom_ctx *ctx = nullptr;
   bool uploaded = false;
   int64_t n2 = 0;                    // 2N unknowns
+  double scale = 1.0;                // scale of the mesh command (b%scale)
   std::vector<std::string> symm;     // named groups of the symmetry group (read_symm)
   int nga = 1;                       // its order
   std::vector<std::vector<double>> x;  // per wavelength: [nsrc][nga][2N] complex, interleaved
@@ -433,6 +435,298 @@ void nfpl(State &s, const std::vector<std::string> &it) {
   std::fflush(stdout);
 }
 
+// ---- field maps in Gmsh post-processing files (mesh.f90:1740-1978) ----
+
+constexpr int kSteps = 25;  // time steps of the harmonic animation (nsteps)
+
+// REAL(v exp(-i 2 pi l / nsteps)) of a complex value (re, im)
+inline double phase_re(const double *v, int l) {
+  const double a = -2.0 * kPi * (double)l / kSteps;
+  return v[0] * std::cos(a) - v[1] * std::sin(a);
+}
+
+// A list-directed record "n value" (WRITE(fid,*) n, ' ', value): the
+// reference leaves its layout to the compiler; written here as an integer
+// and a 17-digit real.
+void list_record(std::FILE *f, int n, double v) { std::fprintf(f, "%12d   %.17E\n", n, v); }
+
+void msh_header(std::FILE *f) { std::fputs("$MeshFormat\n2.1 0 8\n$EndMeshFormat\n", f); }
+
+void msh_node(std::FILE *f, int n, const double *p, double scale) {
+  std::fprintf(f, "%d ", n);
+  for (int i = 0; i < 3; i++) std::fputs(en15_3(p[i] / scale).c_str(), f);
+  std::fputs("\n", f);
+}
+
+// save_vector_fields_msh (mesh.f90:1740-1888): the mesh and, per face, 25
+// animation frames each of Re(E), Re(H) (3 components), Re(En), Re(Hn) and
+// |Re(E)|, |Re(H)|.  e, h: [nfaces][3] complex (6 doubles per face).
+void save_vector_fields_msh(const std::string &path, const std::vector<double> &nodes,
+                            const std::vector<int> &faces, const std::vector<double> &normals,
+                            const std::vector<double> &e, const std::vector<double> &h, double scale) {
+  std::FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) stop("Could not open output file" + path + "!");
+  const int nn = (int)(nodes.size() / 3), nf = (int)(faces.size() / 3);
+  msh_header(f);
+  std::fprintf(f, "$Nodes\n%d\n", nn);
+  for (int n = 0; n < nn; n++) msh_node(f, n + 1, &nodes[3 * (size_t)n], scale);
+  std::fprintf(f, "$EndNodes\n$Elements\n%d\n", nf);
+  for (int n = 0; n < nf; n++)
+    std::fprintf(f, "%d 2 3 0 0 0 %d %d %d\n", n + 1, faces[3 * n] + 1, faces[3 * n + 1] + 1, faces[3 * n + 2] + 1);
+  std::fputs("$EndElements\n", f);
+  for (int which = 0; which < 2; which++) {
+    const std::vector<double> &v = which == 0 ? e : h;
+    for (int l = 1; l <= kSteps; l++) {
+      std::fprintf(f, "$ElementData\n1\n\"Re(%c)\"\n0\n3\n%d\n3\n%d\n", which == 0 ? 'E' : 'H', l - 1, nf);
+      for (int n = 0; n < nf; n++) {
+        std::fprintf(f, "%d ", n + 1);
+        for (int i = 0; i < 3; i++) std::fputs(en15_3(phase_re(&v[6 * (size_t)n + 2 * i], l)).c_str(), f);
+        std::fputs("\n", f);
+      }
+      std::fputs("$EndElementData\n", f);
+    }
+  }
+  for (int which = 0; which < 2; which++) {
+    const std::vector<double> &v = which == 0 ? e : h;
+    for (int l = 1; l <= kSteps; l++) {
+      std::fprintf(f, "$ElementData\n1\n\"Re(%cn)\"\n0\n3\n%d\n1\n%d\n", which == 0 ? 'E' : 'H', l - 1, nf);
+      for (int n = 0; n < nf; n++) {
+        // dotc (linalg.f90:15-21): the real normal against the complex field, no conjugation
+        double fn[2] = {0, 0};
+        for (int i = 0; i < 3; i++) {
+          fn[0] += normals[3 * (size_t)n + i] * v[6 * (size_t)n + 2 * i];
+          fn[1] += normals[3 * (size_t)n + i] * v[6 * (size_t)n + 2 * i + 1];
+        }
+        list_record(f, n + 1, phase_re(fn, l));
+      }
+      std::fputs("$EndElementData\n", f);
+    }
+  }
+  for (int which = 0; which < 2; which++) {
+    const std::vector<double> &v = which == 0 ? e : h;
+    for (int l = 1; l <= kSteps; l++) {
+      std::fprintf(f, "$ElementData\n1\n\"|Re(%c)|\"\n0\n3\n%d\n1\n%d\n", which == 0 ? 'E' : 'H', l - 1, nf);
+      for (int n = 0; n < nf; n++) {
+        double m = 0;
+        for (int i = 0; i < 3; i++) {
+          const double c = phase_re(&v[6 * (size_t)n + 2 * i], l);
+          m += c * c;
+        }
+        list_record(f, n + 1, std::sqrt(m));
+      }
+      std::fputs("$EndElementData\n", f);
+    }
+  }
+  std::fclose(f);
+}
+
+// The nodes (metres) and 0-based face nodes of domain d's submesh.
+void domain_mesh(State &s, int d, std::vector<double> &nodes, std::vector<int> &faces) {
+  mom_mesh m;
+  check(s, mom_problem_domain(s.prob, d, &m), "domain mesh");
+  nodes.assign(m.nodes, m.nodes + 3 * (size_t)m.nnodes);
+  faces.assign(m.face_nodes, m.face_nodes + 3 * (size_t)m.nfaces);
+}
+
+void unit_normal(const double *p1, const double *p2, const double *p3, double *n) {
+  const double a[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]}, b[3] = {p3[0] - p1[0], p3[1] - p1[1],
+                                                                               p3[2] - p1[2]};
+  n[0] = a[1] * b[2] - a[2] * b[1];
+  n[1] = a[2] * b[0] - a[0] * b[2];
+  n[2] = a[0] * b[1] - a[1] * b[0];
+  const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  for (int i = 0; i < 3; i++) n[i] /= l;
+}
+
+void field_indices(State &s, const std::vector<std::string> &it, const char *what, int *w, int *k, int *d) {
+  *w = int_item(it, 1, what);
+  *k = int_item(it, 2, what);
+  *d = int_item(it, 3, what);
+  if (s.x.empty()) stop(std::string("Error: solve (solv) before computing near fields!"));
+  if (*w < 1 || *w > (int)s.wl.size() || *k < 1 || *k > (int)s.src.size() || *d < 1 || *d > (int)s.doms.size())
+    stop(std::string("Error: index out of range in ") + what);
+}
+
+std::string field_name(const State &s, int w, int k, int d) {
+  return s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + "-d" + std::to_string(d) + ".msh";
+}
+
+// read_nfms (interface.f90:772-803) -> field_mesh (nfpost.f90:167-262): the
+// fields on domain d's boundary, on the domain mesh and its images under the
+// symmetry group.
+void nfms(State &s, const std::vector<std::string> &it) {
+  int w, k, d;
+  field_indices(s, it, "nfms", &w, &k, &d);
+  std::printf(" Computing near fields on particle mesh.\n");
+  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  const double ri[2] = {v.real(), v.imag()};
+  std::vector<double> nodes;
+  std::vector<int> faces;
+  domain_mesh(s, d - 1, nodes, faces);
+  const int nn = (int)(nodes.size() / 3), nf = (int)(faces.size() / 3), nga = s.nga;
+  std::vector<double> e(6 * (size_t)nf * nga), h(6 * (size_t)nf * nga);
+  check(s, mom_gpu_surface_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, k - 1, s.x[w - 1].data(), s.n2, e.data(),
+                                  h.data()),
+        "nfms");
+  // the image mesh: nodes J p, faces renumbered per element, normals J n
+  std::vector<double> n2((size_t)3 * nn * nga), nor((size_t)3 * nf * nga);
+  std::vector<int> f2((size_t)3 * nf * nga);
+  for (int g = 0; g < nga; g++) {
+    double J[9], detj;
+    check(s, mom_gpu_group_action(s.ctx, g, J, &detj), "nfms");
+    for (int n = 0; n < nn; n++)
+      for (int i = 0; i < 3; i++)
+        n2[3 * ((size_t)g * nn + n) + i] = J[3 * i] * nodes[3 * (size_t)n] + J[3 * i + 1] * nodes[3 * (size_t)n + 1] +
+                                           J[3 * i + 2] * nodes[3 * (size_t)n + 2];
+    for (int n = 0; n < nf; n++) {
+      double n0[3];
+      unit_normal(&nodes[3 * (size_t)faces[3 * n]], &nodes[3 * (size_t)faces[3 * n + 1]],
+                  &nodes[3 * (size_t)faces[3 * n + 2]], n0);
+      for (int i = 0; i < 3; i++) {
+        f2[3 * ((size_t)g * nf + n) + i] = faces[3 * n + i] + g * nn;
+        nor[3 * ((size_t)g * nf + n) + i] = J[3 * i] * n0[0] + J[3 * i + 1] * n0[1] + J[3 * i + 2] * n0[2];
+      }
+    }
+  }
+  save_vector_fields_msh(field_name(s, w, k, d), n2, f2, nor, e, h, s.scale);
+  double emax = 0;
+  for (size_t n = 0; n < (size_t)nf * nga; n++) {
+    double m = 0;
+    for (int i = 0; i < 6; i++) m += e[6 * n + i] * e[6 * n + i];
+    emax = std::max(emax, std::sqrt(m));
+  }
+  std::printf(" Maximum of |E| is %.15E\n", emax);
+  std::fflush(stdout);
+}
+
+// read_nfem (interface.f90:1010-1090) -> field_external_mesh
+// (nfpost.f90:264-314): scat_fields of domain d at the face centroids of an
+// external mesh (scaled as the problem mesh), plus the incident field when
+// asked.
+void nfem(State &s, const std::vector<std::string> &it) {
+  int w, k, d;
+  field_indices(s, it, "nfem", &w, &k, &d);
+  if (it.size() < 6) stop("Error: nfem needs a mesh file and true/false");
+  const bool addsrc = it[5] == "true";
+  mom_problem *ext = nullptr;
+  check(s, mom_problem_create(&ext), "nfem");
+  if (mom_problem_load_gmsh(ext, it[4].c_str(), s.scale) != MOM_OK) {
+    mom_problem_destroy(ext);
+    stop("Error in nfem: could not read mesh " + it[4]);
+  }
+  std::printf(" Computing near fields on external mesh.\n");
+  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  const double ri[2] = {v.real(), v.imag()};
+  std::vector<double> nodes, pts, nor;
+  std::vector<int> faces;
+  {
+    mom_mesh m;
+    if (mom_problem_domain(ext, -1, &m) != MOM_OK || m.nfaces <= 0) {
+      mom_problem_destroy(ext);
+      stop("Error in nfem: external mesh without faces");
+    }
+    nodes.assign(m.nodes, m.nodes + 3 * (size_t)m.nnodes);
+    faces.assign(m.face_nodes, m.face_nodes + 3 * (size_t)m.nfaces);
+    mom_problem_destroy(ext);
+    const int nf = m.nfaces;
+    pts.resize(3 * (size_t)nf);
+    nor.resize(3 * (size_t)nf);
+    for (int n = 0; n < nf; n++) {
+      const double *p1 = &nodes[3 * (size_t)faces[3 * n]], *p2 = &nodes[3 * (size_t)faces[3 * n + 1]],
+                   *p3 = &nodes[3 * (size_t)faces[3 * n + 2]];
+      for (int i = 0; i < 3; i++) pts[3 * (size_t)n + i] = (p1[i] + p2[i] + p3[i]) / 3.0;
+      unit_normal(p1, p2, p3, &nor[3 * (size_t)n]);
+    }
+  }
+  const int nf = (int)(faces.size() / 3), nsrc = (int)s.src.size();
+  std::vector<double> e(6 * (size_t)nf * nsrc), h(6 * (size_t)nf * nsrc);
+  check(s, mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, addsrc ? s.src.data() : nullptr,
+                               s.x[w - 1].data(), s.n2, nf, pts.data(), e.data(), h.data()),
+        "nfem");
+  std::vector<double> ek(e.begin() + 6 * (size_t)nf * (k - 1), e.begin() + 6 * (size_t)nf * k),
+      hk(h.begin() + 6 * (size_t)nf * (k - 1), h.begin() + 6 * (size_t)nf * k);
+  save_vector_fields_msh(field_name(s, w, k, d), nodes, faces, nor, ek, hk, s.scale);
+  std::fflush(stdout);
+}
+
+// read_nfdm (interface.f90:1092-1139) -> field_domain (nfpost.f90:85-165):
+// scat_fields of domain d on a regular grid of npoints(1:3) points over the
+// box origin +- dsize/2 (fractions (n-1)/(np-1) in default-kind reals), plus
+// the incident field when asked; the points where |E| exceeds 1% of its
+// maximum are written with the domain mesh (save_domain_vector_fields_msh,
+// mesh.f90:1890-1978).
+void nfdm(State &s, const std::vector<std::string> &it) {
+  int w, k, d;
+  field_indices(s, it, "nfdm", &w, &k, &d);
+  if (it.size() < 14) stop("Error: nfdm needs true/false, an origin, a size and three point counts");
+  const bool addsrc = it[4] == "true";
+  double org[3], dsz[3];
+  int np[3];
+  for (int i = 0; i < 3; i++) {
+    org[i] = real_item(it, 5 + i, "nfdm");
+    dsz[i] = real_item(it, 8 + i, "nfdm");
+    np[i] = int_item(it, 11 + i, "nfdm");
+    if (np[i] < 2) stop("Error: nfdm needs at least 2 points per axis");
+  }
+  const int npts = np[0] * np[1] * np[2], nsrc = (int)s.src.size();
+  std::vector<double> pts(3 * (size_t)npts);
+  for (int a = 0; a < np[0]; a++)
+    for (int b = 0; b < np[1]; b++)
+      for (int c = 0; c < np[2]; c++) {
+        const size_t idx = (size_t)c + (size_t)b * np[2] + (size_t)a * np[2] * np[1];
+        const float fr[3] = {(float)a / (float)(np[0] - 1), (float)b / (float)(np[1] - 1),
+                             (float)c / (float)(np[2] - 1)};
+        for (int i = 0; i < 3; i++) pts[3 * idx + i] = org[i] - dsz[i] / 2 + dsz[i] * (double)fr[i];
+      }
+  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  const double ri[2] = {v.real(), v.imag()};
+  std::vector<double> e(6 * (size_t)npts * nsrc), h(6 * (size_t)npts * nsrc);
+  check(s, mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, addsrc ? s.src.data() : nullptr,
+                               s.x[w - 1].data(), s.n2, npts, pts.data(), e.data(), h.data()),
+        "nfdm");
+  const double *ek = &e[6 * (size_t)npts * (k - 1)], *hk = &h[6 * (size_t)npts * (k - 1)];
+  auto mag = [&](size_t n) {
+    double m = 0;
+    for (int i = 0; i < 6; i++) m += ek[6 * n + i] * ek[6 * n + i];
+    return std::sqrt(m);
+  };
+  double emax = 0;
+  for (size_t n = 0; n < (size_t)npts; n++) emax = std::max(emax, mag(n));
+  std::vector<size_t> keep;
+  for (size_t n = 0; n < (size_t)npts; n++)
+    if (mag(n) > emax * 0.01) keep.push_back(n);
+  std::vector<double> nodes;
+  std::vector<int> faces;
+  domain_mesh(s, d - 1, nodes, faces);
+  const int nn = (int)(nodes.size() / 3), nf = (int)(faces.size() / 3), m = (int)keep.size();
+  const std::string path = field_name(s, w, k, d);
+  std::FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) stop("Could not open output file" + path + "!");
+  msh_header(f);
+  std::fprintf(f, "$Nodes\n%d\n", nn + m);
+  for (int n = 0; n < nn; n++) msh_node(f, n + 1, &nodes[3 * (size_t)n], s.scale);
+  for (int n = 0; n < m; n++) msh_node(f, nn + n + 1, &pts[3 * keep[n]], s.scale);
+  std::fprintf(f, "$EndNodes\n$Elements\n%d\n", nf + m);
+  for (int n = 0; n < nf; n++)
+    std::fprintf(f, "%d 2 3 0 0 0 %d %d %d\n", n + 1, faces[3 * n] + 1, faces[3 * n + 1] + 1, faces[3 * n + 2] + 1);
+  for (int n = 0; n < m; n++) std::fprintf(f, "%d 15 3 0 0 0 %d\n", nf + n + 1, nn + n + 1);
+  std::fputs("$EndElements\n", f);
+  for (int which = 0; which < 2; which++) {
+    const double *val = which == 0 ? ek : hk;
+    for (int l = 1; l <= kSteps; l++) {
+      std::fprintf(f, "$NodeData\n1\n\"Re(%c)\"\n0\n3\n%d\n3\n%d\n", which == 0 ? 'E' : 'H', l - 1, m);
+      for (int n = 0; n < m; n++) {
+        std::fprintf(f, "%d ", nn + n + 1);
+        for (int i = 0; i < 3; i++) std::fputs(en15_3(phase_re(&val[6 * keep[n] + 2 * i], l)).c_str(), f);
+        std::fputs("\n", f);
+      }
+      std::fputs("$EndNodeData\n", f);
+    }
+  }
+  std::fclose(f);
+  std::fflush(stdout);
+}
+
 void command(State &s, const std::string &cmd, const std::vector<std::string> &it) {
   if (cmd == "name") {
     if (it.size() < 2) stop("Error: name needs a value");
@@ -445,6 +739,7 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     s.prob = nullptr;
     check(s, mom_problem_create(&s.prob), "mesh");
     check(s, mom_problem_load_gmsh(s.prob, it[1].c_str(), scale), ("mesh " + it[1]).c_str());
+    s.scale = scale;
     s.finalized = s.uploaded = false;
     s.doms.clear();
   } else if (cmd == "wlrg") {
@@ -629,8 +924,14 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     rcst(s, it);
   } else if (cmd == "nfpl") {
     nfpl(s, it);
-  } else if (cmd == "osrc" || cmd == "npgf" || cmd == "ipgw" || cmd == "sbnd" || cmd == "nfms" || cmd == "nfdm" ||
-             cmd == "nfem" || cmd == "nfst" || cmd == "rcs2" || cmd == "rcs3" || cmd == "diff" ||
+  } else if (cmd == "nfms") {
+    nfms(s, it);
+  } else if (cmd == "nfem") {
+    nfem(s, it);
+  } else if (cmd == "nfdm") {
+    nfdm(s, it);
+  } else if (cmd == "osrc" || cmd == "npgf" || cmd == "ipgw" || cmd == "nfst" || cmd == "rcs2" || cmd == "rcs3" ||
+             cmd == "diff" ||
              cmd == "plrz" || cmd == "scan" || cmd == "trns" || cmd == "csca" || cmd == "test" || cmd == "vsol" ||
              cmd == "vext" || cmd == "viem" || cmd == "msrc") {
     stop("Error: command " + cmd + " is outside the linear PMCHWT path that this build implements");

@@ -374,7 +374,7 @@ int32_t mom_problem_ndom(const mom_problem *p) { return p ? (int32_t)p->dom.size
 
 int mom_problem_domain(const mom_problem *p, int32_t dom, mom_mesh *out) {
   if (!p || !out) return MOM_ERR_ARG;
-  if (!p->finalized) return MOM_ERR_STATE;
+  if (dom == -1 ? !p->have_mesh : !p->finalized) return MOM_ERR_STATE;
   if (dom < -1 || dom >= (int)p->dom.size()) return MOM_ERR_ARG;
   const Mesh &m = dom < 0 ? p->master : p->dom[dom];
   out->nnodes = m.nnodes;

@@ -50,6 +50,7 @@ EXPORTS = [
     "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement", "mom_gpu_scat_fields",
     "mom_gpu_set_matrix", "mom_gpu_set_wait_limits", "mom_gpu_set_symmetry", "mom_gpu_group_order",
     "mom_problem_set_lines", "mom_problem_classify_edges", "mom_problem_edge_bnd",
+    "mom_gpu_surface_fields", "mom_gpu_group_action",
 ]
 
 # Boundary types of mesh edges (sbnd; mesh.f90:16-25).
@@ -129,6 +130,8 @@ def lib():
     L.mom_problem_set_lines.argtypes = [vp, C.c_int32, ip, ip]
     L.mom_problem_classify_edges.argtypes = [vp, C.c_int32, C.c_int32, ip]
     L.mom_problem_edge_bnd.argtypes = [vp, ip]
+    L.mom_gpu_surface_fields.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, dp, dp]
+    L.mom_gpu_group_action.argtypes = [vp, C.c_int32, dp, dp]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
     L.mom_gpu_launch_count.argtypes = [vp]
@@ -369,6 +372,10 @@ class Solver:
         self.N = problem.nedges
         self.ndom = problem.ndom
         self.nga = 1
+        self._dom_faces = [problem.domain(d)["face_node"].shape[0] for d in range(problem.ndom)]
+
+    def domain_faces(self, dom):
+        return self._dom_faces[dom]
 
     def set_symmetry(self, names, problem: Problem):
         """read_symm: the product of the named groups ("id", "mxp", "myp", "mzp") with the
@@ -576,6 +583,29 @@ class Solver:
                                            e.ctypes.data_as(C.POINTER(C.c_double)),
                                            h.ctypes.data_as(C.POINTER(C.c_double))), "scat_fields")
         return e, h
+
+    def surface_fields(self, omega, ri, isrc=0, x=None, dom=0):
+        """field_mesh: (e, h), each [nga * nfaces_dom][3] complex, the fields at the
+        centroids of the domain's faces and of their symmetry images (face g F + f is
+        the image of face f under group element g)."""
+        r = _ri(ri)
+        nf = self.domain_faces(dom) * self.nga
+        e = np.zeros((nf, 3), dtype=np.complex128)
+        h = np.zeros_like(e)
+        xp = None
+        if x is not None:
+            x = np.asfortranarray(np.asarray(x, dtype=np.complex128).reshape(2 * self.N, -1, order="F"))
+            xp = x.ctypes.data
+        self._ck(lib().mom_gpu_surface_fields(self.h, dom, omega, _dp(r), isrc, xp, 2 * self.N, e.ctypes.data_as(
+            C.POINTER(C.c_double)), h.ctypes.data_as(C.POINTER(C.c_double))), "surface_fields")
+        return e, h
+
+    def group_action(self, g):
+        """(J [3][3], det J) of group element g."""
+        j = np.zeros(9)
+        d = C.c_double()
+        self._ck(lib().mom_gpu_group_action(self.h, g, _dp(j), C.byref(d)), "group_action")
+        return j.reshape(3, 3), d.value
 
     def rcs(self, omega, ri, ntheta, nphi, isrc=0, x=None, dom=0):
         r = _ri(ri)

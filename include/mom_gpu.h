@@ -168,6 +168,20 @@ int mom_gpu_rcs(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32
 int mom_gpu_scat_fields(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t nsrc, const mom_src *src,
                         const double *x_host, int64_t ldx, int32_t npts, const double *pts, double *e, double *h);
 
+/* Replaces field_mesh (nfpost.f90:167-262, the nfms command): the fields
+ * on the boundary of domain dom (0-based, refractive index ri) at the
+ * centroid of every face of every image of the domain's submesh under the
+ * symmetry group, from the surface currents alone: with n the image normal,
+ * E = n x M + n (div J) / (i omega eps), H = -n x J + n (div M) / (i omega mu0)
+ * (the group's field actions and det J applied as the reference does).
+ * isrc: source column of x_host (2N x nga x nsrc, ldx) or, if NULL, of the
+ * device solutions.  e, h: [nga * nfaces][3] complex; face g * nfaces + f is
+ * the image of face f under group element g (mom_gpu_group_action). */
+int mom_gpu_surface_fields(mom_ctx *ctx, int32_t dom, double omega, const double *ri, int32_t isrc,
+                           const double *x_host, int64_t ldx, double *e, double *h);
+/* Point action j[9] (row-major) and det J of group element g (symmetry.f90:24-40). */
+int mom_gpu_group_action(mom_ctx *ctx, int32_t g, double *j, double *detj);
+
 /* Allocation-free cross sections.  No counterpart in the reference.  For
  * callers that cannot allocate device memory at call time (their device
  * memory is reserved up front by another allocator, or they cannot accept
@@ -317,7 +331,9 @@ int mom_problem_edge_bnd(const mom_problem *p, int32_t *bnd);
 int mom_problem_finalize(mom_problem *p);
 int32_t mom_problem_nedges(const mom_problem *p);
 int32_t mom_problem_ndom(const mom_problem *p);
-/* Flattened view of domain dom (valid until the problem is destroyed). */
+/* Flattened view of domain dom (valid until the problem is destroyed); dom
+ * = -1 gives the master mesh, available from the mesh command on (before
+ * fdom; its edge_parent is not set). */
 int mom_problem_domain(const mom_problem *p, int32_t dom, mom_mesh *out);
 /* Master-mesh node of each submesh node of domain dom: parent[nnodes]. */
 int mom_problem_node_parent(const mom_problem *p, int32_t dom, int32_t *parent);

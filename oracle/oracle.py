@@ -391,6 +391,61 @@ class OracleProblem:
         return dict(nodes=nodes, area=area.value, sign=sign, length=ln, bnode=bn)
 
 
+def field_mesh(P, d, omega, ri, x, group=None):
+    """field_mesh (nfpost.f90:167-262): the fields at the centroid of every face
+    of domain d's submesh (and of its images under the group), from the
+    currents x (2N, nga) alone: E = sum_r ef_g(r) sum_q (beta_q f' + n div f_q
+    alpha_q / (i w eps)), H likewise with -alpha, beta and det J, where f' = J
+    (n0 x f_q(cp)) and n = J n0.  group: (j[nga][3][3], detj[nga],
+    ef[nga][nga]) as group_info returns, default the identity.  Returns
+    (e, h), each [nga * F][3]."""
+    m = P.export(d)
+    nodes, fn_, fe, ef_, eb = m["nodes"], m["face_node"], m["face_edge"], m["edge_face"], m["edge_bnode"]
+    par = m["edge_parent"]
+    N = P.N
+    x = np.asarray(x, dtype=np.complex128).reshape(2 * N, -1)
+    if group is None:
+        J, detj, ef = np.eye(3)[None], np.ones(1), np.ones((1, 1))
+    else:
+        J, detj, ef = group
+    nga = len(detj)
+    eps = ri * ri * EPS0
+    F = len(fn_)
+    e = np.zeros((nga * F, 3), dtype=np.complex128)
+    h = np.zeros_like(e)
+    for f in range(F):
+        p = nodes[fn_[f]]
+        cp = p.mean(axis=0)
+        cr = np.cross(p[1] - p[0], p[2] - p[0])
+        n0 = cr / np.linalg.norm(cr)
+        A = 0.5 * np.linalg.norm(np.cross(-(p[0] - p[2]), p[2] - p[1]))
+        for g in range(nga):
+            nor = J[g] @ n0
+            et = np.zeros(3, complex)
+            ht = np.zeros(3, complex)
+            en = hn = 0j
+            for r in range(nga):
+                gae = ef[g, r]
+                for q in range(3):
+                    ed = fe[f, q]
+                    sign = 1.0 if ef_[ed, 0] == f else -1.0
+                    free = nodes[eb[ed, 0] if sign > 0 else eb[ed, 1]]
+                    L = np.linalg.norm(nodes[m["edge_node"][ed, 0]] - nodes[m["edge_node"][ed, 1]])
+                    fr = sign * L / (2 * A) * (cp - free)
+                    fn = J[g] @ np.cross(n0, fr)
+                    div = sign * L / A
+                    al, be = x[par[ed], r], x[par[ed] + N, r]
+                    ht -= fn * al * gae * detj[g]
+                    hn += div * be * gae * detj[g]
+                    et += fn * be * gae
+                    en += div * al * gae
+            en /= 1j * omega * eps
+            hn /= 1j * omega * MU0
+            e[g * F + f] = et + nor * en
+            h[g * F + f] = ht + nor * hn
+    return e, h
+
+
 def solve(A, q):
     """solve_multi_linsys (linalg.f90:159-180): ZGETRF + ZGETRS('N'), STOP on INFO /= 0."""
     from scipy.linalg import lapack

@@ -64,7 +64,7 @@ def test_unknown_command_is_reported_and_skipped(workdir):
 
 @pytest.mark.parametrize("line,msg", [
     ("symm 1 r4", "rotation symmetry group 'r4'"),
-    ("nfms 1 2 3", "outside the linear PMCHWT path"),
+    ("diff 1 1 0 0 false 0", "outside the linear PMCHWT path"),
 ])
 def test_input_outside_the_path_stops(workdir, line, msg):
     r = run(line + "\nexit\n", workdir)

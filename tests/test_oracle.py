@@ -300,3 +300,32 @@ def test_mirror_group_structure_and_boundary_conditions():
         # a plane edge loses exactly one of J, M in each representation
         assert np.count_nonzero(idv == -1) == len(lines[0]) + len(lines[1])
         assert np.all(idv[:N][idv[N:] == -1] == 0)
+
+
+def test_field_mesh_matches_near_fields_at_the_surface():
+    """field_mesh (nfpost.f90:167-262) gives the fields on the surface from the
+    currents alone; they must agree with the integrated fields (scat_fields, plus
+    the incident field outside) a hundredth of an edge off the surface, on either
+    side, to the discretisation error of the s=2 sphere (measured 1-8%)."""
+    from mom_b200 import workloads as W
+    nodes, faces, ids, doms = W.sphere(2)
+    P = O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+    om = O.omega_of(600e-9)
+    n_in = np.sqrt(W.EPS_AU)
+    src = dict(type="pw", theta=0.0, phi=90 * O.DEGTORAD, psi=0.0)
+    x = O.solve(P.sysmat(om, np.array([1.0, n_in])), P.srcvec(om, 1.0, src)[:, None])
+    e, h = O.field_mesh(P, 0, om, 1.0, x[:, 0])
+    ei, hi = O.field_mesh(P, 1, om, n_in, x[:, 0])
+    nd = np.asarray(nodes) * 1e-9
+    fc = np.asarray(faces)
+    for f in (7, 100, 250):
+        tri = nd[fc[f]]
+        cp = tri.mean(axis=0)
+        nn = np.cross(tri[1] - tri[0], tri[2] - tri[0])
+        nn = nn / np.linalg.norm(nn) * np.sign(nn @ cp)
+        dh = 0.01 * np.linalg.norm(tri[1] - tri[0])
+        eo, ho = P.scat_fields(om, 1.0, x, np.array([cp + dh * nn]), srcs=[src], d=0)
+        en, hn = P.scat_fields(om, n_in, x, np.array([cp - dh * nn]), d=1)
+        for a, b, tol in ((e[f], eo[0, 0], 0.12), (h[f], ho[0, 0], 0.05), (ei[f], en[0, 0], 0.05),
+                          (hi[f], hn[0, 0], 0.02)):
+            assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b), (f, np.linalg.norm(a - b) / np.linalg.norm(b))
