@@ -1719,6 +1719,10 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
   LuWork w;
   MOM_TRY(lu_workspace(c, precision, w));
   Ctx::LuGraph *g = nullptr;
+  // the whole factorisation on the context stream (its wall time, with the
+  // look-ahead stream joined in before the end event)
+  {
+  ProfScope pl(c, kProfLu);
   if (c->use_graph) {
     // Everything the captured launches bake in: sizes, buffer addresses, the
     // SM count (panel grid) and whether timing events are part of the graph.
@@ -1754,6 +1758,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
     c->tc_flops += g->tc_flops;
   } else {
     MOM_TRY(use_lookahead(c, precision) ? lu_enqueue_la<T>(c, A, w) : lu_enqueue<T>(c, A, precision, w));
+  }
   }
   int hinfo[3] = {0, 0, 0};
   MOM_CUDA(c, cudaMemcpyAsync(hinfo, c->dinfo, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));

@@ -253,7 +253,7 @@ inline long long wait_polls(const Ctx *c, int kind) {
 // Kernel categories for the optional timers.
 enum ProfCat {
   kProfPair = 0, kProfNear, kProfGather, kProfPanel, kProfGemm, kProfTrsv, kProfResidual, kProfPost, kProfPivotAux,
-  kProfTc, kProfDiagInv,
+  kProfTc, kProfDiagInv, kProfLu,
   kProfCount
 };
 

@@ -636,7 +636,7 @@ class Solver:
         return lib().mom_gpu_library_calls(self.h)
 
     PROF_CATEGORIES = ("pair", "near", "gather", "panel", "gemm", "trsv", "residual", "post", "pivot_aux", "tc_gemm",
-                       "diag_inv")
+                       "diag_inv", "lu")
 
     @property
     def tensor_flops(self):

@@ -297,7 +297,8 @@ double mom_gpu_tensor_flops(mom_ctx *ctx);
  * assembly), 1 near pairs, 2 gather, 3 LU panel, 4 LU GEMMs, 5 triangular
  * solves, 6 refinement residual, 7 post-processing, 8 row interchanges of
  * the LU, 9 the tensor-core LU update kernel alone, 10 diagonal-block
- * inverses of the LU. */
+ * inverses of the LU, 11 the whole LU factorisation (wall time on the
+ * context stream; the categories inside it overlap under the look-ahead). */
 int mom_gpu_profile(mom_ctx *ctx, int32_t enable);
 int mom_gpu_profile_read(mom_ctx *ctx, int32_t category, double *ms_total, int64_t *launches);
 
