@@ -484,7 +484,8 @@ def run_ours(args, rank, local_rank, world):
         for key, fn in (("sweep", lambda: bench_sweep(M, args.sweep_workers, local_rank)),
                         ("adjoint", lambda: bench_adjoint(M, local_rank)),
                         ("core_shell", lambda: bench_core_shell(M, local_rank)),
-                        ("near_field", lambda: bench_nearfield(M, local_rank, with_cpu=not args.no_cpu))):
+                        ("near_field", lambda: bench_nearfield(M, local_rank, with_cpu=not args.no_cpu)),
+                        ("shg", lambda: bench_shg(M, local_rank, with_cpu=not args.no_cpu))):
             try:
                 line[key] = fn()
             except Exception as exc:  # a side measurement must not cost the bench line
@@ -560,6 +561,66 @@ def bench_nearfield(M, dev, n=101, with_cpu=True):
         out["cpu_baseline"] = {"value": len(idx) / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
                                "sample": "16 of the plane's points"}
         out["max_rel_diff_vs_oracle"] = err
+    return out
+
+
+def bench_shg(M, dev, with_cpu=True):
+    """Second-harmonic generation (solver.f90:143-217) from a surface
+    nonlinearity of the particle (chi_nnn, chi_ntt, chi_ttn = 1, 0.5, 0.2 x
+    1e-18 m^2/V) on the s=4 sphere (15,360 unknowns) at 1000 nm, SH index
+    sqrt(-2 + 3.5i): time of the SH solve (source expansion + assembly at
+    2 omega + LU + solve) after the fundamental solve, FP64 and mixed, and the
+    SH sigma_sca.  With with_cpu, the oracle's restatement on the s=2 sphere
+    (1,920 unknowns, one host thread for the expansion, OpenMP assembly) against
+    the GPU on the same s=2 problem: time and the largest relative difference
+    of the SH solution."""
+    import numpy as np
+    from mom_b200 import workloads as W
+    wl = 1000e-9
+    om = M.omega_of(wl)
+    ri = [1.0, np.sqrt(EPS_IN)]
+    shri = [1.0, np.sqrt(complex(-2.0, 3.5))]
+    chi = (1.0e-18, 0.5e-18, 0.2e-18)
+    src = [M.src_pw(0, 90, 0)]
+    out = {"workload": "icosphere s=4 (15360 unknowns), nlsurf chi (1, 0.5, 0.2)e-18 in the particle, 1000 nm, "
+                       "SH index sqrt(-2+3.5i), x-pol pw +z"}
+    S = M.Solver(dev)
+    nodes, faces, ids, doms = W.sphere(4)
+    S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    for name, prec in (("fp64", M.FP64), ("mixed", M.MIXED)):
+        times = []
+        for rep in range(3):
+            S.solve_wavelength(om, ri, src, prec, 1e-12, 30, want_host=False)
+            S.synchronize()
+            t0 = time.perf_counter()
+            S.shg_solve(om, ri, shri, [None, chi], prec, 1e-12, 30, want_host=False)
+            S.synchronize()
+            times.append(time.perf_counter() - t0)
+        csca, _ = S.cross_sections(2 * om, 1.0, [M.src_none()])
+        out[name] = {"shg_solve_ms": min(times[1:]) * 1e3, "sigma_sca_sh": float(csca[0]),
+                     "refine_iters": S.iters}
+    out["mixed_vs_fp64_sigma_sh"] = abs(out["mixed"]["sigma_sca_sh"] / out["fp64"]["sigma_sca_sh"] - 1)
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        nodes, faces, ids, doms = W.sphere(2)
+        S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+        S.solve_wavelength(om, ri, src, M.FP64, want_host=False)
+        S.synchronize()
+        t0 = time.perf_counter()
+        nlx = S.shg_solve(om, ri, shri, [None, chi], M.FP64)
+        gpu_s = time.perf_counter() - t0
+        P = O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+        osrc = dict(type="pw", theta=0.0, phi=90 * O.DEGTORAD, psi=0.0)
+        x = O.solve(P.sysmat(om, ri), P.srcvec(om, 1.0, osrc)[:, None])
+        t0 = time.perf_counter()
+        nlo = O.shg_solve(P, om, ri, shri, [None, chi], x)
+        cpu_s = time.perf_counter() - t0
+        out["s2"] = {"gpu_shg_solve_ms": gpu_s * 1e3,
+                     "max_rel_diff_vs_oracle": float(np.linalg.norm(nlx[:, 0] - nlo[:, 0]) / np.linalg.norm(nlo[:, 0]))}
+        out["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "SH solves/s", "kind": "port",
+                               "cores": host_cores(), "sample": "the s=2 sphere (1920 unknowns), whole SH solve"}
+    S.close()
     return out
 
 

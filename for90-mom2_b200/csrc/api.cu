@@ -107,6 +107,7 @@ void free_domain(DomDev &D) {
   cudaFree(D.inc_face);
   cudaFree(D.nf_geo);
   cudaFree(D.nf_bn);
+  free_shg(D);
   D = DomDev();
 }
 
@@ -119,6 +120,9 @@ void free_problem(Ctx *c) {
   cudaFree(c->A_all);
   cudaFree(c->A32_all);
   cudaFree(c->blk);
+  cudaFree(c->dmap);
+  c->dmap = nullptr;
+  c->blk_fused = false;
   cudaFree(c->ipiv_all);
   cudaFree(c->perm_all);
   cudaFree(c->invd_all);
@@ -139,6 +143,9 @@ void free_problem(Ctx *c) {
   c->nga = 1;
   c->B = c->X = nullptr;
   c->BX_cap = 0;
+  c->nsrc = 0;
+  c->solved = false;
+  c->shg_slot.clear();
   c->have_problem = false;
   c->assembled = 0;
   c->factored = -1;
@@ -453,6 +460,8 @@ void mom_gpu_destroy(mom_ctx *c) {
   cudaFree(c->adj);
   cudaFree(c->adj_part);
   cudaFree(c->adjW);
+  cudaFree(c->shg_c);
+  cudaFree(c->shg_ws);
   cudaFree(c->dinfo);
   if (c->pinned) cudaFreeHost(c->pinned);
   for (auto *g : c->lu_graphs) {
@@ -519,6 +528,27 @@ int mom_gpu_set_problem(mom_ctx *c, int32_t nedges_total, int32_t ndom, const mo
   c->n = (n2 + c->nb - 1) / c->nb * c->nb;
   c->lda = c->n;
   c->blk_bytes = sizeof(double2) * 18 * maxF * maxF;
+  // Face-pair blocks of all domains at once (one gather writes the matrix)
+  // when they fit beside the matrices with room to spare.
+  {
+    size_t total = 0;
+    c->blk_off.assign(ndom, 0);
+    for (int d = 0; d < ndom; d++) {
+      c->blk_off[d] = total / sizeof(double2);
+      total += sizeof(double2) * 18 * (size_t)c->dom[d].F * c->dom[d].F;
+    }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    const size_t mats = (size_t)c->lda * c->n * (sizeof(double2) + sizeof(float2)) + (size_t(4) << 30);
+    c->blk_fused = ndom <= 8 && fr > total + mats;
+    if (c->blk_fused) {
+      std::vector<int> dm((size_t)ndom * c->N, -1);
+      for (int d = 0; d < ndom; d++)
+        for (int e = 0; e < c->dom[d].Nd; e++) dm[(size_t)d * c->N + c->dom[d].h_epar[e]] = e;
+      MOM_TRY(upload(c, &c->dmap, dm));
+      c->blk_bytes = total;
+    }
+  }
   // the identity group: one element, one representation, nothing removed
   std::memset(c->ga, 0, sizeof c->ga);
   c->ga[0].j[0] = c->ga[0].j[4] = c->ga[0].j[8] = 1.0;
@@ -571,6 +601,7 @@ int mom_gpu_srcvec(mom_ctx *c, double omega, const double *ri1, int32_t nsrc, co
   MOM_TRY(ensure_rhs(c, nsrc * c->nga));
   MOM_TRY(rhs_build(c, omega, ri1, nsrc, src));
   c->nsrc = nsrc;
+  c->solved = false;
   c->srcs.assign(src, src + nsrc);
   c->omega_rhs = omega;
   c->ri1[0] = ri1[0];
@@ -617,6 +648,7 @@ int mom_gpu_solve(mom_ctx *c, int32_t precision, double tol, int32_t maxit, doub
   }
   select_rep(c, 0);
   if (precision == MOM_PREC_FP64) c->assembled = 0;  // the matrices now hold their LU factors
+  c->solved = true;
   if (iters_out) *iters_out = it;
   if (x_host) MOM_TRY(copy_block_to_host(c, c->X, c->nsrc, x_host, ldx));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -631,6 +663,49 @@ int mom_gpu_solve_wavelength(mom_ctx *c, double omega, const double *ri, int32_t
   r = mom_gpu_srcvec(c, omega, ri, nsrc, src, nullptr, 0);
   if (r) return r;
   return mom_gpu_solve(c, precision, tol, maxit, x_host, ldx, iters_out);
+}
+
+int mom_gpu_shg_solve(mom_ctx *c, double omega, const double *ri, const double *shri, const mom_nls *nls,
+                      int32_t precision, double tol, int32_t maxit, double *nlx_host, int64_t ldx,
+                      int32_t *iters_out) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before the second-harmonic solve");
+  if (!ri || !shri || !nls || !(omega > 0)) return fail(c, MOM_ERR_ARG, "invalid omega, refractive indices or media");
+  MOM_TRY(check_prec(c, precision));
+  if (c->nga != 1) return fail(c, MOM_ERR_ARG, "the second-harmonic solve supports the identity symmetry group only");
+  if (c->nsrc <= 0 || !c->solved) return fail(c, MOM_ERR_STATE, "solve at the fundamental frequency first");
+  if (nlx_host && ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
+  if (precision == MOM_PREC_MIXED && (maxit <= 0 || !(tol > 0)))
+    return fail(c, MOM_ERR_ARG, "mixed solve needs tol > 0, maxit > 0");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  if (precision == MOM_PREC_MIXED) MOM_TRY(ensure_a32(c));
+  int it = 0;
+  c->solved = false;  // the device solutions become the second harmonic's
+  const int rc = shg_solve(c, omega, ri, shri, nls, precision, tol, maxit, &it);
+  if (rc != MOM_OK) {
+    c->factored = -1;
+    return rc;
+  }
+  if (iters_out) *iters_out = it;
+  if (nlx_host) MOM_TRY(copy_block_to_host(c, c->X, c->nsrc, nlx_host, ldx));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
+}
+
+int mom_gpu_shg_source_coef(mom_ctx *c, int32_t dom, double *coef_host, int64_t ldc) {
+  if (!c) return MOM_ERR_ARG;
+  std::lock_guard<std::mutex> g(c->mu);
+  if (!c->have_problem || dom < 0 || dom >= c->ndom || !coef_host || ldc < 2 * (int64_t)c->N)
+    return fail(c, MOM_ERR_ARG, "invalid domain or output for the second-harmonic source coefficients");
+  if (dom >= (int)c->shg_slot.size() || c->shg_slot[dom] < 0 || !c->shg_c)
+    return fail(c, MOM_ERR_STATE, "no second-harmonic source coefficients for this domain");
+  MOM_CUDA(c, cudaSetDevice(c->device));
+  const double2 *src = (const double2 *)c->shg_c + (size_t)c->shg_slot[dom] * c->n * c->nsrc;
+  MOM_CUDA(c, cudaMemcpy2DAsync(coef_host, sizeof(double2) * ldc, src, sizeof(double2) * c->n,
+                                sizeof(double2) * 2 * (size_t)c->N, c->nsrc, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return MOM_OK;
 }
 
 int mom_gpu_sweep(mom_ctx *c, int32_t nwl, const double *omega, const double *ri, int32_t nsrc, const mom_src *src,
@@ -721,7 +796,8 @@ static int adjoint_currents(mom_ctx *c, int32_t precision, double omega, const d
                             const mom_src *src, double tol, int32_t maxit, double2 **G, double2 **lam,
                             double2 **xo, int32_t *iters) {
   MOM_TRY(check_prec(c, precision));
-  if (c->factored != precision) return fail(c, MOM_ERR_STATE, "the adjoint needs the factors of a solve in this precision");
+  if (c->factored != precision || !c->solved)
+    return fail(c, MOM_ERR_STATE, "the adjoint needs the factors and solutions of a solve in this precision");
   if (nsrc != c->nsrc || nsrc <= 0 || !src || !ri || !(omega > 0))
     return fail(c, MOM_ERR_ARG, "the adjoint sources must be those of the last solve");
   if (precision == MOM_PREC_MIXED && (maxit <= 0 || !(tol > 0))) return fail(c, MOM_ERR_ARG, "mixed adjoint needs tol > 0, maxit > 0");

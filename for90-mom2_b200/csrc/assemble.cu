@@ -661,6 +661,94 @@ __global__ void __launch_bounds__(256) gather_kernel(GatherArgs a) {
   A[r + (c + N) * a.lda] = t;
 }
 
+constexpr int kGatherDoms = 8;
+
+struct GatherAllArgs {
+  int N, ndom;
+  const int *dmap;  // [ndom][N]: domain edge of each global edge, -1 if none
+  const double2 *blk[kGatherDoms];
+  const int *eh[kGatherDoms];
+  int F[kGatherDoms];
+  Cd Zsi[kGatherDoms];
+  double2 *A;       // FP64 matrix, written (not accumulated)
+  float2 *A32;      // FP32 copy, or null
+  int64_t lda;
+};
+
+// Thread per global edge pair (g1 fastest): the four PMCHWT blocks summed
+// over the domains in order (sysmat.f90:70-99, identity group), each domain's
+// S and K from its face-pair blocks over the (+,-) halves of both edges;
+// written once into A (and its FP32 copy), so the matrix needs no clearing,
+// no read-modify-write per domain and no separate conversion.
+__global__ void __launch_bounds__(256) gather_all_kernel(GatherAllArgs a) {
+  const int g1 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g2 = blockIdx.y;
+  if (g1 >= a.N) return;
+  double2 jj = make_double2(0, 0), mm = jj, mj = jj, jm = jj;
+  for (int d = 0; d < a.ndom; d++) {
+    const int e1 = a.dmap[(size_t)d * a.N + g1], e2 = a.dmap[(size_t)d * a.N + g2];
+    if (e1 < 0 || e2 < 0) continue;
+    const int *eh = a.eh[d];
+    const int h1[2] = {eh[2 * e1], eh[2 * e1 + 1]};
+    const int h2[2] = {eh[2 * e2], eh[2 * e2 + 1]};
+    double sr = 0, si = 0, kr = 0, ki = 0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      if (h1[i] < 0) continue;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (h2[j] < 0) continue;
+        const int m = h1[i] / 3, p = h1[i] % 3, n = h2[j] / 3, q = h2[j] % 3;
+        const double4 v =
+            *reinterpret_cast<const double4 *>(a.blk[d] + ((size_t)n * a.F[d] + m) * 18 + 2 * (3 * p + q));
+        sr += v.x;
+        si += v.y;
+        kr += v.z;
+        ki += v.w;
+      }
+    }
+    // the coefficients of the identity action: 1, Zsi, 1, -1
+    const Cd z = a.Zsi[d];
+    jj.x += 1.0 * sr - 0.0 * si;
+    jj.y += 1.0 * si + 0.0 * sr;
+    mm.x += z.re * sr - z.im * si;
+    mm.y += z.re * si + z.im * sr;
+    mj.x += 1.0 * kr - 0.0 * ki;
+    mj.y += 1.0 * ki + 0.0 * kr;
+    jm.x += -1.0 * kr - 0.0 * ki;
+    jm.y += -1.0 * ki + 0.0 * kr;
+  }
+  const int64_t r = g1, c = g2, N = a.N, ld = a.lda;
+  a.A[r + c * ld] = jj;
+  a.A[(r + N) + (c + N) * ld] = mm;
+  a.A[(r + N) + c * ld] = mj;
+  a.A[r + (c + N) * ld] = jm;
+  if (a.A32) {
+    a.A32[r + c * ld] = make_float2((float)jj.x, (float)jj.y);
+    a.A32[(r + N) + (c + N) * ld] = make_float2((float)mm.x, (float)mm.y);
+    a.A32[(r + N) + c * ld] = make_float2((float)mj.x, (float)mj.y);
+    a.A32[r + (c + N) * ld] = make_float2((float)jm.x, (float)jm.y);
+  }
+}
+
+// The padding rows and columns 2N..n-1 of a matrix the gather writes
+// without clearing: zero, with ones on the diagonal.  Thread per (row,
+// padding index) of both strips.
+template <class T>
+__global__ void pad_strips_kernel(T *A, int64_t lda, int64_t n2, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t k = n2 + blockIdx.y;
+  if (i >= n) return;
+  T z{};
+  A[i + k * lda] = z;  // column k
+  A[k + i * lda] = z;  // row k
+  if (i == k) {
+    T one{};
+    one.x = 1;
+    A[k + k * lda] = one;
+  }
+}
+
 // Rows/columns 2N..n-1 pad the matrix to a multiple of the panel width with
 // an identity block, which leaves the LU of the leading 2N x 2N part as is.
 __global__ void pad_identity(double2 *A, int64_t lda, int64_t n2, int64_t n) {
@@ -849,7 +937,7 @@ int action_precompute(Ctx *c, int d, int g) {
 // precision, near pairs in FP64) are gathered into the four PMCHWT blocks of
 // every representation (sysmat.f90:56-100; the identity group has one
 // action and one representation).
-int assemble(Ctx *c, double omega, const double *ri, int precision) {
+int assemble_begin(Ctx *c) {
   const int64_t n = c->n, lda = c->lda;
   const size_t mat = (size_t)lda * n;
   const int nga = c->nga;
@@ -860,21 +948,41 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
       pad_identity<<<(unsigned)((n - n2 + 127) / 128), 128, 0, c->stream>>>(c->A_all + r * mat, lda, n2, n);
       c->launches++;
     }
-  for (int d = 0; d < c->ndom; d++) {
-    DomDev &D = c->dom[d];
-    const Cd rid = {ri[2 * d], ri[2 * d + 1]};
-    // k = ri omega / c0 ; c1 = -i omega mu0 ; c2 = -1/(i omega eps0 ri^2) ; Zsi = ri^2/eta0^2
-    const double kr = rid.re * omega / kC0, ki = rid.im * omega / kC0;
-    const Cd c1 = {0.0, -omega * kMu0};
-    const Cd ri2 = {rid.re * rid.re - rid.im * rid.im, 2 * rid.re * rid.im};
-    const Cd den = {-omega * kEps0 * ri2.im, omega * kEps0 * ri2.re};  // i omega eps0 ri^2
-    const double dn2 = den.re * den.re + den.im * den.im;
-    const Cd c2 = {-den.re / dn2, den.im / dn2};
-    const Cd Zsi = {ri2.re / (kEta0 * kEta0), ri2.im / (kEta0 * kEta0)};
-    const double L0 = (precision == MOM_PREC_MIXED) ? D.avelen : 1.0;
-    for (int g = 0; g < nga; g++) {
+  return MOM_OK;
+}
+
+// Medium constants of domain d: k = ri omega / c0, c1 = -i omega mu0,
+// c2 = -1/(i omega eps0 ri^2), Zsi = ri^2/eta0^2.
+struct MediumConsts {
+  double kr, ki;
+  Cd c1, c2, Zsi;
+};
+
+MediumConsts medium_consts(double omega, const double *ri, int d) {
+  const Cd rid = {ri[2 * d], ri[2 * d + 1]};
+  MediumConsts m;
+  m.kr = rid.re * omega / kC0;
+  m.ki = rid.im * omega / kC0;
+  m.c1 = {0.0, -omega * kMu0};
+  const Cd ri2 = {rid.re * rid.re - rid.im * rid.im, 2 * rid.re * rid.im};
+  const Cd den = {-omega * kEps0 * ri2.im, omega * kEps0 * ri2.re};  // i omega eps0 ri^2
+  const double dn2 = den.re * den.re + den.im * den.im;
+  m.c2 = {-den.re / dn2, den.im / dn2};
+  m.Zsi = {ri2.re / (kEta0 * kEta0), ri2.im / (kEta0 * kEta0)};
+  return m;
+}
+
+// The face-pair blocks of domain d under group action g (pair_kernel for
+// every pair, then near_kernel over the near pairs) into blk.
+int domain_blocks(Ctx *c, int d, int g, double omega, const double *ri, int precision, double2 *blk) {
+  DomDev &D = c->dom[d];
+  const MediumConsts mc = medium_consts(omega, ri, d);
+  const double kr = mc.kr, ki = mc.ki;
+  const Cd c1 = mc.c1, c2 = mc.c2;
+  const double L0 = (precision == MOM_PREC_MIXED) ? D.avelen : 1.0;
+  {
+    {
       const bool ident = g == 0;
-      if (!ident && !D.act[g].admissible) continue;
       const double *tqrel = ident ? D.qrel : D.act[g].qrel, *tcp = ident ? D.cp : D.act[g].cp,
                    *tmu = ident ? D.mu : D.act[g].mu;
       const int64_t nnear = ident ? D.nnear : D.act[g].nnear;
@@ -894,7 +1002,7 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
       pa.fD = {c1.re * L0 * L0 * L0 * kOofpi / 4.0, c1.im * L0 * L0 * L0 * kOofpi / 4.0};
       pa.fH = {c2.re * L0 * kOofpi, c2.im * L0 * kOofpi};
       pa.fK = L0 * L0 * kOofpi / 4.0;
-      pa.blk = c->blk;
+      pa.blk = blk;
       dim3 grid((D.F + kPairThreads - 1) / kPairThreads, (D.F + kTestPerCta - 1) / kTestPerCta);
       {
         ProfScope ps(c, kProfPair);
@@ -924,7 +1032,7 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
         na.c1 = c1;
         na.c2 = c2;
         na.k2 = {kr * kr - ki * ki, 2 * kr * ki};
-        na.blk = c->blk;
+        na.blk = blk;
         const unsigned blocks = (unsigned)((nnear + 127) / 128);
         ProfScope ps(c, kProfNear);
         switch (c->nq) {
@@ -938,6 +1046,21 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
         c->launches++;
         MOM_CUDA(c, cudaGetLastError());
       }
+    }
+  }
+  return MOM_OK;
+}
+
+int assemble_domain(Ctx *c, int d, double omega, const double *ri, int precision) {
+  const int64_t n = c->n, lda = c->lda;
+  const size_t mat = (size_t)lda * n;
+  const int nga = c->nga;
+  {
+    DomDev &D = c->dom[d];
+    const Cd Zsi = medium_consts(omega, ri, d).Zsi;
+    for (int g = 0; g < nga; g++) {
+      if (g > 0 && !D.act[g].admissible) continue;
+      MOM_TRY(domain_blocks(c, d, g, omega, ri, precision, c->blk));
       const double detj = c->ga[g].detj;
       for (int r = 0; r < nga; r++) {
         const double e = c->ga[g].ef[r];
@@ -962,6 +1085,12 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
       }
     }
   }
+  return MOM_OK;
+}
+
+int assemble_end(Ctx *c, int precision) {
+  const size_t mat = (size_t)c->lda * c->n;
+  const int nga = c->nga;
   for (int r = 0; r < nga && nga > 1; r++) MOM_TRY(apply_bc_matrix(c, r));
   if (precision == MOM_PREC_MIXED) {
     convert_to_fp32<<<c->nsm * 8, 256, 0, c->stream>>>(c->A_all, c->A32_all, (int64_t)mat * nga);
@@ -971,6 +1100,54 @@ int assemble(Ctx *c, double omega, const double *ri, int precision) {
   c->assembled = 1;
   c->factored = -1;
   return MOM_OK;
+}
+
+// The identity-group assembly when every domain's face-pair blocks fit at
+// once: pair and near kernels per domain into its own block buffer, then one
+// gather over the global edge pairs that writes A (and A32) once.
+int assemble_fused(Ctx *c, double omega, const double *ri, int precision) {
+  GatherAllArgs ga;
+  ga.N = c->N;
+  ga.ndom = c->ndom;
+  ga.dmap = c->dmap;
+  for (int d = 0; d < c->ndom; d++) {
+    double2 *blk = c->blk + c->blk_off[d];
+    MOM_TRY(domain_blocks(c, d, 0, omega, ri, precision, blk));
+    ga.blk[d] = blk;
+    ga.eh[d] = c->dom[d].eh;
+    ga.F[d] = c->dom[d].F;
+    ga.Zsi[d] = medium_consts(omega, ri, d).Zsi;
+  }
+  ga.A = c->A_all;
+  ga.A32 = precision == MOM_PREC_MIXED ? c->A32_all : nullptr;
+  ga.lda = c->lda;
+  {
+    ProfScope ps(c, kProfGather);
+    gather_all_kernel<<<dim3((c->N + 255) / 256, c->N), 256, 0, c->stream>>>(ga);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  const int64_t n = c->n, n2 = 2 * (int64_t)c->N;
+  if (n > n2) {
+    const dim3 pg((unsigned)((n + 255) / 256), (unsigned)(n - n2));
+    pad_strips_kernel<double2><<<pg, 256, 0, c->stream>>>(c->A_all, c->lda, n2, n);
+    c->launches++;
+    if (ga.A32) {
+      pad_strips_kernel<float2><<<pg, 256, 0, c->stream>>>(c->A32_all, c->lda, n2, n);
+      c->launches++;
+    }
+    MOM_CUDA(c, cudaGetLastError());
+  }
+  c->assembled = 1;
+  c->factored = -1;
+  return MOM_OK;
+}
+
+int assemble(Ctx *c, double omega, const double *ri, int precision) {
+  if (c->blk_fused && c->nga == 1 && c->ndom <= kGatherDoms) return assemble_fused(c, omega, ri, precision);
+  MOM_TRY(assemble_begin(c));
+  for (int d = 0; d < c->ndom; d++) MOM_TRY(assemble_domain(c, d, omega, ri, precision));
+  return assemble_end(c, precision);
 }
 
 // A caller's 2N x 2N matrix (host, column-major, lda) in place of an

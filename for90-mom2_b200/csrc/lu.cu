@@ -1217,6 +1217,24 @@ __global__ void residual_kernel(const double2 *B, int64_t ldb, const double2 *pa
   if (threadIdx.x == 0) rn2[(size_t)s * gridDim.x + blockIdx.x] = red[0];
 }
 
+// Y[s] += sign * (sum of partials)
+__global__ void acc_partials_kernel(double2 *Y, int64_t ldy, const double2 *partial, int nchunk, int64_t n, int nrhs,
+                                    double sign) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= n) return;
+  double2 acc = make_double2(0, 0);
+  for (int c = 0; c < nchunk; c++) {
+    const double2 p = partial[((size_t)c * nrhs + s) * n + i];
+    acc.x += p.x;
+    acc.y += p.y;
+  }
+  double2 y = Y[(size_t)s * ldy + i];
+  y.x += sign * acc.x;
+  y.y += sign * acc.y;
+  Y[(size_t)s * ldy + i] = y;
+}
+
 __global__ void axpy_kernel(double2 *X, const double2 *D, int64_t count) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t st = (int64_t)gridDim.x * blockDim.x;
@@ -2268,6 +2286,29 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
     char buf[160];
     snprintf(buf, sizeof buf, "iterative refinement stopped at relative residual %.3e > %.3e", worst, tol);
     return fail(c, MOM_ERR_NOCONV, buf);
+  }
+  return MOM_OK;
+}
+
+int matvec_acc(Ctx *c, const double2 *X, int nrhs, double2 *Y, double sign) {
+  const int64_t n = c->n;
+  const int nchunk = (int)((n + kGemvCols - 1) / kGemvCols);
+  const int rblocks = (int)((n + kGemvRows - 1) / kGemvRows);
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, sizeof(double2) * (size_t)nchunk * 8 * n));
+  double2 *Pp = (double2 *)c->ws;
+  for (int s0 = 0, ns = 0; s0 < nrhs; s0 += ns) {
+    ns = 8;
+    while (ns > nrhs - s0) ns >>= 1;
+    const double2 *xs0 = X + (size_t)s0 * n;
+    const dim3 gg(rblocks, nchunk);
+    if (ns == 1) gemv_partial_kernel<1><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+    else if (ns == 2) gemv_partial_kernel<2><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+    else if (ns == 4) gemv_partial_kernel<4><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+    else gemv_partial_kernel<8><<<gg, kGemvRows, 0, c->stream>>>(c->A, c->lda, n, xs0, n, Pp);
+    acc_partials_kernel<<<dim3((unsigned)((n + 255) / 256), ns), 256, 0, c->stream>>>(Y + (size_t)s0 * n, n, Pp,
+                                                                                     nchunk, n, ns, sign);
+    c->launches += 2;
+    MOM_CUDA(c, cudaGetLastError());
   }
   return MOM_OK;
 }

@@ -99,6 +99,13 @@ struct DomDev {
   // Symmetry group actions on this domain, [nga] (element 0 is the identity,
   // which uses the arrays above).
   std::vector<ActDev> act;
+  // Second-harmonic sources (uploaded on first use): free vertex of each
+  // local edge, the domain edge of each local edge, and the RWG Gram matrix
+  // <f_m, f_n> as 5 entries per row (the diagonal first).
+  double *shg_bn = nullptr;    // [F][3][3]
+  int *shg_fedge = nullptr;    // [F][3]
+  int *gram_col = nullptr;     // [Nd][5]
+  double *gram_val = nullptr;  // [Nd][5]
 };
 
 struct Ctx {
@@ -115,8 +122,10 @@ struct Ctx {
   void *blas_ws2 = nullptr;
   cudaEvent_t la_ev[3] = {nullptr, nullptr, nullptr};
   int lookahead = 1;       // MOM_LOOKAHEAD=0 turns it off
-  int la_ctas = 0;         // MOM_LA_CTAS: CTA cap of the look-ahead panels (0: the smallest that fits)
-  double la_from = 0.9;    // MOM_LA_FROM: overlap blocks whose height is below this fraction of n
+  // Defaults from a sweep on a B200 at n = 30,720 (the cap 32/48/64 and the
+  // fraction 0.9/0.95/all within 3% of each other; these were the fastest).
+  int la_ctas = 64;        // MOM_LA_CTAS: CTA cap of the look-ahead panels (0: the smallest that fits)
+  double la_from = 1.0;    // MOM_LA_FROM: overlap blocks whose trailing height is below this fraction of n
   std::mutex mu;
   std::string last_error;
   int64_t launches = 0;
@@ -152,7 +161,10 @@ struct Ctx {
   float2 *A32 = nullptr;   // FP32 copy (LU in place in mixed mode)
   size_t A_bytes = 0, A32_bytes = 0;
   double2 *blk = nullptr;  // face-pair blocks [source F][test F][9][2] of the largest domain
-  size_t blk_bytes = 0;
+  size_t blk_bytes = 0;    //   or, when blk_fused, of every domain at blk + blk_off[d]
+  bool blk_fused = false;
+  std::vector<size_t> blk_off;  // [ndom], in double2
+  int *dmap = nullptr;     // [ndom][N]: domain edge of each global edge, -1 if none
   int *ipiv = nullptr;     // [n]
   int *perm = nullptr;     // [n] composed row permutation of the factorisation
   double2 *invd = nullptr; // inverses of diagonal blocks (L then U), FP64
@@ -169,6 +181,7 @@ struct Ctx {
 
   // Right-hand sides / solutions
   int nsrc = 0;
+  bool solved = false;     // X holds the solutions of the current right-hand sides
   double2 *B = nullptr;    // [nsrc][n] right-hand sides
   double2 *X = nullptr;    // [nsrc][n] solutions
   size_t BX_cap = 0;
@@ -233,6 +246,14 @@ struct Ctx {
   size_t adj_part_bytes = 0;
   void *adjW = nullptr;
   size_t adjW_bytes = 0;
+
+  // Second-harmonic solve: source coefficients of the nonlinear domains and
+  // the scratch of their expansion.
+  void *shg_c = nullptr;
+  size_t shg_c_bytes = 0;
+  std::vector<int> shg_slot;  // [ndom]: slot of the domain's coefficients in shg_c, -1 for a linear domain
+  void *shg_ws = nullptr;
+  size_t shg_ws_bytes = 0;
 
   // Host-side staging (pinned)
   double *pinned = nullptr;
@@ -305,6 +326,11 @@ inline void select_rep(Ctx *c, int r) {
 int upload_quadrature(Ctx *c);
 int near_precompute(Ctx *c, int d);
 int assemble(Ctx *c, double omega, const double *ri, int precision);
+// The steps of assemble(): clear (and pad) the matrices; add domain d's
+// D, H and K blocks; boundary conditions, FP32 copy and state.
+int assemble_begin(Ctx *c);
+int assemble_domain(Ctx *c, int d, double omega, const double *ri, int precision);
+int assemble_end(Ctx *c, int precision);
 // The test faces of domain d mapped by group action g (J^T), their near
 // pairs and closed-form integrals (set-up of a symmetry group).
 int action_precompute(Ctx *c, int d, int g);
@@ -321,6 +347,14 @@ int lu_factor(Ctx *c, int precision);
 int lu_solve(Ctx *c, int precision, double tol, int maxit, int *iters);
 int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, int nrhs, double tol, int maxit,
                 int *iters);
+// Y[:, s] += sign * A X[:, s] with the FP64 matrix of the current
+// representation (n rows, ld n columns for X and Y).
+int matvec_acc(Ctx *c, const double2 *X, int nrhs, double2 *Y, double sign);
+
+// shg.cu: the second-harmonic solve (mom_gpu_shg_solve)
+int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const mom_nls *nls, int precision,
+              double tol, int maxit, int *iters);
+void free_shg(DomDev &D);
 
 // tc_gemm.cu: C -= L U (complex FP32) on the tensor cores, 3xTF32
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,

@@ -71,6 +71,10 @@ __device__ __forceinline__ void zx(const Zc *a, const Zc *b, Zc *r) {
 
 // pw_fields / pw_fields_elliptic (source.f90:84-125)
 __device__ void na_fields(const NaSrc &S, Zc k, double omega, const double *pt, Zc *ef, Zc *hf) {
+  if (S.type == MOM_SRC_NONE) {  // no incident field
+    for (int i = 0; i < 3; i++) ef[i] = hf[i] = {0, 0};
+    return;
+  }
   const double kd = S.dir[0] * pt[0] + S.dir[1] * pt[1] + S.dir[2] * pt[2];
   double sn, cs;
   sincos(k.re * kd, &sn, &cs);
@@ -234,8 +238,8 @@ extern "C" int mom_gpu_cross_sections_noalloc(mom_ctx *c, int32_t dom, double om
   NaSrc hs[kNaMaxSrc];
   for (int i = 0; i < nsrc; i++) {
     const mom_src &s = src[i];
-    if (s.type != MOM_SRC_PW && s.type != MOM_SRC_PW_ELLIPTIC)
-      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+    if (s.type != MOM_SRC_PW && s.type != MOM_SRC_PW_ELLIPTIC && s.type != MOM_SRC_NONE)
+      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw, pw_elliptic and none)");
     // get_dir / get_pol (aux.f90:245-261)
     const double th = s.theta, ph = s.phi, ps = (s.type == MOM_SRC_PW) ? s.psi : 0.0;
     hs[i].dir[0] = sin(th) * cos(ph);

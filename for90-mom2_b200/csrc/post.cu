@@ -8,6 +8,7 @@
 // deterministic (the reference adds them in face order).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -61,6 +62,10 @@ __device__ __forceinline__ Z zexp_i(Z k, double s) {  // exp(i k s)
 
 // pw_fields / pw_fields_elliptic (source.f90:84-125) at point pt.
 __device__ void src_fields(const SrcDev &S, Z k, double omega, const double *pt, Z *ef, Z *hf) {
+  if (S.type == MOM_SRC_NONE) {  // no incident field (src_fields, source.f90:328-329)
+    for (int i = 0; i < 3; i++) ef[i] = hf[i] = {0, 0};
+    return;
+  }
   const double kd = S.dir[0] * pt[0] + S.dir[1] * pt[1] + S.dir[2] * pt[2];
   const Z ph = zexp_i(k, kd);
   Z dc[3] = {{S.dir[0], 0}, {S.dir[1], 0}, {S.dir[2], 0}};
@@ -394,13 +399,16 @@ __global__ void ff_current_kernel(FfArgs a) {
 constexpr int kFfThreads = 128;
 constexpr int kFfTile = 128;
 
-// One thread per direction: N and L radiation vectors by the phasor sum over
-// all weighted quadrature points, then E_theta, E_phi at r = 1 m.
-__global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const double4 *cur, const double *pos,
-                                                            int ntheta, int nphi, Z k, Z ri, double *rcs) {
+// One thread per direction, the points split over blockIdx.y: partial N and
+// L radiation vectors (theta, phi components) by the phasor sum over the
+// split's weighted quadrature points, into part[split][direction][4].
+__global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, int per_split, const double4 *cur,
+                                                            const double *pos, int ntheta, int nphi, Z k,
+                                                            double2 *part) {
   __shared__ double4 s_cur[kFfTile][3];
   __shared__ double s_pos[kFfTile][3];
   const int dirx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p0 = blockIdx.y * per_split, p1 = min(npts, p0 + per_split);
   const int nd = ntheta * nphi;
   const int it = dirx % ntheta, ip = dirx / ntheta;
   const double theta = kPi * (double)it / (double)(ntheta - 1);
@@ -410,17 +418,17 @@ __global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const doub
   sincos(phi, &sp, &cp);
   const double ux = st * cp, uy = st * sp, uz = ct;
   Z Nt = {0, 0}, Np = {0, 0}, Lt = {0, 0}, Lp = {0, 0};
-  for (int base = 0; base < npts; base += kFfTile) {
+  for (int base = p0; base < p1; base += kFfTile) {
     __syncthreads();
     for (int i = threadIdx.x; i < kFfTile; i += blockDim.x) {
       const int j = base + i;
       for (int c = 0; c < 3; c++) {
-        s_cur[i][c] = (j < npts) ? cur[(size_t)j * 3 + c] : make_double4(0, 0, 0, 0);
-        s_pos[i][c] = (j < npts) ? pos[(size_t)j * 3 + c] : 0.0;
+        s_cur[i][c] = (j < p1) ? cur[(size_t)j * 3 + c] : make_double4(0, 0, 0, 0);
+        s_pos[i][c] = (j < p1) ? pos[(size_t)j * 3 + c] : 0.0;
       }
     }
     __syncthreads();
-    const int cnt = min(kFfTile, npts - base);
+    const int cnt = min(kFfTile, p1 - base);
     for (int i = 0; i < cnt; i++) {
       const double s = s_pos[i][0] * ux + s_pos[i][1] * uy + s_pos[i][2] * uz;
       // phasor = exp(-i k s)
@@ -441,6 +449,27 @@ __global__ void __launch_bounds__(kFfThreads) ff_dir_kernel(int npts, const doub
     }
   }
   if (dirx >= nd) return;
+  double2 *o = part + ((size_t)blockIdx.y * nd + dirx) * 4;
+  o[0] = make_double2(Nt.re, Nt.im);
+  o[1] = make_double2(Np.re, Np.im);
+  o[2] = make_double2(Lt.re, Lt.im);
+  o[3] = make_double2(Lp.re, Lp.im);
+}
+
+// Thread per direction: the splits' partial radiation vectors summed in
+// split order, then E_theta, E_phi at r = 1 m and the RCS.
+__global__ void ff_finish_kernel(int nd, int nsplit, const double2 *part, int ntheta, Z k, Z ri, double *rcs) {
+  const int dirx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dirx >= nd) return;
+  Z Nt = {0, 0}, Np = {0, 0}, Lt = {0, 0}, Lp = {0, 0};
+  for (int sp = 0; sp < nsplit; sp++) {
+    const double2 *o = part + ((size_t)sp * nd + dirx) * 4;
+    Nt = zadd(Nt, Z{o[0].x, o[0].y});
+    Np = zadd(Np, Z{o[1].x, o[1].y});
+    Lt = zadd(Lt, Z{o[2].x, o[2].y});
+    Lp = zadd(Lp, Z{o[3].x, o[3].y});
+  }
+  const int it = dirx % ntheta, ip = dirx / ntheta;
   // prefix = i k exp(i k r) / (4 pi r), r = 1
   const Z e = zexp_i(k, 1.0);
   const Z ik = {-k.im, k.re};
@@ -727,8 +756,8 @@ void make_src(const mom_src &s, SrcDev &d) {
 int upload_sources(Ctx *c, int nsrc, const mom_src *src, SrcDev **out) {
   std::vector<SrcDev> h(nsrc);
   for (int i = 0; i < nsrc; i++) {
-    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC)
-      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC && src[i].type != MOM_SRC_NONE)
+      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw, pw_elliptic and none)");
     make_src(src[i], h[i]);
   }
   const size_t bytes = sizeof(SrcDev) * nsrc;
@@ -885,8 +914,16 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   const int nd = ntheta * nphi;
   const size_t cur_bytes = sizeof(double4) * 3 * (size_t)npts;
   const size_t pos_bytes = sizeof(double) * 3 * (size_t)npts;
-  const size_t out_bytes = sizeof(double) * (size_t)nd;
-  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, cur_bytes + pos_bytes + out_bytes + 512));
+  const size_t out_bytes = ((sizeof(double) * (size_t)nd + 255) / 256) * 256;
+  // split the points so that about 8 CTAs per SM are in flight, at least
+  // 1024 points per split
+  const int dir_ctas = (nd + kFfThreads - 1) / kFfThreads;
+  int nsplit = std::max(1, (8 * c->nsm + dir_ctas - 1) / dir_ctas);
+  nsplit = std::min(nsplit, std::max(1, npts / 1024));
+  const int per_split = (npts + nsplit - 1) / nsplit;
+  nsplit = (npts + per_split - 1) / per_split;
+  const size_t part_bytes = sizeof(double2) * 4 * (size_t)nd * nsplit;
+  MOM_TRY(ensure_buffer(c, &c->ws, &c->ws_bytes, cur_bytes + pos_bytes + out_bytes + part_bytes + 512));
   FfArgs a;
   for (int i = 0; i < kMaxQ; i++) a.w[i] = c->qw[i];
   a.F = D.F;
@@ -902,6 +939,7 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   a.cur = reinterpret_cast<double4 *>(c->ws);
   a.pos = reinterpret_cast<double *>((char *)c->ws + cur_bytes);
   double *dout = reinterpret_cast<double *>((char *)c->ws + cur_bytes + pos_bytes);
+  double2 *dpart = reinterpret_cast<double2 *>((char *)c->ws + cur_bytes + pos_bytes + out_bytes);
   {
   ProfScope ps(c, kProfPost);
   if (c->nga > 1) ff_current_sym_kernel<<<(npts + 127) / 128, 128, 0, c->stream>>>(a, group_arg(c), xrep);
@@ -910,9 +948,10 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   MOM_CUDA(c, cudaGetLastError());
   const Z k = {ri[0] * omega / kC0, ri[1] * omega / kC0};
   const Z rz = {ri[0], ri[1]};
-  ff_dir_kernel<<<(nd + kFfThreads - 1) / kFfThreads, kFfThreads, 0, c->stream>>>(npts, a.cur, a.pos, ntheta, nphi,
-                                                                                 k, rz, dout);
-  c->launches++;
+  ff_dir_kernel<<<dim3(dir_ctas, nsplit), kFfThreads, 0, c->stream>>>(npts, per_split, a.cur, a.pos, ntheta, nphi,
+                                                                       k, dpart);
+  ff_finish_kernel<<<(nd + 127) / 128, 128, 0, c->stream>>>(nd, nsplit, dpart, ntheta, k, rz, dout);
+  c->launches += 2;
   MOM_CUDA(c, cudaGetLastError());
   }
   MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -964,8 +1003,8 @@ int add_incident_fields(Ctx *c, double omega, const double *ri, int nsrc, const 
   static_assert(sizeof(SrcDev) <= 128, "source record larger than the caller's scratch");
   std::vector<SrcDev> h(nsrc);
   for (int i = 0; i < nsrc; i++) {
-    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC)
-      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw and pw_elliptic)");
+    if (src[i].type != MOM_SRC_PW && src[i].type != MOM_SRC_PW_ELLIPTIC && src[i].type != MOM_SRC_NONE)
+      return fail(c, MOM_ERR_ARG, "unsupported source type (only pw, pw_elliptic and none)");
     make_src(src[i], h[i]);
   }
   SrcDev *d = reinterpret_cast<SrcDev *>(srcbuf);

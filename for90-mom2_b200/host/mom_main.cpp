@@ -23,12 +23,16 @@
 // field-component files of read_nfpl.
 //
 // Symmetry groups are products of id and the mirror groups mxp, myp, mzp
-// with the xplane / yplane / zplane boundaries of sbnd.  Commands of the
-// reference outside this path (rotation groups, periodic boundaries and
-// Green's functions, volume domains, second-harmonic media,
-// near fields, diffraction, polarizability, the VIE solver, source offsets
-// and scans) print an error and stop, as the reference does on invalid
-// input, instead of producing results this build does not compute.
+// with the xplane / yplane / zplane boundaries of sbnd.  Media may carry a
+// centrosymmetric surface nonlinearity (`smed m nlsurf value chi_nnn chi_ntt
+// chi_ttn`, identity group only): solv then also solves the second harmonic
+// (solver.f90:143-217) and crst, rcst, nfms, nfem, nfdm and nfpl also write
+// its results (-sh files).  Commands of the reference outside this path
+// (rotation groups, periodic boundaries and Green's functions, volume
+// domains, bulk nonlinearities, diffraction, polarizability, the VIE
+// solver, source offsets and scans) print an error and stop, as the
+// reference does on invalid input, instead of producing results this build
+// does not compute.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -199,7 +203,26 @@ struct State {
   std::vector<std::string> symm;     // named groups of the symmetry group (read_symm)
   int nga = 1;                       // its order
   std::vector<std::vector<double>> x;  // per wavelength: [nsrc][nga][2N] complex, interleaved
+  // Second harmonic: per medium the refractive indices at half the
+  // wavelength (prop%shri) and the surface nonlinearity; per wavelength the
+  // SH solutions and, per domain, the source coefficients of nonlinear ones.
+  std::vector<std::vector<cplx>> media_sh;  // [medium][wavelength]
+  std::vector<mom_nls> nls;                 // [medium]
+  std::vector<std::vector<double>> nlx;     // per wavelength, as x
+  std::vector<std::vector<std::vector<double>>> shc;  // [wavelength][domain]: empty if linear
 };
+
+void clear_solutions(State &s) {
+  s.x.clear();
+  s.nlx.clear();
+  s.shc.clear();
+}
+
+bool any_nls(const State &s) {
+  for (const auto &m : s.nls)
+    if (m.active) return true;
+  return false;
+}
 
 void check(State &s, int st, const char *what) {
   if (st == MOM_OK) return;
@@ -259,14 +282,19 @@ void ensure_ctx(State &s) {
   check(s, mom_gpu_create(s.device, &s.ctx), "mom_gpu_create");
 }
 
-std::vector<double> ri_table(const State &s, size_t n) {
+std::vector<double> ri_table(const State &s, size_t n, bool sh = false) {
   std::vector<double> ri(2 * s.doms.size());
   for (size_t d = 0; d < s.doms.size(); d++) {
-    const cplx v = s.media[s.doms[d].medium - 1][n];
+    const cplx v = (sh ? s.media_sh : s.media)[s.doms[d].medium - 1][n];
     ri[2 * d] = v.real();
     ri[2 * d + 1] = v.imag();
   }
   return ri;
+}
+
+// Refractive index of domain d's medium (1-based), fundamental or second harmonic.
+cplx dom_ri(const State &s, int d, int w, bool sh) {
+  return (sh ? s.media_sh : s.media)[s.doms[d - 1].medium - 1][w - 1];
 }
 
 // solve_batch (solver.f90:17-142): every wavelength, all sources.
@@ -312,6 +340,28 @@ void solve_batch(State &s) {
                                    s.maxit, s.x[n].data(), s.n2, &iters),
           "solv");
     if (s.precision == MOM_PREC_MIXED) std::printf(" Refinement steps: %d\n", iters);
+    if (any_nls(s)) {
+      // the second-harmonic branch of solve_batch (solver.f90:143-217)
+      std::printf(" Solving nonlinear scattering from centrosymmetric material\n");
+      if (s.nlx.size() != s.wl.size()) {
+        s.nlx.assign(s.wl.size(), std::vector<double>());
+        s.shc.assign(s.wl.size(), std::vector<std::vector<double>>(s.doms.size()));
+      }
+      const std::vector<double> shri = ri_table(s, n, true);
+      std::vector<mom_nls> dn(s.doms.size());
+      for (size_t d = 0; d < s.doms.size(); d++) dn[d] = s.nls[s.doms[d].medium - 1];
+      s.nlx[n].assign((size_t)2 * s.n2 * s.nga * nsrc, 0.0);
+      check(s,
+            mom_gpu_shg_solve(s.ctx, omega_of(s.wl[n]), ri.data(), shri.data(), dn.data(), s.precision, s.tol,
+                              s.maxit, s.nlx[n].data(), s.n2, &iters),
+            "solv (second harmonic)");
+      for (size_t d = 0; d < s.doms.size(); d++) {
+        s.shc[n][d].clear();
+        if (!dn[d].active) continue;
+        s.shc[n][d].assign((size_t)2 * s.n2 * nsrc, 0.0);
+        check(s, mom_gpu_shg_source_coef(s.ctx, (int32_t)d, s.shc[n][d].data(), s.n2), "solv (second harmonic)");
+      }
+    }
   }
   std::fflush(stdout);
 }
@@ -343,6 +393,21 @@ void crst(State &s, const std::vector<std::string> &it) {
     std::printf(" Wavelength %zu of %zu\n", n + 1, s.wl.size());
   }
   for (int k = 0; k < nsrc; k++) write_data(s.name + "-s" + std::to_string(k + 1) + ".crs", data[k]);
+  if (!s.nlx.empty()) {
+    // second harmonic: no incident field, 2 omega, the medium's SH index
+    const std::vector<mom_src> none(nsrc, mom_src{MOM_SRC_NONE, 0, 0, 0, 0, 0});
+    for (size_t n = 0; n < s.wl.size(); n++) {
+      const cplx v = s.media_sh[medium - 1][n];
+      const double ri[2] = {v.real(), v.imag()};
+      check(s,
+            mom_gpu_cross_sections(s.ctx, domain - 1, 2.0 * omega_of(s.wl[n]), ri, nsrc, none.data(),
+                                   s.nlx[n].data(), s.n2, csca.data(), cabs.data()),
+            "crst");
+      for (int k = 0; k < nsrc; k++) data[k][n] = {s.wl[n], csca[k] * factor, cabs[k] * factor};
+      std::printf(" Wavelength %zu of %zu\n", n + 1, s.wl.size());
+    }
+    for (int k = 0; k < nsrc; k++) write_data(s.name + "-s" + std::to_string(k + 1) + "-sh.crs", data[k]);
+  }
   std::fflush(stdout);
 }
 
@@ -354,15 +419,20 @@ void rcst(State &s, const std::vector<std::string> &it) {
   if (w < 1 || w > (int)s.wl.size() || k < 1 || k > (int)s.src.size() || nt < 1 || np < 1)
     stop("Error: index or grid size out of range in rcst!");
   std::printf(" Computing radar cross-sections\n");
-  const cplx v = s.media[s.doms[0].medium - 1][w - 1];
-  const double ri[2] = {v.real(), v.imag()};
-  std::vector<double> out((size_t)nt * np);
-  check(s, mom_gpu_rcs(s.ctx, 0, omega_of(s.wl[w - 1]), ri, k - 1, s.x[w - 1].data(), s.n2, nt, np, out.data()),
-        "rcst");
-  std::vector<std::vector<double>> rows(nt, std::vector<double>(np));
-  for (int i = 0; i < nt; i++)
-    for (int j = 0; j < np; j++) rows[i][j] = out[(size_t)j * nt + i];  // rcsdata(1:nt, 1:np), column-major
-  write_data(s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + ".rcs", rows);
+  for (int sh = 0; sh < (s.nlx.empty() ? 1 : 2); sh++) {
+    // the second pass: the SH solutions at 2 omega with domain 1's SH index
+    const cplx v = dom_ri(s, 1, w, sh);
+    const double ri[2] = {v.real(), v.imag()};
+    std::vector<double> out((size_t)nt * np);
+    check(s,
+          mom_gpu_rcs(s.ctx, 0, (sh ? 2.0 : 1.0) * omega_of(s.wl[w - 1]), ri, k - 1,
+                      (sh ? s.nlx : s.x)[w - 1].data(), s.n2, nt, np, out.data()),
+          "rcst");
+    std::vector<std::vector<double>> rows(nt, std::vector<double>(np));
+    for (int i = 0; i < nt; i++)
+      for (int j = 0; j < np; j++) rows[i][j] = out[(size_t)j * nt + i];  // rcsdata(1:nt, 1:np), column-major
+    write_data(s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + (sh ? "-sh.rcs" : ".rcs"), rows);
+  }
   std::fflush(stdout);
 }
 
@@ -370,6 +440,9 @@ void rcst(State &s, const std::vector<std::string> &it) {
 // fields of domain d on the n1 x n2 grid origin + i/(n1-1) v1 + j/(n2-1) v2,
 // plus the incident field in domain 1, expressed in the basis (v1/|v1|,
 // v2/|v2|, their cross product); 12 files per source, each n2 rows of n1.
+void nfpl_pass(State &s, int w, int d, int sh, const double *v1, const double *v2, int n1, int n2,
+               const std::vector<double> &pts, const std::string &tag);
+
 void nfpl(State &s, const std::vector<std::string> &it) {
   const int w = int_item(it, 1, "nfpl"), d = int_item(it, 2, "nfpl");
   double o[3], v1[3], v2[3];
@@ -384,19 +457,31 @@ void nfpl(State &s, const std::vector<std::string> &it) {
   if (s.x.empty()) stop("Error: solve (solv) before computing near fields!");
   if (w < 1 || w > (int)s.wl.size() || d < 1 || d > (int)s.doms.size() || n1 < 2 || n2 < 2)
     stop("Error: index or grid size out of range in nfpl (grids need at least 2 x 2 points)");
-  const int nsrc = (int)s.src.size(), npts = n1 * n2;
+  const int npts = n1 * n2;
   std::vector<double> pts(3 * (size_t)npts);
   for (int a = 0; a < n1; a++)
     for (int b = 0; b < n2; b++)
       for (int i = 0; i < 3; i++)
         pts[3 * ((size_t)a * n2 + b) + i] = o[i] + (double)a / (n1 - 1) * v1[i] + (double)b / (n2 - 1) * v2[i];
-  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  std::printf(" Computing near fields on a plane\n");
+  for (int sh = 0; sh < (s.nlx.empty() ? 1 : 2); sh++)
+    nfpl_pass(s, w, d, sh, v1, v2, n1, n2, pts, tag);
+  std::fflush(stdout);
+}
+
+// One pass of nfpl: the fundamental (incident field added in domain 1) or,
+// with sh, the second harmonic (2 omega, SH index, no incident field; file
+// stems end in -sh, interface.f90:855-888).
+void nfpl_pass(State &s, int w, int d, int sh, const double *v1, const double *v2, int n1, int n2,
+               const std::vector<double> &pts, const std::string &tag) {
+  const int nsrc = (int)s.src.size(), npts = n1 * n2;
+  const cplx v = dom_ri(s, d, w, sh);
   const double ri[2] = {v.real(), v.imag()};
   std::vector<double> e(6 * (size_t)npts * nsrc), h(6 * (size_t)npts * nsrc);
-  std::printf(" Computing near fields on a plane\n");
   check(s,
-        mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, d == 1 ? s.src.data() : nullptr,
-                            s.x[w - 1].data(), s.n2, npts, pts.data(), e.data(), h.data()),
+        mom_gpu_scat_fields(s.ctx, d - 1, (sh ? 2.0 : 1.0) * omega_of(s.wl[w - 1]), ri, nsrc,
+                            (d == 1 && !sh) ? s.src.data() : nullptr, (sh ? s.nlx : s.x)[w - 1].data(), s.n2, npts,
+                            pts.data(), e.data(), h.data()),
         "nfpl");
   double b1[3], b2[3], b3[3];
   const double l1 = std::sqrt(v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2]);
@@ -412,7 +497,7 @@ void nfpl(State &s, const std::vector<std::string> &it) {
   const char *comp[3] = {"x", "y", "z"};
   for (int k = 0; k < nsrc; k++) {
     const std::string stem = s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k + 1) + "-d" +
-                             std::to_string(d) + "-" + tag + "-";
+                             std::to_string(d) + "-" + tag + (sh ? "-sh-" : "-");
     for (int f = 0; f < 2; f++) {
       const std::vector<double> &src = f == 0 ? e : h;
       std::vector<std::vector<std::vector<double>>> R(3, std::vector<std::vector<double>>(n2, std::vector<double>(n1)));
@@ -432,7 +517,6 @@ void nfpl(State &s, const std::vector<std::string> &it) {
       for (int c = 0; c < 3; c++) write_data(stem + fl + comp[c] + "-im.dat", I[c]);
     }
   }
-  std::fflush(stdout);
 }
 
 // ---- field maps in Gmsh post-processing files (mesh.f90:1740-1978) ----
@@ -547,9 +631,16 @@ void field_indices(State &s, const std::vector<std::string> &it, const char *wha
     stop(std::string("Error: index out of range in ") + what);
 }
 
-std::string field_name(const State &s, int w, int k, int d) {
-  return s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + "-d" + std::to_string(d) + ".msh";
+std::string field_name(const State &s, int w, int k, int d, bool sh = false) {
+  return s.name + "-wl" + std::to_string(w) + "-s" + std::to_string(k) + "-d" + std::to_string(d) +
+         (sh ? "-sh.msh" : ".msh");
 }
+
+// Number of passes of a field command: the fundamental, then the second
+// harmonic when solv solved one.
+int passes(const State &s) { return s.nlx.empty() ? 1 : 2; }
+
+void nfms_pass(State &s, int w, int k, int d, int sh);
 
 // read_nfms (interface.f90:772-803) -> field_mesh (nfpost.f90:167-262): the
 // fields on domain d's boundary, on the domain mesh and its images under the
@@ -558,15 +649,23 @@ void nfms(State &s, const std::vector<std::string> &it) {
   int w, k, d;
   field_indices(s, it, "nfms", &w, &k, &d);
   std::printf(" Computing near fields on particle mesh.\n");
-  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  for (int sh = 0; sh < passes(s); sh++) nfms_pass(s, w, k, d, sh);
+  std::fflush(stdout);
+}
+
+// One pass of nfms; the second harmonic's at 2 omega with the SH index
+// (read_nfms, interface.f90:794-801).
+void nfms_pass(State &s, int w, int k, int d, int sh) {
+  const cplx v = dom_ri(s, d, w, sh);
   const double ri[2] = {v.real(), v.imag()};
   std::vector<double> nodes;
   std::vector<int> faces;
   domain_mesh(s, d - 1, nodes, faces);
   const int nn = (int)(nodes.size() / 3), nf = (int)(faces.size() / 3), nga = s.nga;
   std::vector<double> e(6 * (size_t)nf * nga), h(6 * (size_t)nf * nga);
-  check(s, mom_gpu_surface_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, k - 1, s.x[w - 1].data(), s.n2, e.data(),
-                                  h.data()),
+  check(s,
+        mom_gpu_surface_fields(s.ctx, d - 1, (sh ? 2.0 : 1.0) * omega_of(s.wl[w - 1]), ri, k - 1,
+                               (sh ? s.nlx : s.x)[w - 1].data(), s.n2, e.data(), h.data()),
         "nfms");
   // the image mesh: nodes J p, faces renumbered per element, normals J n
   std::vector<double> n2((size_t)3 * nn * nga), nor((size_t)3 * nf * nga);
@@ -588,7 +687,7 @@ void nfms(State &s, const std::vector<std::string> &it) {
       }
     }
   }
-  save_vector_fields_msh(field_name(s, w, k, d), n2, f2, nor, e, h, s.scale);
+  save_vector_fields_msh(field_name(s, w, k, d, sh), n2, f2, nor, e, h, s.scale);
   double emax = 0;
   for (size_t n = 0; n < (size_t)nf * nga; n++) {
     double m = 0;
@@ -596,7 +695,6 @@ void nfms(State &s, const std::vector<std::string> &it) {
     emax = std::max(emax, std::sqrt(m));
   }
   std::printf(" Maximum of |E| is %.15E\n", emax);
-  std::fflush(stdout);
 }
 
 // read_nfem (interface.f90:1010-1090) -> field_external_mesh
@@ -615,8 +713,6 @@ void nfem(State &s, const std::vector<std::string> &it) {
     stop("Error in nfem: could not read mesh " + it[4]);
   }
   std::printf(" Computing near fields on external mesh.\n");
-  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
-  const double ri[2] = {v.real(), v.imag()};
   std::vector<double> nodes, pts, nor;
   std::vector<int> faces;
   {
@@ -639,15 +735,29 @@ void nfem(State &s, const std::vector<std::string> &it) {
     }
   }
   const int nf = (int)(faces.size() / 3), nsrc = (int)s.src.size();
-  std::vector<double> e(6 * (size_t)nf * nsrc), h(6 * (size_t)nf * nsrc);
-  check(s, mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, addsrc ? s.src.data() : nullptr,
-                               s.x[w - 1].data(), s.n2, nf, pts.data(), e.data(), h.data()),
-        "nfem");
-  std::vector<double> ek(e.begin() + 6 * (size_t)nf * (k - 1), e.begin() + 6 * (size_t)nf * k),
-      hk(h.begin() + 6 * (size_t)nf * (k - 1), h.begin() + 6 * (size_t)nf * k);
-  save_vector_fields_msh(field_name(s, w, k, d), nodes, faces, nor, ek, hk, s.scale);
+  for (int sh = 0; sh < passes(s); sh++) {
+    // second harmonic: 2 omega, the SH index, no incident field, and in a
+    // nonlinear domain the source coefficients added to nlx
+    // (interface.f90:1050-1085)
+    const cplx v = dom_ri(s, d, w, sh);
+    const double ri[2] = {v.real(), v.imag()};
+    std::vector<double> xs = (sh ? s.nlx : s.x)[w - 1];
+    if (sh && !s.shc[w - 1][d - 1].empty())
+      for (size_t i = 0; i < xs.size(); i++) xs[i] += s.shc[w - 1][d - 1][i];
+    std::vector<double> e(6 * (size_t)nf * nsrc), h(6 * (size_t)nf * nsrc);
+    check(s,
+          mom_gpu_scat_fields(s.ctx, d - 1, (sh ? 2.0 : 1.0) * omega_of(s.wl[w - 1]), ri, nsrc,
+                              (addsrc && !sh) ? s.src.data() : nullptr, xs.data(), s.n2, nf, pts.data(), e.data(),
+                              h.data()),
+          "nfem");
+    std::vector<double> ek(e.begin() + 6 * (size_t)nf * (k - 1), e.begin() + 6 * (size_t)nf * k),
+        hk(h.begin() + 6 * (size_t)nf * (k - 1), h.begin() + 6 * (size_t)nf * k);
+    save_vector_fields_msh(field_name(s, w, k, d, sh), nodes, faces, nor, ek, hk, s.scale);
+  }
   std::fflush(stdout);
 }
+
+void nfdm_pass(State &s, int w, int k, int d, int sh, bool addsrc, const std::vector<double> &pts);
 
 // read_nfdm (interface.f90:1092-1139) -> field_domain (nfpost.f90:85-165):
 // scat_fields of domain d on a regular grid of npoints(1:3) points over the
@@ -668,7 +778,7 @@ void nfdm(State &s, const std::vector<std::string> &it) {
     np[i] = int_item(it, 11 + i, "nfdm");
     if (np[i] < 2) stop("Error: nfdm needs at least 2 points per axis");
   }
-  const int npts = np[0] * np[1] * np[2], nsrc = (int)s.src.size();
+  const int npts = np[0] * np[1] * np[2];
   std::vector<double> pts(3 * (size_t)npts);
   for (int a = 0; a < np[0]; a++)
     for (int b = 0; b < np[1]; b++)
@@ -678,11 +788,22 @@ void nfdm(State &s, const std::vector<std::string> &it) {
                              (float)c / (float)(np[2] - 1)};
         for (int i = 0; i < 3; i++) pts[3 * idx + i] = org[i] - dsz[i] / 2 + dsz[i] * (double)fr[i];
       }
-  const cplx v = s.media[s.doms[d - 1].medium - 1][w - 1];
+  for (int sh = 0; sh < passes(s); sh++)
+    nfdm_pass(s, w, k, d, sh, addsrc && !sh, pts);
+  std::fflush(stdout);
+}
+
+// One pass of nfdm; the second harmonic's at 2 omega with the SH index and
+// no incident field (interface.f90:1126-1137).
+void nfdm_pass(State &s, int w, int k, int d, int sh, bool addsrc, const std::vector<double> &pts) {
+  const int npts = (int)(pts.size() / 3), nsrc = (int)s.src.size();
+  const cplx v = dom_ri(s, d, w, sh);
   const double ri[2] = {v.real(), v.imag()};
   std::vector<double> e(6 * (size_t)npts * nsrc), h(6 * (size_t)npts * nsrc);
-  check(s, mom_gpu_scat_fields(s.ctx, d - 1, omega_of(s.wl[w - 1]), ri, nsrc, addsrc ? s.src.data() : nullptr,
-                               s.x[w - 1].data(), s.n2, npts, pts.data(), e.data(), h.data()),
+  check(s,
+        mom_gpu_scat_fields(s.ctx, d - 1, (sh ? 2.0 : 1.0) * omega_of(s.wl[w - 1]), ri, nsrc,
+                            addsrc ? s.src.data() : nullptr, (sh ? s.nlx : s.x)[w - 1].data(), s.n2, npts, pts.data(),
+                            e.data(), h.data()),
         "nfdm");
   const double *ek = &e[6 * (size_t)npts * (k - 1)], *hk = &h[6 * (size_t)npts * (k - 1)];
   auto mag = [&](size_t n) {
@@ -699,7 +820,7 @@ void nfdm(State &s, const std::vector<std::string> &it) {
   std::vector<int> faces;
   domain_mesh(s, d - 1, nodes, faces);
   const int nn = (int)(nodes.size() / 3), nf = (int)(faces.size() / 3), m = (int)keep.size();
-  const std::string path = field_name(s, w, k, d);
+  const std::string path = field_name(s, w, k, d, sh);
   std::FILE *f = std::fopen(path.c_str(), "w");
   if (!f) stop("Could not open output file" + path + "!");
   msh_header(f);
@@ -724,7 +845,6 @@ void nfdm(State &s, const std::vector<std::string> &it) {
     }
   }
   std::fclose(f);
-  std::fflush(stdout);
 }
 
 void command(State &s, const std::string &cmd, const std::vector<std::string> &it) {
@@ -749,14 +869,14 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     if (n < 1) stop("Error: wlrg needs at least one wavelength");
     s.wl.assign(n, a);
     for (int i = 0; n > 1 && i < n; i++) s.wl[i] = a + (b - a) * ((double)i / (double)(n - 1));
-    s.x.clear();
+    clear_solutions(s);
   } else if (cmd == "wlls") {
     // read_wllist (interface.f90:391-406)
     const int n = int_item(it, 1, "wlls");
     if (n < 1) stop("Error: wlls needs at least one wavelength");
     s.wl.resize(n);
     for (int i = 0; i < n; i++) s.wl[i] = real_item(it, 2 + i, "wlls");
-    s.x.clear();
+    clear_solutions(s);
   } else if (cmd == "symm") {
     // read_symm (interface.f90:160-210): products of id and the mirror
     // groups mxp, myp, mzp (the rotation groups rN are not supported)
@@ -779,7 +899,7 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     if (order > MOM_MAX_GROUP) stop("Error: symmetry group too large");
     s.symm = order > 1 ? names : std::vector<std::string>();
     s.uploaded = false;
-    s.x.clear();
+    clear_solutions(s);
     std::printf(" Created a symmetry group with %d elements.\n", order);
   } else if (cmd == "sbnd") {
     // read_sbnd (interface.f90:125-157) -> classify_edges (mesh.f90:155-175)
@@ -807,9 +927,13 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     }
     const int n = int_item(it, 1, "nmed");
     s.media.assign(n, std::vector<cplx>(s.wl.size(), cplx(1.0, 0.0)));
+    s.media_sh = s.media;
+    s.nls.assign(n, mom_nls{0, {0, 0}, {0, 0}, {0, 0}});
+    clear_solutions(s);
     std::printf(" Allocated %d media.\n", n);
   } else if (cmd == "smed") {
-    // read_smed (interface.f90:234-355): linear media only
+    // read_smed (interface.f90:234-355): linear media (refractive indices at
+    // the wavelength and at half of it) and surface nonlinearities
     if (s.media.empty()) {
       std::printf(" Error: no media allocated!\n");
       return;
@@ -817,14 +941,32 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     const int m = int_item(it, 1, "smed");
     if (m < 1 || m > (int)s.media.size()) stop("Error: medium index out of range in smed");
     if (it.size() < 4) stop("Error: smed needs a type, a method and a value");
-    if (it[2] != "linear") stop("Error: medium type '" + it[2] + "' is not supported by this build (only linear)");
-    if (it[3] == "value") {
+    if (it[2] != "linear" && it[2] != "nlsurf") {
+      if (it[2] == "nlbulk-nonlocal" || it[2] == "nlbulk-dipole")
+        stop("Error: medium type '" + it[2] + "' is not supported by this build (linear, nlsurf)");
+      std::printf(" Unrecognized material type!\n");
+      return;
+    }
+    s.nls[m - 1].active = 0;  // every smed first makes the medium linear
+    clear_solutions(s);
+    if (it[2] == "nlsurf") {
+      if (it[3] != "value") {
+        std::printf(" Unrecongnized method for retrieveing medium properties!\n");
+        return;
+      }
+      const cplx a = complex_item(it, 4, "smed"), b = complex_item(it, 5, "smed"), c = complex_item(it, 6, "smed");
+      s.nls[m - 1] = mom_nls{1, {a.real(), a.imag()}, {b.real(), b.imag()}, {c.real(), c.imag()}};
+    } else if (it[3] == "value") {
       const cplx v = complex_item(it, 4, "smed");
       for (auto &r : s.media[m - 1]) r = v;
+      for (auto &r : s.media_sh[m - 1]) r = v;
       std::printf("Set medium %d refractive index to (%6.3f,%6.3f)\n", m, v.real(), v.imag());
     } else if (it[3] == "file") {
       if (it.size() < 5) stop("Error: smed file needs a file name");
-      for (size_t n = 0; n < s.wl.size(); n++) s.media[m - 1][n] = refind_from_file(it[4], s.wl[n]);
+      for (size_t n = 0; n < s.wl.size(); n++) {
+        s.media[m - 1][n] = refind_from_file(it[4], s.wl[n]);
+        s.media_sh[m - 1][n] = refind_from_file(it[4], s.wl[n] * 0.5);
+      }
       std::printf("Set medium %d refractive index to %s\n", m, it[4].c_str());
     } else {
       std::printf(" Unrecongnized method for retrieveing medium properties!\n");
@@ -871,7 +1013,7 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
     if (n < 1) stop("Error: nsrc needs at least one source");
     s.src.assign(n, mom_src());
     s.src_set.assign(n, false);
-    s.x.clear();
+    clear_solutions(s);
     std::printf(" Allocated %d sources.\n", n);
   } else if (cmd == "ssrc") {
     // read_ssrc (interface.f90:486-550): plane waves only
@@ -897,7 +1039,7 @@ void command(State &s, const std::string &cmd, const std::vector<std::string> &i
       stop("Error: source type '" + it[2] + "' is not supported by this build (pw, pw_elliptic)");
     }
     s.src_set[k - 1] = true;
-    s.x.clear();
+    clear_solutions(s);
   } else if (cmd == "quad") {
     // read_quad (interface.f90:18-30): the triangle rule; the tetrahedron rule
     // belongs to the volume solver

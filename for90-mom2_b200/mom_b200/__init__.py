@@ -30,7 +30,7 @@ MOM_OK = 0
 MOM_ERR_ARG, MOM_ERR_ALLOC, MOM_ERR_CUDA, MOM_ERR_SINGULAR, MOM_ERR_TIMEOUT = 1, 2, 3, 4, 5
 MOM_ERR_STATE, MOM_ERR_MESH, MOM_ERR_NOCONV, MOM_ERR_IO = 6, 7, 8, 9
 FP64, MIXED = 0, 1
-SRC_PW, SRC_PW_ELLIPTIC = 1, 10
+SRC_NONE, SRC_PW, SRC_PW_ELLIPTIC = 0, 1, 10
 
 # constants.f90:8-14 (pi is a single-precision literal in the reference)
 PI_F = float(np.float32(3.141592653589))
@@ -50,7 +50,8 @@ EXPORTS = [
     "mom_gpu_sweep", "mom_gpu_sweep_many", "mom_gpu_autotune_result", "mom_gpu_autotune_placement", "mom_gpu_scat_fields",
     "mom_gpu_set_matrix", "mom_gpu_set_wait_limits", "mom_gpu_set_symmetry", "mom_gpu_group_order",
     "mom_problem_set_lines", "mom_problem_classify_edges", "mom_problem_edge_bnd",
-    "mom_gpu_surface_fields", "mom_gpu_group_action",
+    "mom_gpu_surface_fields", "mom_gpu_group_action", "mom_gpu_shg_solve",
+    "mom_gpu_shg_source_coef",
 ]
 
 # Boundary types of mesh edges (sbnd; mesh.f90:16-25).
@@ -75,6 +76,11 @@ class MomMesh(C.Structure):
 class MomSrc(C.Structure):
     _fields_ = [("type", C.c_int32), ("theta", C.c_double), ("phi", C.c_double), ("psi", C.c_double),
                 ("phase_re", C.c_double), ("phase_im", C.c_double)]
+
+
+class MomNls(C.Structure):
+    _fields_ = [("active", C.c_int32), ("chi_nnn", C.c_double * 2), ("chi_ntt", C.c_double * 2),
+                ("chi_ttn", C.c_double * 2)]
 
 
 _lib = None
@@ -132,6 +138,9 @@ def lib():
     L.mom_problem_edge_bnd.argtypes = [vp, ip]
     L.mom_gpu_surface_fields.argtypes = [vp, C.c_int32, C.c_double, dp, C.c_int32, vp, C.c_int64, dp, dp]
     L.mom_gpu_group_action.argtypes = [vp, C.c_int32, dp, dp]
+    L.mom_gpu_shg_solve.argtypes = [vp, C.c_double, dp, dp, C.POINTER(MomNls), C.c_int32, C.c_double, C.c_int32,
+                                    vp, C.c_int64, ip]
+    L.mom_gpu_shg_source_coef.argtypes = [vp, C.c_int32, vp, C.c_int64]
     L.mom_gpu_device_solution.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_int64), ip]
     L.mom_gpu_synchronize.argtypes = [vp]
     L.mom_gpu_launch_count.argtypes = [vp]
@@ -205,12 +214,19 @@ def src_pw_elliptic(theta_deg: float, phi_deg: float, phase: complex) -> dict:
     return dict(type="pw_elliptic", theta=theta_deg * DEGTORAD, phi=phi_deg * DEGTORAD, phase=complex(phase))
 
 
+def src_none() -> dict:
+    """No incident field (nlsrc%type = 0): the cross sections of second-harmonic solutions."""
+    return dict(type="none")
+
+
 def _srcs(srcs):
     if isinstance(srcs, dict):
         srcs = [srcs]
     arr = (MomSrc * len(srcs))()
     for i, s in enumerate(srcs):
-        if s["type"] == "pw":
+        if s["type"] == "none":
+            arr[i] = MomSrc(SRC_NONE, 0.0, 0.0, 0.0, 0.0, 0.0)
+        elif s["type"] == "pw":
             arr[i] = MomSrc(SRC_PW, s["theta"], s["phi"], s["psi"], 0.0, 0.0)
         else:
             ph = complex(s["phase"])
@@ -442,6 +458,39 @@ class Solver:
                  "solve_wavelength")
         self.nsrc = ns
         self.iters = it.value
+        return x
+
+    def shg_solve(self, omega, ri, shri, nls, precision=FP64, tol=1e-12, maxit=30, want_host=True):
+        """The second-harmonic solve after solve_wavelength at the fundamental
+        frequency omega (solver.f90:143-217): nls[d] is None for a linear domain or
+        (chi_nnn, chi_ntt, chi_ttn) of its surface nonlinearity (``smed m nlsurf
+        value ...``); ri / shri are the fundamental and second-harmonic refractive
+        indices per domain.  Returns nlx (2N x nsrc); afterwards the device
+        solutions are the second harmonic's (cross sections with src_none() at
+        2 omega and shri)."""
+        if len(nls) != self.ndom:
+            raise ValueError("nls needs one entry per domain")
+        arr = (MomNls * self.ndom)()
+        for d, v in enumerate(nls):
+            if v is None:
+                arr[d] = MomNls(0, (0.0, 0.0), (0.0, 0.0), (0.0, 0.0))
+            else:
+                c = [complex(t) for t in v]
+                arr[d] = MomNls(1, (c[0].real, c[0].imag), (c[1].real, c[1].imag), (c[2].real, c[2].imag))
+        r, rs = _ri(ri), _ri(shri)
+        x = self._cols(self.nsrc) if want_host else None
+        it = C.c_int32()
+        self._ck(lib().mom_gpu_shg_solve(self.h, omega, _dp(r), _dp(rs), arr, precision, tol, maxit,
+                                         x.ctypes.data if x is not None else None, 2 * self.N, C.byref(it)),
+                 "shg_solve")
+        self.iters = it.value
+        return x
+
+    def shg_source_coef(self, dom):
+        """The source coefficients (cJ on rows [0, N), cM on [N, 2N)) of nonlinear
+        domain dom from the last shg_solve, 2N x nsrc."""
+        x = self._cols(self.nsrc)
+        self._ck(lib().mom_gpu_shg_source_coef(self.h, dom, x.ctypes.data, 2 * self.N), "shg_source_coef")
         return x
 
     def cross_sections(self, omega, ri, srcs, x=None, dom=0):

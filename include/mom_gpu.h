@@ -48,7 +48,10 @@ extern "C" {
 /* Largest symmetry group (three mirror planes). */
 #define MOM_MAX_GROUP 8
 
-/* Source types (source.f90:20-30). */
+/* Source types (source.f90:20-30).  MOM_SRC_NONE has no incident field: the
+ * reference's cross sections of second-harmonic solutions use it
+ * (nlsrc%type = 0, interface.f90:1441-1458). */
+#define MOM_SRC_NONE 0
 #define MOM_SRC_PW 1
 #define MOM_SRC_PW_ELLIPTIC 10
 
@@ -71,10 +74,18 @@ typedef struct mom_mesh {
 
 /* Excitation (srcdata, source.f90:36-58); angles in radians. */
 typedef struct mom_src {
-  int32_t type;           /* MOM_SRC_PW or MOM_SRC_PW_ELLIPTIC */
+  int32_t type;           /* MOM_SRC_PW, MOM_SRC_PW_ELLIPTIC or MOM_SRC_NONE */
   double theta, phi, psi; /* psi unused for pw_elliptic */
   double phase_re, phase_im; /* pw_elliptic Ex/Ey phase factor */
 } mom_src;
+
+/* Surface second-order nonlinearity of a domain's medium (medium_nls,
+ * nlsurf.f90:14-18; `smed m nlsurf value chi_nnn chi_ntt chi_ttn`).  The
+ * susceptibilities are complex (re, im); active = 0 marks a linear medium. */
+typedef struct mom_nls {
+  int32_t active;
+  double chi_nnn[2], chi_ntt[2], chi_ttn[2];
+} mom_nls;
 
 /* Context on one CUDA device.  Owns a stream, cuBLAS handle and the device
  * copies of the problem, the system matrix, its LU factors and solutions. */
@@ -140,6 +151,34 @@ int mom_gpu_solve(mom_ctx *ctx, int32_t precision, double tol, int32_t maxit, do
 int mom_gpu_solve_wavelength(mom_ctx *ctx, double omega, const double *ri, int32_t nsrc, const mom_src *src,
                              int32_t precision, double tol, int32_t maxit, double *x_host, int64_t ldx,
                              int32_t *iters_out);
+
+/* The second-harmonic branch of solve_batch for centrosymmetric surface
+ * nonlinearities (solver.f90:143-217): after a solve at the fundamental
+ * frequency omega (the device solutions of its nsrc sources), for every
+ * domain with nls[d].active the source coefficients and source vector of
+ * nlsurf_coef (nlsurf.f90:137-338: the surface polarisation of the
+ * fundamental field inside domain d, expanded in the domain's RWG functions),
+ * the system matrix at 2 omega with the second-harmonic refractive indices
+ * shri [ndom][2] and its source terms (sysmat_pmchwt_nls, sysmat.f90:112-229),
+ * then the solve.  ri [ndom][2] are the fundamental indices (the field
+ * inside domain d and the selvedge permittivity of determine_epsp,
+ * solver.f90:393-433).  Afterwards the device solutions, matrix and factors
+ * are those of the second harmonic: cross sections with MOM_SRC_NONE
+ * sources at 2 omega and shri give the reference's -sh.crs values.
+ * nlx_host (2N x nsrc, ldx) may be NULL.  Identity symmetry group only
+ * (MOM_ERR_ARG otherwise); a domain face that no other domain shares gives
+ * MOM_ERR_ARG ("Could not find epsp!"). */
+int mom_gpu_shg_solve(mom_ctx *ctx, double omega, const double *ri, const double *shri, const mom_nls *nls,
+                      int32_t precision, double tol, int32_t maxit, double *nlx_host, int64_t ldx,
+                      int32_t *iters_out);
+
+/* The source coefficients of domain dom from the last mom_gpu_shg_solve
+ * (src_coef(:, dom, 1, :), nlsurf.f90:137-338) on the global unknowns: cJ on
+ * the domain's edges in rows [0, N), cM in rows [N, 2N), zero elsewhere;
+ * 2N x nsrc, ldc.  The fields inside a nonlinear domain come from nlx plus
+ * these (read_nfem, interface.f90:1060-1078).  MOM_ERR_STATE if dom was not
+ * nonlinear in that solve. */
+int mom_gpu_shg_source_coef(mom_ctx *ctx, int32_t dom, double *coef_host, int64_t ldc);
 
 /* Replaces cs_prtsrf (cs.f90:14-104) for nsrc sources: scattering and
  * absorption cross sections from the surface currents on domain dom

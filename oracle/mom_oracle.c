@@ -1064,6 +1064,10 @@ static void src_fields(const osrc *s, double omega, cplx ri, const double *pt, c
   double dir[3], pol[3];
   cplx k = ri * omega / O_C0;
   cplx dc[3];
+  if (s->type != 1 && s->type != 10) { /* no source (type 0, the SH cross sections): zero fields */
+    for (int i = 0; i < 3; i++) ef[i] = hf[i] = 0;
+    return;
+  }
   get_dir(s->theta, s->phi, dir);
   for (int i = 0; i < 3; i++) dc[i] = dir[i];
   if (s->type == 1) {

@@ -166,7 +166,10 @@ class OSrc(C.Structure):
 
 def make_src(src: dict) -> OSrc:
     """src: {'type': 'pw', 'theta', 'phi', 'psi'} or {'type': 'pw_elliptic', 'theta', 'phi', 'phase'},
-    angles in radians (``ssrc`` converts degrees with the float-rounded pi, interface.f90:486-515)."""
+    angles in radians (``ssrc`` converts degrees with the float-rounded pi, interface.f90:486-515);
+    {'type': 'none'}: no incident field (type 0, the second-harmonic cross sections)."""
+    if src["type"] == "none":
+        return OSrc(0, 0.0, 0.0, 0.0, 0.0, 0.0)
     if src["type"] == "pw":
         return OSrc(1, src["theta"], src["phi"], src["psi"], 0.0, 0.0)
     ph = complex(src["phase"])
@@ -444,6 +447,192 @@ def field_mesh(P, d, omega, ri, x, group=None):
             e[g * F + f] = et + nor * en
             h[g * F + f] = ht + nor * hn
     return e, h
+
+
+# ---- second-harmonic generation from a centrosymmetric surface nonlinearity ----
+
+def _domain_geometry(P, d, qd):
+    """Per face of domain d: vertices, centroid, normal, area, quadrature points;
+    per (face, local edge): domain edge index, sign, length, free vertex."""
+    m = P.export(d)
+    nodes, fnode, fedge = m["nodes"], m["face_node"], m["face_edge"]
+    w, qn = qd
+    F = len(fnode)
+    g = dict(m=m, F=F, w=w)
+    p = nodes[fnode]  # [F][3][3]
+    g["n"] = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    g["n"] /= np.linalg.norm(g["n"], axis=1)[:, None]
+    g["A"] = 0.5 * np.linalg.norm(np.cross(-(p[:, 0] - p[:, 2]), p[:, 2] - p[:, 1]), axis=1)
+    # quad_tri_points (quad.f90:352-367): qn[2] p1 + qn[0] p2 + qn[1] p3
+    g["qp"] = (qn[None, :, 2, None] * p[:, None, 0] + qn[None, :, 0, None] * p[:, None, 1]
+               + qn[None, :, 1, None] * p[:, None, 2])
+    g["edge"] = fedge
+    sign = np.where(m["edge_face"][fedge, 0] == np.arange(F)[:, None], 1.0, -1.0)
+    g["sign"] = sign
+    en = m["edge_node"][fedge]
+    g["len"] = np.linalg.norm(nodes[en[..., 0]] - nodes[en[..., 1]], axis=-1)
+    g["free"] = nodes[np.where(sign > 0, m["edge_bnode"][fedge, 0], m["edge_bnode"][fedge, 1])]
+    return g
+
+
+def _rwg(g, f, q, r):
+    """rwg (rwgf.f90:13-49) of local edge q of face f at points r [..., 3]."""
+    return g["sign"][f, q] * g["len"][f, q] / (2 * g["A"][f]) * (r - g["free"][f, q])
+
+
+def rwg_moments(g):
+    """rwg_moments (rwgf.f90:148-221): the Gram matrix <f_m, f_n> of the domain's
+    RWG functions (diagonal over both faces of an edge; off-diagonal over the
+    first common face)."""
+    Nd = len(g["m"]["edge_node"])
+    Fm = np.zeros((Nd, Nd))
+    for f in range(g["F"]):
+        for q in range(3):
+            for p_ in range(3):
+                a = _rwg(g, f, q, g["qp"][f])
+                b = _rwg(g, f, p_, g["qp"][f])
+                Fm[g["edge"][f, q], g["edge"][f, p_]] += g["A"][f] * np.sum(g["w"] * np.einsum("ri,ri->r", a, b))
+    return Fm
+
+
+def nlsurf_coef(P, d, qd, omega_ff, ri_ff, epsp, xff, chi2):
+    """nlsurf_coef (nlsurf.f90:137-338, identity group, the expansion method):
+    the surface polarisation P = eps0 (chi_nnn En^2 + chi_ntt Et.Et) n
+    + 2 eps0 chi_ttn Et En of the fundamental surface field (efield,
+    nlsurf.f90:22-51), projected on the domain's RWG functions and expanded
+    through the Gram matrix.  Returns (src_coef (cM, cJ), src_vec (E0, H0)),
+    each 2 Nd in the domain's edge numbering."""
+    g = _domain_geometry(P, d, qd)
+    m = g["m"]
+    N, Nd = P.N, len(m["edge_node"])
+    par = m["edge_parent"]
+    chi_nnn, chi_ntt, chi_ttn = chi2
+    omega_sh = 2.0 * omega_ff
+    eps = ri_ff ** 2 * EPS0
+    coef = np.zeros(Nd, complex)
+    sc = np.zeros(2 * Nd, complex)
+    sv = np.zeros(2 * Nd, complex)
+    for f in range(g["F"]):
+        nor = g["n"][f]
+        qp = g["qp"][f]
+        # efield at the quadrature points
+        divj = sum(xff[par[g["edge"][f, q]]] * g["sign"][f, q] * g["len"][f, q] / g["A"][f] for q in range(3))
+        ms = sum(xff[N + par[g["edge"][f, q]]] * _rwg(g, f, q, qp) for q in range(3))
+        en_ = divj / (1j * omega_ff * eps)
+        e = np.cross(nor, ms) + nor[None, :] * en_
+        en = e @ nor
+        et = e - en[:, None] * nor[None, :]
+        Pn_ = EPS0 * (chi_nnn * en ** 2 + chi_ntt * np.sum(et * et, axis=1))
+        Pt_ = 2.0 * EPS0 * chi_ttn * et * en[:, None]
+        Pfull = Pt_ + Pn_[:, None] * nor[None, :]
+        Pn = Pfull @ nor
+        Pt = Pfull - Pn[:, None] * nor[None, :]
+        for q in range(3):
+            fmdiv = g["sign"][f, q] * g["len"][f, q] / g["A"][f]
+            fm = _rwg(g, f, q, qp)
+            int1 = -np.sum(g["w"] * fmdiv * Pn)
+            int2 = np.sum(g["w"] * np.sum(fm * np.cross(Pt, nor[None, :]), axis=1))
+            int3 = np.sum(g["w"] * np.sum(fm * Pt, axis=1))
+            idx = g["edge"][f, q]
+            coef[idx] += int1 * g["A"][f] / epsp[f]
+            sc[idx + Nd] += int3 * g["A"][f]
+            sv[idx + Nd] += int2 * g["A"][f]
+    sc[Nd:] = -sc[Nd:] * 1j * omega_sh
+    sv[:Nd] = 0.5 * coef
+    sv[Nd:] = 0.5 * 1j * omega_sh * sv[Nd:]
+    Fm = rwg_moments(g)
+    sol = np.linalg.solve(Fm, np.stack([coef, sc[Nd:]], axis=1))
+    coef = sol[:, 0]
+    sc[Nd:] = sol[:, 1]
+    cm = np.zeros(Nd, complex)
+    for f in range(g["F"]):
+        nor = g["n"][f]
+        qp = g["qp"][f]
+        ex = sum(_rwg(g, f, q, qp) * coef[g["edge"][f, q]] for q in range(3))
+        ncr = np.cross(nor[None, :], ex)
+        for q in range(3):
+            cm[g["edge"][f, q]] += g["A"][f] * np.sum(g["w"] * np.sum(_rwg(g, f, q, qp) * ncr, axis=1))
+    sc[:Nd] = np.linalg.solve(Fm, cm)
+    return sc, sv
+
+
+def epsp_of(P, d, ri):
+    """determine_epsp (solver.f90:393-433): per face of domain d, eps0 ri^2 of the
+    first other domain that contains the same face."""
+    md = P.export(d)
+    key = lambda nodes, fn: [tuple(sorted(map(tuple, np.round(nodes[f], 20)))) for f in fn]
+    mine = key(md["nodes"], md["face_node"])
+    out = np.zeros(len(mine), complex)
+    found = np.zeros(len(mine), bool)
+    for d2 in range(P.ndom):
+        if d2 == d:
+            continue
+        m2 = P.export(d2)
+        other = set(key(m2["nodes"], m2["face_node"]))
+        for i, k in enumerate(mine):
+            if not found[i] and k in other:
+                out[i] = complex(ri[d2]) ** 2 * EPS0
+                found[i] = True
+    if not found.all():
+        raise RuntimeError("Could not find epsp!")
+    return out
+
+
+def domain_matrix(P, d, omega, ri_d):
+    """The PMCHWT blocks of domain d alone (sysmat.f90:70-99 for one domain,
+    identity group), 2N x 2N."""
+    m = P.export(d)
+    par = m["edge_parent"]
+    N = P.N
+    S = P.operator(d, 0, omega, ri_d) + P.operator(d, 1, omega, ri_d)
+    K = P.operator(d, 2, omega, ri_d)
+    Zsi = ri_d ** 2 / ETA0 ** 2
+    A = np.zeros((2 * N, 2 * N), complex)
+    ix = np.ix_(par, par)
+    A[ix] += S
+    A[np.ix_(par + N, par + N)] += Zsi * S
+    A[np.ix_(par + N, par)] += K
+    A[np.ix_(par, par + N)] -= K
+    return A
+
+
+def shg_solve(P, omega, ri, shri, nls, x, qd_name="tri_gl13", coef_out=None):
+    """The nonlinear branch of solve_batch for a centrosymmetric surface
+    nonlinearity (solver.f90:143-217, identity group): for every domain d with
+    nls[d] = (chi_nnn, chi_ntt, chi_ttn) the source coefficients of
+    nlsurf_coef, the source vector E0, H0 and the matrix terms of
+    sysmat_pmchwt_nls (sysmat.f90:112-229) at 2 omega with the SH refractive
+    indices, then the SH solve.  x: fundamental solutions [2N][nsrc].
+    Returns nlx [2N][nsrc]; coef_out (a dict), if given, receives per
+    nonlinear domain the source coefficients on the global unknowns (cJ in
+    rows [0, N), cM in rows [N, 2N)), [2N][nsrc]."""
+    qd = tri_rule(qd_name)
+    N = P.N
+    x = np.asarray(x, dtype=np.complex128).reshape(2 * N, -1)
+    nsrc = x.shape[1]
+    nlx = np.zeros((2 * N, nsrc), complex)
+    for d in range(P.ndom):
+        if nls[d] is None:
+            continue
+        m = P.export(d)
+        par = m["edge_parent"]
+        Nd = len(par)
+        epsp = epsp_of(P, d, ri)
+        Ad = domain_matrix(P, d, 2.0 * omega, complex(shri[d]))
+        if coef_out is not None:
+            coef_out[d] = np.zeros((2 * N, nsrc), complex)
+        for s in range(nsrc):
+            sc, sv = nlsurf_coef(P, d, qd, omega, complex(ri[d]), epsp, x[:, s], nls[d])
+            nlx[par, s] += sv[:Nd]
+            nlx[par + N, s] += sv[Nd:]
+            c = np.zeros(2 * N, complex)
+            c[par] = sc[Nd:]      # cJ on the J columns
+            c[par + N] = sc[:Nd]  # cM on the M columns
+            nlx[:, s] -= Ad @ c
+            if coef_out is not None:
+                coef_out[d][:, s] = c
+    A = P.sysmat(2.0 * omega, [complex(v) for v in shri])
+    return solve(A, nlx)
 
 
 def solve(A, q):

@@ -145,7 +145,12 @@ def test_field_map_commands(solver, tmp_path):
         "ndom 2", "sdom 1 1 1 0 1 -1", "sdom 2 1 -1 0 2 -1", "fdom", "nsrc 1", "ssrc 1 'pw' 0 90 0",
         "solv", "nfms 1 1 1", "nfem 1 1 1 'ext.msh' true", "nfdm 1 1 1 true 0 0 0 200d-9 200d-9 200d-9 5 4 3",
         "exit"]) + "\n"
-    r = subprocess.run([EXE], input=script, capture_output=True, text=True, cwd=tmp_path, timeout=600)
+    # nfms, nfem and nfdm write the same file name in turn: run the script up to
+    # each command alone
+    nfem_cmd = "nfem 1 1 1 'ext.msh' true\n"
+    nfdm_cmd = "nfdm 1 1 1 true 0 0 0 200d-9 200d-9 200d-9 5 4 3\n"
+    r = subprocess.run([EXE], input=script.replace(nfem_cmd, "").replace(nfdm_cmd, ""), capture_output=True,
+                       text=True, cwd=tmp_path, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:]
     om = M.omega_of(WL)
     solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
@@ -161,9 +166,8 @@ def test_field_map_commands(solver, tmp_path):
     got = np.array([data[("$ElementData", "Re(H)", 24)][i + 1] for i in range(len(faces))])
     assert close_en(got, h.real)
     assert len([k for k in data if k[1] == "|Re(E)|"]) == 25
-    # nfem and nfdm write the same file name in turn; rerun the script up to each command
     for cmd in ("nfem", "nfdm"):
-        sc = script.replace("nfms 1 1 1\n", "").replace("nfem 1 1 1 'ext.msh' true\n" if cmd == "nfdm" else "nfdm 1 1 1 true 0 0 0 200d-9 200d-9 200d-9 5 4 3\n", "")
+        sc = script.replace("nfms 1 1 1\n", "").replace(nfem_cmd if cmd == "nfdm" else nfdm_cmd, "")
         r = subprocess.run([EXE], input=sc, capture_output=True, text=True, cwd=tmp_path, timeout=600)
         assert r.returncode == 0, r.stdout[-2000:]
         nd, el, data = read_msh_blocks(path)

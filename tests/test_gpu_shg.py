@@ -1,0 +1,221 @@
+"""Second-harmonic generation from a centrosymmetric surface nonlinearity
+(solver.f90:143-217, nlsurf_coef nlsurf.f90:137-338, sysmat_pmchwt_nls
+sysmat.f90:112-229) through mom_gpu_shg_solve, against the oracle's
+restatement (oracle.shg_solve) on the same spheres.
+
+Tolerances: FP64 SH solutions 1e-9 relative (the Gram systems are solved by
+conjugate gradients to a relative residual of 1e-14 on the GPU and by LU in
+the oracle), SH cross sections 1e-9; mixed precision 1e-6 on the cross
+sections (the mixed path's far-pair rounding, as for the linear solve)."""
+import numpy as np
+import pytest
+
+import mom_b200 as M
+import oracle as O
+from mom_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+WL = 1000e-9
+CHI = (1.0e-18 + 0.3e-18j, 0.5e-18, -0.2e-18 + 0.1e-18j)
+SRCS = [M.src_pw(0, 90, 0), M.src_pw_elliptic(35, 20, np.exp(0.4j))]
+OSRCS = [dict(type="pw", theta=0.0, phi=90 * O.DEGTORAD, psi=0.0),
+         dict(type="pw_elliptic", theta=35 * O.DEGTORAD, phi=20 * O.DEGTORAD, phase=np.exp(0.4j))]
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def solver(built):
+    s = M.Solver(0)
+    yield s
+    s.close()
+
+
+def setup(s):
+    nodes, faces, ids, doms = W.sphere(s)
+    return nodes, faces, ids, doms, O.OracleProblem(nodes, faces, ids, 1e-9, doms)
+
+
+@pytest.mark.parametrize("s,nls_doms", [(1, (1,)), (2, (1,)), (2, (0, 1))])
+def test_shg_fp64_matches_oracle(solver, s, nls_doms):
+    nodes, faces, ids, doms, P = setup(s)
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU)]
+    shri = [1.0, np.sqrt(complex(-2.0, 3.5))]
+    nls = [CHI if d in nls_doms else None for d in range(2)]
+    A = P.sysmat(om, ri)
+    x = O.solve(A, np.stack([P.srcvec(om, 1.0, q) for q in OSRCS], axis=1))
+    coef_o = {}
+    nlx_o = O.shg_solve(P, om, ri, shri, nls, x, coef_out=coef_o)
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, SRCS, M.FP64, want_host=False)
+    nlx = solver.shg_solve(om, ri, shri, nls, M.FP64)
+    for k in range(2):
+        assert rel(nlx[:, k], nlx_o[:, k]) <= 1e-9, (k, rel(nlx[:, k], nlx_o[:, k]))
+    for d in range(2):
+        if nls[d] is None:
+            with pytest.raises(M.MomError):
+                solver.shg_source_coef(d)
+        else:
+            assert rel(solver.shg_source_coef(d), coef_o[d]) <= 1e-10, d
+    none = [M.src_none()] * 2
+    csca, cabs = solver.cross_sections(2 * om, shri[0], none)
+    for k in range(2):
+        so, ao = P.cs(2 * om, shri[0], nlx_o[:, k], dict(type="none"))
+        assert abs(csca[k] - so) <= 1e-9 * abs(so) and abs(cabs[k] - ao) <= 1e-9 * abs(ao), (k, csca[k], so)
+    # the same cross sections through host solutions
+    c2, a2 = solver.cross_sections(2 * om, shri[0], none, x=nlx)
+    assert np.allclose(c2, csca, rtol=1e-13, atol=0) and np.allclose(a2, cabs, rtol=1e-13, atol=0)
+
+
+def test_shg_mixed_cross_sections(solver):
+    nodes, faces, ids, doms, P = setup(2)
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU)]
+    shri = [1.0, np.sqrt(complex(-2.0, 3.5))]
+    nls = [None, CHI]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, SRCS, M.FP64, want_host=False)
+    solver.shg_solve(om, ri, shri, nls, M.FP64, want_host=False)
+    ref = solver.cross_sections(2 * om, shri[0], [M.src_none()] * 2)
+    solver.solve_wavelength(om, ri, SRCS, M.MIXED, 1e-12, 30, want_host=False)
+    solver.shg_solve(om, ri, shri, nls, M.MIXED, 1e-12, 30, want_host=False)
+    got = solver.cross_sections(2 * om, shri[0], [M.src_none()] * 2)
+    for a, b in zip(got, ref):
+        assert np.all(np.abs(a / b - 1) <= 1e-6), (a, b)
+
+
+def test_shg_scaling_laws(solver):
+    """nlx is linear in the susceptibilities: doubling all three doubles nlx."""
+    nodes, faces, ids, doms, _ = setup(1)
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU)]
+    shri = [1.0, np.sqrt(complex(-2.0, 3.5))]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, SRCS[:1], M.FP64, want_host=False)
+    a = solver.shg_solve(om, ri, shri, [None, CHI], M.FP64)
+    solver.solve_wavelength(om, ri, SRCS[:1], M.FP64, want_host=False)
+    b = solver.shg_solve(om, ri, shri, [None, tuple(2 * c for c in CHI)], M.FP64)
+    assert rel(b, 2 * a) <= 1e-12
+
+
+def test_shg_errors(solver):
+    nodes, faces, ids, doms, _ = setup(1)
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU)]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    with pytest.raises(M.MomError) as e:
+        solver.shg_solve(om, ri, ri, [None, CHI], M.FP64)
+    assert e.value.status == M.MOM_ERR_STATE
+    # symmetry groups are not supported by the second-harmonic path
+    from mom_b200 import meshgen
+    fn, ff, lines = meshgen.symmetry_fragment(*meshgen.octasphere(1, 50.0), [0])
+    prob = M.Problem.from_arrays(fn, ff, np.ones(len(ff), int), 1e-9, [[1], [-1]])
+    prob.set_lines(np.asarray(lines[0], np.int32).reshape(-1, 2), np.full(len(lines[0]), 10, np.int32))
+    prob.classify_edges(10, "xplane")
+    solver.set_problem(prob)
+    solver.set_symmetry(["mxp"], prob)
+    solver.solve_wavelength(om, ri, SRCS[:1], M.FP64, want_host=False)
+    with pytest.raises(M.MomError) as e:
+        solver.shg_solve(om, ri, ri, [None, CHI], M.FP64)
+    assert e.value.status == M.MOM_ERR_ARG and "identity" in str(e.value)
+    # the adjoint after a second-harmonic solve: its factors are not the fundamental's
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, SRCS[:1], M.FP64, want_host=False)
+    solver.shg_solve(om, ri, ri, [None, CHI], M.FP64, want_host=False)
+    with pytest.raises(M.MomError) as e:
+        solver.adjoint(om, ri, SRCS[:1], M.FP64, eps_dom=1)
+    assert e.value.status == M.MOM_ERR_STATE
+
+
+def test_shg_command_script(solver, tmp_path):
+    """The `mom` interpreter with `smed 2 nlsurf value ...`: solv also solves the
+    second harmonic, and crst / rcst / nfms / nfem write -sh files whose values
+    match the C ABI's (to the printed EN15.3 precision)."""
+    import os
+    import subprocess
+    from mom_b200 import meshgen
+    nodes, faces, ids, doms = W.sphere(2)
+    meshgen.write_gmsh22(str(tmp_path / "ico2.msh"), nodes, faces, ids)
+    en, ef = meshgen.icosphere(1, 80.0)
+    meshgen.write_gmsh22(str(tmp_path / "ext.msh"), en, ef, np.ones(len(ef), int))
+    n_in = np.sqrt(W.EPS_AU)
+    cx = lambda z: "(%.17g, %.17g)" % (complex(z).real, complex(z).imag)
+    script = "\n".join([
+        "name 'shg'", "mesh 'ico2.msh' 1d-9", "wlls 1 1000d-9", "nmed 2",
+        "smed 1 linear value (1.0, 0.0)", "smed 2 linear value " + cx(n_in),
+        "smed 2 nlsurf value " + " ".join(cx(c) for c in CHI),
+        "ndom 2", "sdom 1 1 1 0 1 -1", "sdom 2 1 -1 0 2 -1", "fdom", "nsrc 1", "ssrc 1 'pw' 0 90 0",
+        "solv", "crst", "rcst 1 1 7 9", "nfms 1 1 1", "nfem 1 1 2 'ext.msh' false", "exit"]) + "\n"
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "for90-mom2_b200", "bin",
+                       "mom_b200")
+    r = subprocess.run([exe], input=script, capture_output=True, text=True, cwd=tmp_path, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:]
+    assert "Solving nonlinear scattering from centrosymmetric material" in r.stdout
+    om = M.omega_of(WL)
+    ri = [1.0, n_in]
+    src = [M.src_pw(0, 90, 0)]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, src, M.FP64, want_host=False)
+    nlx = solver.shg_solve(om, ri, ri, [None, CHI], M.FP64)  # `smed ... value` sets shri = ri
+    cs, ca = solver.cross_sections(2 * om, 1.0, [M.src_none()], x=nlx)
+    row = [float(v) for v in open(tmp_path / "shg-s1-sh.crs").read().split()]
+    assert abs(row[0] - WL) <= 1e-3 * WL
+    assert abs(row[1] - cs[0]) <= 5e-4 * abs(cs[0]) and abs(row[2] - ca[0]) <= 5e-4 * abs(ca[0]), (row, cs, ca)
+    rc = solver.rcs(2 * om, 1.0, 7, 9, isrc=0, x=nlx)
+    got = np.array([[float(v) for v in ln.split()] for ln in open(tmp_path / "shg-wl1-s1-sh.rcs").read().split("\n")
+                    if ln.strip()])
+    assert got.shape == (7, 9)
+    assert np.all(np.abs(got - rc) <= 5e-4 * np.abs(rc) + 1e-30)
+    assert os.path.exists(tmp_path / "shg-wl1-s1-d1-sh.msh")
+    # nfem in the nonlinear domain: the fields of nlx plus its source coefficients
+    coef = solver.shg_source_coef(1)
+    cp = en[ef].mean(axis=1) * 1e-9
+    ee, _ = solver.scat_fields(2 * om, n_in, cp, x=nlx + coef, dom=1)
+    lines = open(tmp_path / "shg-wl1-s1-d2-sh.msh").read().split("\n")
+    i = lines.index('"Re(E)"')
+    assert int(lines[i + 3]) == 0
+    n = int(lines[i + 5])
+    got = np.array([[float(v) for v in lines[i + 6 + j].split()[1:4]] for j in range(n)])
+    assert got.shape == (len(ef), 3)
+    # the first frame is Re(E exp(-2 pi i / 25))
+    ph = np.exp(-2j * np.pi / 25)
+    want = (ee[0] * ph).real
+    assert np.all(np.abs(got - want) <= 5e-4 * np.abs(want) + 1e-3 * np.abs(want).max())
+
+
+def sh_power_ratio(solver, s, chi):
+    """sigma_sca of the SH solution (the Poynting flux through the particle
+    surface, cs_prtsrf) over the far-field power (the RCS integrated over
+    directions)."""
+    nodes, faces, ids, doms = W.sphere(s)
+    om = M.omega_of(WL)
+    ri = [1.0, np.sqrt(W.EPS_AU)]
+    shri = [1.0, np.sqrt(complex(-2.0, 3.5))]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+    solver.solve_wavelength(om, ri, SRCS[:1], M.FP64, want_host=False)
+    solver.shg_solve(om, ri, shri, [None, chi], M.FP64, want_host=False)
+    csca, _ = solver.cross_sections(2 * om, shri[0], [M.src_none()])
+    nt, nph = 91, 73  # rcs grids: theta on [0, pi], phi on [0, 2 pi], both ends included
+    r = solver.rcs(2 * om, shri[0], nt, nph, isrc=0)
+    th = np.linspace(0, np.pi, nt)
+    wt = np.sin(th) * (th[1] - th[0])
+    wp = np.full(nph, 2 * np.pi / (nph - 1))
+    wp[0] *= 0.5
+    wp[-1] *= 0.5
+    return csca[0] / (wt @ r @ wp)
+
+
+@pytest.mark.parametrize("k", range(3))
+def test_shg_energy_balance_converges(solver, k):
+    """Energy balance of the second harmonic: the power through the surface
+    approaches the radiated far-field power as the mesh is refined (within 10%
+    at 5120 triangles; the coarse meshes miss it by far more)."""
+    chi = [0.0, 0.0, 0.0]
+    chi[k] = 1e-18
+    coarse = abs(sh_power_ratio(solver, 2, tuple(chi)) - 1)
+    fine = abs(sh_power_ratio(solver, 4, tuple(chi)) - 1)
+    assert fine <= 0.1 and fine < coarse, (k, coarse, fine)
