@@ -780,7 +780,9 @@ def run_kernel_cases(subdiv):
     (pair_kernel<double>, near_kernel, gather_kernel), srcvec, cs_prtsrf,
     the 91 x 180 far field, a 41 x 41 near-field plane, the FP64 eps adjoint
     (adj_pair_kernel), then the mixed solve (pair_kernel<float>, the FP64
-    refinement residual gemv_partial_kernel)."""
+    refinement residual gemv_partial_kernel) and an FP64 second-harmonic solve
+    with a surface nonlinearity of the particle (nls_face_kernel,
+    gram_cg_kernel, nls_cm_kernel)."""
     import numpy as np
     import mom_b200 as M
     nodes, faces, ids, doms = make_problem(M, subdiv)
@@ -797,6 +799,9 @@ def run_kernel_cases(subdiv):
     S.scat_fields(om, 1.0, pts, srcs=src, dom=0)
     S.adjoint(om, ri, src, M.FP64, eps_dom=1)
     S.solve_wavelength(om, ri, src, M.MIXED, TOL, MAXIT, want_host=False)
+    S.solve_wavelength(om, ri, src, M.FP64, want_host=False)
+    S.shg_solve(om, ri, [1.0, np.sqrt(complex(-2.0, 3.5))], [None, (1.0e-18, 0.5e-18, 0.2e-18)], M.FP64,
+                want_host=False)
     S.synchronize()
     S.close()
     print(json.dumps({"kernel_cases": workload_name(subdiv), "sigma_ext_fp64": float(a[0] + b[0])}), flush=True)

@@ -444,6 +444,8 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (ec) c->la_ctas = std::max(0, std::atoi(ec));
   const char *ef = std::getenv("MOM_LA_FROM");
   if (ef) c->la_from = std::atof(ef);
+  const char *ft = std::getenv("MOM_FUSED_TRSM");
+  if (ft) c->fused_trsm = std::atoi(ft) != 0;
   *out = c;
   return MOM_OK;
 }
@@ -540,7 +542,8 @@ int mom_gpu_set_problem(mom_ctx *c, int32_t nedges_total, int32_t ndom, const mo
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     const size_t mats = (size_t)c->lda * c->n * (sizeof(double2) + sizeof(float2)) + (size_t(4) << 30);
-    c->blk_fused = ndom <= 8 && fr > total + mats;
+    const char *fg = std::getenv("MOM_FUSED_GATHER");
+    c->blk_fused = ndom <= 8 && fr > total + mats && !(fg && std::atoi(fg) == 0);
     if (c->blk_fused) {
       std::vector<int> dm((size_t)ndom * c->N, -1);
       for (int d = 0; d < ndom; d++)

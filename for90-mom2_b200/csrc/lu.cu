@@ -1244,6 +1244,85 @@ __global__ void axpy_kernel(double2 *X, const double2 *D, int64_t count) {
   }
 }
 
+// U12 of an outer block in one launch: B <- inv(L11) B for the np panels'
+// rows [J0, J0 + np nb) and the columns [c0, c0 + ncol), L11 unit lower
+// triangular.  Per panel p: X_p = inv(L_pp) B_p with the diagonal block's
+// inverse (diag_inv_kernel), then B_q -= L_qp X_p for every panel q below.
+// One CTA per kBtCols columns keeps its np nb x kBtCols tile in shared
+// memory; the 64 x 64 factor blocks are staged one at a time.  FP32 complex
+// products with FP32 accumulation, as the library CGEMM it replaces.
+constexpr int kBtCols = 32;
+constexpr int kBtThreads = 256;
+constexpr int kBtMaxPanels = 4;
+constexpr int kBtLd = 65;             // padded row stride of the staged factor block
+constexpr int kBtLdB = kBtCols + 1;   // padded row stride of the column tile
+constexpr size_t kBtSmem = sizeof(float2) * ((size_t)kBtMaxPanels * 64 * kBtLdB + 64 * kBtLd);
+
+__global__ void __launch_bounds__(kBtThreads) block_trsm_kernel(float2 *A, int64_t lda, int64_t J0, int np,
+                                                                int64_t c0, int ncol, const float2 *invL) {
+  extern __shared__ float2 bt_smem[];
+  float2 *Bs = bt_smem;                                  // [np * 64][kBtLdB]
+  float2 *Ms = bt_smem + (size_t)kBtMaxPanels * 64 * kBtLdB;  // [64][kBtLd], row-major
+  const int t = threadIdx.x, j = t % kBtCols, rg = t / kBtCols;  // 8 rows per thread
+  const int jc = blockIdx.x * kBtCols;
+  const int rows = np * 64;
+  for (int idx = t; idx < rows * kBtCols; idx += kBtThreads) {
+    const int r = idx % rows, cc = idx / rows;
+    Bs[r * kBtLdB + cc] = (jc + cc < ncol) ? A[(J0 + r) + (c0 + jc + cc) * lda] : make_float2(0.f, 0.f);
+  }
+  for (int p = 0; p < np; p++) {
+    // X_p = inv(L_pp) B_p
+    __syncthreads();
+    const float2 *inv = invL + (size_t)p * 64 * 64;  // column-major 64 x 64
+    for (int idx = t; idx < 64 * 64; idx += kBtThreads) Ms[(idx % 64) * kBtLd + idx / 64] = inv[idx];
+    __syncthreads();
+    float2 acc[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) acc[r] = make_float2(0.f, 0.f);
+    for (int k = 0; k < 64; k++) {
+      const float2 b = Bs[(p * 64 + k) * kBtLdB + j];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const float2 m = Ms[(rg * 8 + r) * kBtLd + k];
+        acc[r].x = fmaf(m.x, b.x, fmaf(-m.y, b.y, acc[r].x));
+        acc[r].y = fmaf(m.x, b.y, fmaf(m.y, b.x, acc[r].y));
+      }
+    }
+    __syncthreads();  // every read of B_p done
+#pragma unroll
+    for (int r = 0; r < 8; r++) Bs[(p * 64 + rg * 8 + r) * kBtLdB + j] = acc[r];
+    // B_q -= L_qp X_p
+    for (int q = p + 1; q < np; q++) {
+      __syncthreads();
+      const float2 *L = A + (J0 + q * 64) + (J0 + p * 64) * lda;
+      for (int idx = t; idx < 64 * 64; idx += kBtThreads) Ms[(idx % 64) * kBtLd + idx / 64] = L[(idx % 64) + (idx / 64) * lda];
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; r++) acc[r] = make_float2(0.f, 0.f);
+      for (int k = 0; k < 64; k++) {
+        const float2 x = Bs[(p * 64 + k) * kBtLdB + j];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+          const float2 m = Ms[(rg * 8 + r) * kBtLd + k];
+          acc[r].x = fmaf(m.x, x.x, fmaf(-m.y, x.y, acc[r].x));
+          acc[r].y = fmaf(m.x, x.y, fmaf(m.y, x.x, acc[r].y));
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        float2 &v = Bs[(q * 64 + rg * 8 + r) * kBtLdB + j];
+        v.x -= acc[r].x;
+        v.y -= acc[r].y;
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = t; idx < rows * kBtCols; idx += kBtThreads) {
+    const int r = idx % rows, cc = idx / rows;
+    if (jc + cc < ncol) A[(J0 + r) + (c0 + jc + cc) * lda] = Bs[r * kBtLdB + cc];
+  }
+}
+
 struct LuWork {
   int *info, *timeout;
   unsigned long long *rec;
@@ -1542,8 +1621,10 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
 // block's interchanges to the columns outside it after its factorisation
 // (instead of panel by panel) gives the same factors; the columns left of
 // the block are swapped at the same time (they hold L of earlier blocks,
-// which nothing reads any more).  Blocks taller than la_from * n run without
-// the overlap (the panel would take too many SMs from the larger GEMM).
+// which nothing reads any more).  Blocks whose trailing height is above
+// la_from * n, or whose panels need more than half of the SMs (over about
+// 15,400 rows: at most 208 rows per panel CTA), run without the overlap
+// (the panel would take too many SMs from the larger GEMM).
 template <typename T>
 int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
   const int64_t n = c->n, lda = c->lda;
@@ -1604,7 +1685,14 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       const int64_t rest = J0 + NBc - (j0 + nb);
       if (rest > 0) {
         ProfScope pg(c, kProfGemm, st);
-        MOM_TRY(trsm_l(h, st, (T *)w.W2, j0, j0 + nb, rest));
+        if (c->fused_trsm && nb == 64) {
+          block_trsm_kernel<<<(unsigned)((rest + kBtCols - 1) / kBtCols), kBtThreads, kBtSmem, st>>>(
+              reinterpret_cast<float2 *>(A), lda, j0, 1, j0 + nb, (int)rest, w.invL32 + (size_t)kb * nb * nb);
+          c->launches++;
+          MOM_CUDA(c, cudaGetLastError());
+        } else {
+          MOM_TRY(trsm_l(h, st, (T *)w.W2, j0, j0 + nb, rest));
+        }
         MOM_TRY(gemm(h, n - j0 - nb, rest, nb, -1.0f, A + (j0 + nb) + j0 * lda, lda, A + j0 + (j0 + nb) * lda, lda,
                      1.0f, A + (j0 + nb) + (j0 + nb) * lda, lda));
       }
@@ -1616,11 +1704,18 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     if (ncol <= 0) return MOM_OK;
     const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc;
     ProfScope pg(c, kProfGemm);
-    for (int64_t j0 = J0; j0 < t0; j0 += nb) {
-      MOM_TRY(trsm_l(c->blas, sa, (T *)w.W, j0, c0, ncol));
-      const int64_t below = t0 - (j0 + nb);
-      MOM_TRY(gemm(c->blas, below, ncol, nb, -1.0f, A + (j0 + nb) + j0 * lda, lda, A + j0 + c0 * lda, lda, 1.0f,
-                   A + (j0 + nb) + c0 * lda, lda));
+    if (c->fused_trsm && NBc <= (int64_t)kBtMaxPanels * nb && nb == 64) {
+      block_trsm_kernel<<<(unsigned)((ncol + kBtCols - 1) / kBtCols), kBtThreads, kBtSmem, sa>>>(
+          reinterpret_cast<float2 *>(A), lda, J0, (int)(NBc / nb), c0, (int)ncol, w.invL32 + (size_t)(J0 / nb) * nb * nb);
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+    } else {
+      for (int64_t j0 = J0; j0 < t0; j0 += nb) {
+        MOM_TRY(trsm_l(c->blas, sa, (T *)w.W, j0, c0, ncol));
+        const int64_t below = t0 - (j0 + nb);
+        MOM_TRY(gemm(c->blas, below, ncol, nb, -1.0f, A + (j0 + nb) + j0 * lda, lda, A + j0 + c0 * lda, lda, 1.0f,
+                     A + (j0 + nb) + c0 * lda, lda));
+      }
     }
     MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(A + t0 + c0 * lda), lda,
                             reinterpret_cast<const float2 *>(A + t0 + J0 * lda), lda,
@@ -1647,7 +1742,9 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     if (nc <= 0) break;
     const int64_t L = std::min<int64_t>(NB, nc);
     MOM_TRY(trailing(J0, t0, L, 0));
-    const bool overlap = (double)nc < c->la_from * (double)n && nc > L;
+    // overlap only where the next block's panels leave the GEMM at least half
+    // of the SMs (a panel holds at most 208 rows per CTA)
+    const bool overlap = (double)nc < c->la_from * (double)n && nc > L && (nc + 207) / 208 <= c->nsm / 2;
     if (overlap) {
       // panel CTAs of the next block (the tallest of its panels), the GEMM gets the rest
       int P = panel_ctas(c, nc);
@@ -1751,7 +1848,7 @@ int lu_factor_t(Ctx *c, T *A, int precision) {
                                         (uintptr_t)tune_hash(c), (uintptr_t)c->outer_panels, (uintptr_t)c->inv32,
                                         (uintptr_t)wait_polls(c, 0), (uintptr_t)wait_polls(c, 1),
                                         (uintptr_t)use_lookahead(c, precision), (uintptr_t)c->la_ctas,
-                                        (uintptr_t)(c->la_from * 1e6)};
+                                        (uintptr_t)(c->la_from * 1e6), (uintptr_t)c->fused_trsm};
     for (Ctx::LuGraph *h : c->lu_graphs)
       if (h->exec && h->key == key) g = h;
     if (!g) {
@@ -1927,6 +2024,7 @@ int lu_init_kernels(Ctx *c) {
   MOM_CUDA(c, set_smem(diag_inv_kernel<double2, 1>));
   MOM_CUDA(c, set_smem(diag_inv_kernel<float2, 1>));
   MOM_CUDA(c, set_smem(compose_pivots_kernel));
+  MOM_CUDA(c, cudaFuncSetAttribute(block_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBtSmem));
   MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 1, false>));
   MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 2, false>));
   MOM_CUDA(c, set_smem(trsv_flow_kernel<double2, 4, false>));

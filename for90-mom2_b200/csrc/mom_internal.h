@@ -220,6 +220,10 @@ struct Ctx {
   int panel_cluster = 0;
   int outer_panels = 4;  // panels per outer block of the LU (MOM_LU_OUTER): trailing GEMMs have K = 64 * this
   int small_tc = 0;      // mixed path: K = 64 updates on the tensor cores too (MOM_SMALL_TC=1), else library FP32 GEMM
+  // Look-ahead path: the block TRSMs of an outer block by block_trsm_kernel
+  // (MOM_FUSED_TRSM=1) instead of library CGEMMs; measured slower at
+  // 15,360 unknowns (158.6 against 155.0 ms per solve), so off by default.
+  int fused_trsm = 0;
   bool autotune = true;
   struct Tuned {
     int64_t n;

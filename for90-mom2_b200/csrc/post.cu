@@ -954,7 +954,7 @@ int far_field(Ctx *c, int dom, double omega, const double *ri, const double2 *xd
   c->launches += 2;
   MOM_CUDA(c, cudaGetLastError());
   }
-  MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+  MOM_CUDA(c, cudaMemcpyAsync(rcs, dout, sizeof(double) * (size_t)nd, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));
   return MOM_OK;
 }
