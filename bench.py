@@ -17,8 +17,9 @@ Data are synthetic (a seeded icosphere; no dataset exists for this path).  The
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-For N > 1 (torchrun) every rank solves its own replica (the path has no data
-exchange: "replicas only"); the step time is the max over ranks.
+For N > 1 (torchrun) every rank solves its own wavelength, a shard of a
+wavelength sweep (the path has no data exchange at one wavelength); the step
+time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -38,6 +39,7 @@ sys.path.insert(0, PKG)
 
 METRIC = "solves/s (assemble+LU+solve), mixed vs FP64 on 1 B200 at sigma_ext rel err <=1e-6"
 WL = 600e-9
+SHARD_DWL = 5e-9  # with N ranks, rank r solves the wavelength WL + SHARD_DWL r (a wavelength-sweep shard)
 EPS_IN = complex(-9.0, 1.3)
 SUBDIV = 4
 RADIUS_NM = 50.0
@@ -266,7 +268,8 @@ def bench_config(subdiv, world):
     """The workload description shared by both arms (identical dicts)."""
     return {"workload": workload_name(subdiv), "refine_tol": TOL,
             "l2": "matrix %.2f GB > 126 MB L2, no flush" % (16.0 * (3 * 20 * 4 ** subdiv) ** 2 / 1e9),
-            "parallelism": "replicas x%d" % world}
+            "parallelism": ("wavelength shards x%d (rank r at 600 + %g r nm, one solve per rank per step)"
+                            % (world, SHARD_DWL * 1e9) if world > 1 else "replicas x1")}
 
 
 def run_reference(args, rank, world):
@@ -309,7 +312,9 @@ def run_ours(args, rank, local_rank, world):
     nodes, faces, ids, doms = make_problem(M, args.subdiv)
     S = M.Solver(local_rank)
     S.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
-    om = M.omega_of(WL)
+    # each rank solves its own wavelength of a sweep of N wavelengths
+    # WL + SHARD_DWL i (unit i on rank i); rank 0's is the 600 nm of the sigma fixture
+    om = M.omega_of(WL + SHARD_DWL * rank)
     ri = [1.0, np.sqrt(EPS_IN)]
     src = [M.src_pw(0, 90, 0)]
     stream = torch.cuda.ExternalStream(S.stream)

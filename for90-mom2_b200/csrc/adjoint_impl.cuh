@@ -202,10 +202,11 @@ __device__ void face_build(const AdjTopo &t, int f, int snode, int scoord, FaceA
   }
 }
 
-// blocks_from_moments in the scalar type S throughout.
-template <typename S>
-__device__ void blocks_generic(const Moments<S> &M, const S mu[3][3], const S nu[3][3], const S slp[3], const S slq[3],
-                               const S d[3], Cx<S> fD, Cx<S> fH, double fK, bool self, Cx<S> *Sb, Cx<S> *Kb) {
+// blocks_from_moments in the scalar type S, with the geometry in type G (S
+// by default).
+template <typename S, typename G = S>
+__device__ void blocks_generic(const Moments<S> &M, const G mu[3][3], const G nu[3][3], const G slp[3], const G slq[3],
+                               const G d[3], Cx<S> fD, Cx<S> fH, double fK, bool self, Cx<S> *Sb, Cx<S> *Kb) {
   Cx<S> KBv[3], KDmF[3];
   KBv[0] = {d[1] * M.KF[2].re - d[2] * M.KF[1].re + M.KE[0].re, d[1] * M.KF[2].im - d[2] * M.KF[1].im + M.KE[0].im};
   KBv[1] = {d[2] * M.KF[0].re - d[0] * M.KF[2].re + M.KE[1].re, d[2] * M.KF[0].im - d[0] * M.KF[2].im + M.KE[1].im};
@@ -218,10 +219,10 @@ __device__ void blocks_generic(const Moments<S> &M, const S mu[3][3], const S nu
   Cx<S> beta[3], bq[3], cq[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    const S *v = nu[q];
+    const G *v = nu[q];
     beta[q] = {v[0] * M.TB[0].re + v[1] * M.TB[1].re + v[2] * M.TB[2].re,
                v[0] * M.TB[0].im + v[1] * M.TB[1].im + v[2] * M.TB[2].im};
-    S dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
+    G dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
     bq[q] = {dn[0] * M.KC[0].re + dn[1] * M.KC[1].re + dn[2] * M.KC[2].re,
              dn[0] * M.KC[0].im + dn[1] * M.KC[1].im + dn[2] * M.KC[2].im};
     cq[q] = {v[0] * M.KE[0].re + v[1] * M.KE[1].re + v[2] * M.KE[2].re,
@@ -229,7 +230,7 @@ __device__ void blocks_generic(const Moments<S> &M, const S mu[3][3], const S nu
   }
 #pragma unroll
   for (int p = 0; p < 3; p++) {
-    const S *u = mu[p];
+    const G *u = mu[p];
     const Cx<S> alpha = {u[0] * M.TC[0].re + u[1] * M.TC[1].re + u[2] * M.TC[2].re,
                          u[0] * M.TC[0].im + u[1] * M.TC[1].im + u[2] * M.TC[2].im};
     const Cx<S> ap = {u[0] * KBv[0].re + u[1] * KBv[1].re + u[2] * KBv[2].re,
@@ -239,17 +240,17 @@ __device__ void blocks_generic(const Moments<S> &M, const S mu[3][3], const S nu
                         {u[0] * KDmF[1].re - u[1] * KDmF[0].re, u[0] * KDmF[1].im - u[1] * KDmF[0].im}};
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const S *v = nu[q];
-      const S uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
-      const S ss = slp[p] * slq[q];
+      const G *v = nu[q];
+      const G uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+      const G ss = slp[p] * slq[q];
       const Cx<S> cD = {M.TA.re - beta[q].re - alpha.re + uv * M.TD.re, M.TA.im - beta[q].im - alpha.im + uv * M.TD.im};
       const Cx<S> s12 = cxa(cxm(fD, cD), cxm(fH, M.TD));
-      Sb[3 * p + q] = cxr(s12, ss);
+      Sb[3 * p + q] = cxr(s12, S(ss));
       Cx<S> kv = {S(0.0), S(0.0)};
       if (!self) {
         const Cx<S> cK = {-dKE.re - ap.re - bq[q].re + cq[q].re + v[0] * Z[0].re + v[1] * Z[1].re + v[2] * Z[2].re,
                           -dKE.im - ap.im - bq[q].im + cq[q].im + v[0] * Z[0].im + v[1] * Z[1].im + v[2] * Z[2].im};
-        kv = cxr(cK, ss * fK);
+        kv = cxr(cK, S(ss * fK));
       }
       Kb[3 * p + q] = kv;
     }
@@ -392,6 +393,133 @@ __global__ void __launch_bounds__(kAdjThreads) adj_pair_kernel(AdjPairArgs a) {
     }
     __syncthreads();
   }
+}
+
+// ---- permittivity mode on plain geometry ---------------------------------
+//
+// The permittivity moves only k, c2 and Zsi: the geometry carries no
+// derivative, so the face data come as FP64 from the assembly's arrays and
+// only the values that depend on k are dual numbers.  Same pairs, same
+// contraction and the same deterministic block sums as adj_pair_kernel in
+// eps mode, without the dual face records (which spill at 255 registers).
+
+struct AdjEpsArgs {
+  int F;
+  int64_t n, N;
+  const double *qrel, *qabs, *cp, *area, *mu, *sl, *bn;  // assembly geometry; bn: [F][3][3] free vertices
+  const FaceGeo *geo;  // [F] vertices, edge vectors and normals
+  const int *hpar;
+  const unsigned *near_bits;
+  Dual kr, ki;
+  Cx<Dual> c1, c2, Zsi;
+  int R;
+  const double2 *lam, *xv, *W;
+  double *part;  // [gridDim.y][gridDim.x][max(R,1)][2]
+};
+
+// The closed-form singular terms of a near pair: geometry only, scaled by
+// the dual coefficients (as pair_eval does for near pairs).
+template <int NQ>
+__device__ __noinline__ void eps_near_terms(const AdjEpsArgs &a, int m, int n, Cx<Dual> *Sb, Cx<Dual> *Kb) {
+  double st[6][9];
+  static_terms<double, NQ>(reinterpret_cast<const double(*)[3]>(a.qabs + (size_t)m * NQ * 3), a.area[m], a.sl + 3 * m,
+                           reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)m), a.geo[n], a.area[n],
+                           a.sl + 3 * n, reinterpret_cast<const double(*)[3]>(a.bn + 9 * (size_t)n), m == n, st);
+  const double f4 = 1.0 / (4.0 * kPi);
+  const Cx<Dual> f8 = {(a.kr * a.kr - a.ki * a.ki) / (8.0 * kPi), (2.0 * a.kr * a.ki) / (8.0 * kPi)};
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const Cx<Dual> dterm = {f4 * st[0][i] - f8.re * st[1][i], -f8.im * st[1][i]};
+    const Cx<Dual> hterm = {f4 * st[2][i] - f8.re * st[3][i], -f8.im * st[3][i]};
+    const Cx<Dual> kterm = {f4 * st[4][i] - f8.re * st[5][i], -f8.im * st[5][i]};
+    Sb[i] = cxa(Sb[i], cxa(cxm(a.c1, dterm), cxm(a.c2, hterm)));
+    Kb[i] = cxa(Kb[i], kterm);
+  }
+}
+
+// One thread per source face, one CTA row per test face.
+template <int NQ>
+__global__ void __launch_bounds__(kAdjThreads) adj_eps_kernel(AdjEpsArgs a) {
+  const int m = blockIdx.y;
+  const int x = blockIdx.x * kAdjThreads + threadIdx.x;
+  Cd acc[kAdjMaxObj];
+#pragma unroll
+  for (int o = 0; o < kAdjMaxObj; o++) acc[o] = {0.0, 0.0};
+  if (x < a.F) {
+    const int64_t bit = (int64_t)m * a.F + x;
+    const bool near = (a.near_bits[bit >> 5] >> (bit & 31)) & 1u;
+    double d[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) d[i] = a.cp[3 * m + i] - a.cp[3 * x + i];
+    Moments<Dual> M;
+    if (near)
+      pair_moments<Dual, NQ, true, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d, a.kr,
+                                                  a.ki, M);
+    else
+      pair_moments<Dual, NQ, false, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d,
+                                                   a.kr, a.ki, M);
+    const Cx<Dual> fD = {a.c1.re * (kOofpi / 4.0), a.c1.im * (kOofpi / 4.0)};
+    const Cx<Dual> fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
+    Cx<Dual> Sb[9], Kb[9];
+    blocks_generic<Dual, double>(M, reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)m),
+                                 reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)x), a.sl + 3 * m,
+                                 a.sl + 3 * x, d, fD, fH, kOofpi / 4.0, m == x, Sb, Kb);
+    if (near) eps_near_terms<NQ>(a, m, x, Sb, Kb);
+    const int64_t N = a.N, ld = a.n;
+#pragma unroll 1
+    for (int p = 0; p < 3; p++) {
+      const int64_t r = a.hpar[3 * m + p];
+#pragma unroll 1
+      for (int q = 0; q < 3; q++) {
+        const int64_t cI = a.hpar[3 * x + q];
+        const Cd dS = dpart(Sb[3 * p + q]), dZ = dpart(cxm(a.Zsi, Sb[3 * p + q])), dK = dpart(Kb[3 * p + q]);
+        if (a.R == 0) {
+          const double2 wjj = a.W[r + cI * ld], wmm = a.W[(r + N) + (cI + N) * ld];
+          const double2 wmj = a.W[(r + N) + cI * ld], wjm = a.W[r + (cI + N) * ld];
+          const Cd t1 = cdm(dS, wjj), t2 = cdm(dZ, wmm), t3 = cdm(dK, make_double2(wmj.x - wjm.x, wmj.y - wjm.y));
+          acc[0].re += t1.re + t2.re + t3.re;
+          acc[0].im += t1.im + t2.im + t3.im;
+        } else {
+          for (int o = 0; o < a.R; o++) {
+            const double2 *l = a.lam + (size_t)o * ld, *xo = a.xv + (size_t)o * ld;
+            const double2 lr = l[r], lrN = l[r + N], xc = xo[cI], xcN = xo[cI + N];
+            const double2 jj = make_double2(lr.x * xc.x - lr.y * xc.y, lr.x * xc.y + lr.y * xc.x);
+            const double2 mm = make_double2(lrN.x * xcN.x - lrN.y * xcN.y, lrN.x * xcN.y + lrN.y * xcN.x);
+            const double2 mj = make_double2(lrN.x * xc.x - lrN.y * xc.y, lrN.x * xc.y + lrN.y * xc.x);
+            const double2 jm = make_double2(lr.x * xcN.x - lr.y * xcN.y, lr.x * xcN.y + lr.y * xcN.x);
+            const Cd t1 = cdm(dS, jj), t2 = cdm(dZ, mm), t3 = cdm(dK, make_double2(mj.x - jm.x, mj.y - jm.y));
+            acc[o].re += t1.re + t2.re + t3.re;
+            acc[o].im += t1.im + t2.im + t3.im;
+          }
+        }
+      }
+    }
+  }
+  __shared__ double red[kAdjThreads][2];
+  const int nobj = a.R == 0 ? 1 : a.R;
+  for (int o = 0; o < nobj; o++) {
+    red[threadIdx.x][0] = acc[o].re;
+    red[threadIdx.x][1] = acc[o].im;
+    __syncthreads();
+    for (int w = kAdjThreads / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) {
+        red[threadIdx.x][0] += red[threadIdx.x + w][0];
+        red[threadIdx.x][1] += red[threadIdx.x + w][1];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      double *out = a.part + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * nobj + o) * 2;
+      out[0] = red[0][0];
+      out[1] = red[0][1];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NQ>
+void launch_adj_eps(const dim3 &grid, cudaStream_t s, const AdjEpsArgs &a) {
+  adj_eps_kernel<NQ><<<grid, kAdjThreads, 0, s>>>(a);
 }
 
 // ---- explicit geometry terms of the exterior surface: q and sigma --------

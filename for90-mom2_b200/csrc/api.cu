@@ -444,6 +444,8 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (ec) c->la_ctas = std::max(0, std::atoi(ec));
   const char *ef = std::getenv("MOM_LA_FROM");
   if (ef) c->la_from = std::atof(ef);
+  const char *ae = std::getenv("MOM_ADJ_EPS_PLAIN");
+  if (ae) c->adj_eps_plain = std::atoi(ae) != 0;
   const char *ft = std::getenv("MOM_FUSED_TRSM");
   if (ft) c->fused_trsm = std::atoi(ft) != 0;
   *out = c;

@@ -79,9 +79,11 @@ __device__ __forceinline__ void zero(Cx<T> &a) {
 
 // Point-pair loop.  rho_t: test point offsets (stride 3), rho_s: source
 // offsets with stride sstride between coordinates; w from constant memory.
-// SMOOTH selects the singularity-subtracted kernels (green.f90:40-97).
-template <typename T, int NQ, bool SMOOTH, bool LOSSLESS = false>
-__device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int sstride, const T d[3], T kr, T ki,
+// SMOOTH selects the singularity-subtracted kernels (green.f90:40-97).  The
+// geometry has its own type G (the value type T by default): the adjoint's
+// permittivity derivative runs T = dual numbers on plain FP64 geometry.
+template <typename T, int NQ, bool SMOOTH, bool LOSSLESS = false, typename G = T>
+__device__ __forceinline__ void pair_moments(const G *rho_t, const G *rho_s, int sstride, const G d[3], T kr, T ki,
                                              Moments<T> &M) {
   zero(M.TA);
   zero(M.TD);
@@ -98,26 +100,26 @@ __device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int
   const T k2r = kr * kr - ki * ki, k2i = 2 * kr * ki;
 #pragma unroll 1
   for (int t = 0; t < NQ; t++) {
-    const T rx = rho_t[3 * t], ry = rho_t[3 * t + 1], rz = rho_t[3 * t + 2];
-    const T wt = (T)c_qw[t];
-    const T ax = d[0] + rx, ay = d[1] + ry, az = d[2] + rz;
+    const G rx = rho_t[3 * t], ry = rho_t[3 * t + 1], rz = rho_t[3 * t + 2];
+    const G wt = (G)c_qw[t];
+    const G ax = d[0] + rx, ay = d[1] + ry, az = d[2] + rz;
     Cx<T> G0 = {0, 0}, P0 = {0, 0}, G1[3] = {{0, 0}, {0, 0}, {0, 0}}, P1[3] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
     for (int s = 0; s < NQ; s++) {
-      const T sx = rho_s[(3 * s) * sstride], sy = rho_s[(3 * s + 1) * sstride], sz = rho_s[(3 * s + 2) * sstride];
-      const T ws = (T)c_qw[s];
-      const T dx = ax - sx, dy = ay - sy, dz = az - sz;
-      const T R2 = dx * dx + dy * dy + dz * dz;
+      const G sx = rho_s[(3 * s) * sstride], sy = rho_s[(3 * s + 1) * sstride], sz = rho_s[(3 * s + 2) * sstride];
+      const G ws = (G)c_qw[s];
+      const G dx = ax - sx, dy = ay - sy, dz = az - sz;
+      const G R2 = dx * dx + dy * dy + dz * dz;
       T gre, gim, pre, pim;
       if (R2 > 0) {
-        const T iR = frsqrt(R2);
-        const T R = R2 * iR;
+        const G iR = frsqrt(R2);
+        const G R = R2 * iR;
         T sn, cs;
         fsincos(kr * R, &sn, &cs);
         const T ea = LOSSLESS ? (T)1 : fexp(-ki * R);  // real k: no decay factor
         const T er = ea * cs, ei = ea * sn;  // e^{ikR}
-        const T iR2 = iR * iR;
-        const T iR3 = iR2 * iR;
+        const G iR2 = iR * iR;
+        const G iR3 = iR2 * iR;
         // q = 1/R^3 - i k / R^2 = (iR3 + ki iR2) - i kr iR2
         const T qr = iR3 + ki * iR2, qi = -kr * iR2;
         if (SMOOTH) {
@@ -127,7 +129,7 @@ __device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int
           pre = (er * qr - ei * qi - iR3 - (T)0.5 * k2r * iR) * ws;
           pim = (er * qi + ei * qr - (T)0.5 * k2i * iR) * ws;
         } else {
-          const T g = iR * ws;
+          const G g = iR * ws;
           gre = er * g;
           gim = ei * g;
           pre = (er * qr - ei * qi) * ws;
@@ -156,7 +158,7 @@ __device__ __forceinline__ void pair_moments(const T *rho_t, const T *rho_s, int
       P1[2].re += pre * sz; P1[2].im += pim * sz;
     }
     // Test-side sums.
-    const T rr[3] = {rx, ry, rz};
+    const G rr[3] = {rx, ry, rz};
     M.TA.re += wt * (rx * G1[0].re + ry * G1[1].re + rz * G1[2].re);
     M.TA.im += wt * (rx * G1[0].im + ry * G1[1].im + rz * G1[2].im);
     M.TD.re += wt * G0.re;
@@ -1298,7 +1300,46 @@ int adjoint_eps(Ctx *c, double omega, const double *ri, int d, int R, const doub
   const size_t nvals = (size_t)grid.x * grid.y * nobj * 2;
   MOM_TRY(ensure_buffer(c, &c->adj_part, &c->adj_part_bytes, sizeof(double) * nvals));
   a.part = (double *)c->adj_part;
-  MOM_TRY(adj_launch_pair(c, grid, a));
+  if (c->adj_eps_plain) {
+    // the same sums with FP64 geometry and dual numbers only where k enters
+    MOM_TRY(nfield_geometry(c, D));
+    AdjEpsArgs e;
+    e.F = D.F;
+    e.n = c->n;
+    e.N = c->N;
+    e.qrel = D.qrel;
+    e.qabs = D.qabs;
+    e.cp = D.cp;
+    e.area = D.area;
+    e.mu = D.mu;
+    e.sl = D.sl;
+    e.bn = D.nf_bn;
+    e.geo = reinterpret_cast<const FaceGeo *>(D.nf_geo);
+    e.hpar = D.hpar;
+    e.near_bits = D.near_bits;
+    e.kr = a.kr;
+    e.ki = a.ki;
+    e.c1 = a.c1;
+    e.c2 = a.c2;
+    e.Zsi = a.Zsi;
+    e.R = R;
+    e.lam = lam;
+    e.xv = xv;
+    e.W = W;
+    e.part = a.part;
+    switch (c->nq) {
+      case 1: launch_adj_eps<1>(grid, c->stream, e); break;
+      case 3: launch_adj_eps<3>(grid, c->stream, e); break;
+      case 4: launch_adj_eps<4>(grid, c->stream, e); break;
+      case 7: launch_adj_eps<7>(grid, c->stream, e); break;
+      case 13: launch_adj_eps<13>(grid, c->stream, e); break;
+      default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+    }
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+  } else {
+    MOM_TRY(adj_launch_pair(c, grid, a));
+  }
   std::vector<double> h(nvals);
   MOM_CUDA(c, cudaMemcpyAsync(h.data(), a.part, sizeof(double) * nvals, cudaMemcpyDeviceToHost, c->stream));
   MOM_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -224,6 +224,9 @@ struct Ctx {
   // (MOM_FUSED_TRSM=1) instead of library CGEMMs; measured slower at
   // 15,360 unknowns (158.6 against 155.0 ms per solve), so off by default.
   int fused_trsm = 0;
+  // Permittivity gradients by adj_eps_kernel (FP64 geometry, dual numbers in
+  // k only); MOM_ADJ_EPS_PLAIN=0 selects the all-dual adj_pair_kernel.
+  int adj_eps_plain = 1;
   bool autotune = true;
   struct Tuned {
     int64_t n;

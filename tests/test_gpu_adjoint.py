@@ -71,6 +71,29 @@ def test_eps_gradient_matches_fd(solver, prec):
             assert abs(g[k, j] - fd[k]) <= 1e-5 * abs(fd[k]), (prec, j, k, g[k, j], fd[k])
 
 
+def test_eps_gradient_plain_geometry_matches_dual(solver, monkeypatch):
+    """The permittivity gradient of adj_eps_kernel (FP64 geometry, dual numbers
+    in k only) equals that of the all-dual adj_pair_kernel (MOM_ADJ_EPS_PLAIN=0),
+    on one and on several objectives and with the dense-W contraction."""
+    geo = core_shell(1)
+    ri = ri_of([EPS, 2.13])
+    srcs = [M.src_pw(30, 40, 0), M.src_pw_elliptic(120, 250, 0.3 + 0.4j)]
+    om = M.omega_of(WL)
+    sigmas(solver, geo, ri, M.FP64, srcs)
+    plain = solver.adjoint(om, ri, srcs, M.FP64, eps_dom=1)["deps"]
+    plain_mean = solver.adjoint_mean_eps(om, ri, srcs, M.FP64, eps_dom=1)
+    monkeypatch.setenv("MOM_ADJ_EPS_PLAIN", "0")
+    other = M.Solver(0)
+    try:
+        sigmas(other, geo, ri, M.FP64, srcs)
+        dual = other.adjoint(om, ri, srcs, M.FP64, eps_dom=1)["deps"]
+        dual_mean = other.adjoint_mean_eps(om, ri, srcs, M.FP64, eps_dom=1)
+    finally:
+        other.close()
+    assert np.allclose(plain, dual, rtol=1e-11, atol=0), np.max(np.abs(plain / dual - 1))
+    assert np.allclose(plain_mean, dual_mean, rtol=1e-11, atol=0)
+
+
 def test_eps_gradient_core_shell_mean(solver):
     """d(mean sigma)/d(shell eps) over several incidences, dense-W contraction."""
     geo = core_shell(1)
