@@ -29,7 +29,6 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
-#include <map>
 #include <set>
 #include <vector>
 
