@@ -202,11 +202,13 @@ __device__ void face_build(const AdjTopo &t, int f, int snode, int scoord, FaceA
   }
 }
 
-// blocks_from_moments in the scalar type S, with the geometry in type G (S
-// by default).
-template <typename S, typename G = S>
-__device__ void blocks_generic(const Moments<S> &M, const G mu[3][3], const G nu[3][3], const G slp[3], const G slq[3],
-                               const G d[3], Cx<S> fD, Cx<S> fH, double fK, bool self, Cx<S> *Sb, Cx<S> *Kb) {
+// blocks_from_moments in the scalar type S, with the test face's geometry in
+// type GM, the source face's in GN and the centroid offset in GD (S by
+// default).
+template <typename S, typename GM = S, typename GN = GM, typename GD = GM>
+__device__ void blocks_generic(const Moments<S> &M, const GM mu[3][3], const GN nu[3][3], const GM slp[3],
+                               const GN slq[3], const GD d[3], Cx<S> fD, Cx<S> fH, double fK, bool self, Cx<S> *Sb,
+                               Cx<S> *Kb) {
   Cx<S> KBv[3], KDmF[3];
   KBv[0] = {d[1] * M.KF[2].re - d[2] * M.KF[1].re + M.KE[0].re, d[1] * M.KF[2].im - d[2] * M.KF[1].im + M.KE[0].im};
   KBv[1] = {d[2] * M.KF[0].re - d[0] * M.KF[2].re + M.KE[1].re, d[2] * M.KF[0].im - d[0] * M.KF[2].im + M.KE[1].im};
@@ -219,18 +221,18 @@ __device__ void blocks_generic(const Moments<S> &M, const G mu[3][3], const G nu
   Cx<S> beta[3], bq[3], cq[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    const G *v = nu[q];
+    const GN *v = nu[q];
     beta[q] = {v[0] * M.TB[0].re + v[1] * M.TB[1].re + v[2] * M.TB[2].re,
                v[0] * M.TB[0].im + v[1] * M.TB[1].im + v[2] * M.TB[2].im};
-    G dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
-    bq[q] = {dn[0] * M.KC[0].re + dn[1] * M.KC[1].re + dn[2] * M.KC[2].re,
-             dn[0] * M.KC[0].im + dn[1] * M.KC[1].im + dn[2] * M.KC[2].im};
+    const auto dn0 = d[1] * v[2] - d[2] * v[1], dn1 = d[2] * v[0] - d[0] * v[2], dn2 = d[0] * v[1] - d[1] * v[0];
+    bq[q] = {dn0 * M.KC[0].re + dn1 * M.KC[1].re + dn2 * M.KC[2].re,
+             dn0 * M.KC[0].im + dn1 * M.KC[1].im + dn2 * M.KC[2].im};
     cq[q] = {v[0] * M.KE[0].re + v[1] * M.KE[1].re + v[2] * M.KE[2].re,
              v[0] * M.KE[0].im + v[1] * M.KE[1].im + v[2] * M.KE[2].im};
   }
 #pragma unroll
   for (int p = 0; p < 3; p++) {
-    const G *u = mu[p];
+    const GM *u = mu[p];
     const Cx<S> alpha = {u[0] * M.TC[0].re + u[1] * M.TC[1].re + u[2] * M.TC[2].re,
                          u[0] * M.TC[0].im + u[1] * M.TC[1].im + u[2] * M.TC[2].im};
     const Cx<S> ap = {u[0] * KBv[0].re + u[1] * KBv[1].re + u[2] * KBv[2].re,
@@ -240,9 +242,9 @@ __device__ void blocks_generic(const Moments<S> &M, const G mu[3][3], const G nu
                         {u[0] * KDmF[1].re - u[1] * KDmF[0].re, u[0] * KDmF[1].im - u[1] * KDmF[0].im}};
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const G *v = nu[q];
-      const G uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
-      const G ss = slp[p] * slq[q];
+      const GN *v = nu[q];
+      const auto uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+      const auto ss = slp[p] * slq[q];
       const Cx<S> cD = {M.TA.re - beta[q].re - alpha.re + uv * M.TD.re, M.TA.im - beta[q].im - alpha.im + uv * M.TD.im};
       const Cx<S> s12 = cxa(cxm(fD, cD), cxm(fH, M.TD));
       Sb[3 * p + q] = cxr(s12, S(ss));
@@ -302,9 +304,38 @@ struct AdjPairArgs {
   const double2 *lam, *xv;  // [R][n]
   const double2 *W;         // [n][n] column-major, W(r, c) = sum_o lambda_o[r] x_o[c]
   double *part;    // [gridDim.y][gridDim.x][max(R,1)][2]
+  // the assembly's FP64 geometry (partner faces that carry no derivative)
+  const double *qrel, *cp, *mu, *sl;
 };
 
 __device__ __forceinline__ Cd cdm(Cd a, double2 b) { return {a.re * b.x - a.im * b.y, a.re * b.y + a.im * b.x}; }
+
+// Adds the derivative blocks Sb, Kb of the pair (test m, source n) contracted
+// with the objectives into acc (the loop of pair_contract).
+__device__ __forceinline__ void contract_blocks(const AdjPairArgs &a, int m, int n, const Cx<Dual> *Sb,
+                                                const Cx<Dual> *Kb, Cd *acc) {
+  const int64_t N = a.t.N, ld = a.n;
+#pragma unroll 1
+  for (int p = 0; p < 3; p++) {
+    const int64_t r = a.t.hpar[3 * m + p];
+#pragma unroll 1
+    for (int q = 0; q < 3; q++) {
+      const int64_t cI = a.t.hpar[3 * n + q];
+      const Cd dS = dpart(Sb[3 * p + q]), dZ = dpart(cxm(a.Zsi, Sb[3 * p + q])), dK = dpart(Kb[3 * p + q]);
+      for (int o = 0; o < a.R; o++) {
+        const double2 *l = a.lam + (size_t)o * ld, *x = a.xv + (size_t)o * ld;
+        const double2 lr = l[r], lrN = l[r + N], xc = x[cI], xcN = x[cI + N];
+        const double2 jj = make_double2(lr.x * xc.x - lr.y * xc.y, lr.x * xc.y + lr.y * xc.x);
+        const double2 mm = make_double2(lrN.x * xcN.x - lrN.y * xcN.y, lrN.x * xcN.y + lrN.y * xcN.x);
+        const double2 mj = make_double2(lrN.x * xc.x - lrN.y * xc.y, lrN.x * xc.y + lrN.y * xc.x);
+        const double2 jm = make_double2(lr.x * xcN.x - lr.y * xcN.y, lr.x * xcN.y + lr.y * xcN.x);
+        const Cd t1 = cdm(dS, jj), t2 = cdm(dZ, mm), t3 = cdm(dK, make_double2(mj.x - jm.x, mj.y - jm.y));
+        acc[o].re += t1.re + t2.re + t3.re;
+        acc[o].im += t1.im + t2.im + t3.im;
+      }
+    }
+  }
+}
 
 // Adds d/dp (lambda_o^T A x_o) of pair (m, n) into acc[o] for the four
 // PMCHWT blocks [JJ] S, [MM] Zsi S, [MJ] K, [JM] -K (sysmat.f90:70-99).
@@ -393,6 +424,95 @@ __global__ void __launch_bounds__(kAdjThreads) adj_pair_kernel(AdjPairArgs a) {
     }
     __syncthreads();
   }
+}
+
+// ---- vertex mode with one dual face ---------------------------------------
+//
+// Item (vertex v, incident face f, axis): only the faces that touch v carry a
+// derivative.  The CTA builds f's dual record once in shared memory; a
+// partner x that does not touch v is read as FP64 from the assembly's arrays
+// and the far pairs (f, x) and (x, f) run with one dual and one plain face.
+// Partners that touch v, and near pairs (closed-form singular terms), take
+// the all-dual evaluation of adj_pair_kernel.  Same pairs, same contraction
+// and the same deterministic block sums.
+
+template <int NQ>
+__device__ __noinline__ void vertex_pairs_dual(const AdjPairArgs &a, int f, int x, int snode, int scoord,
+                                               const FaceAll<Dual, NQ> &ff, bool touches, Cd *acc) {
+  FaceAll<Dual, NQ> fx;
+  face_build<NQ>(a.t, x, snode, scoord, fx);
+  pair_contract<NQ>(a, f, x, ff, fx, acc);
+  if (!touches) pair_contract<NQ>(a, x, f, fx, ff, acc);
+}
+
+template <int NQ>
+__global__ void __launch_bounds__(kAdjThreads) adj_vertex_kernel(AdjPairArgs a) {
+  // the seeded face's dual record, built once per CTA (raw storage: Dual has
+  // a constructor, which a __shared__ object may not run)
+  __shared__ __align__(16) unsigned char ff_raw[sizeof(FaceAll<Dual, NQ>)];
+  FaceAll<Dual, NQ> &ff = *reinterpret_cast<FaceAll<Dual, NQ> *>(ff_raw);
+  const int item = blockIdx.y;
+  const int f = a.inc_face[item / 3], snode = a.inc_node[item / 3], scoord = item % 3;
+  if (threadIdx.x == 0) face_build<NQ>(a.t, f, snode, scoord, ff);
+  __syncthreads();
+  const int x = blockIdx.x * kAdjThreads + threadIdx.x;
+  Cd acc[kAdjMaxObj];
+#pragma unroll
+  for (int o = 0; o < kAdjMaxObj; o++) acc[o] = {0.0, 0.0};
+  if (x < a.t.F) {
+    const bool touches = a.t.fnode[3 * x] == snode || a.t.fnode[3 * x + 1] == snode || a.t.fnode[3 * x + 2] == snode;
+    const int64_t b1 = (int64_t)f * a.t.F + x, b2 = (int64_t)x * a.t.F + f;
+    const bool near = ((a.t.near_bits[b1 >> 5] >> (b1 & 31)) & 1u) || ((a.t.near_bits[b2 >> 5] >> (b2 & 31)) & 1u);
+    if (touches || near) {
+      vertex_pairs_dual<NQ>(a, f, x, snode, scoord, ff, touches, acc);
+    } else {
+      const double *qx = a.qrel + (size_t)x * NQ * 3;
+      const double *mux = a.mu + 9 * (size_t)x, *slx = a.sl + 3 * (size_t)x;
+      const Cx<Dual> fD = {a.c1.re * (kOofpi / 4.0), a.c1.im * (kOofpi / 4.0)};
+      const Cx<Dual> fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
+      Dual d[3];
+      Cx<Dual> Sb[9], Kb[9];
+      Moments<Dual> M;
+      // (f, x): dual test face, plain source
+#pragma unroll
+      for (int i = 0; i < 3; i++) d[i] = ff.cp[i] - a.cp[3 * x + i];
+      pair_moments<Dual, NQ, false, false, Dual, double, Dual>(&ff.qr[0][0], qx, 1, d, a.kr, a.ki, M);
+      blocks_generic<Dual, Dual, double, Dual>(M, ff.mu, reinterpret_cast<const double(*)[3]>(mux), ff.sl, slx, d, fD,
+                                               fH, kOofpi / 4.0, false, Sb, Kb);
+      contract_blocks(a, f, x, Sb, Kb, acc);
+      // (x, f): plain test face, dual source
+#pragma unroll
+      for (int i = 0; i < 3; i++) d[i] = a.cp[3 * x + i] - ff.cp[i];
+      pair_moments<Dual, NQ, false, false, double, Dual, Dual>(qx, &ff.qr[0][0], 1, d, a.kr, a.ki, M);
+      blocks_generic<Dual, double, Dual, Dual>(M, reinterpret_cast<const double(*)[3]>(mux), ff.mu, slx, ff.sl, d, fD,
+                                               fH, kOofpi / 4.0, false, Sb, Kb);
+      contract_blocks(a, x, f, Sb, Kb, acc);
+    }
+  }
+  __shared__ double red[kAdjThreads][2];
+  for (int o = 0; o < a.R; o++) {
+    red[threadIdx.x][0] = acc[o].re;
+    red[threadIdx.x][1] = acc[o].im;
+    __syncthreads();
+    for (int w = kAdjThreads / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) {
+        red[threadIdx.x][0] += red[threadIdx.x + w][0];
+        red[threadIdx.x][1] += red[threadIdx.x + w][1];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      double *out = a.part + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * a.R + o) * 2;
+      out[0] = red[0][0];
+      out[1] = red[0][1];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NQ>
+void launch_adj_vertex(const dim3 &grid, cudaStream_t s, const AdjPairArgs &a) {
+  adj_vertex_kernel<NQ><<<grid, kAdjThreads, 0, s>>>(a);
 }
 
 // ---- permittivity mode on plain geometry ---------------------------------

@@ -446,8 +446,10 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (ef) c->la_from = std::atof(ef);
   const char *ae = std::getenv("MOM_ADJ_EPS_PLAIN");
   if (ae) c->adj_eps_plain = std::atoi(ae) != 0;
+  const char *av = std::getenv("MOM_ADJ_VERTEX_PLAIN");
+  if (av) c->adj_vertex_plain = std::atoi(av) != 0;
   const char *ft = std::getenv("MOM_FUSED_TRSM");
-  if (ft) c->fused_trsm = std::atoi(ft) != 0;
+  if (ft) c->fused_trsm = std::max(0, std::min(2, std::atoi(ft)));
   *out = c;
   return MOM_OK;
 }

@@ -80,10 +80,12 @@ __device__ __forceinline__ void zero(Cx<T> &a) {
 // Point-pair loop.  rho_t: test point offsets (stride 3), rho_s: source
 // offsets with stride sstride between coordinates; w from constant memory.
 // SMOOTH selects the singularity-subtracted kernels (green.f90:40-97).  The
-// geometry has its own type G (the value type T by default): the adjoint's
-// permittivity derivative runs T = dual numbers on plain FP64 geometry.
-template <typename T, int NQ, bool SMOOTH, bool LOSSLESS = false, typename G = T>
-__device__ __forceinline__ void pair_moments(const G *rho_t, const G *rho_s, int sstride, const G d[3], T kr, T ki,
+// geometry has its own types (the value type T by default): G for the test
+// points, GS for the source points, GD for the centroid offset; the adjoint
+// runs T = dual numbers on plain FP64 geometry (permittivity) or on one dual
+// and one plain face (vertex coordinates).
+template <typename T, int NQ, bool SMOOTH, bool LOSSLESS = false, typename G = T, typename GS = G, typename GD = G>
+__device__ __forceinline__ void pair_moments(const G *rho_t, const GS *rho_s, int sstride, const GD d[3], T kr, T ki,
                                              Moments<T> &M) {
   zero(M.TA);
   zero(M.TD);
@@ -102,24 +104,24 @@ __device__ __forceinline__ void pair_moments(const G *rho_t, const G *rho_s, int
   for (int t = 0; t < NQ; t++) {
     const G rx = rho_t[3 * t], ry = rho_t[3 * t + 1], rz = rho_t[3 * t + 2];
     const G wt = (G)c_qw[t];
-    const G ax = d[0] + rx, ay = d[1] + ry, az = d[2] + rz;
+    const auto ax = d[0] + rx, ay = d[1] + ry, az = d[2] + rz;
     Cx<T> G0 = {0, 0}, P0 = {0, 0}, G1[3] = {{0, 0}, {0, 0}, {0, 0}}, P1[3] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
     for (int s = 0; s < NQ; s++) {
-      const G sx = rho_s[(3 * s) * sstride], sy = rho_s[(3 * s + 1) * sstride], sz = rho_s[(3 * s + 2) * sstride];
-      const G ws = (G)c_qw[s];
-      const G dx = ax - sx, dy = ay - sy, dz = az - sz;
-      const G R2 = dx * dx + dy * dy + dz * dz;
+      const GS sx = rho_s[(3 * s) * sstride], sy = rho_s[(3 * s + 1) * sstride], sz = rho_s[(3 * s + 2) * sstride];
+      const GS ws = (GS)c_qw[s];
+      const auto dx = ax - sx, dy = ay - sy, dz = az - sz;
+      const auto R2 = dx * dx + dy * dy + dz * dz;
       T gre, gim, pre, pim;
       if (R2 > 0) {
-        const G iR = frsqrt(R2);
-        const G R = R2 * iR;
+        const auto iR = frsqrt(R2);
+        const auto R = R2 * iR;
         T sn, cs;
         fsincos(kr * R, &sn, &cs);
         const T ea = LOSSLESS ? (T)1 : fexp(-ki * R);  // real k: no decay factor
         const T er = ea * cs, ei = ea * sn;  // e^{ikR}
-        const G iR2 = iR * iR;
-        const G iR3 = iR2 * iR;
+        const auto iR2 = iR * iR;
+        const auto iR3 = iR2 * iR;
         // q = 1/R^3 - i k / R^2 = (iR3 + ki iR2) - i kr iR2
         const T qr = iR3 + ki * iR2, qi = -kr * iR2;
         if (SMOOTH) {
@@ -129,7 +131,7 @@ __device__ __forceinline__ void pair_moments(const G *rho_t, const G *rho_s, int
           pre = (er * qr - ei * qi - iR3 - (T)0.5 * k2r * iR) * ws;
           pim = (er * qi + ei * qr - (T)0.5 * k2i * iR) * ws;
         } else {
-          const G g = iR * ws;
+          const auto g = iR * ws;
           gre = er * g;
           gim = ei * g;
           pre = (er * qr - ei * qi) * ws;
@@ -807,17 +809,43 @@ int near_setup(Ctx *c, DomDev &D, const double *tcp, const double *tqabs, const 
                int64_t *nnear, int **near_m, int **near_n, double **near_static) {
   const int F = D.F;
   const double thr = D.avelen * 3;
+  // near_faces (sysmat.f90:233-260): |cp_m - cp_n| < 3 avelen.  The source
+  // centroids are binned in cubes of side 3 avelen, so the partners of a test
+  // face lie in the 27 cubes around its own; the pairs come out in the order
+  // of the all-pairs loop (m, then n ascending) with the same distance test.
   std::vector<int> nm, nn;
+  auto cell = [&](double v) { return (int64_t)std::floor(v / thr); };
+  auto key = [](int64_t i, int64_t j, int64_t k) {
+    return ((i & 0x1FFFFF) << 42) | ((j & 0x1FFFFF) << 21) | (k & 0x1FFFFF);
+  };
+  std::vector<std::pair<int64_t, int>> bins(F);
+  for (int n = 0; n < F; n++) {
+    const double *cn = &D.h_cp[3 * (size_t)n];
+    bins[n] = {key(cell(cn[0]), cell(cn[1]), cell(cn[2])), n};
+  }
+  std::sort(bins.begin(), bins.end());
+  std::vector<int> cand;
   for (int m = 0; m < F; m++) {
     const double *cm = tcp + 3 * (size_t)m;
-    for (int n = 0; n < F; n++) {
-      const double *cn = &D.h_cp[3 * (size_t)n];
-      const double d0 = cm[0] - cn[0], d1 = cm[1] - cn[1], d2 = cm[2] - cn[2];
-      const double distsq = d0 * d0 + d1 * d1 + d2 * d2;
-      if (distsq < thr * thr) {
-        nm.push_back(m);
-        nn.push_back(n);
-      }
+    const int64_t ci = cell(cm[0]), cj = cell(cm[1]), ck = cell(cm[2]);
+    cand.clear();
+    for (int64_t a = -1; a <= 1; a++)
+      for (int64_t b = -1; b <= 1; b++)
+        for (int64_t e = -1; e <= 1; e++) {
+          const int64_t k = key(ci + a, cj + b, ck + e);
+          auto it = std::lower_bound(bins.begin(), bins.end(), std::make_pair(k, -1));
+          for (; it != bins.end() && it->first == k; ++it) {
+            const int n = it->second;
+            const double *cn = &D.h_cp[3 * (size_t)n];
+            const double d0 = cm[0] - cn[0], d1 = cm[1] - cn[1], d2 = cm[2] - cn[2];
+            const double distsq = d0 * d0 + d1 * d1 + d2 * d2;
+            if (distsq < thr * thr) cand.push_back(n);
+          }
+        }
+    std::sort(cand.begin(), cand.end());
+    for (int n : cand) {
+      nm.push_back(m);
+      nn.push_back(n);
     }
   }
   *nnear = (int64_t)nm.size();
@@ -1291,6 +1319,10 @@ int adjoint_eps(Ctx *c, double omega, const double *ri, int d, int R, const doub
   medium_duals(omega, ri, d, true, a);
   a.mode = 0;
   a.inc_node = a.inc_face = nullptr;
+  a.qrel = D.qrel;
+  a.cp = D.cp;
+  a.mu = D.mu;
+  a.sl = D.sl;
   a.R = R;
   a.lam = lam;
   a.xv = xv;
@@ -1381,11 +1413,28 @@ int adjoint_nodes(Ctx *c, double omega, const double *ri, int R, const double2 *
     a.lam = lam;
     a.xv = xv;
     a.W = nullptr;
+    a.qrel = D.qrel;
+    a.cp = D.cp;
+    a.mu = D.mu;
+    a.sl = D.sl;
     const dim3 grid((D.F + kAdjThreads - 1) / kAdjThreads, 3 * D.ninc);
     const size_t nvals = (size_t)grid.x * grid.y * R * 2;
     MOM_TRY(ensure_buffer(c, &c->adj_part, &c->adj_part_bytes, sizeof(double) * nvals));
     a.part = (double *)c->adj_part;
-    MOM_TRY(adj_launch_pair(c, grid, a));
+    if (c->adj_vertex_plain) {
+      switch (c->nq) {
+        case 1: launch_adj_vertex<1>(grid, c->stream, a); break;
+        case 3: launch_adj_vertex<3>(grid, c->stream, a); break;
+        case 4: launch_adj_vertex<4>(grid, c->stream, a); break;
+        case 7: launch_adj_vertex<7>(grid, c->stream, a); break;
+        case 13: launch_adj_vertex<13>(grid, c->stream, a); break;
+        default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
+      }
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+    } else {
+      MOM_TRY(adj_launch_pair(c, grid, a));
+    }
     std::vector<double> h(nvals);
     std::vector<int> inode(D.ninc);
     MOM_CUDA(c, cudaMemcpyAsync(h.data(), a.part, sizeof(double) * nvals, cudaMemcpyDeviceToHost, c->stream));

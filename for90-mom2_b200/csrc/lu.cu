@@ -577,13 +577,17 @@ __global__ void laswp_range_kernel(T *A, int64_t lda, int64_t c0, int64_t ncols,
 }
 
 // The interchanges of the np panels of an outer block [J0, J0 + NBc), in
-// panel order, on every column outside that block: one warp per column,
-// maps at pm + 260 p (dst[128], src[128], count).
+// panel order, on the columns outside that block: one warp per column, maps
+// at pm + 260 p (dst[128], src[128], count).  The outside columns are
+// numbered 0 .. n - NBc - 1 (those right of the block shifted by NBc); the
+// launch covers [c_lo, c_hi) of that numbering without [s_lo, s_hi).
 template <typename T>
-__global__ void laswp_block_kernel(T *A, int64_t lda, int64_t n, int64_t J0, int64_t NBc, const int *pm, int np) {
+__global__ void laswp_block_kernel(T *A, int64_t lda, int64_t n, int64_t J0, int64_t NBc, const int *pm, int np,
+                                   int64_t c_lo, int64_t c_hi, int64_t s_lo, int64_t s_hi) {
   const int lane = threadIdx.x & 31;
-  int64_t col = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (col >= n - NBc) return;
+  int64_t col = c_lo + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (col >= c_hi || col >= n - NBc) return;
+  if (col >= s_lo && col < s_hi) return;
   if (col >= J0) col += NBc;
   T *a = A + col * lda;
   for (int p = 0; p < np; p++) {
@@ -1685,7 +1689,7 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       const int64_t rest = J0 + NBc - (j0 + nb);
       if (rest > 0) {
         ProfScope pg(c, kProfGemm, st);
-        if (c->fused_trsm && nb == 64) {
+        if (c->fused_trsm != 0 && nb == 64) {
           block_trsm_kernel<<<(unsigned)((rest + kBtCols - 1) / kBtCols), kBtThreads, kBtSmem, st>>>(
               reinterpret_cast<float2 *>(A), lda, j0, 1, j0 + nb, (int)rest, w.invL32 + (size_t)kb * nb * nb);
           c->launches++;
@@ -1704,7 +1708,8 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     if (ncol <= 0) return MOM_OK;
     const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc;
     ProfScope pg(c, kProfGemm);
-    if (c->fused_trsm && NBc <= (int64_t)kBtMaxPanels * nb && nb == 64) {
+    if ((c->fused_trsm == 1 || (c->fused_trsm == 2 && ncol <= NB)) && NBc <= (int64_t)kBtMaxPanels * nb &&
+        nb == 64) {
       block_trsm_kernel<<<(unsigned)((ncol + kBtCols - 1) / kBtCols), kBtThreads, kBtSmem, sa>>>(
           reinterpret_cast<float2 *>(A), lda, J0, (int)(NBc / nb), c0, (int)ncol, w.invL32 + (size_t)(J0 / nb) * nb * nb);
       c->launches++;
@@ -1731,16 +1736,24 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     const int J = (int)(J0 / NB);
     const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc, nc = n - t0;
     int *pmJ = w.pmb + 260 * 16 * (J & 1), *pmN = w.pmb + 260 * 16 * ((J + 1) & 1);
-    {
-      ProfScope pz(c, kProfPivotAux);
-      if (n > NBc) {
-        laswp_block_kernel<T><<<(unsigned)(((n - NBc) * 32 + 255) / 256), 256, 0, sa>>>(A, lda, n, J0, NBc, pmJ,
-                                                                                         (int)(NBc / nb));
-        c->launches++;
-      }
-    }
-    if (nc <= 0) break;
     const int64_t L = std::min<int64_t>(NB, nc);
+    // block J's interchanges: first on the next block's L columns (outside
+    // numbering [J0, J0 + L)), which its panels need; the other columns follow
+    // beside those panels
+    auto swaps = [&](int64_t lo, int64_t hi, int64_t slo, int64_t shi) -> int {
+      if (hi <= lo) return MOM_OK;
+      ProfScope pz(c, kProfPivotAux);
+      laswp_block_kernel<T><<<(unsigned)(((hi - lo) * 32 + 255) / 256), 256, 0, sa>>>(A, lda, n, J0, NBc, pmJ,
+                                                                                      (int)(NBc / nb), lo, hi, slo, shi);
+      c->launches++;
+      MOM_CUDA(c, cudaGetLastError());
+      return MOM_OK;
+    };
+    if (nc <= 0) {
+      MOM_TRY(swaps(0, n - NBc, 0, 0));
+      break;
+    }
+    MOM_TRY(swaps(J0, J0 + L, 0, 0));
     MOM_TRY(trailing(J0, t0, L, 0));
     // overlap only where the next block's panels leave the GEMM at least half
     // of the SMs (a panel holds at most 208 rows per CTA)
@@ -1755,9 +1768,11 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       MOM_CUDA(c, cudaStreamWaitEvent(sb, c->la_ev[1], 0));
       MOM_TRY(factor_block(t0, sb, c->blas2, pmN, pcap));
       MOM_CUDA(c, cudaEventRecord(c->la_ev[2], sb));
+      MOM_TRY(swaps(0, n - NBc, J0, J0 + L));
       MOM_TRY(trailing(J0, t0 + L, nc - L, std::max(8, c->nsm - P)));
       MOM_CUDA(c, cudaStreamWaitEvent(sa, c->la_ev[2], 0));
     } else {
+      MOM_TRY(swaps(0, n - NBc, J0, J0 + L));
       MOM_TRY(trailing(J0, t0 + L, nc - L, 0));
       MOM_TRY(factor_block(t0, sa, c->blas, pmN, 0));
     }

@@ -221,12 +221,17 @@ struct Ctx {
   int outer_panels = 4;  // panels per outer block of the LU (MOM_LU_OUTER): trailing GEMMs have K = 64 * this
   int small_tc = 0;      // mixed path: K = 64 updates on the tensor cores too (MOM_SMALL_TC=1), else library FP32 GEMM
   // Look-ahead path: the block TRSMs of an outer block by block_trsm_kernel
-  // (MOM_FUSED_TRSM=1) instead of library CGEMMs; measured slower at
-  // 15,360 unknowns (158.6 against 155.0 ms per solve), so off by default.
+  // instead of library CGEMMs: MOM_FUSED_TRSM=1 everywhere (measured slower
+  // at 15,360 unknowns: 158.6 against 155.0 ms per solve), 2 only for the
+  // narrow updates on the panels' critical path (the next block's columns and
+  // the in-block updates), 0 (default) nowhere.
   int fused_trsm = 0;
   // Permittivity gradients by adj_eps_kernel (FP64 geometry, dual numbers in
   // k only); MOM_ADJ_EPS_PLAIN=0 selects the all-dual adj_pair_kernel.
   int adj_eps_plain = 1;
+  // Vertex gradients by adj_vertex_kernel (the seeded face dual in shared
+  // memory, plain partners); MOM_ADJ_VERTEX_PLAIN=0 selects adj_pair_kernel.
+  int adj_vertex_plain = 1;
   bool autotune = true;
   struct Tuned {
     int64_t n;

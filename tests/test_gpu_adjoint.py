@@ -94,6 +94,28 @@ def test_eps_gradient_plain_geometry_matches_dual(solver, monkeypatch):
     assert np.allclose(plain_mean, dual_mean, rtol=1e-11, atol=0)
 
 
+def test_vertex_gradient_plain_partners_matches_dual(solver, monkeypatch):
+    """Vertex gradients of adj_vertex_kernel (the seeded face dual, partner faces
+    in plain FP64) equal those of the all-dual adj_pair_kernel
+    (MOM_ADJ_VERTEX_PLAIN=0) on the perturbed s=2 sphere, two objectives."""
+    geo = sphere(2, perturbed=True)
+    ri = ri_of([EPS])
+    srcs = [M.src_pw(0, 90, 0), M.src_pw_elliptic(50, 20, 1j)]
+    om = M.omega_of(WL)
+    sigmas(solver, geo, ri, M.FP64, srcs)
+    plain = solver.adjoint(om, ri, srcs, M.FP64, nodes=True)["dnodes"]
+    monkeypatch.setenv("MOM_ADJ_VERTEX_PLAIN", "0")
+    other = M.Solver(0)
+    try:
+        sigmas(other, geo, ri, M.FP64, srcs)
+        dual = other.adjoint(om, ri, srcs, M.FP64, nodes=True)["dnodes"]
+    finally:
+        other.close()
+    for a, b in zip(plain, dual):
+        scale = np.abs(b).max()
+        assert np.abs(a - b).max() <= 1e-11 * scale, np.abs(a - b).max() / scale
+
+
 def test_eps_gradient_core_shell_mean(solver):
     """d(mean sigma)/d(shell eps) over several incidences, dense-W contraction."""
     geo = core_shell(1)
