@@ -680,7 +680,6 @@ int mom_gpu_shg_solve(mom_ctx *c, double omega, const double *ri, const double *
   if (!c->have_problem) return fail(c, MOM_ERR_STATE, "set the problem before the second-harmonic solve");
   if (!ri || !shri || !nls || !(omega > 0)) return fail(c, MOM_ERR_ARG, "invalid omega, refractive indices or media");
   MOM_TRY(check_prec(c, precision));
-  if (c->nga != 1) return fail(c, MOM_ERR_ARG, "the second-harmonic solve supports the identity symmetry group only");
   if (c->nsrc <= 0 || !c->solved) return fail(c, MOM_ERR_STATE, "solve at the fundamental frequency first");
   if (nlx_host && ldx < 2 * (int64_t)c->N) return fail(c, MOM_ERR_ARG, "ldx < 2N");
   if (precision == MOM_PREC_MIXED && (maxit <= 0 || !(tol > 0)))
@@ -708,11 +707,8 @@ int mom_gpu_shg_source_coef(mom_ctx *c, int32_t dom, double *coef_host, int64_t 
   if (dom >= (int)c->shg_slot.size() || c->shg_slot[dom] < 0 || !c->shg_c)
     return fail(c, MOM_ERR_STATE, "no second-harmonic source coefficients for this domain");
   MOM_CUDA(c, cudaSetDevice(c->device));
-  const double2 *src = (const double2 *)c->shg_c + (size_t)c->shg_slot[dom] * c->n * c->nsrc;
-  MOM_CUDA(c, cudaMemcpy2DAsync(coef_host, sizeof(double2) * ldc, src, sizeof(double2) * c->n,
-                                sizeof(double2) * 2 * (size_t)c->N, c->nsrc, cudaMemcpyDeviceToHost, c->stream));
-  MOM_CUDA(c, cudaStreamSynchronize(c->stream));
-  return MOM_OK;
+  const double2 *src = (const double2 *)c->shg_c + (size_t)c->shg_slot[dom] * c->n * c->nsrc * c->nga;
+  return copy_block_to_host(c, src, c->nsrc, coef_host, ldc);
 }
 
 int mom_gpu_sweep(mom_ctx *c, int32_t nwl, const double *omega, const double *ri, int32_t nsrc, const mom_src *src,

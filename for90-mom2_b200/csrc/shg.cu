@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstring>
 #include <set>
 #include <vector>
 
@@ -60,63 +61,106 @@ __device__ __forceinline__ void rwg_at(const double *r, const double *bn, double
   for (int i = 0; i < 3; i++) f[i] = s * (r[i] - bn[i]);
 }
 
+// The symmetry group as kernel argument (point actions J row-major, det J,
+// field actions ef[g][r]: real for the mirror groups).
+struct ShgGroup {
+  int nga;
+  double j[kMaxGroup][9];
+  double detj[kMaxGroup];
+  double ef[kMaxGroup][kMaxGroup];
+};
+
 struct FaceArgs {
   double w[kMaxQ];
-  int F, nq, N;
-  int64_t ldx;
+  int F, nq, N, nsrc;
+  int64_t ldx, xrep;    // solutions: source s, representation m at X + m xrep + s ldx
   const double *qabs, *area, *nrm, *sl, *bn;
   const int *hpar;
-  const double2 *X;     // fundamental solutions [nsrc][ldx]
+  const double2 *X;     // fundamental solutions
   const double2 *epsp;  // [F] selvedge permittivity
   Z iwe;                // i omega eps of the medium at the fundamental
   Z chi_nnn, chi_ntt, chi_ttn;
-  double2 *half;        // [nsrc][F][3][3]: int1 A / epsp, int3 A, int2 A
+  ShgGroup G;
+  double2 *half;        // [nga][nsrc][F][3][3]: int1 A / epsp, int3 A, int2 A
 };
 
-// Thread per (face, source).
-__global__ void nls_face_kernel(FaceArgs a) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y;
-  if (f >= a.F) return;
-  const double A = a.area[f];
-  const double nor[3] = {a.nrm[3 * f], a.nrm[3 * f + 1], a.nrm[3 * f + 2]};
-  const double2 *x = a.X + (size_t)s * a.ldx;
-  Z xj[3], xm[3];
-  double slq[3];
+// efield (nlsurf.f90:22-51) of solution x on face f at a point: n x M + n
+// div J / (i omega eps), with the RWG values fq at the point.
+__device__ __forceinline__ void face_efield(const FaceArgs &a, const double2 *x, int f, const double *nor,
+                                            const double slq[3], double A, const double fq[3][3], Z *e) {
+  Z divj = {0, 0}, ms[3] = {{0, 0}, {0, 0}, {0, 0}};
   for (int q = 0; q < 3; q++) {
     const int g = a.hpar[3 * f + q];
-    xj[q] = {x[g].x, x[g].y};
-    xm[q] = {x[a.N + g].x, x[a.N + g].y};
-    slq[q] = a.sl[3 * f + q];
+    const Z xj = {x[g].x, x[g].y}, xm = {x[a.N + g].x, x[a.N + g].y};
+    divj = zadd(divj, zrs(xj, slq[q] / A));
+    for (int i = 0; i < 3; i++) ms[i] = zadd(ms[i], zrs(xm, fq[q][i]));
   }
-  // divergence of the electric current on this face (efield)
-  Z divj = {0, 0};
-  for (int q = 0; q < 3; q++) divj = zadd(divj, zrs(xj[q], slq[q] / A));
   const Z en0 = zdiv(divj, a.iwe);
+  e[0] = zadd(zsub(zrs(ms[2], nor[1]), zrs(ms[1], nor[2])), zrs(en0, nor[0]));
+  e[1] = zadd(zsub(zrs(ms[0], nor[2]), zrs(ms[2], nor[0])), zrs(en0, nor[1]));
+  e[2] = zadd(zsub(zrs(ms[1], nor[0]), zrs(ms[0], nor[1])), zrs(en0, nor[2]));
+}
+
+// Pnls_invmap's polarisation (nlsurf.f90:76-103) of the field e with the
+// normal nn: eps0 (chi_nnn En^2 + chi_ntt Et.Et) nn + 2 eps0 chi_ttn Et En.
+__device__ __forceinline__ void surface_polarisation(const FaceArgs &a, const Z *e, const double *nn, Z *P) {
+  Z en = {0, 0};
+  for (int i = 0; i < 3; i++) en = zadd(en, zrs(e[i], nn[i]));
+  Z et[3];
+  for (int i = 0; i < 3; i++) et[i] = zsub(e[i], zrs(en, nn[i]));
+  Z ett = {0, 0};
+  for (int i = 0; i < 3; i++) ett = zadd(ett, zmul(et[i], et[i]));
+  const Z pn = zrs(zadd(zmul(a.chi_nnn, zmul(en, en)), zmul(a.chi_ntt, ett)), kEps0);
+  const Z ttn = zrs(a.chi_ttn, 2.0 * kEps0);
+  for (int i = 0; i < 3; i++) P[i] = zadd(zmul(zmul(ttn, et[i]), en), zrs(pn, nn[i]));
+}
+
+// Thread per (face, source, representation nf): the polarisation of
+// representation nf (Pnls_frag, nlsurf.f90:106-125: for every element n the
+// field of the image point, sum_m ef_n(m) J_n^T E_m, with the normal
+// J_n^T n, and the sum over n of ef_n(nf) J_n P_n / nga; for the identity
+// group simply P(E)) and its three moments per local edge.
+__global__ void nls_face_kernel(FaceArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y, nf = blockIdx.z;
+  if (f >= a.F) return;
+  const int nga = a.G.nga;
+  const double A = a.area[f];
+  const double nor[3] = {a.nrm[3 * f], a.nrm[3 * f + 1], a.nrm[3 * f + 2]};
+  double slq[3];
+  for (int q = 0; q < 3; q++) slq[q] = a.sl[3 * f + q];
   Z i1[3] = {{0, 0}, {0, 0}, {0, 0}}, i2[3] = {{0, 0}, {0, 0}, {0, 0}}, i3[3] = {{0, 0}, {0, 0}, {0, 0}};
   for (int r = 0; r < a.nq; r++) {
     const double *pt = a.qabs + ((size_t)f * a.nq + r) * 3;
     double fq[3][3];
     for (int q = 0; q < 3; q++) rwg_at(pt, a.bn + 9 * (size_t)f + 3 * q, slq[q], A, fq[q]);
-    Z ms[3] = {{0, 0}, {0, 0}, {0, 0}};
-    for (int q = 0; q < 3; q++)
-      for (int i = 0; i < 3; i++) ms[i] = zadd(ms[i], zrs(xm[q], fq[q][i]));
-    // e = n x ms + n en
-    Z e[3];
-    e[0] = zadd(zsub(zrs(ms[2], nor[1]), zrs(ms[1], nor[2])), zrs(en0, nor[0]));
-    e[1] = zadd(zsub(zrs(ms[0], nor[2]), zrs(ms[2], nor[0])), zrs(en0, nor[1]));
-    e[2] = zadd(zsub(zrs(ms[1], nor[0]), zrs(ms[0], nor[1])), zrs(en0, nor[2]));
-    // Pnls_invmap: normal and tangential parts of E, the polarisation
-    Z en = {0, 0};
-    for (int i = 0; i < 3; i++) en = zadd(en, zrs(e[i], nor[i]));
-    Z et[3];
-    for (int i = 0; i < 3; i++) et[i] = zsub(e[i], zrs(en, nor[i]));
-    Z ett = {0, 0};
-    for (int i = 0; i < 3; i++) ett = zadd(ett, zmul(et[i], et[i]));
-    const Z pn = zrs(zadd(zmul(a.chi_nnn, zmul(en, en)), zmul(a.chi_ntt, ett)), kEps0);
-    const Z ttn = zrs(a.chi_ttn, 2.0 * kEps0);
     Z P[3];
-    for (int i = 0; i < 3; i++) P[i] = zadd(zmul(zmul(ttn, et[i]), en), zrs(pn, nor[i]));
+    if (nga == 1) {
+      Z e[3];
+      face_efield(a, a.X + (size_t)s * a.ldx, f, nor, slq, A, fq, e);
+      surface_polarisation(a, e, nor, P);
+    } else {
+      Z Em[kMaxGroup][3];
+      for (int m = 0; m < nga; m++) face_efield(a, a.X + (size_t)m * a.xrep + (size_t)s * a.ldx, f, nor, slq, A, fq, Em[m]);
+      for (int i = 0; i < 3; i++) P[i] = {0, 0};
+      for (int n = 0; n < nga; n++) {
+        const double *J = a.G.j[n];
+        Z e[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int m = 0; m < nga; m++) {
+          const double c = a.G.ef[n][m];  // conj of a real character
+          for (int i = 0; i < 3; i++)  // (J^T E)_i = sum_k J[k][i] E_k
+            e[i] = zadd(e[i], zrs(zadd(zadd(zrs(Em[m][0], J[i]), zrs(Em[m][1], J[3 + i])), zrs(Em[m][2], J[6 + i])), c));
+        }
+        double nn[3];
+        for (int i = 0; i < 3; i++) nn[i] = J[i] * nor[0] + J[3 + i] * nor[1] + J[6 + i] * nor[2];
+        Z Pn_[3];
+        surface_polarisation(a, e, nn, Pn_);
+        const double c = a.G.ef[n][nf];
+        for (int i = 0; i < 3; i++)  // J P
+          P[i] = zadd(P[i], zrs(zadd(zadd(zrs(Pn_[0], J[3 * i]), zrs(Pn_[1], J[3 * i + 1])), zrs(Pn_[2], J[3 * i + 2])), c));
+      }
+      for (int i = 0; i < 3; i++) P[i] = zrs(P[i], 1.0 / nga);
+    }
     // nlsurf_coef: Pn = n . P, Pt = P - Pn n
     Z Pn = {0, 0};
     for (int i = 0; i < 3; i++) Pn = zadd(Pn, zrs(P[i], nor[i]));
@@ -141,7 +185,7 @@ __global__ void nls_face_kernel(FaceArgs a) {
     }
   }
   const Z ep = {a.epsp[f].x, a.epsp[f].y};
-  double2 *o = a.half + ((size_t)s * a.F + f) * 9;
+  double2 *o = a.half + (((size_t)nf * a.nsrc + s) * a.F + f) * 9;
   for (int q = 0; q < 3; q++) {
     const Z c = zdiv(zrs(i1[q], A), ep);
     o[3 * q] = make_double2(c.re, c.im);
@@ -256,6 +300,12 @@ struct CgArgs {
   double *x;         // [nv][Nd]
   double *work;      // [nv][3][Nd]: r, p, q
   int *status;       // [nv]: iterations, or -1 if the residual did not reach tol ||b||
+  // Symmetry-plane boundary conditions (edge_bc): keep[rep][Nd] = 0 removes
+  // an unknown (identity row and column, zero right-hand side, so it stays
+  // 0, as reduce_system / expand_solution leave it); vector v belongs to
+  // representation (v / vec_per_col) / nsrc.  Null: nothing removed.
+  const unsigned char *keep;
+  int vec_per_col, nsrc;
 };
 
 __device__ __forceinline__ void block_sum2(double &a, double &b, double *red) {
@@ -286,9 +336,12 @@ __global__ void __launch_bounds__(kCgThreads) gram_cg_kernel(CgArgs a) {
   const double *b = a.b + (size_t)v * n;
   double *x = a.x + (size_t)v * n;
   double *r = a.work + (size_t)v * 3 * n, *p = r + n, *q = p + n;
+  const unsigned char *km = a.keep ? a.keep + (size_t)((v / a.vec_per_col) / a.nsrc) * n : nullptr;
+  auto kept = [&](int i) { return km == nullptr || km[i] != 0; };
+  auto diag = [&](int i) { return kept(i) ? a.val[(size_t)i * kEll] : 1.0; };
   double rz = 0, bb = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double bi = b[i], zi = bi / a.val[(size_t)i * kEll];
+    const double bi = kept(i) ? b[i] : 0.0, zi = bi / diag(i);
     x[i] = 0;
     r[i] = bi;
     p[i] = zi;
@@ -297,7 +350,7 @@ __global__ void __launch_bounds__(kCgThreads) gram_cg_kernel(CgArgs a) {
   }
   block_sum2(rz, bb, red);
   int it = 0;
-  bool done = !(bb > 0);
+  bool done = bb == 0.0;  // a zero right-hand side: x = 0; a NaN one never converges
   const double lim = a.tol * a.tol * bb;
   while (!done && it < a.maxit) {
     __syncthreads();  // p complete before the product reads neighbours
@@ -306,8 +359,15 @@ __global__ void __launch_bounds__(kCgThreads) gram_cg_kernel(CgArgs a) {
       const int *ci = a.col + (size_t)i * kEll;
       const double *vi = a.val + (size_t)i * kEll;
       double s = 0;
+      if (km == nullptr) {
 #pragma unroll
-      for (int k = 0; k < kEll; k++) s += vi[k] * p[ci[k]];
+        for (int k = 0; k < kEll; k++) s += vi[k] * p[ci[k]];
+      } else if (km[i]) {
+#pragma unroll
+        for (int k = 0; k < kEll; k++) s += km[ci[k]] ? vi[k] * p[ci[k]] : 0.0;
+      } else {
+        s = p[i];
+      }
       q[i] = s;
       pq += p[i] * s;
     }
@@ -319,7 +379,7 @@ __global__ void __launch_bounds__(kCgThreads) gram_cg_kernel(CgArgs a) {
       const double ri = r[i] - alpha * q[i];
       r[i] = ri;
       rr += ri * ri;
-      rzn += ri * ri / a.val[(size_t)i * kEll];
+      rzn += ri * ri / diag(i);
     }
     block_sum2(rr, rzn, red);
     it++;
@@ -329,7 +389,7 @@ __global__ void __launch_bounds__(kCgThreads) gram_cg_kernel(CgArgs a) {
     }
     const double beta = rzn / rz;
     rz = rzn;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = r[i] / a.val[(size_t)i * kEll] + beta * p[i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = r[i] / diag(i) + beta * p[i];
   }
   if (threadIdx.x == 0) a.status[v] = done ? it : -1;
 }
@@ -516,8 +576,12 @@ ShgBuf shg_layout(int F, int Nd, int nsrc) {
 constexpr int kCgMaxIt = 20000;
 constexpr double kCgTol = 1e-14;
 
-int run_cg(Ctx *c, const DomDev &D, int nv, const double *b, double *x, double *work, int *status) {
+int run_cg(Ctx *c, const DomDev &D, int nv, const double *b, double *x, double *work, int *status,
+           const unsigned char *keep, int vec_per_col, int nsrc) {
   CgArgs g;
+  g.keep = keep;
+  g.vec_per_col = vec_per_col;
+  g.nsrc = nsrc;
   g.Nd = D.Nd;
   g.maxit = kCgMaxIt;
   g.tol = kCgTol;
@@ -553,7 +617,8 @@ void free_shg(DomDev &D) {
 
 int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const mom_nls *nls, int precision,
               double tol, int maxit, int *iters) {
-  const int nsrc = c->nsrc;
+  const int nsrc = c->nsrc, nga = c->nga;
+  const int ncol = nga * nsrc;  // (representation, source) columns: column r nsrc + s at X, B + (r nsrc + s) n
   const int64_t n = c->n;
   const double omega_sh = 2.0 * omega;
   std::vector<int> nl;
@@ -563,32 +628,59 @@ int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const 
       c->shg_slot[d] = (int)nl.size();
       nl.push_back(d);
     }
-  // source coefficients of every nonlinear domain, [nl][nsrc][n]
-  MOM_TRY(ensure_buffer(c, &c->shg_c, &c->shg_c_bytes, sizeof(double2) * (size_t)n * nsrc * std::max<size_t>(nl.size(), 1)));
+  // source coefficients of every nonlinear domain, [nl][ncol][n]
+  MOM_TRY(ensure_buffer(c, &c->shg_c, &c->shg_c_bytes, sizeof(double2) * (size_t)n * ncol * std::max<size_t>(nl.size(), 1)));
   double2 *Call = (double2 *)c->shg_c;
-  MOM_CUDA(c, cudaMemsetAsync(Call, 0, sizeof(double2) * (size_t)n * nsrc * nl.size(), c->stream));
-  MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * (size_t)n * nsrc, c->stream));
+  MOM_CUDA(c, cudaMemsetAsync(Call, 0, sizeof(double2) * (size_t)n * ncol * nl.size(), c->stream));
+  MOM_CUDA(c, cudaMemsetAsync(c->B, 0, sizeof(double2) * (size_t)n * ncol, c->stream));
+  ShgGroup G;
+  std::memset(&G, 0, sizeof G);
+  G.nga = nga;
+  for (int g = 0; g < nga; g++) {
+    for (int i = 0; i < 9; i++) G.j[g][i] = c->ga[g].j[i];
+    G.detj[g] = c->ga[g].detj;
+    for (int r = 0; r < nga; r++) G.ef[g][r] = c->ga[g].ef[r];
+  }
   for (size_t k = 0; k < nl.size(); k++) {
     const int d = nl[k];
     MOM_TRY(shg_setup(c, d));
     const DomDev &D = c->dom[d];
     std::vector<double2> epsp;
     MOM_TRY(face_epsp(c, d, ri, epsp));
-    const ShgBuf L = shg_layout(D.F, D.Nd, nsrc);
-    MOM_TRY(ensure_buffer(c, &c->shg_ws, &c->shg_ws_bytes, L.total));
+    // edge_bc on the domain mesh per representation: the E-type unknowns (coef
+    // and cJ) and the H-type ones (cM) that the symmetry planes remove
+    std::vector<unsigned char> keep;
+    if (nga > 1) {
+      keep.assign(2 * (size_t)nga * D.Nd, 1);
+      for (int r = 0; r < nga; r++) {
+        std::vector<char> rem(2 * (size_t)c->N, 0);
+        for (int u : c->removed[r]) rem[u] = 1;
+        for (int e = 0; e < D.Nd; e++) {
+          keep[(size_t)r * D.Nd + e] = !rem[D.h_epar[e]];
+          keep[((size_t)nga + r) * D.Nd + e] = !rem[c->N + D.h_epar[e]];
+        }
+      }
+    }
+    const ShgBuf L = shg_layout(D.F, D.Nd, ncol);
+    const size_t keep_off = (L.total + 255) / 256 * 256;
+    MOM_TRY(ensure_buffer(c, &c->shg_ws, &c->shg_ws_bytes, keep_off + keep.size() + 256));
     char *ws = (char *)c->shg_ws;
     double2 *half = (double2 *)(ws + L.off_half), *dep = (double2 *)(ws + L.off_epsp);
     double *rhs = (double *)(ws + L.off_rhs), *x1 = (double *)(ws + L.off_x1), *rhs2 = (double *)(ws + L.off_rhs2),
            *x2 = (double *)(ws + L.off_x2), *work = (double *)(ws + L.off_work);
     int *st = (int *)(ws + L.off_st);
+    unsigned char *dkeep = keep.empty() ? nullptr : (unsigned char *)(ws + keep_off);
     MOM_CUDA(c, cudaMemcpyAsync(dep, epsp.data(), sizeof(double2) * D.F, cudaMemcpyHostToDevice, c->stream));
+    if (dkeep) MOM_CUDA(c, cudaMemcpyAsync(dkeep, keep.data(), keep.size(), cudaMemcpyHostToDevice, c->stream));
     const mom_nls &m = nls[d];
     FaceArgs fa;
     for (int i = 0; i < kMaxQ; i++) fa.w[i] = c->qw[i];
     fa.F = D.F;
     fa.nq = c->nq;
     fa.N = c->N;
+    fa.nsrc = nsrc;
     fa.ldx = n;
+    fa.xrep = (int64_t)nsrc * n;
     fa.qabs = D.qabs;
     fa.area = D.area;
     fa.nrm = D.nrm;
@@ -604,10 +696,11 @@ int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const 
     fa.chi_nnn = {m.chi_nnn[0], m.chi_nnn[1]};
     fa.chi_ntt = {m.chi_ntt[0], m.chi_ntt[1]};
     fa.chi_ttn = {m.chi_ttn[0], m.chi_ttn[1]};
+    fa.G = G;
     fa.half = half;
     {
       ProfScope ps(c, kProfPost);
-      nls_face_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(fa);
+      nls_face_kernel<<<dim3((D.F + 127) / 128, nsrc, nga), 128, 0, c->stream>>>(fa);
       c->launches++;
       MOM_CUDA(c, cudaGetLastError());
     }
@@ -622,10 +715,10 @@ int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const 
     ea.omega_sh = omega_sh;
     ea.B = c->B;
     ea.rhs = rhs;
-    nls_edge_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(ea);
+    nls_edge_kernel<<<dim3((D.Nd + 127) / 128, ncol), 128, 0, c->stream>>>(ea);
     c->launches++;
     MOM_CUDA(c, cudaGetLastError());
-    MOM_TRY(run_cg(c, D, 4 * nsrc, rhs, x1, work, st));
+    MOM_TRY(run_cg(c, D, 4 * ncol, rhs, x1, work, st, dkeep, 4, nsrc));
     CmArgs ca;
     for (int i = 0; i < kMaxQ; i++) ca.w[i] = c->qw[i];
     ca.F = D.F;
@@ -639,25 +732,35 @@ int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const 
     ca.fedge = D.shg_fedge;
     ca.coef = x1;
     ca.half = half;
-    nls_cm_kernel<<<dim3((D.F + 127) / 128, nsrc), 128, 0, c->stream>>>(ca);
-    nls_cm_edge_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(D.F, D.Nd, D.eh, half, rhs2);
+    nls_cm_kernel<<<dim3((D.F + 127) / 128, ncol), 128, 0, c->stream>>>(ca);
+    nls_cm_edge_kernel<<<dim3((D.Nd + 127) / 128, ncol), 128, 0, c->stream>>>(D.F, D.Nd, D.eh, half, rhs2);
     c->launches += 2;
     MOM_CUDA(c, cudaGetLastError());
-    MOM_TRY(run_cg(c, D, 2 * nsrc, rhs2, x2, work, st));
-    nls_scatter_kernel<<<dim3((D.Nd + 127) / 128, nsrc), 128, 0, c->stream>>>(D.Nd, c->N, n, D.epar, x1, x2,
-                                                                               Call + k * (size_t)n * nsrc);
+    MOM_TRY(run_cg(c, D, 2 * ncol, rhs2, x2, work, st, dkeep ? dkeep + (size_t)nga * D.Nd : nullptr, 2, nsrc));
+    nls_scatter_kernel<<<dim3((D.Nd + 127) / 128, ncol), 128, 0, c->stream>>>(D.Nd, c->N, n, D.epar, x1, x2,
+                                                                               Call + k * (size_t)n * ncol);
     c->launches++;
     MOM_CUDA(c, cudaGetLastError());
   }
   // sysmat_pmchwt_nls: the nonlinear domains first, each block applied to
-  // its own coefficients as A_after c - A_before c, then the other domains.
+  // its own coefficients as A_after c - A_before c in every representation,
+  // then the other domains.
+  const size_t col_rep = (size_t)nsrc * n;
+  auto apply = [&](const double2 *Ck, double sign) -> int {
+    for (int r = 0; r < nga; r++) {
+      select_rep(c, r);
+      MOM_TRY(matvec_acc(c, Ck + r * col_rep, nsrc, c->B + r * col_rep, sign));
+    }
+    select_rep(c, 0);
+    return MOM_OK;
+  };
   select_rep(c, 0);
   MOM_TRY(assemble_begin(c));
   for (size_t k = 0; k < nl.size(); k++) {
-    const double2 *Ck = Call + k * (size_t)n * nsrc;
-    if (k > 0) MOM_TRY(matvec_acc(c, Ck, nsrc, c->B, 1.0));
+    const double2 *Ck = Call + k * (size_t)n * ncol;
+    if (k > 0) MOM_TRY(apply(Ck, 1.0));
     MOM_TRY(assemble_domain(c, nl[k], omega_sh, shri, precision));
-    MOM_TRY(matvec_acc(c, Ck, nsrc, c->B, -1.0));
+    MOM_TRY(apply(Ck, -1.0));
   }
   for (int d = 0; d < c->ndom; d++)
     if (!nls[d].active) MOM_TRY(assemble_domain(c, d, omega_sh, shri, precision));
@@ -665,8 +768,30 @@ int shg_solve(Ctx *c, double omega, const double *ri, const double *shri, const 
   c->omega_rhs = omega_sh;
   c->ri1[0] = shri[0];
   c->ri1[1] = shri[1];
-  MOM_TRY(lu_factor(c, precision));
-  MOM_TRY(lu_solve_ex(c, precision, 0, c->B, c->X, nsrc, tol, maxit, iters));
+  // solve_systems per representation: the removed unknowns' right-hand
+  // sides are zero (identity rows), one factorisation and solve each
+  int it = 0;
+  for (int r = 0; r < nga && nga > 1; r++) MOM_TRY(apply_bc_rhs(c, r, c->B + r * col_rep, nsrc));
+  for (int r = 0; r < nga; r++) {
+    select_rep(c, r);
+    const int rc = lu_factor(c, precision);
+    if (rc != MOM_OK) {
+      select_rep(c, 0);
+      return rc;
+    }
+  }
+  for (int r = 0; r < nga; r++) {
+    select_rep(c, r);
+    int itr = 0;
+    const int rc = lu_solve_ex(c, precision, 0, c->B + r * col_rep, c->X + r * col_rep, nsrc, tol, maxit, &itr);
+    if (rc != MOM_OK) {
+      select_rep(c, 0);
+      return rc;
+    }
+    it = std::max(it, itr);
+  }
+  select_rep(c, 0);
+  if (iters) *iters = it;
   if (precision == MOM_PREC_FP64) c->assembled = 0;
   return MOM_OK;
 }

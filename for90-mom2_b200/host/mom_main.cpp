@@ -25,8 +25,8 @@
 // Symmetry groups are products of id and the mirror groups mxp, myp, mzp
 // with the xplane / yplane / zplane boundaries of sbnd.  Media may carry a
 // centrosymmetric surface nonlinearity (`smed m nlsurf value chi_nnn chi_ntt
-// chi_ttn`, identity group only): solv then also solves the second harmonic
-// (solver.f90:143-217) and crst, rcst, nfms, nfem, nfdm and nfpl also write
+// chi_ttn`, with the mirror groups too): solv then also solves the second
+// harmonic (solver.f90:143-217) and crst, rcst, nfms, nfem, nfdm and nfpl also write
 // its results (-sh files).  Commands of the reference outside this path
 // (rotation groups, periodic boundaries and Green's functions, volume
 // domains, bulk nonlinearities, diffraction, polarizability, the VIE
@@ -358,7 +358,7 @@ void solve_batch(State &s) {
       for (size_t d = 0; d < s.doms.size(); d++) {
         s.shc[n][d].clear();
         if (!dn[d].active) continue;
-        s.shc[n][d].assign((size_t)2 * s.n2 * nsrc, 0.0);
+        s.shc[n][d].assign((size_t)2 * s.n2 * s.nga * nsrc, 0.0);
         check(s, mom_gpu_shg_source_coef(s.ctx, (int32_t)d, s.shc[n][d].data(), s.n2), "solv (second harmonic)");
       }
     }

@@ -465,9 +465,10 @@ class Solver:
         frequency omega (solver.f90:143-217): nls[d] is None for a linear domain or
         (chi_nnn, chi_ntt, chi_ttn) of its surface nonlinearity (``smed m nlsurf
         value ...``); ri / shri are the fundamental and second-harmonic refractive
-        indices per domain.  Returns nlx (2N x nsrc); afterwards the device
-        solutions are the second harmonic's (cross sections with src_none() at
-        2 omega and shri)."""
+        indices per domain.  Returns nlx (2N x nsrc, or 2N x nga x nsrc with a
+        mirror group: the polarisation projected on each representation);
+        afterwards the device solutions are the second harmonic's (cross sections
+        with src_none() at 2 omega and shri)."""
         if len(nls) != self.ndom:
             raise ValueError("nls needs one entry per domain")
         arr = (MomNls * self.ndom)()
@@ -488,7 +489,7 @@ class Solver:
 
     def shg_source_coef(self, dom):
         """The source coefficients (cJ on rows [0, N), cM on [N, 2N)) of nonlinear
-        domain dom from the last shg_solve, 2N x nsrc."""
+        domain dom from the last shg_solve, 2N x nsrc (2N x nga x nsrc with a group)."""
         x = self._cols(self.nsrc)
         self._ck(lib().mom_gpu_shg_source_coef(self.h, dom, x.ctypes.data, 2 * self.N), "shg_source_coef")
         return x

@@ -165,17 +165,20 @@ int mom_gpu_solve_wavelength(mom_ctx *ctx, double omega, const double *ri, int32
  * solver.f90:393-433).  Afterwards the device solutions, matrix and factors
  * are those of the second harmonic: cross sections with MOM_SRC_NONE
  * sources at 2 omega and shri give the reference's -sh.crs values.
- * nlx_host (2N x nsrc, ldx) may be NULL.  Identity symmetry group only
- * (MOM_ERR_ARG otherwise); a domain face that no other domain shares gives
- * MOM_ERR_ARG ("Could not find epsp!"). */
+ * With a symmetry group the polarisation is projected on every
+ * representation (Pnls_frag, nlsurf.f90:106-125) and the Gram systems and
+ * the SH solves keep the representations' boundary conditions; nlx_host is
+ * then (2N, nga, nsrc).  nlx_host (ldx) may be NULL.  A domain face that no
+ * other domain shares gives MOM_ERR_ARG ("Could not find epsp!"); a Gram
+ * system that does not converge (NaN input) MOM_ERR_NOCONV. */
 int mom_gpu_shg_solve(mom_ctx *ctx, double omega, const double *ri, const double *shri, const mom_nls *nls,
                       int32_t precision, double tol, int32_t maxit, double *nlx_host, int64_t ldx,
                       int32_t *iters_out);
 
 /* The source coefficients of domain dom from the last mom_gpu_shg_solve
- * (src_coef(:, dom, 1, :), nlsurf.f90:137-338) on the global unknowns: cJ on
+ * (src_coef(:, dom, :, :), nlsurf.f90:137-338) on the global unknowns: cJ on
  * the domain's edges in rows [0, N), cM in rows [N, 2N), zero elsewhere;
- * 2N x nsrc, ldc.  The fields inside a nonlinear domain come from nlx plus
+ * 2N x nsrc (2N x nga x nsrc with a symmetry group), ldc.  The fields inside a nonlinear domain come from nlx plus
  * these (read_nfem, interface.f90:1060-1078).  MOM_ERR_STATE if dom was not
  * nonlinear in that solve. */
 int mom_gpu_shg_source_coef(mom_ctx *ctx, int32_t dom, double *coef_host, int64_t ldc);

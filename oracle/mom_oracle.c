@@ -1570,14 +1570,17 @@ static void compute_op_g(int op, double omega, cplx ri, const omesh *m, const oq
 }
 
 /* sysmat.f90:18-105 sysmat_pmchwt with the problem's group: one 2N x 2N
- * matrix per representation, A[nf] at A + nf (2N)^2 (column-major). */
-void oracle_sysmat_sym(void *p, double omega, const double *ri_ri, cplx *A, int nthreads) {
+ * matrix per representation, A[nf] at A + nf (2N)^2 (column-major); the
+ * blocks of domain `dom` alone when dom >= 0 (sysmat_pmchwt_nls needs the
+ * nonlinear domain's blocks apart, sysmat.f90:112-229). */
+void oracle_sysmat_sym_dom(void *p, double omega, const double *ri_ri, cplx *A, int nthreads, int dom) {
   oproblem *P = p;
   if (nthreads > 0) omp_set_num_threads(nthreads);
   const int N = P->master.nedges, nga = P->nga;
   const size_t n2 = 2 * (size_t)N;
   memset(A, 0, sizeof(cplx) * n2 * n2 * nga);
   for (int d = 0; d < P->ndom; d++) {
+    if (dom >= 0 && d != dom) continue;
     omesh *m = P->dom + d;
     cplx ri = ri_ri[2 * d] + I * ri_ri[2 * d + 1];
     cplx Zsi = (ri * ri) / (O_ETA0 * O_ETA0);
@@ -1608,6 +1611,10 @@ void oracle_sysmat_sym(void *p, double omega, const double *ri_ri, cplx *A, int 
     }
     free(M);
   }
+}
+
+void oracle_sysmat_sym(void *p, double omega, const double *ri_ri, cplx *A, int nthreads) {
+  oracle_sysmat_sym_dom(p, omega, ri_ri, A, nthreads, -1);
 }
 
 /* source.f90:250-315 src_field_frags: the source at J^T pt for each element,

@@ -143,6 +143,7 @@ def lib():
         L.oracle_problem_classify_edges.argtypes = [C.c_void_p, C.c_int, ip, C.c_int]
         L.oracle_edge_bc.argtypes = [C.c_void_p, C.c_int, ip, C.c_void_p]
         L.oracle_sysmat_sym.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_int]
+        L.oracle_sysmat_sym_dom.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_int, C.c_int]
         L.oracle_srcvec_sym.argtypes = [C.c_void_p, C.c_double, dp, C.c_void_p, C.c_void_p]
         L.oracle_cs_sym.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_void_p, C.c_void_p, dp, dp]
         L.oracle_scat_fields.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, C.c_int, C.c_void_p, C.c_int64,
@@ -312,6 +313,15 @@ class OracleProblem:
         n = getattr(self, "nga", 1)
         A = np.zeros((n, 2 * self.N, 2 * self.N), dtype=np.complex128)  # [nf] column-major blocks
         lib().oracle_sysmat_sym(self.h, omega, _dp(rr), A.ctypes.data, nthreads)
+        return np.ascontiguousarray(A.transpose(0, 2, 1))
+
+    def sysmat_sym_dom(self, omega, ri, d, nthreads=0):
+        """The blocks of domain d alone in every representation (sysmat_pmchwt_nls's
+        per-domain terms, sysmat.f90:112-229): A[nga][2N][2N]."""
+        rr = np.array([[complex(v).real, complex(v).imag] for v in ri]).ravel()
+        n = getattr(self, "nga", 1)
+        A = np.zeros((n, 2 * self.N, 2 * self.N), dtype=np.complex128)
+        lib().oracle_sysmat_sym_dom(self.h, omega, _dp(rr), A.ctypes.data, nthreads, d)
         return np.ascontiguousarray(A.transpose(0, 2, 1))
 
     def srcvec_sym(self, omega, ri, src):
@@ -554,6 +564,124 @@ def nlsurf_coef(P, d, qd, omega_ff, ri_ff, epsp, xff, chi2):
             cm[g["edge"][f, q]] += g["A"][f] * np.sum(g["w"] * np.sum(_rwg(g, f, q, qp) * ncr, axis=1))
     sc[:Nd] = np.linalg.solve(Fm, cm)
     return sc, sv
+
+
+def nlsurf_coef_sym(P, d, qd, omega_ff, ri_ff, epsp, xff, chi2, nf, group, keep_e, keep_h):
+    """nlsurf_coef (nlsurf.f90:137-338) in representation nf of a symmetry group:
+    the polarisation of Pnls_frag (nlsurf.f90:106-125) from the fundamental
+    solutions of every representation (efield_invmap / Pnls_invmap,
+    nlsurf.f90:54-103: the field of the image J_n r from sum_m conj(ef_n(m))
+    J_n^T E_m(r), the normal J_n^T n), and the Gram systems under the
+    representation's boundary conditions (edge_bc on the domain mesh: the
+    E-type unknowns keep_e for coef and cJ, the H-type keep_h for cM; removed
+    unknowns are zero, as reduce_system / expand_solution leave them).
+    xff: [nga][2N]; group: (J[nga][3][3], detj[nga], ef[nga][nga])."""
+    g = _domain_geometry(P, d, qd)
+    m = g["m"]
+    N, Nd = P.N, len(m["edge_node"])
+    par = m["edge_parent"]
+    Jg, detj, efg = group
+    nga = len(detj)
+    chi_nnn, chi_ntt, chi_ttn = chi2
+    omega_sh = 2.0 * omega_ff
+    eps = ri_ff ** 2 * EPS0
+    coef = np.zeros(Nd, complex)
+    sc = np.zeros(2 * Nd, complex)
+    sv = np.zeros(2 * Nd, complex)
+    for f in range(g["F"]):
+        nor = g["n"][f]
+        qp = g["qp"][f]
+        # the fields of every representation at the quadrature points (efield)
+        Em = []
+        for mm in range(nga):
+            x = xff[mm]
+            divj = sum(x[par[g["edge"][f, q]]] * g["sign"][f, q] * g["len"][f, q] / g["A"][f] for q in range(3))
+            ms = sum(x[N + par[g["edge"][f, q]]] * _rwg(g, f, q, qp) for q in range(3))
+            en_ = divj / (1j * omega_ff * eps)
+            Em.append(np.cross(nor, ms) + nor[None, :] * en_)
+        Pf = np.zeros((len(qp), 3), complex)
+        for n in range(nga):
+            e = sum(np.conj(efg[n][mm]) * (Em[mm] @ Jg[n]) for mm in range(nga))  # J^T E, row vectors
+            nn = Jg[n].T @ nor
+            en = e @ nn
+            et = e - en[:, None] * nn[None, :]
+            Pn_ = EPS0 * (chi_nnn * en ** 2 + chi_ntt * np.sum(et * et, axis=1))
+            Pt_ = 2.0 * EPS0 * chi_ttn * et * en[:, None]
+            Pv = Pt_ + Pn_[:, None] * nn[None, :]
+            Pf += efg[n][nf] * (Pv @ Jg[n].T)  # J P, row vectors
+        Pf /= nga
+        Pn = Pf @ nor
+        Pt = Pf - Pn[:, None] * nor[None, :]
+        for q in range(3):
+            fmdiv = g["sign"][f, q] * g["len"][f, q] / g["A"][f]
+            fm = _rwg(g, f, q, qp)
+            int1 = -np.sum(g["w"] * fmdiv * Pn)
+            int2 = np.sum(g["w"] * np.sum(fm * np.cross(Pt, nor[None, :]), axis=1))
+            int3 = np.sum(g["w"] * np.sum(fm * Pt, axis=1))
+            idx = g["edge"][f, q]
+            coef[idx] += int1 * g["A"][f] / epsp[f]
+            sc[idx + Nd] += int3 * g["A"][f]
+            sv[idx + Nd] += int2 * g["A"][f]
+    sc[Nd:] = -sc[Nd:] * 1j * omega_sh
+    sv[:Nd] = 0.5 * coef
+    sv[Nd:] = 0.5 * 1j * omega_sh * sv[Nd:]
+    Fm = rwg_moments(g)
+    ke = np.nonzero(keep_e)[0]
+    sol = np.zeros((Nd, 2), complex)
+    sol[ke] = np.linalg.solve(Fm[np.ix_(ke, ke)], np.stack([coef, sc[Nd:]], axis=1)[ke])
+    coef = sol[:, 0]
+    sc[Nd:] = sol[:, 1]
+    cm = np.zeros(Nd, complex)
+    for f in range(g["F"]):
+        nor = g["n"][f]
+        qp = g["qp"][f]
+        ex = sum(_rwg(g, f, q, qp) * coef[g["edge"][f, q]] for q in range(3))
+        ncr = np.cross(nor[None, :], ex)
+        for q in range(3):
+            cm[g["edge"][f, q]] += g["A"][f] * np.sum(g["w"] * np.sum(_rwg(g, f, q, qp) * ncr, axis=1))
+    kh = np.nonzero(keep_h)[0]
+    sc[:Nd] = 0
+    sc[kh] = np.linalg.solve(Fm[np.ix_(kh, kh)], cm[kh])
+    return sc, sv
+
+
+def shg_solve_sym(P, omega, ri, shri, nls, x, qd_name="tri_gl13", coef_out=None):
+    """The nonlinear branch of solve_batch with the problem's symmetry group
+    (solver.f90:143-217): per representation nf the source terms of every
+    nonlinear domain (nlsurf_coef_sym, and -A_{d,nf} c_{d,nf} with the domain's
+    blocks, sysmat.f90:112-229), the matrices at 2 omega with the SH indices
+    and solve_sym.  x: fundamental solutions [nga][2N] for one source.  Returns
+    nlx [nga][2N]."""
+    qd = tri_rule(qd_name)
+    N = P.N
+    J, detj, ef = P.group_info()
+    nga = len(detj)
+    x = np.asarray(x, dtype=np.complex128).reshape(nga, 2 * N)
+    nlx = np.zeros((nga, 2 * N), complex)
+    for d in range(P.ndom):
+        if nls[d] is None:
+            continue
+        m = P.export(d)
+        par = m["edge_parent"]
+        Nd = len(par)
+        epsp = epsp_of(P, d, ri)
+        Ad = P.sysmat_sym_dom(2.0 * omega, [complex(v) for v in shri], d)
+        for nf in range(nga):
+            idv, _ = P.edge_bc(nf)
+            keep_e = idv[par] != -1
+            keep_h = idv[N + par] != -1
+            sc, sv = nlsurf_coef_sym(P, d, qd, omega, complex(ri[d]), epsp, x, nls[d], nf, (J, detj, ef), keep_e,
+                                     keep_h)
+            nlx[nf, par] += sv[:Nd]
+            nlx[nf, par + N] += sv[Nd:]
+            c = np.zeros(2 * N, complex)
+            c[par] = sc[Nd:]
+            c[par + N] = sc[:Nd]
+            nlx[nf] -= Ad[nf] @ c
+            if coef_out is not None:
+                coef_out.setdefault(d, np.zeros((nga, 2 * N), complex))[nf] = c
+    A = P.sysmat_sym(2.0 * omega, [complex(v) for v in shri])
+    return P.solve_sym(A, nlx)
 
 
 def epsp_of(P, d, ri):

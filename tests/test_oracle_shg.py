@@ -99,3 +99,30 @@ def test_epsp(sphere1):
     assert np.allclose(e, O.EPS0 * complex(RI[0]) ** 2, rtol=0, atol=0)
     e = O.epsp_of(P, 0, RI)
     assert np.allclose(e, O.EPS0 * complex(RI[1]) ** 2, rtol=1e-15, atol=0)
+
+
+def test_shg_with_mirror_group_reproduces_full_sphere():
+    """The second harmonic of the eighth of the mirror-symmetric s=1 sphere with
+    the group mxp x myp x mzp (the boundary conditions of edge_bc on the plane
+    edges, the polarisation projected on each representation) equals the full
+    sphere's without a group: SH cross sections through cs_prtsrf with no
+    incident field."""
+    from mom_b200 import meshgen
+    nodes, faces = meshgen.octasphere(1, 50.0)
+    om = O.omega_of(WL)
+    chi = (1e-18 + 0.3e-18j, 0.5e-18, -0.2e-18)
+    src = dict(type="pw", theta=0.4, phi=0.3, psi=0.2)
+    full = O.OracleProblem(nodes, faces, np.ones(len(faces), int), 1e-9, [[1], [-1]])
+    x = O.solve(full.sysmat(om, RI), full.srcvec(om, 1.0, src)[:, None])
+    nlx = O.shg_solve(full, om, RI, SHRI, [None, chi], x)
+    ref = full.cs(2 * om, SHRI[0], nlx[:, 0], dict(type="none"))
+    fn, ff, lines = meshgen.symmetry_fragment(nodes, faces, [0, 1, 2])
+    Q = O.OracleProblem(fn, ff, np.ones(len(ff), int), 1e-9, [[1], [-1]])
+    Q.set_symmetry(["mxp", "myp", "mzp"])
+    for ax, name in enumerate(("xplane", "yplane", "zplane")):
+        Q.classify_edges(lines[ax], name)
+    A = Q.sysmat_sym(om, RI)
+    xs = Q.solve_sym(A, Q.srcvec_sym(om, 1.0, src))
+    Q_nlx = O.shg_solve_sym(Q, om, RI, SHRI, [None, chi], xs)
+    got = Q.cs_sym(2 * om, SHRI[0], Q_nlx, dict(type="none"))
+    assert abs(got[0] / ref[0] - 1) <= 1e-10 and abs(got[1] / ref[1] - 1) <= 1e-10, (got, ref)
