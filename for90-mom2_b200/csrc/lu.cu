@@ -37,6 +37,29 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double cabs1(float2 a) { return (double)(fabsf(a.x) + fabsf(a.y)); }
+__device__ __forceinline__ void st2(float2 *p, float2 v) { *p = v; }
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
+template <typename E> __device__ __forceinline__ E from_d2(double2 v);
+template <> __device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 from_d2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <typename E> __device__ __forceinline__ E ld_slab(const double2 *p) { return from_d2<E>(*p); }
+template <typename E> __device__ __forceinline__ E ld_slab(const float2 *p);
+template <> __device__ __forceinline__ float2 ld_slab<float2>(const float2 *p) { return *p; }
+template <> __device__ __forceinline__ double2 ld_slab<double2>(const float2 *p) { return to_d2(*p); }
+
+// Element type of a panel's shared-memory slab: the FP64 factorisation works
+// in FP64; the mixed path's FP32 factors are factored in FP32 arithmetic
+// (what the tensor-core trailing updates keep), which halves the slab and so
+// the CTAs a panel needs.
+template <typename T> struct SlabOf { using type = double2; };
+template <> struct SlabOf<float2> { using type = float2; };
+// Rows per CTA that fit a 64-column slab in the 222 KB the panel kernel gets.
+template <typename T> constexpr int64_t kPanelMaxRows = sizeof(typename SlabOf<T>::type) == 8 ? 416 : 208;
 
 constexpr int kPanelThreads = 512;
 constexpr long long kSpinLimit = 1LL << 26;  // default bound of a barrier wait (a few seconds)
@@ -101,11 +124,13 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k)
 // row swap, scaling and the rank-1 update of the CTA's rows.
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
-  extern __shared__ double2 slab[];  // [nb][rpc] column-major within the CTA
+  using E = typename SlabOf<T>::type;
+  extern __shared__ __align__(16) unsigned char panel_smem[];
+  E *slab = reinterpret_cast<E *>(panel_smem);  // [nb][rpc] column-major within the CTA
   __shared__ unsigned long long w_key[kPanelThreads / 32];
-  __shared__ double2 s_prow_data[64];
-  __shared__ double2 s_l[kPanelThreads];
-  __shared__ double2 s_rp;
+  __shared__ E s_prow_data[64];
+  __shared__ E s_l[kPanelThreads];
+  __shared__ E s_rp;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;
   const int nb = a.nb, rpc = a.rpc;
@@ -114,12 +139,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   const int64_t rem = a.n - row0;
   const int nrow = rem <= 0 ? 0 : (rem < rpc ? (int)rem : rpc);
   for (int base = tid; base < nb * rpc; base += 8 * kPanelThreads) {
-    double2 v[8];
+    E v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * kPanelThreads;
       const int c = idx / rpc, i = idx % rpc;
-      v[u] = (idx < nb * rpc && i < nrow) ? ld2(A + (row0 + i) + (a.j0 + c) * a.lda) : make_double2(0, 0);
+      v[u] = (idx < nb * rpc && i < nrow) ? ld_slab<E>(A + (row0 + i) + (a.j0 + c) * a.lda)
+                                          : from_d2<E>(make_double2(0, 0));
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
@@ -146,11 +172,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       //    record; the release store orders the whole warp's stores before it
       if (bkey != 0ull) {
         const int li = (int)(0xffffffu - (unsigned)((bkey >> 8) & 0xffffffu)) - (int)(row0 - a.j0);
-        for (int j = lane; j < nb; j += 32) a.cand_data[((size_t)par * a.P + cta) * nb + j] = slab[j * rpc + li];
+        for (int j = lane; j < nb; j += 32) a.cand_data[((size_t)par * a.P + cta) * nb + j] = to_d2(slab[j * rpc + li]);
       }
       if (col >= row0 && col < row0 + nrow) {
         const int li = (int)(col - row0);
-        for (int j = lane; j < nb; j += 32) a.col_data[(size_t)par * nb + j] = slab[j * rpc + li];
+        for (int j = lane; j < nb; j += 32) a.col_data[(size_t)par * nb + j] = to_d2(slab[j * rpc + li]);
       }
       __syncwarp();
       unsigned long long *rec = a.rec + (size_t)par * a.P;
@@ -228,12 +254,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         for (int j = lane; j < nb; j += 32) {
           const double2 pv = none ? __ldcg(cdat + j) : have ? (j < 32 ? pf0 : pf1) : __ldcg(pdat + j);
           const double2 cvv = own_p ? __ldcg(cdat + j) : make_double2(0, 0);
-          s_prow_data[j] = pv;
-          if (own_p) slab[j * rpc + (gr - (int)row0)] = cvv;  // row prow <- old row col
-          if (own_c) slab[j * rpc + (int)(col - row0)] = pv;  // row col  <- pivot row
+          s_prow_data[j] = from_d2<E>(pv);
+          if (own_p) slab[j * rpc + (gr - (int)row0)] = from_d2<E>(cvv);  // row prow <- old row col
+          if (own_c) slab[j * rpc + (int)(col - row0)] = from_d2<E>(pv);  // row col  <- pivot row
           if (j == c) {
+            // 1 / pivot, formed in FP64 (|pivot|^2 cannot underflow)
             const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
-            s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
+            s_rp = from_d2<E>(pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0));
             if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
           }
         }
@@ -244,10 +271,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     __syncthreads();
     if (!s_ok) return;
     // 4. scale column c of the rows below the pivot (one thread per row) ...
-    const double2 rp = s_rp;
-    const bool live = mine && g > col && (rp.x != 0.0 || rp.y != 0.0);
+    const E rp = s_rp;
+    const bool live = mine && g > col && (rp.x != 0 || rp.y != 0);
     if (live && sph == 0) {
-      const double2 l = cmul(slab[c * rpc + i], rp);
+      const E l = cmul(slab[c * rpc + i], rp);
       slab[c * rpc + i] = l;
       s_l[i] = l;
     }
@@ -258,16 +285,16 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     if (mine && g > col) {
       const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
       if (live) {
-        const double2 l = s_l[i];
+        const E l = s_l[i];
         for (int j = jst; j < nb; j += 4 * S) {
-          double2 x[4];
+          E x[4];
 #pragma unroll
           for (int u = 0; u < 4; u++)
             if (j + u * S < nb) x[u] = slab[(j + u * S) * rpc + i];
 #pragma unroll
           for (int u = 0; u < 4; u++)
             if (j + u * S < nb) {
-              const double2 uu = s_prow_data[j + u * S];
+              const E uu = s_prow_data[j + u * S];
               x[u].x -= l.x * uu.x - l.y * uu.y;
               x[u].y -= l.x * uu.y + l.y * uu.x;
               slab[(j + u * S) * rpc + i] = x[u];
@@ -1396,8 +1423,8 @@ uint64_t tune_hash(const Ctx *c) {
 
 // CTAs for a panel of m rows: the autotuned table's entry at the nearest
 // probed height (log scale), else a cap, else one CTA per SM; never fewer
-// than needed for rpc <= 208 rows.
-int panel_ctas(const Ctx *c, int64_t m) {
+// than needed for rpc <= max_rows rows (what one CTA's slab holds).
+int panel_ctas(const Ctx *c, int64_t m, int64_t max_rows) {
   int P = c->nsm;
   if (c->panel_cap_env > 0) {
     P = std::min(c->panel_cap_env, c->nsm);
@@ -1412,7 +1439,7 @@ int panel_ctas(const Ctx *c, int64_t m) {
     }
   }
   P = (int)std::min<int64_t>(P, (m + 7) / 8);
-  return (int)std::min<int64_t>(c->nsm, std::max<int64_t>(P, (m + 207) / 208));
+  return (int)std::min<int64_t>(c->nsm, std::max<int64_t>(P, (m + max_rows - 1) / max_rows));
 }
 
 // One panel (rows j0 .. n of columns j0 .. j0+nb) on P CTAs.
@@ -1460,7 +1487,7 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
   }
   const int rpc = (int)((m + P - 1) / P);
   P = (int)((m + rpc - 1) / rpc);
-  const size_t smem = sizeof(double2) * (size_t)nb * rpc;
+  const size_t smem = sizeof(typename SlabOf<T>::type) * (size_t)nb * rpc;
   if (smem > 222 * 1024 || rpc > kPanelThreads || nb > 64 || P > 256)
     return fail(c, MOM_ERR_ARG, "panel does not fit in shared memory (matrix order too large)");
   PanelArgs pa;
@@ -1540,7 +1567,7 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
       const int64_t m = n - j0;
       {
         ProfScope ps(c, kProfPanel);
-        MOM_TRY(launch_panel<T>(c, A, lda, n, j0, panel_ctas(c, m), c->ipiv, w.info, w));
+        MOM_TRY(launch_panel<T>(c, A, lda, n, j0, panel_ctas(c, m, kPanelMaxRows<T>), c->ipiv, w.info, w));
       }
       {
         ProfScope pz(c, kProfPivotAux);
@@ -1627,7 +1654,7 @@ int lu_enqueue(Ctx *c, T *A, int precision, const LuWork &w) {
 // the block are swapped at the same time (they hold L of earlier blocks,
 // which nothing reads any more).  Blocks whose trailing height is above
 // la_from * n, or whose panels need more than half of the SMs (over about
-// 15,400 rows: at most 208 rows per panel CTA), run without the overlap
+// 30,800 rows: at most 416 rows per FP32 panel CTA), run without the overlap
 // (the panel would take too many SMs from the larger GEMM).
 template <typename T>
 int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
@@ -1664,8 +1691,8 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     for (int64_t j0 = J0; j0 < J0 + NBc; j0 += nb) {
       const int p = (int)((j0 - J0) / nb), kb = (int)(j0 / nb);
       const int64_t m = n - j0;
-      int P = panel_ctas(c, m);
-      if (pcap > 0) P = (int)std::max<int64_t>(std::min(P, pcap), (m + 207) / 208);
+      int P = panel_ctas(c, m, kPanelMaxRows<T>);
+      if (pcap > 0) P = (int)std::max<int64_t>(std::min(P, pcap), (m + kPanelMaxRows<T> - 1) / kPanelMaxRows<T>);
       {
         ProfScope ps(c, kProfPanel, st);
         MOM_TRY(launch_panel<T>(c, A, lda, n, j0, P, c->ipiv, w.info, w, st));
@@ -1756,13 +1783,14 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     MOM_TRY(swaps(J0, J0 + L, 0, 0));
     MOM_TRY(trailing(J0, t0, L, 0));
     // overlap only where the next block's panels leave the GEMM at least half
-    // of the SMs (a panel holds at most 208 rows per CTA)
-    const bool overlap = (double)nc < c->la_from * (double)n && nc > L && (nc + 207) / 208 <= c->nsm / 2;
+    // of the SMs
+    constexpr int64_t R = kPanelMaxRows<T>;
+    const bool overlap = (double)nc < c->la_from * (double)n && nc > L && (nc + R - 1) / R <= c->nsm / 2;
     if (overlap) {
       // panel CTAs of the next block (the tallest of its panels), the GEMM gets the rest
-      int P = panel_ctas(c, nc);
+      int P = panel_ctas(c, nc, R);
       const int pcap = c->la_ctas > 0 ? c->la_ctas : 1;
-      P = (int)std::max<int64_t>(std::min(P, pcap), (nc + 207) / 208);
+      P = (int)std::max<int64_t>(std::min(P, pcap), (nc + R - 1) / R);
       if (c->panel_cluster > 0 && nc <= (int64_t)kClusterRows * c->panel_cluster) P = c->panel_cluster;
       MOM_CUDA(c, cudaEventRecord(c->la_ev[1], sa));
       MOM_CUDA(c, cudaStreamWaitEvent(sb, c->la_ev[1], 0));
@@ -2117,7 +2145,8 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
     const bool clustered = c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster;
     for (int cand : cands) {
       if (clustered && cand != cands[0]) break;
-      const int P0 = (int)std::min<int64_t>(c->nsm, std::max<int64_t>(std::min<int64_t>(cand, (m + 7) / 8), (m + 207) / 208));
+      const int P0 = (int)std::min<int64_t>(
+          c->nsm, std::max<int64_t>(std::min<int64_t>(cand, (m + 7) / 8), (m + kPanelMaxRows<T> - 1) / kPanelMaxRows<T>));
       const int rpc = (int)((m + P0 - 1) / P0);
       const int P = (int)((m + rpc - 1) / rpc);
       if (P == last) continue;
