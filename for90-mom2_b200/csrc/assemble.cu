@@ -274,25 +274,43 @@ struct PairArgs {
   double2 *blk;        // [F source][F test][18]
 };
 
-// One thread per source face n; the CTA walks kTestPerCta test faces.
-template <typename T, int NQ, bool LOSSLESS>
-__global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
+// One thread per source face n; the CTA walks kTestPerCta test faces.  In the
+// FP32 kernel the source face's FP64 geometry (centroid, edge vectors, edge
+// lengths) waits in shared memory while the point-pair loop runs, so it holds
+// no registers there (the FP64 kernel's point sources already fill the 48 KB
+// of static shared memory and keep it in registers).  MINB CTAs of 128
+// threads share an SM (the register cap follows).
+template <typename T, int NQ, bool LOSSLESS, int MINB = 3>
+__global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
+  constexpr bool kGeoShared = sizeof(T) == sizeof(float);
   __shared__ T s_src[NQ * 3][kPairThreads];
   __shared__ T s_tst[NQ * 3];
   __shared__ double s_tmu[9], s_tsl[3], s_tcp[3];
+  // per source face: cp[3], mu[3][3] / L0, sl[3] / L0
+  __shared__ double s_ngeo[kGeoShared ? 15 : 1][kPairThreads];
+  double r_ngeo[kGeoShared ? 1 : 15];
   const int tid = threadIdx.x;
+  auto ngeo = [&](int i) -> double {
+    if constexpr (kGeoShared) return s_ngeo[i][tid];
+    else return r_ngeo[i];
+  };
   const int n = blockIdx.x * kPairThreads + tid;
   const bool active = n < a.F;
-  double ncp[3] = {0, 0, 0}, nu[3][3], slq[3];
   if (active) {
 #pragma unroll
     for (int i = 0; i < NQ * 3; i++) s_src[i][tid] = (T)(a.qrel[(size_t)n * NQ * 3 + i] * a.inv_unit);
+    double g[15];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      ncp[i] = a.cp[3 * n + i];
-      slq[i] = a.sl[3 * n + i] * a.inv_unit;
+      g[i] = a.cp[3 * n + i];
+      g[12 + i] = a.sl[3 * n + i] * a.inv_unit;
 #pragma unroll
-      for (int j = 0; j < 3; j++) nu[i][j] = a.mu[9 * n + 3 * i + j] * a.inv_unit;
+      for (int j = 0; j < 3; j++) g[3 + 3 * i + j] = a.mu[9 * n + 3 * i + j] * a.inv_unit;
+    }
+#pragma unroll
+    for (int i = 0; i < 15; i++) {
+      if constexpr (kGeoShared) s_ngeo[i][tid] = g[i];
+      else r_ngeo[i] = g[i];
     }
   }
   const int m0 = blockIdx.y * kTestPerCta;
@@ -308,21 +326,22 @@ __global__ void __launch_bounds__(kPairThreads, 3) pair_kernel(PairArgs a) {
     }
     __syncthreads();
     if (!active) continue;
-    double dd[3];
     T dT[3];
 #pragma unroll
-    for (int i = 0; i < 3; i++) {
-      dd[i] = (s_tcp[i] - ncp[i]) * a.inv_unit;
-      dT[i] = (T)dd[i];
-    }
+    for (int i = 0; i < 3; i++) dT[i] = (T)((s_tcp[i] - ngeo(i)) * a.inv_unit);
     Moments<T> Mt;
     pair_moments<T, NQ, false, LOSSLESS>(s_tst, &s_src[0][tid], kPairThreads, dT, (T)a.kr, (T)a.ki, Mt);
-    double mu[3][3], slp[3];
+    double mu[3][3], slp[3], nu[3][3], slq[3], dd[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
       slp[i] = s_tsl[i];
+      slq[i] = ngeo(12 + i);
+      dd[i] = (s_tcp[i] - ngeo(i)) * a.inv_unit;
 #pragma unroll
-      for (int j = 0; j < 3; j++) mu[i][j] = s_tmu[3 * i + j];
+      for (int j = 0; j < 3; j++) {
+        mu[i][j] = s_tmu[3 * i + j];
+        nu[i][j] = ngeo(3 + 3 * i + j);
+      }
     }
     blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
                            a.blk + ((size_t)n * a.F + m) * 18);
@@ -776,7 +795,13 @@ int launch_pair_k(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
     case 3: pair_kernel<T, 3, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
     case 4: pair_kernel<T, 4, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
     case 7: pair_kernel<T, 7, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
-    case 13: pair_kernel<T, 13, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
+    case 13:
+      // the FP64 kernel keeps 3 CTAs per SM (168 registers, no spills)
+      if (sizeof(T) == sizeof(float) && c->pair_ctas == 4)
+        pair_kernel<T, 13, LOSSLESS, 4><<<grid, kPairThreads, 0, c->stream>>>(a);
+      else
+        pair_kernel<T, 13, LOSSLESS, 3><<<grid, kPairThreads, 0, c->stream>>>(a);
+      break;
     default: return fail(c, MOM_ERR_ARG, "unsupported number of quadrature points");
   }
   c->launches++;

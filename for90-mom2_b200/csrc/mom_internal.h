@@ -124,6 +124,7 @@ struct Ctx {
   int lookahead = 1;       // MOM_LOOKAHEAD=0 turns it off
   // Defaults from a sweep on a B200 at n = 30,720 (the cap 32/48/64 and the
   // fraction 0.9/0.95/all within 3% of each other; these were the fastest).
+  int pair_ctas = 3;       // MOM_PAIR_CTAS: resident CTAs per SM of the 13-point FP32 far-pair kernel (3 or 4)
   int la_ctas = 48;        // MOM_LA_CTAS: CTA cap of the look-ahead panels (0: the smallest that fits)
   double la_from = 1.0;    // MOM_LA_FROM: overlap blocks whose trailing height is below this fraction of n
   std::mutex mu;
