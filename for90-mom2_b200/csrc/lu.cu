@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   E *slab = reinterpret_cast<E *>(panel_smem);  // [nb][rpc] column-major within the CTA
   __shared__ unsigned long long w_key[kPanelThreads / 32];
   __shared__ E s_prow_data[64];
-  __shared__ E s_l[kPanelThreads];
+  __shared__ E s_rpc[64];  // 1 / pivot of each column (0: failed pivot)
   __shared__ E s_rp;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;
@@ -261,6 +261,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
             // 1 / pivot, formed in FP64 (|pivot|^2 cannot underflow)
             const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
             s_rp = from_d2<E>(pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0));
+            s_rpc[c] = s_rp;
             if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
           }
         }
@@ -270,22 +271,18 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     }
     __syncthreads();
     if (!s_ok) return;
-    // 4. scale column c of the rows below the pivot (one thread per row) ...
+    // 4. rank-1 update of columns c+1 .. nb, S threads per row, with the
+    //    multiplier l = a(i, c) / pivot formed by each of them; column c keeps
+    //    a(i, c) until the final store scales it (the same product, so the
+    //    factors are unchanged) and needs no barrier of its own
     const E rp = s_rp;
     const bool live = mine && g > col && (rp.x != 0 || rp.y != 0);
-    if (live && sph == 0) {
-      const E l = cmul(slab[c * rpc + i], rp);
-      slab[c * rpc + i] = l;
-      s_l[i] = l;
-    }
-    __syncthreads();
-    // ... and the rank-1 update of columns c+1 .. nb, S threads per row
     cv = -1.0;
     const int own = (c + 1) % S;  // phase of the thread that holds column c+1
     if (mine && g > col) {
       const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
       if (live) {
-        const E l = s_l[i];
+        const E l = cmul(slab[c * rpc + i], rp);
         for (int j = jst; j < nb; j += 4 * S) {
           E x[4];
 #pragma unroll
@@ -305,9 +302,14 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     }
   }
   __syncthreads();
+  // L below the diagonal scaled by its column's 1 / pivot on the way out
   for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
     const int c = idx / rpc, ii = idx % rpc;
-    if (ii < nrow) st2(A + (row0 + ii) + (a.j0 + c) * a.lda, slab[idx]);
+    if (ii < nrow) {
+      const E v = slab[idx], rp = s_rpc[c];
+      const bool low = row0 + ii > a.j0 + c && (rp.x != 0 || rp.y != 0);
+      st2(A + (row0 + ii) + (a.j0 + c) * a.lda, low ? cmul(v, rp) : v);
+    }
   }
 }
 
@@ -355,7 +357,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
   __shared__ unsigned long long w_key[kPanelThreads / 32];
   __shared__ unsigned long long c_key[2][kMaxCluster];
   __shared__ double2 s_prow_data[64];
-  __shared__ double2 s_l[kPanelThreads];
+  __shared__ double2 s_rpc[64];  // 1 / pivot of each column (0: failed pivot)
   __shared__ double2 s_rp;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;  // cta == cluster rank
   const int nb = a.nb, rpc = a.rpc, P = a.P;
@@ -437,27 +439,23 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
         if (j == c) {
           const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
           s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
+          s_rpc[c] = s_rp;
           if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
         }
       }
       if (lane == 0 && cta == 0) a.ipiv[col] = gr;
     }
     __syncthreads();
-    // 3. scale column c, rank-1 update of columns c+1 ..
+    // 3. rank-1 update of columns c+1 .. with l = a(i, c) / pivot formed by
+    //    each thread of the row (column c is scaled at the final store)
     const double2 rp = s_rp;
     const bool live = mine && g > col && (rp.x != 0.0 || rp.y != 0.0);
-    if (live && sph == 0) {
-      const double2 l = cmul(slab[c * rpc + i], rp);
-      slab[c * rpc + i] = l;
-      s_l[i] = l;
-    }
-    __syncthreads();
     cv = -1.0;
     const int own = (c + 1) % S;
     if (mine && g > col) {
       const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
       if (live) {
-        const double2 l = s_l[i];
+        const double2 l = cmul(slab[c * rpc + i], rp);
         for (int j = jst; j < nb; j += 4 * S) {
           double2 x[4];
 #pragma unroll
@@ -479,7 +477,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
   __syncthreads();
   for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
     const int c = idx / rpc, ii = idx % rpc;
-    if (ii < nrow) st2(A + (row0 + ii) + (a.j0 + c) * a.lda, slab[idx]);
+    if (ii < nrow) {
+      const double2 v = slab[idx], rp = s_rpc[c];
+      const bool low = row0 + ii > a.j0 + c && (rp.x != 0.0 || rp.y != 0.0);
+      st2(A + (row0 + ii) + (a.j0 + c) * a.lda, low ? cmul(v, rp) : v);
+    }
   }
   cluster_sync();  // no CTA leaves while another may still address its shared memory
 }
