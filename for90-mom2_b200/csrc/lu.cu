@@ -1732,8 +1732,10 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     }
     return MOM_OK;
   };
-  // trailing update of block J0 on columns [c0, c0 + ncol), stream 1
-  auto trailing = [&](int64_t J0, int64_t c0, int64_t ncol, int gemm_ctas) -> int {
+  // trailing update of block J0 on columns [c0, c0 + ncol), stream 1;
+  // reuse_a: the previous trailing call was for the same block (its expanded
+  // L21 is still in the work buffer: nothing between them writes L21 or it)
+  auto trailing = [&](int64_t J0, int64_t c0, int64_t ncol, int gemm_ctas, bool reuse_a) -> int {
     if (ncol <= 0) return MOM_OK;
     const int64_t NBc = std::min<int64_t>(NB, n - J0), t0 = J0 + NBc;
     ProfScope pg(c, kProfGemm);
@@ -1754,7 +1756,7 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
     MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(A + t0 + c0 * lda), lda,
                             reinterpret_cast<const float2 *>(A + t0 + J0 * lda), lda,
                             reinterpret_cast<const float2 *>(A + J0 + c0 * lda), lda, (int)(n - t0), (int)ncol,
-                            (int)NBc, w.tcw, c->dinfo + 2, gemm_ctas));
+                            (int)NBc, w.tcw, c->dinfo + 2, gemm_ctas, reuse_a));
     return MOM_OK;
   };
   // stream 2 joins the stream (and any capture open on it)
@@ -1783,7 +1785,7 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       break;
     }
     MOM_TRY(swaps(J0, J0 + L, 0, 0));
-    MOM_TRY(trailing(J0, t0, L, 0));
+    MOM_TRY(trailing(J0, t0, L, 0, false));
     // overlap only where the next block's panels leave the GEMM at least half
     // of the SMs
     constexpr int64_t R = kPanelMaxRows<T>;
@@ -1799,11 +1801,11 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       MOM_TRY(factor_block(t0, sb, c->blas2, pmN, pcap));
       MOM_CUDA(c, cudaEventRecord(c->la_ev[2], sb));
       MOM_TRY(swaps(0, n - NBc, J0, J0 + L));
-      MOM_TRY(trailing(J0, t0 + L, nc - L, std::max(8, c->nsm - P)));
+      MOM_TRY(trailing(J0, t0 + L, nc - L, std::max(8, c->nsm - P), true));
       MOM_CUDA(c, cudaStreamWaitEvent(sa, c->la_ev[2], 0));
     } else {
       MOM_TRY(swaps(0, n - NBc, J0, J0 + L));
-      MOM_TRY(trailing(J0, t0 + L, nc - L, 0));
+      MOM_TRY(trailing(J0, t0 + L, nc - L, 0, true));
       MOM_TRY(factor_block(t0, sa, c->blas, pmN, 0));
     }
   }

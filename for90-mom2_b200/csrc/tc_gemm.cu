@@ -358,16 +358,20 @@ int make_map(Ctx *c, CUtensorMap *m, const float *base, int64_t rows, int64_t co
 // C (m x nc complex FP32, ldc) -= L (m x k, ldl) * U (k x nc, ldu) with the
 // 3xTF32 tensor-core kernel.  m must be a multiple of 64, k of 16.
 // work: >= (4 m k + 4 k nc) * 4 bytes of device scratch.  max_ctas > 0
-// caps the persistent grid.
+// caps the persistent grid.  reuse_a: work already holds the expansion of
+// this L (the previous call on the same stream had the same L, m and k).
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
-                    int nc, int k, float *work, int *err, int max_ctas) {
+                    int nc, int k, float *work, int *err, int max_ctas, bool reuse_a) {
   if (m <= 0 || nc <= 0 || k <= 0) return MOM_OK;
   if ((2 * m) % kBM != 0 || (2 * k) % kBK != 0) return fail(c, MOM_ERR_ARG, "tc_cgemm_update: unsupported shape");
   const int Mr = 2 * m, Kr = 2 * k;
   float *ahi = work, *alo = ahi + (size_t)Mr * Kr, *bhi = alo + (size_t)Mr * Kr, *blo = bhi + (size_t)nc * Kr;
-  expand_a_kernel<<<(unsigned)(((int64_t)m * k + 255) / 256), 256, 0, c->stream>>>(L, ldl, m, k, ahi, alo);
+  if (!reuse_a) {
+    expand_a_kernel<<<(unsigned)(((int64_t)m * k + 255) / 256), 256, 0, c->stream>>>(L, ldl, m, k, ahi, alo);
+    c->launches++;
+  }
   split_b_kernel<<<(unsigned)(((int64_t)k * nc + 255) / 256), 256, 0, c->stream>>>(U, ldu, k, nc, bhi, blo);
-  c->launches += 2;
+  c->launches++;
   CUtensorMap mAhi, mAlo, mBhi, mBlo;
   MOM_TRY(make_map(c, &mAhi, ahi, Mr, Kr, kBM));
   MOM_TRY(make_map(c, &mAlo, alo, Mr, Kr, kBM));
