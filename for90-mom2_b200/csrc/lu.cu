@@ -2226,6 +2226,7 @@ int lu_factor(Ctx *c, int precision) {
 namespace {
 
 constexpr int kMultiRhs = 16;  // from this many right-hand sides on, the solves are GEMM based
+constexpr int kMultiTc = 64;   // ... and with the FP32 factors, the block updates on the tensor cores
 
 // Y = P X (mode 0), Y = X (mode 1) or Y[perm[i]] = X[i] (mode 2), with a
 // type conversion, for nrhs columns.
@@ -2275,10 +2276,17 @@ int getrs_multi(Ctx *c, const T *F, double2 *X, int nrhs, int trans) {
   const int64_t n = c->n, lda = c->lda;
   const int nb = c->nb, nblk = (int)(n / nb);
   const bool f32 = sizeof(T) == sizeof(float2);
+  // FP32 factors and many right-hand sides: 256-row blocks whose updates run
+  // on the tensor cores (3xTF32, FP32-accurate like the rest of the solve)
+  const bool tc = f32 && nrhs >= kMultiTc;
+  const int64_t NBt = 4 * (int64_t)nb;
   const size_t ybytes = sizeof(T) * (size_t)n * nrhs, tbytes = sizeof(T) * (size_t)nb * nrhs;
-  MOM_TRY(ensure_buffer(c, &c->ws2, &c->ws2_bytes, ybytes + tbytes + 1024));
+  const size_t o_t = ((ybytes + 255) / 256) * 256, o_w = o_t + ((tbytes + 255) / 256) * 256;
+  const size_t wbytes = tc ? tc_cgemm_work_bytes((int)n, nrhs, (int)NBt) : 0;
+  MOM_TRY(ensure_buffer(c, &c->ws2, &c->ws2_bytes, o_w + wbytes + 1024));
   T *Y = (T *)c->ws2;
-  T *Tm = (T *)((char *)c->ws2 + ((ybytes + 255) / 256) * 256);
+  T *Tm = (T *)((char *)c->ws2 + o_t);
+  float *tw = (float *)((char *)c->ws2 + o_w);
   const T *inv = f32 ? (const T *)c->inv32 : (const T *)c->invd;
   ProfScope ps(c, kProfTrsv);
   const dim3 pg((unsigned)((n + 255) / 256), nrhs);
@@ -2296,6 +2304,48 @@ int getrs_multi(Ctx *c, const T *F, double2 *X, int nrhs, int trans) {
                                   cudaMemcpyDeviceToDevice, c->stream));
     return MOM_OK;
   };
+  if (tc) {
+    // forward: L (unit lower), or U^T; 64-row blocks inside a 256-row block
+    // with the library GEMM, the rows below the 256-row block on the tensor cores
+    for (int64_t K0 = 0; K0 < n; K0 += NBt) {
+      const int64_t K1 = std::min<int64_t>(K0 + NBt, n);
+      for (int64_t k0 = K0; k0 < K1; k0 += nb) {
+        MOM_TRY(diag((int)(k0 / nb), trans ? 1 : 0));
+        const int64_t mi = K1 - k0 - nb;
+        if (mi > 0) {
+          const T *Ab = trans ? F + k0 + (k0 + nb) * lda : F + (k0 + nb) + k0 * lda;
+          MOM_TRY(blas_gemm<T>(c, op, (int)mi, nrhs, nb, -1.0, Ab, lda, Tm, nb, 1.0, Y + k0 + nb, n));
+        }
+      }
+      if (K1 < n) {
+        const T *Ab = trans ? F + K0 + K1 * lda : F + K1 + K0 * lda;
+        MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(Y + K1), n, reinterpret_cast<const float2 *>(Ab), lda,
+                                reinterpret_cast<const float2 *>(Y + K0), n, (int)(n - K1), nrhs, (int)(K1 - K0), tw,
+                                c->dinfo + 2, 0, false, trans != 0));
+      }
+    }
+    // backward: U, or L^T (unit upper)
+    for (int64_t K0 = ((n - 1) / NBt) * NBt; K0 >= 0; K0 -= NBt) {
+      const int64_t K1 = std::min<int64_t>(K0 + NBt, n);
+      for (int64_t k0 = K1 - nb; k0 >= K0; k0 -= nb) {
+        MOM_TRY(diag((int)(k0 / nb), trans ? 0 : 1));
+        if (k0 > K0) {
+          const T *Ab = trans ? F + k0 + K0 * lda : F + K0 + k0 * lda;
+          MOM_TRY(blas_gemm<T>(c, op, (int)(k0 - K0), nrhs, nb, -1.0, Ab, lda, Tm, nb, 1.0, Y + K0, n));
+        }
+      }
+      if (K0 > 0) {
+        const T *Ab = trans ? F + K0 : F + K0 * lda;
+        MOM_TRY(tc_cgemm_update(c, reinterpret_cast<float2 *>(Y), n, reinterpret_cast<const float2 *>(Ab), lda,
+                                reinterpret_cast<const float2 *>(Y + K0), n, (int)K0, nrhs, (int)(K1 - K0), tw,
+                                c->dinfo + 2, 0, false, trans != 0));
+      }
+    }
+    permute_rows_kernel<T, double2><<<pg, 256, 0, c->stream>>>(Y, n, X, n, n, c->perm, trans ? 2 : 1);
+    c->launches++;
+    MOM_CUDA(c, cudaGetLastError());
+    return MOM_OK;
+  }
   // forward: L (unit lower), or U^T; backward: U, or L^T (unit upper)
   for (int kb = 0; kb < nblk; kb++) {
     const int64_t k0 = (int64_t)kb * nb, m = n - k0 - nb;
@@ -2415,10 +2465,11 @@ int lu_solve_ex(Ctx *c, int precision, int trans, const double2 *B, double2 *X, 
     }
     MOM_CUDA(c, cudaGetLastError());
     MOM_CUDA(c, cudaMemcpyAsync(h.data(), rn2, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-    int tmo = 0;
-    MOM_CUDA(c, cudaMemcpyAsync(&tmo, c->dinfo + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    int tmo[2] = {0, 0};
+    MOM_CUDA(c, cudaMemcpyAsync(tmo, c->dinfo + 1, sizeof(int) * 2, cudaMemcpyDeviceToHost, c->stream));
     MOM_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (tmo) return fail(c, MOM_ERR_TIMEOUT, "triangular solve barrier timed out");
+    if (tmo[0]) return fail(c, MOM_ERR_TIMEOUT, "triangular solve barrier timed out");
+    if (tmo[1]) return fail(c, MOM_ERR_TIMEOUT, "tensor-core GEMM wait timed out");
     worst = 0;
     for (int s = 0; s < nrhs; s++) {
       double t = 0;

@@ -371,7 +371,8 @@ void free_shg(DomDev &D);
 
 // tc_gemm.cu: C -= L U (complex FP32) on the tensor cores, 3xTF32
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
-                    int nc, int k, float *work, int *err, int max_ctas = 0, bool reuse_a = false);
+                    int nc, int k, float *work, int *err, int max_ctas = 0, bool reuse_a = false,
+                    bool trans_l = false);
 size_t tc_cgemm_work_bytes(int m, int nc, int k);
 int tc_init_kernels(Ctx *c);
 

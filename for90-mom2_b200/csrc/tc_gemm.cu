@@ -283,12 +283,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
-// Ahat_hi / Ahat_lo (Mr x Kr, row-major) from the complex block L (m x k, ld).
-__global__ void expand_a_kernel(const float2 *L, int64_t ld, int m, int k, float *hi, float *lo) {
+// Ahat_hi / Ahat_lo (Mr x Kr, row-major) from the complex block L (m x k, ld),
+// or (tr) from the transpose of a k x m block: L(i, l) = P[l + i ld].
+__global__ void expand_a_kernel(const float2 *L, int64_t ld, int m, int k, float *hi, float *lo, bool tr) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)m * k) return;
   const int i = (int)(idx / k), l = (int)(idx % k);
-  const float2 z = L[i + (int64_t)l * ld];
+  const float2 z = tr ? L[l + (int64_t)i * ld] : L[i + (int64_t)l * ld];
   const int64_t Kr = 2 * (int64_t)k;
   const float vals[4] = {z.x, -z.y, z.y, z.x};
   const int64_t pos[4] = {(2 * i) * Kr + 2 * l, (2 * i) * Kr + 2 * l + 1, (2 * i + 1) * Kr + 2 * l,
@@ -360,14 +361,15 @@ int make_map(Ctx *c, CUtensorMap *m, const float *base, int64_t rows, int64_t co
 // work: >= (4 m k + 4 k nc) * 4 bytes of device scratch.  max_ctas > 0
 // caps the persistent grid.  reuse_a: work already holds the expansion of
 // this L (the previous call on the same stream had the same L, m and k).
+// trans_l: L is given as its k x m transpose at L (ld ldl).
 int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl, const float2 *U, int64_t ldu, int m,
-                    int nc, int k, float *work, int *err, int max_ctas, bool reuse_a) {
+                    int nc, int k, float *work, int *err, int max_ctas, bool reuse_a, bool trans_l) {
   if (m <= 0 || nc <= 0 || k <= 0) return MOM_OK;
   if ((2 * m) % kBM != 0 || (2 * k) % kBK != 0) return fail(c, MOM_ERR_ARG, "tc_cgemm_update: unsupported shape");
   const int Mr = 2 * m, Kr = 2 * k;
   float *ahi = work, *alo = ahi + (size_t)Mr * Kr, *bhi = alo + (size_t)Mr * Kr, *blo = bhi + (size_t)nc * Kr;
   if (!reuse_a) {
-    expand_a_kernel<<<(unsigned)(((int64_t)m * k + 255) / 256), 256, 0, c->stream>>>(L, ldl, m, k, ahi, alo);
+    expand_a_kernel<<<(unsigned)(((int64_t)m * k + 255) / 256), 256, 0, c->stream>>>(L, ldl, m, k, ahi, alo, trans_l);
     c->launches++;
   }
   split_b_kernel<<<(unsigned)(((int64_t)k * nc + 255) / 256), 256, 0, c->stream>>>(U, ldu, k, nc, bhi, blo);
