@@ -430,7 +430,14 @@ def run_ours(args, rank, local_rank, world):
                           "peak_note": "%s; latency-bound: one device-wide pivot exchange per column" % peak_src}
     ms, cnt = prof["pair"]
     if cnt:
-        flop = 17914.0 * F * F * cnt  # 17,914 FLOP per face pair, F^2 pairs per launch (one domain)
+        # 169 point pairs x 88 FLOP per unordered face pair (each evaluated once and
+        # used for both blocks) + a 3,042-FLOP contraction per block, F^2 blocks per
+        # launch (one domain); 17,914 FLOP per face pair when every ordered pair is
+        # evaluated (MOM_PAIR_SYM=0)
+        if os.environ.get("MOM_PAIR_SYM", "1") != "0":
+            flop = (14872.0 * F * (F + 1) / 2.0 + 3042.0 * F * F) * cnt
+        else:
+            flop = 17914.0 * F * F * cnt
         ach = flop / (ms * 1e-3) / 1e12
         peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         roofs["pair"] = {"kernel": "pair_kernel<float,13> (far-pair assembly, FP32 pipe)", "bound": "fp32",

@@ -267,6 +267,7 @@ struct PairArgs {
   const double *sl;    // [F][3]
   const double *tqrel, *tcp, *tmu;  // test faces (mapped by J^T for a group action g != identity)
   int ident;           // identity action: the self pair m == n has no K term
+  int sym;             // identity action: each unordered pair once, both blocks written
   double inv_unit;     // 1/L0
   double kr, ki;       // k * L0
   Cd fD, fH;
@@ -314,6 +315,8 @@ __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
     }
   }
   const int m0 = blockIdx.y * kTestPerCta;
+  // with sym, a CTA whose test faces all come after its source faces has no work
+  if (a.sym && (int64_t)m0 > (int64_t)blockIdx.x * kPairThreads + kPairThreads - 1) return;
   for (int mi = 0; mi < kTestPerCta; mi++) {
     const int m = m0 + mi;
     if (m >= a.F) break;
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
       s_tcp[tid] = a.tcp[3 * m + tid];
     }
     __syncthreads();
-    if (!active) continue;
+    if (!active || (a.sym && m > n)) continue;
     T dT[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) dT[i] = (T)((s_tcp[i] - ngeo(i)) * a.inv_unit);
@@ -345,6 +348,27 @@ __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
     }
     blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
                            a.blk + ((size_t)n * a.F + m) * 18);
+    if (a.sym && m < n) {
+      // the block of test face n and source face m from the same point pairs:
+      // G and the gradient phasor depend on |r - r'| only, so its moments are
+      // these with the two faces' roles exchanged (TB <-> TC, KC <-> KF,
+      // KE -> -KE; TA, TD, KG unchanged) and the centroid offset negated
+      Moments<T> Ms;
+      Ms.TA = Mt.TA;
+      Ms.TD = Mt.TD;
+      Ms.KG = Mt.KG;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        Ms.TB[i] = Mt.TC[i];
+        Ms.TC[i] = Mt.TB[i];
+        Ms.KC[i] = Mt.KF[i];
+        Ms.KF[i] = Mt.KC[i];
+        Ms.KE[i].re = -Mt.KE[i].re;
+        Ms.KE[i].im = -Mt.KE[i].im;
+        dd[i] = -dd[i];
+      }
+      blocks_from_moments<T>(Ms, nu, mu, slq, slp, dd, a.fD, a.fH, a.fK, false, a.blk + ((size_t)m * a.F + n) * 18);
+    }
   }
 }
 
@@ -1051,6 +1075,7 @@ int domain_blocks(Ctx *c, int d, int g, double omega, const double *ri, int prec
       pa.tcp = tcp;
       pa.tmu = tmu;
       pa.ident = ident ? 1 : 0;
+      pa.sym = ident && c->pair_sym ? 1 : 0;
       pa.inv_unit = 1.0 / L0;
       pa.kr = kr * L0;
       pa.ki = ki * L0;
