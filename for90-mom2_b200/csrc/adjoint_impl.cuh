@@ -480,10 +480,11 @@ __global__ void __launch_bounds__(kAdjThreads) adj_vertex_kernel(AdjPairArgs a) 
       blocks_generic<Dual, Dual, double, Dual>(M, ff.mu, reinterpret_cast<const double(*)[3]>(mux), ff.sl, slx, d, fD,
                                                fH, kOofpi / 4.0, false, Sb, Kb);
       contract_blocks(a, f, x, Sb, Kb, acc);
-      // (x, f): plain test face, dual source
+      // (x, f): plain test face, dual source; the same point pairs, so its
+      // moments are those of (f, x) with the faces' roles exchanged
 #pragma unroll
-      for (int i = 0; i < 3; i++) d[i] = a.cp[3 * x + i] - ff.cp[i];
-      pair_moments<Dual, NQ, false, false, double, Dual, Dual>(qx, &ff.qr[0][0], 1, d, a.kr, a.ki, M);
+      for (int i = 0; i < 3; i++) d[i] = -d[i];
+      exchange_roles(M);
       blocks_generic<Dual, double, Dual, Dual>(M, reinterpret_cast<const double(*)[3]>(mux), ff.mu, slx, ff.sl, d, fD,
                                                fH, kOofpi / 4.0, false, Sb, Kb);
       contract_blocks(a, x, f, Sb, Kb, acc);

@@ -71,6 +71,24 @@ struct Moments {
   Cx<T> TB[3], TC[3], KC[3], KE[3], KF[3];
 };
 
+// The moments of the face pair with the two faces' roles exchanged (test <->
+// source): G and the gradient phasor depend on |r - r'| only, so TB <-> TC,
+// KC <-> KF, KE -> -KE, and TA, TD, KG stay (the centroid offset of the
+// exchanged pair is the negated one).  Both faces use the same point rule.
+template <typename T>
+__device__ __forceinline__ void exchange_roles(Moments<T> &M) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const Cx<T> tb = M.TB[i], kc = M.KC[i];
+    M.TB[i] = M.TC[i];
+    M.TC[i] = tb;
+    M.KC[i] = M.KF[i];
+    M.KF[i] = kc;
+    M.KE[i].re = -M.KE[i].re;
+    M.KE[i].im = -M.KE[i].im;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void zero(Cx<T> &a) {
   a.re = 0;
@@ -349,24 +367,11 @@ __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
     blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
                            a.blk + ((size_t)n * a.F + m) * 18);
     if (a.sym && m < n) {
-      // the block of test face n and source face m from the same point pairs:
-      // G and the gradient phasor depend on |r - r'| only, so its moments are
-      // these with the two faces' roles exchanged (TB <-> TC, KC <-> KF,
-      // KE -> -KE; TA, TD, KG unchanged) and the centroid offset negated
-      Moments<T> Ms;
-      Ms.TA = Mt.TA;
-      Ms.TD = Mt.TD;
-      Ms.KG = Mt.KG;
+      // the block of test face n and source face m from the same point pairs
+      Moments<T> Ms = Mt;
+      exchange_roles(Ms);
 #pragma unroll
-      for (int i = 0; i < 3; i++) {
-        Ms.TB[i] = Mt.TC[i];
-        Ms.TC[i] = Mt.TB[i];
-        Ms.KC[i] = Mt.KF[i];
-        Ms.KF[i] = Mt.KC[i];
-        Ms.KE[i].re = -Mt.KE[i].re;
-        Ms.KE[i].im = -Mt.KE[i].im;
-        dd[i] = -dd[i];
-      }
+      for (int i = 0; i < 3; i++) dd[i] = -dd[i];
       blocks_from_moments<T>(Ms, nu, mu, slq, slp, dd, a.fD, a.fH, a.fK, false, a.blk + ((size_t)m * a.F + n) * 18);
     }
   }
