@@ -558,7 +558,11 @@ __device__ __noinline__ void eps_near_terms(const AdjEpsArgs &a, int m, int n, C
   }
 }
 
-// One thread per source face, one CTA row per test face.
+// One thread per source face, one CTA row per test face.  A far pair is
+// evaluated once, by the thread with m < x, which contracts both its blocks
+// ((m, x) and, with the faces' roles exchanged, (x, m)); near pairs (their
+// closed-form terms are not symmetric in the two faces) and the self pair
+// are evaluated in each order.
 template <int NQ>
 __global__ void __launch_bounds__(kAdjThreads) adj_eps_kernel(AdjEpsArgs a) {
   const int m = blockIdx.y;
@@ -566,33 +570,15 @@ __global__ void __launch_bounds__(kAdjThreads) adj_eps_kernel(AdjEpsArgs a) {
   Cd acc[kAdjMaxObj];
 #pragma unroll
   for (int o = 0; o < kAdjMaxObj; o++) acc[o] = {0.0, 0.0};
-  if (x < a.F) {
-    const int64_t bit = (int64_t)m * a.F + x;
-    const bool near = (a.near_bits[bit >> 5] >> (bit & 31)) & 1u;
-    double d[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) d[i] = a.cp[3 * m + i] - a.cp[3 * x + i];
-    Moments<Dual> M;
-    if (near)
-      pair_moments<Dual, NQ, true, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d, a.kr,
-                                                  a.ki, M);
-    else
-      pair_moments<Dual, NQ, false, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d,
-                                                   a.kr, a.ki, M);
-    const Cx<Dual> fD = {a.c1.re * (kOofpi / 4.0), a.c1.im * (kOofpi / 4.0)};
-    const Cx<Dual> fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
-    Cx<Dual> Sb[9], Kb[9];
-    blocks_generic<Dual, double>(M, reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)m),
-                                 reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)x), a.sl + 3 * m,
-                                 a.sl + 3 * x, d, fD, fH, kOofpi / 4.0, m == x, Sb, Kb);
-    if (near) eps_near_terms<NQ>(a, m, x, Sb, Kb);
+  // dZ/deps-weighted blocks of test face tm, source face tx into acc
+  auto contract = [&](int tm, int tx, const Cx<Dual> *Sb, const Cx<Dual> *Kb) {
     const int64_t N = a.N, ld = a.n;
 #pragma unroll 1
     for (int p = 0; p < 3; p++) {
-      const int64_t r = a.hpar[3 * m + p];
+      const int64_t r = a.hpar[3 * tm + p];
 #pragma unroll 1
       for (int q = 0; q < 3; q++) {
-        const int64_t cI = a.hpar[3 * x + q];
+        const int64_t cI = a.hpar[3 * tx + q];
         const Cd dS = dpart(Sb[3 * p + q]), dZ = dpart(cxm(a.Zsi, Sb[3 * p + q])), dK = dpart(Kb[3 * p + q]);
         if (a.R == 0) {
           const double2 wjj = a.W[r + cI * ld], wmm = a.W[(r + N) + (cI + N) * ld];
@@ -614,6 +600,37 @@ __global__ void __launch_bounds__(kAdjThreads) adj_eps_kernel(AdjEpsArgs a) {
           }
         }
       }
+    }
+  };
+  const int64_t bit = (int64_t)m * a.F + x;
+  const bool near = x < a.F && ((a.near_bits[bit >> 5] >> (bit & 31)) & 1u);
+  if (x < a.F && (near || m <= x)) {
+    double d[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) d[i] = a.cp[3 * m + i] - a.cp[3 * x + i];
+    Moments<Dual> M;
+    if (near)
+      pair_moments<Dual, NQ, true, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d, a.kr,
+                                                  a.ki, M);
+    else
+      pair_moments<Dual, NQ, false, false, double>(a.qrel + (size_t)m * NQ * 3, a.qrel + (size_t)x * NQ * 3, 1, d,
+                                                   a.kr, a.ki, M);
+    const Cx<Dual> fD = {a.c1.re * (kOofpi / 4.0), a.c1.im * (kOofpi / 4.0)};
+    const Cx<Dual> fH = {a.c2.re * kOofpi, a.c2.im * kOofpi};
+    Cx<Dual> Sb[9], Kb[9];
+    blocks_generic<Dual, double>(M, reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)m),
+                                 reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)x), a.sl + 3 * m,
+                                 a.sl + 3 * x, d, fD, fH, kOofpi / 4.0, m == x, Sb, Kb);
+    if (near) eps_near_terms<NQ>(a, m, x, Sb, Kb);
+    contract(m, x, Sb, Kb);
+    if (!near && m < x) {
+      exchange_roles(M);
+#pragma unroll
+      for (int i = 0; i < 3; i++) d[i] = -d[i];
+      blocks_generic<Dual, double>(M, reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)x),
+                                   reinterpret_cast<const double(*)[3]>(a.mu + 9 * (size_t)m), a.sl + 3 * x,
+                                   a.sl + 3 * m, d, fD, fH, kOofpi / 4.0, false, Sb, Kb);
+      contract(x, m, Sb, Kb);
     }
   }
   __shared__ double red[kAdjThreads][2];
