@@ -442,6 +442,8 @@ int mom_gpu_create(int32_t device, mom_ctx **out) {
   if (el) c->lookahead = el[0] != '0';
   const char *es = std::getenv("MOM_PAIR_SYM");
   if (es) c->pair_sym = es[0] != '0';
+  const char *ee = std::getenv("MOM_PAIR_E32");
+  if (ee) c->pair_e32 = ee[0] != '0';
   const char *ep3 = std::getenv("MOM_PAIR_CTAS");
   if (ep3) c->pair_ctas = std::atoi(ep3) == 3 ? 3 : 4;
   const char *ec = std::getenv("MOM_LA_CTAS");

@@ -39,6 +39,8 @@
 #include <cstdio>
 #include <vector>
 
+#include <type_traits>
+
 #include "mom_internal.h"
 
 namespace mom {
@@ -211,14 +213,28 @@ struct Cd {
 };
 __device__ __forceinline__ Cd cmul(Cd a, Cd b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
 
-// Closed-form 3x3 blocks from the moments (FP64).  mu[p][3], nu[q][3], d in
-// the kernel's length unit; fD, fH, fK carry c1, c2, 1/(16 pi) and the unit
-// scale.  Writes S = D + H and K, interleaved, 18 double2 values.
-template <typename T>
+template <typename R>
+struct Cr {
+  R re, im;
+};
+template <typename R>
+__device__ __forceinline__ Cr<R> cmul(Cr<R> a, Cr<R> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// Closed-form 3x3 blocks from the moments, in the real type R (FP64, or FP32
+// for FP32 moments).  mu[p][3], nu[q][3], d in the kernel's length unit; fD,
+// fH, fK carry c1, c2, 1/(16 pi) and the unit scale.  Writes S = D + H and K,
+// interleaved, 18 double2 values.
+template <typename T, typename R = double>
 __device__ __forceinline__ void blocks_from_moments(const Moments<T> &Mt, const double mu[3][3], const double nu[3][3],
-                                                    const double slp[3], const double slq[3], const double d[3],
-                                                    Cd fD, Cd fH, double fK, bool self, double2 *out) {
-  auto cv = [](const Cx<T> &a) -> Cd { return {(double)a.re, (double)a.im}; };
+                                                    const double slp[3], const double slq[3], const double d_[3],
+                                                    Cd fD_, Cd fH_, double fK_, bool self, double2 *out) {
+  using Cd = Cr<R>;
+  const R d[3] = {(R)d_[0], (R)d_[1], (R)d_[2]};
+  const Cd fD = {(R)fD_.re, (R)fD_.im}, fH = {(R)fH_.re, (R)fH_.im};
+  const R fK = (R)fK_;
+  auto cv = [](const Cx<T> &a) -> Cd { return {(R)a.re, (R)a.im}; };
   Cd TA = cv(Mt.TA), TD = cv(Mt.TD), KG = cv(Mt.KG);
   Cd TB[3], TC[3], KC[3], KE[3], KF[3];
 #pragma unroll
@@ -242,15 +258,15 @@ __device__ __forceinline__ void blocks_from_moments(const Moments<T> &Mt, const 
   Cd beta[3], bq[3], cq[3];
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    const double *v = nu[q];
+    const R v[3] = {(R)nu[q][0], (R)nu[q][1], (R)nu[q][2]};
     beta[q] = {v[0] * TB[0].re + v[1] * TB[1].re + v[2] * TB[2].re, v[0] * TB[0].im + v[1] * TB[1].im + v[2] * TB[2].im};
-    double dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
+    R dn[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
     bq[q] = {dn[0] * KC[0].re + dn[1] * KC[1].re + dn[2] * KC[2].re, dn[0] * KC[0].im + dn[1] * KC[1].im + dn[2] * KC[2].im};
     cq[q] = {v[0] * KE[0].re + v[1] * KE[1].re + v[2] * KE[2].re, v[0] * KE[0].im + v[1] * KE[1].im + v[2] * KE[2].im};
   }
 #pragma unroll
   for (int p = 0; p < 3; p++) {
-    const double *u = mu[p];
+    const R u[3] = {(R)mu[p][0], (R)mu[p][1], (R)mu[p][2]};
     Cd alpha = {u[0] * TC[0].re + u[1] * TC[1].re + u[2] * TC[2].re, u[0] * TC[0].im + u[1] * TC[1].im + u[2] * TC[2].im};
     Cd ap = {u[0] * KBv[0].re + u[1] * KBv[1].re + u[2] * KBv[2].re, u[0] * KBv[0].im + u[1] * KBv[1].im + u[2] * KBv[2].im};
     // Z_p = mu_p x (KDv - KF)
@@ -259,17 +275,17 @@ __device__ __forceinline__ void blocks_from_moments(const Moments<T> &Mt, const 
                {u[0] * KDmF[1].re - u[1] * KDmF[0].re, u[0] * KDmF[1].im - u[1] * KDmF[0].im}};
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const double *v = nu[q];
-      const double uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
-      const double ss = slp[p] * slq[q];
+      const R v[3] = {(R)nu[q][0], (R)nu[q][1], (R)nu[q][2]};
+      const R uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+      const R ss = (R)slp[p] * (R)slq[q];
       Cd cD = {TA.re - beta[q].re - alpha.re + uv * TD.re, TA.im - beta[q].im - alpha.im + uv * TD.im};
       Cd S1 = cmul(fD, cD), S2 = cmul(fH, TD);
-      double2 sv = make_double2(ss * (S1.re + S2.re), ss * (S1.im + S2.im));
+      double2 sv = make_double2((double)(ss * (S1.re + S2.re)), (double)(ss * (S1.im + S2.im)));
       double2 kv = make_double2(0.0, 0.0);
       if (!self) {
         Cd cK = {-dKE.re - ap.re - bq[q].re + cq[q].re + v[0] * Z[0].re + v[1] * Z[1].re + v[2] * Z[2].re,
                  -dKE.im - ap.im - bq[q].im + cq[q].im + v[0] * Z[0].im + v[1] * Z[1].im + v[2] * Z[2].im};
-        kv = make_double2(ss * fK * cK.re, ss * fK * cK.im);
+        kv = make_double2((double)(ss * fK * cK.re), (double)(ss * fK * cK.im));
       }
       out[2 * (3 * p + q)] = sv;
       out[2 * (3 * p + q) + 1] = kv;
@@ -299,8 +315,9 @@ struct PairArgs {
 // no registers there (the FP64 kernel's point sources already fill the 48 KB
 // of static shared memory and keep it in registers).  MINB CTAs of 128
 // threads share an SM (the register cap follows).
-template <typename T, int NQ, bool LOSSLESS, int MINB = 3>
+template <typename T, int NQ, bool LOSSLESS, int MINB = 3, bool E32 = false>
 __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
+  using R = typename std::conditional<E32, float, double>::type;  // the block contraction's type
   constexpr bool kGeoShared = sizeof(T) == sizeof(float);
   __shared__ T s_src[NQ * 3][kPairThreads];
   __shared__ T s_tst[NQ * 3];
@@ -364,15 +381,15 @@ __global__ void __launch_bounds__(kPairThreads, MINB) pair_kernel(PairArgs a) {
         nu[i][j] = ngeo(3 + 3 * i + j);
       }
     }
-    blocks_from_moments<T>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
-                           a.blk + ((size_t)n * a.F + m) * 18);
+    blocks_from_moments<T, R>(Mt, mu, nu, slp, slq, dd, a.fD, a.fH, a.fK, a.ident && m == n,
+                              a.blk + ((size_t)n * a.F + m) * 18);
     if (a.sym && m < n) {
       // the block of test face n and source face m from the same point pairs
       Moments<T> Ms = Mt;
       exchange_roles(Ms);
 #pragma unroll
       for (int i = 0; i < 3; i++) dd[i] = -dd[i];
-      blocks_from_moments<T>(Ms, nu, mu, slq, slp, dd, a.fD, a.fH, a.fK, false, a.blk + ((size_t)m * a.F + n) * 18);
+      blocks_from_moments<T, R>(Ms, nu, mu, slq, slp, dd, a.fD, a.fH, a.fK, false, a.blk + ((size_t)m * a.F + n) * 18);
     }
   }
 }
@@ -826,8 +843,12 @@ int launch_pair_k(Ctx *c, int nq, dim3 grid, const PairArgs &a) {
     case 7: pair_kernel<T, 7, LOSSLESS><<<grid, kPairThreads, 0, c->stream>>>(a); break;
     case 13:
       // the FP64 kernel keeps 3 CTAs per SM (168 registers, no spills)
-      if (sizeof(T) == sizeof(float) && c->pair_ctas == 4)
+      if (sizeof(T) == sizeof(float) && c->pair_ctas == 4 && c->pair_e32)
+        pair_kernel<T, 13, LOSSLESS, 4, true><<<grid, kPairThreads, 0, c->stream>>>(a);
+      else if (sizeof(T) == sizeof(float) && c->pair_ctas == 4)
         pair_kernel<T, 13, LOSSLESS, 4><<<grid, kPairThreads, 0, c->stream>>>(a);
+      else if (sizeof(T) == sizeof(float) && c->pair_e32)
+        pair_kernel<T, 13, LOSSLESS, 3, true><<<grid, kPairThreads, 0, c->stream>>>(a);
       else
         pair_kernel<T, 13, LOSSLESS, 3><<<grid, kPairThreads, 0, c->stream>>>(a);
       break;

@@ -125,6 +125,7 @@ struct Ctx {
   // Defaults from a sweep on a B200 at n = 30,720 (the cap 32/48/64 and the
   // fraction 0.9/0.95/all within 3% of each other; these were the fastest).
   bool pair_sym = true;    // MOM_PAIR_SYM: far pairs once per unordered pair (identity action), both blocks written
+  bool pair_e32 = false;   // MOM_PAIR_E32: FP32 block contraction in the FP32 far-pair kernel
   int pair_ctas = 3;       // MOM_PAIR_CTAS: resident CTAs per SM of the 13-point FP32 far-pair kernel (3 or 4)
   int la_ctas = 48;        // MOM_LA_CTAS: CTA cap of the look-ahead panels (0: the smallest that fits)
   double la_from = 1.0;    // MOM_LA_FROM: overlap blocks whose trailing height is below this fraction of n
