@@ -119,3 +119,27 @@ def test_mixed_precision_refinement(solver, case):
     ext, ext_r = csca[0] + cabs[0], sr + ar
     # FP32 far-pair assembly perturbs the matrix itself; sigma_ext stays within 1e-6
     assert abs(ext - ext_r) <= 1e-6 * abs(ext_r), (abs(ext - ext_r) / abs(ext_r), solver.iters)
+
+
+def test_far_pairs_once_per_unordered_pair_match_ordered(built):
+    """The assembly evaluates each unordered far face pair once and writes both
+    blocks from the moments with the faces' roles exchanged; the matrices
+    (FP64, and the mixed path's FP32 far pairs) equal those of the ordered
+    evaluation (MOM_PAIR_SYM=0, read when a context is created) to rounding."""
+    import os
+    nodes, faces, ids, doms, ri = core_shell_case(2)
+    om = M.omega_of(WL)
+    mats = {}
+    for sym in ("1", "0"):
+        os.environ["MOM_PAIR_SYM"] = sym
+        try:
+            s = M.Solver(0)
+        finally:
+            del os.environ["MOM_PAIR_SYM"]
+        try:
+            s.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
+            mats[sym] = (s.sysmat(om, ri, M.FP64, want_host=True), s.sysmat(om, ri, M.MIXED, want_host=True))
+        finally:
+            s.close()
+    assert rel(mats["1"][0], mats["0"][0]) <= 1e-13
+    assert rel(mats["1"][1], mats["0"][1]) <= 1e-6  # FP32 moments, summed in a transposed order
