@@ -316,7 +316,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
 // ---- short panels: one thread-block cluster, exchange in distributed shared memory ----
 
 constexpr int kMaxCluster = 16;
-constexpr int kClusterRows = 176;  // rows per CTA of a cluster panel (FP64 slab + pushed rows in shared memory)
+// rows per CTA of a cluster panel (slab + pushed rows in shared memory): 176
+// with the FP64 slab, 352 with the FP32 slab of the mixed path
+template <typename T> constexpr int kClusterRows = sizeof(typename SlabOf<T>::type) == 8 ? 352 : 176;
 
 __device__ __forceinline__ unsigned map_shared(const void *p, unsigned rank) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(p);
@@ -341,9 +343,12 @@ __device__ __forceinline__ void cluster_sync() {
 __device__ __forceinline__ void st_cluster_d2(unsigned addr, double2 v) {
   asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y) : "memory");
 }
+__device__ __forceinline__ void st_cluster_d2(unsigned addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
 
 // The same panel factorisation as panel_kernel for panels of at most
-// kClusterRows * kMaxCluster rows, on a grid that is exactly one cluster of
+// kClusterRows<T> * kMaxCluster rows, on a grid that is exactly one cluster of
 // P CTAs (all co-scheduled by the hardware).  Per column each CTA pushes
 // its packed candidate key and the candidate row (and the owner of row col
 // that row) into every CTA's shared memory, then one cluster barrier; the
@@ -353,27 +358,30 @@ __device__ __forceinline__ void st_cluster_d2(unsigned addr, double2 v) {
 // the cluster executes the same sequence of cluster barriers.
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelArgs a) {
-  extern __shared__ double2 slab[];  // [nb][rpc] column-major, then the pushed rows
+  using E = typename SlabOf<T>::type;
+  extern __shared__ __align__(16) unsigned char cluster_smem[];
+  E *slab = reinterpret_cast<E *>(cluster_smem);  // [nb][rpc] column-major, then the pushed rows
   __shared__ unsigned long long w_key[kPanelThreads / 32];
   __shared__ unsigned long long c_key[2][kMaxCluster];
-  __shared__ double2 s_prow_data[64];
-  __shared__ double2 s_rpc[64];  // 1 / pivot of each column (0: failed pivot)
-  __shared__ double2 s_rp;
+  __shared__ E s_prow_data[64];
+  __shared__ E s_rpc[64];  // 1 / pivot of each column (0: failed pivot)
+  __shared__ E s_rp;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, cta = blockIdx.x;  // cta == cluster rank
   const int nb = a.nb, rpc = a.rpc, P = a.P;
-  double2 *recv_row = slab + (size_t)nb * rpc;           // [2][P][nb] candidate rows by sender
-  double2 *recv_col = recv_row + (size_t)2 * P * nb;    // [2][nb] row col, from its owner
+  E *recv_row = slab + (size_t)nb * rpc;           // [2][P][nb] candidate rows by sender
+  E *recv_col = recv_row + (size_t)2 * P * nb;    // [2][nb] row col, from its owner
   T *A = reinterpret_cast<T *>(a.A);
   const int64_t row0 = a.j0 + (int64_t)cta * rpc;
   const int64_t rem = a.n - row0;
   const int nrow = rem <= 0 ? 0 : (rem < rpc ? (int)rem : rpc);
   for (int base = tid; base < nb * rpc; base += 8 * kPanelThreads) {
-    double2 v[8];
+    E v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int idx = base + u * kPanelThreads;
       const int c = idx / rpc, i = idx % rpc;
-      v[u] = (idx < nb * rpc && i < nrow) ? ld2(A + (row0 + i) + (a.j0 + c) * a.lda) : make_double2(0, 0);
+      v[u] = (idx < nb * rpc && i < nrow) ? ld_slab<E>(A + (row0 + i) + (a.j0 + c) * a.lda)
+                                          : from_d2<E>(make_double2(0, 0));
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
@@ -399,22 +407,22 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
       if (lane < P) st_cluster_u64(map_shared(&c_key[par][cta], (unsigned)lane), bkey);
       if (bkey != 0ull) {
         const int li = (int)(0xffffffu - (unsigned)((bkey >> 8) & 0xffffffu)) - (int)(row0 - a.j0);
-        const double2 v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
-        double2 *dst = recv_row + ((size_t)par * P + cta) * nb;
+        const E v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
+        E *dst = recv_row + ((size_t)par * P + cta) * nb;
         for (int t = 0; t < P; t++) {
           const unsigned base = map_shared(dst, (unsigned)t);
-          st_cluster_d2(base + (unsigned)lane * 16u, v0);
-          st_cluster_d2(base + (unsigned)(lane + 32) * 16u, v1);
+          st_cluster_d2(base + (unsigned)(lane * sizeof(E)), v0);
+          st_cluster_d2(base + (unsigned)((lane + 32) * sizeof(E)), v1);
         }
       }
       if (col >= row0 && col < row0 + nrow) {
         const int li = (int)(col - row0);
-        const double2 v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
-        double2 *dst = recv_col + (size_t)par * nb;
+        const E v0 = slab[lane * rpc + li], v1 = slab[(lane + 32) * rpc + li];
+        E *dst = recv_col + (size_t)par * nb;
         for (int t = 0; t < P; t++) {
           const unsigned base = map_shared(dst, (unsigned)t);
-          st_cluster_d2(base + (unsigned)lane * 16u, v0);
-          st_cluster_d2(base + (unsigned)(lane + 32) * 16u, v1);
+          st_cluster_d2(base + (unsigned)(lane * sizeof(E)), v0);
+          st_cluster_d2(base + (unsigned)((lane + 32) * sizeof(E)), v1);
         }
       }
     }
@@ -430,15 +438,17 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
       const int gr = none ? (int)col : (int)a.j0 + (int)(0xffffffu - (unsigned)((gkey >> 8) & 0xffffffu));
       const bool own_p = gr != col && gr >= row0 && gr < row0 + nrow;
       const bool own_c = col >= row0 && col < row0 + nrow;
-      const double2 *prow = recv_row + ((size_t)par * P + gsrc) * nb, *crow = recv_col + (size_t)par * nb;
+      const E *prow = recv_row + ((size_t)par * P + gsrc) * nb, *crow = recv_col + (size_t)par * nb;
       for (int j = lane; j < nb; j += 32) {
-        const double2 pv = none ? crow[j] : prow[j];
+        const E pv = none ? crow[j] : prow[j];
         s_prow_data[j] = pv;
         if (own_p) slab[j * rpc + (gr - (int)row0)] = crow[j];  // row prow <- old row col
         if (own_c) slab[j * rpc + (int)(col - row0)] = pv;      // row col  <- pivot row
         if (j == c) {
-          const double pa = none ? 0.0 : pv.x * pv.x + pv.y * pv.y;
-          s_rp = pa != 0.0 ? make_double2(pv.x / pa, -pv.y / pa) : make_double2(0, 0);  // 1 / pivot
+          // 1 / pivot, formed in FP64
+          const double2 pd = to_d2(pv);
+          const double pa = none ? 0.0 : pd.x * pd.x + pd.y * pd.y;
+          s_rp = from_d2<E>(pa != 0.0 ? make_double2(pd.x / pa, -pd.y / pa) : make_double2(0, 0));
           s_rpc[c] = s_rp;
           if (cta == 0 && pa == 0.0) atomicCAS(a.info, 0, (int)col + 1);
         }
@@ -448,23 +458,23 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
     __syncthreads();
     // 3. rank-1 update of columns c+1 .. with l = a(i, c) / pivot formed by
     //    each thread of the row (column c is scaled at the final store)
-    const double2 rp = s_rp;
-    const bool live = mine && g > col && (rp.x != 0.0 || rp.y != 0.0);
+    const E rp = s_rp;
+    const bool live = mine && g > col && (rp.x != 0 || rp.y != 0);
     cv = -1.0;
     const int own = (c + 1) % S;
     if (mine && g > col) {
       const int jst = c + 1 + ((sph - (c + 1)) % S + S) % S;
       if (live) {
-        const double2 l = cmul(slab[c * rpc + i], rp);
+        const E l = cmul(slab[c * rpc + i], rp);
         for (int j = jst; j < nb; j += 4 * S) {
-          double2 x[4];
+          E x[4];
 #pragma unroll
           for (int u = 0; u < 4; u++)
             if (j + u * S < nb) x[u] = slab[(j + u * S) * rpc + i];
 #pragma unroll
           for (int u = 0; u < 4; u++)
             if (j + u * S < nb) {
-              const double2 uu = s_prow_data[j + u * S];
+              const E uu = s_prow_data[j + u * S];
               x[u].x -= l.x * uu.x - l.y * uu.y;
               x[u].y -= l.x * uu.y + l.y * uu.x;
               slab[(j + u * S) * rpc + i] = x[u];
@@ -478,8 +488,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_cluster_kernel(PanelAr
   for (int idx = tid; idx < nb * rpc; idx += kPanelThreads) {
     const int c = idx / rpc, ii = idx % rpc;
     if (ii < nrow) {
-      const double2 v = slab[idx], rp = s_rpc[c];
-      const bool low = row0 + ii > a.j0 + c && (rp.x != 0.0 || rp.y != 0.0);
+      const E v = slab[idx], rp = s_rpc[c];
+      const bool low = row0 + ii > a.j0 + c && (rp.x != 0 || rp.y != 0);
       st2(A + (row0 + ii) + (a.j0 + c) * a.lda, low ? cmul(v, rp) : v);
     }
   }
@@ -1451,10 +1461,10 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
   if (!st) st = c->stream;
   const int nb = c->nb;
   const int64_t m = n - j0;
-  if (c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster) {
+  if (c->panel_cluster > 0 && m <= (int64_t)kClusterRows<T> * c->panel_cluster) {
     // short panel: one cluster, the smallest power of two with <= kClusterRows rows per CTA
     int CL = 1;
-    while ((int64_t)kClusterRows * CL < m) CL *= 2;
+    while ((int64_t)kClusterRows<T> * CL < m) CL *= 2;
     const int rpc = (int)((m + CL - 1) / CL);
     PanelArgs pa;
     pa.A = A;
@@ -1474,7 +1484,7 @@ int launch_panel(Ctx *c, T *A, int64_t lda, int64_t n, int64_t j0, int P, int *i
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(CL);
     cfg.blockDim = dim3(kPanelThreads);
-    cfg.dynamicSmemBytes = sizeof(double2) * ((size_t)nb * rpc + (size_t)2 * CL * nb + 2 * nb);
+    cfg.dynamicSmemBytes = sizeof(typename SlabOf<T>::type) * ((size_t)nb * rpc + (size_t)2 * CL * nb + 2 * nb);
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1795,7 +1805,7 @@ int lu_enqueue_la(Ctx *c, T *A, const LuWork &w) {
       int P = panel_ctas(c, nc, R);
       const int pcap = c->la_ctas > 0 ? c->la_ctas : 1;
       P = (int)std::max<int64_t>(std::min(P, pcap), (nc + R - 1) / R);
-      if (c->panel_cluster > 0 && nc <= (int64_t)kClusterRows * c->panel_cluster) P = c->panel_cluster;
+      if (c->panel_cluster > 0 && nc <= (int64_t)kClusterRows<T> * c->panel_cluster) P = c->panel_cluster;
       MOM_CUDA(c, cudaEventRecord(c->la_ev[1], sa));
       MOM_CUDA(c, cudaStreamWaitEvent(sb, c->la_ev[1], 0));
       MOM_TRY(factor_block(t0, sb, c->blas2, pmN, pcap));
@@ -2042,7 +2052,7 @@ int max_panel_cluster() {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cl);
     cfg.blockDim = dim3(kPanelThreads);
-    cfg.dynamicSmemBytes = sizeof(double2) * (64 * kClusterRows + 2 * cl * 64 + 2 * 64);
+    cfg.dynamicSmemBytes = sizeof(typename SlabOf<T>::type) * (64 * kClusterRows<T> + 2 * cl * 64 + 2 * 64);
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = cl;
@@ -2146,7 +2156,7 @@ int tune_panels(Ctx *c, const T *A, Ctx::Tuned &t) {
     int best = c->nsm, last = -1;
     double best_ms = 1e30;
     // heights that run on one cluster have nothing to tune: one timed trial
-    const bool clustered = c->panel_cluster > 0 && m <= (int64_t)kClusterRows * c->panel_cluster;
+    const bool clustered = c->panel_cluster > 0 && m <= (int64_t)kClusterRows<T> * c->panel_cluster;
     for (int cand : cands) {
       if (clustered && cand != cands[0]) break;
       const int P0 = (int)std::min<int64_t>(

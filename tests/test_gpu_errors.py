@@ -67,10 +67,17 @@ def test_refinement_no_convergence(small):
 
 
 def test_bounded_waits_time_out_and_recover(built):
-    """cfg1 sphere (3840 unknowns): tall panels use the device-wide exchange,
-    the trailing updates use the tensor-core GEMM."""
+    """cfg1 sphere (3840 unknowns) with the one-cluster panel kernel off
+    (MOM_PANEL_CLUSTER=0, read when the context is created; with it, every
+    mixed panel of this order fits one cluster, which has no spin-wait): the
+    panels use the device-wide exchange, the trailing updates the tensor-core
+    GEMM."""
     ref = np.load(os.path.join(HERE, "golden", "oracle_sphere_s3.npz"))
-    s = M.Solver(0)
+    os.environ["MOM_PANEL_CLUSTER"] = "0"
+    try:
+        s = M.Solver(0)
+    finally:
+        del os.environ["MOM_PANEL_CLUSTER"]
     try:
         nodes, faces, ids, doms = W.sphere(3)
         s.set_problem(M.Problem.from_arrays(nodes, faces, ids, 1e-9, doms))
