@@ -106,7 +106,7 @@ def test_closed_form_singular_integrals(p1, where):
                    K41=-(wts[:, None] * np.cross(d / R[:, None], f)).sum(0))
         for k, v in num.items():
             err = np.linalg.norm(np.atleast_1d(res[k] - v))
-            # (r - p) x K3 can vanish by symmetry; judge K4m1 / K41 on the scale of the f/R, f R terms
+            # (r - p) x K3 can vanish by symmetry; assess K4m1 / K41 on the scale of the f/R, f R terms
             scale = {"K4m1": np.linalg.norm(num["K2m1"]) / L, "K41": np.linalg.norm(num["K21"]) / L}.get(k, 0.0)
             assert err <= 1e-6 * max(np.linalg.norm(np.atleast_1d(v)), scale), (k, e, err)
 
