@@ -175,3 +175,52 @@ def test_command_script_with_mirror_groups(solver, tmp_path):
     solver.solve_wavelength(om, [1.0, N_IN], src, M.FP64, want_host=False)
     csca, cabs = solver.cross_sections(om, 1.0, src)
     assert abs(row[1] - csca[0]) <= 5e-4 * csca[0] and abs(row[2] - cabs[0]) <= 5e-4 * cabs[0], (row, csca, cabs)
+
+
+def test_command_script_second_harmonic_with_mirror_groups(solver, tmp_path):
+    """The `mom` interpreter with symm 3 mxp myp mzp, sbnd and a surface
+    nonlinearity (`smed 2 nlsurf value ...`) on the eighth of the s=1 sphere:
+    its -sh.crs file matches the full sphere's second-harmonic cross sections
+    (C ABI, no group) to the printed EN15.3 precision."""
+    import os
+    import subprocess
+    chi = (1e-18 + 0.2e-18j, 0.5e-18, -0.3e-18)
+    cx = lambda z: "(%.17g, %.17g)" % (complex(z).real, complex(z).imag)
+    nodes, faces = meshgen.octasphere(1, 50.0)
+    fn, ff, lines = fragment(1, [0, 1, 2])
+    with open(tmp_path / "eighth.msh", "w") as fh:
+        fh.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(fn))
+        for i, p in enumerate(fn):
+            fh.write("%d %.17g %.17g %.17g\n" % (i + 1, p[0], p[1], p[2]))
+        ne = sum(len(lines[ax]) for ax in range(3)) + len(ff)
+        fh.write("$EndNodes\n$Elements\n%d\n" % ne)
+        k = 1
+        for ax in range(3):
+            for a, b in lines[ax]:
+                fh.write("%d 1 2 %d %d %d %d\n" % (k, 10 + ax, 10 + ax, a + 1, b + 1))
+                k += 1
+        for f in ff:
+            fh.write("%d 2 2 1 1 %d %d %d\n" % (k, f[0] + 1, f[1] + 1, f[2] + 1))
+            k += 1
+        fh.write("$EndElements\n")
+    script = "\n".join([
+        "name 'eighth'", "symm 3 mxp myp mzp", "mesh 'eighth.msh' 1d-9",
+        "sbnd 10 xplane", "sbnd 11 yplane", "sbnd 12 zplane", "wlls 1 600d-9", "nmed 2",
+        "smed 1 linear value (1.0, 0.0)", "smed 2 linear value " + cx(N_IN),
+        "smed 2 nlsurf value " + " ".join(cx(c) for c in chi),
+        "ndom 2", "sdom 1 1 1 0 1 -1", "sdom 2 1 -1 0 2 -1", "fdom", "nsrc 1", "ssrc 1 'pw' 0 90 0",
+        "solv", "crst", "exit"]) + "\n"
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "for90-mom2_b200", "bin",
+                       "mom_b200")
+    r = subprocess.run([exe], input=script, capture_output=True, text=True, cwd=tmp_path, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:]
+    assert "Solving nonlinear scattering from centrosymmetric material" in r.stdout
+    row = [float(v) for v in open(tmp_path / "eighth-s1-sh.crs").read().split()]
+    om = M.omega_of(WL)
+    ri = [1.0, N_IN]
+    src = [M.src_pw(0, 90, 0)]
+    solver.set_problem(M.Problem.from_arrays(nodes, faces, np.ones(len(faces), int), 1e-9, [[1], [-1]]))
+    solver.solve_wavelength(om, ri, src, M.FP64, want_host=False)
+    solver.shg_solve(om, ri, ri, [None, chi], M.FP64, want_host=False)  # `smed ... value`: the SH index is ri
+    cs, ca = solver.cross_sections(2 * om, 1.0, [M.src_none()])
+    assert abs(row[1] - cs[0]) <= 5e-4 * abs(cs[0]) and abs(row[2] - ca[0]) <= 5e-4 * abs(ca[0]), (row, cs, ca)
