@@ -284,23 +284,42 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 // Ahat_hi / Ahat_lo (Mr x Kr, row-major) from the complex block L (m x k, ld),
-// or (tr) from the transpose of a k x m block: L(i, l) = P[l + i ld].
-__global__ void expand_a_kernel(const float2 *L, int64_t ld, int m, int k, float *hi, float *lo, bool tr) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)m * k) return;
-  const int i = (int)(idx / k), l = (int)(idx % k);
-  const float2 z = tr ? L[l + (int64_t)i * ld] : L[i + (int64_t)l * ld];
+// or (tr) from the transpose of a k x m block: L(i, l) = P[l + i ld].  In
+// 32 x 32 tiles through shared memory: the complex block is read along its
+// contiguous direction and the expanded rows are written as FP32 pairs
+// (block 32 x 8 threads).
+__global__ void __launch_bounds__(256) expand_a_tiled_kernel(const float2 *L, int64_t ld, int m, int k, float *hi,
+                                                             float *lo, bool tr) {
+  __shared__ float2 t[32][33];  // [l][i] of the tile
+  const int i0 = blockIdx.y * 32, l0 = blockIdx.x * 32, tx = threadIdx.x;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    if (!tr) {
+      const int i = i0 + tx, l = l0 + r;
+      t[r][tx] = (i < m && l < k) ? L[i + (int64_t)l * ld] : make_float2(0.f, 0.f);
+    } else {
+      const int l = l0 + tx, i = i0 + r;
+      t[tx][r] = (i < m && l < k) ? L[l + (int64_t)i * ld] : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
   const int64_t Kr = 2 * (int64_t)k;
-  const float vals[4] = {z.x, -z.y, z.y, z.x};
-  const int64_t pos[4] = {(2 * i) * Kr + 2 * l, (2 * i) * Kr + 2 * l + 1, (2 * i + 1) * Kr + 2 * l,
-                          (2 * i + 1) * Kr + 2 * l + 1};
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = i0 + r, l = l0 + tx;
+    if (i >= m || l >= k) continue;
+    const float2 z = t[tx][r];
+    const float v[4] = {z.x, -z.y, z.y, z.x};  // rows 2i and 2i + 1, columns 2l and 2l + 1
+    float h[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    uint32_t h;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(vals[q]));
-    const float hf = __uint_as_float(h);
-    hi[pos[q]] = hf;
-    lo[pos[q]] = vals[q] - hf;
+    for (int q = 0; q < 4; q++) {
+      uint32_t u;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v[q]));
+      h[q] = __uint_as_float(u);
+    }
+    const int64_t p0 = (2 * (int64_t)i) * Kr + 2 * l, p1 = p0 + Kr;
+    *reinterpret_cast<float2 *>(hi + p0) = make_float2(h[0], h[1]);
+    *reinterpret_cast<float2 *>(hi + p1) = make_float2(h[2], h[3]);
+    *reinterpret_cast<float2 *>(lo + p0) = make_float2(v[0] - h[0], v[1] - h[1]);
+    *reinterpret_cast<float2 *>(lo + p1) = make_float2(v[2] - h[2], v[3] - h[3]);
   }
 }
 
@@ -369,7 +388,8 @@ int tc_cgemm_update(Ctx *c, float2 *C, int64_t ldc, const float2 *L, int64_t ldl
   const int Mr = 2 * m, Kr = 2 * k;
   float *ahi = work, *alo = ahi + (size_t)Mr * Kr, *bhi = alo + (size_t)Mr * Kr, *blo = bhi + (size_t)nc * Kr;
   if (!reuse_a) {
-    expand_a_kernel<<<(unsigned)(((int64_t)m * k + 255) / 256), 256, 0, c->stream>>>(L, ldl, m, k, ahi, alo, trans_l);
+    expand_a_tiled_kernel<<<dim3((unsigned)((k + 31) / 32), (unsigned)((m + 31) / 32)), dim3(32, 8), 0, c->stream>>>(
+        L, ldl, m, k, ahi, alo, trans_l);
     c->launches++;
   }
   split_b_kernel<<<(unsigned)(((int64_t)k * nc + 255) / 256), 256, 0, c->stream>>>(U, ldu, k, nc, bhi, blo);
